@@ -1,0 +1,386 @@
+"""Benchmark of the LM normal-equation / Schur / block-Jacobi-PCG hot path on B200.
+
+Step (the unit timed): one Levenberg-Marquardt linear step of the large Schur LM
+workload -- P=4,000 primary 6-dof blocks, L=2,000,000 eliminated 3-dof blocks, each
+observed by 2+Poisson(4) distinct primaries from a wrapped window of 40 (about 12.0M
+2-dim residuals, Jacobians N(0,1), residuals N(0,0.5^2) with 5% N(0,20^2) outliers,
+Huber delta 1, LM lambda 1e-3).  From device-resident Jacobians the step computes the
+Huber-weighted normal equations, the damped Schur complement and its block-Jacobi
+preconditioner, solves the reduced system to an FP64 true relative residual of 1e-8
+and back-substitutes the eliminated step.  The headline pipeline is mixed precision
+(FP64 assembly, FP32 inner PCG with FP64 dots, FP64 refinement); the plain FP64
+pipeline is timed beside it.  Synthetic, seeded inputs (no dataset).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun (N>1) every rank solves its own system (replicas: the path has no
+exchange step), time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+P_FULL, L_FULL = 4000, 2_000_000
+LAMBDA, TOL = 1e-3, 1e-8
+WORKLOAD = ("schur_lm_P4000_L2000000: P=4,000 x 6-dof, L=2,000,000 x 3-dof, 2+Poisson(4) primaries "
+            "per eliminated block from a wrapped window of 40, 2-dim residuals, Huber delta 1, "
+            "lambda 1e-3, FP64 true relative residual 1e-8")
+METRIC = "Schur-PCG ms to 1e-8 FP64 rel. residual: learned+mixed vs plain; SpMV HBM GB/s"
+REF_SAMPLE_L = 100_000  # eliminated blocks of the reference CPU sample (5% of the full system)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--eliminated", type=int, default=L_FULL, help="L (eliminated blocks)")
+    ap.add_argument("--no-extras", action="store_true", help="skip SpMV / e2e / CPU-baseline legs")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks during the timed region
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device_index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ reference arm / CPU baseline
+def reference_sample_ms(seed: int = 0, eliminated: int = REF_SAMPLE_L):
+    """Reference CPU library (oracle/_ref, built from the reference sources): accumulation of
+    the sample's observations + solveDampedSchurComplement(Cpu).  Returns (ms, report)."""
+    import oracle
+    from plamatrix_b200 import workloads as W
+    prob = W.large_bundle(seed=seed, P=P_FULL, L=eliminated)
+    t0 = time.perf_counter()
+    ne = oracle.normal_equations_from_observations(prob, impl="ref")
+    dp, dl, rep = ne.solve(LAMBDA, relative_tolerance=TOL, max_iterations=200)
+    ms = (time.perf_counter() - t0) * 1e3
+    return ms, rep, len(prob["obs_primary"])
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    if not oracle.available("ref"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU library oracle/_ref not built"}))
+        return
+    scale = L_FULL / REF_SAMPLE_L
+    for _ in range(args.warmup):
+        reference_sample_ms(seed=0)
+    times = []
+    reps = []
+    for k in range(args.steps):
+        ms, rep, nobs = reference_sample_ms(seed=k)
+        times.append(ms * scale)
+        reps.append(rep)
+    value = statistics.mean(times)
+    sample = (f"reference CPU library (oracle/_ref, compiled from the reference sources): Huber-weighted "
+              f"BlockNormalEquations accumulation + solveDampedSchurComplement(Cpu backend, tol 1e-8) on "
+              f"P=4,000, L={REF_SAMPLE_L:,} ({nobs:,} observations, 5% of the full system, same distributions), "
+              f"time scaled x{scale:.0f} to L=2,000,000; single thread (the reference's path has no threading)")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_eliminated_blocks": REF_SAMPLE_L},
+        "iterations": [r["iterations"] for r in reps],
+        "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+
+    from plamatrix_b200 import _native as N
+    from plamatrix_b200 import schur as SC
+    from plamatrix_b200 import sparse as S
+    from plamatrix_b200 import workloads as W
+
+    L = args.eliminated
+    prob = W.large_bundle(seed=rank, P=P_FULL, L=L)
+    nobs = len(prob["obs_primary"])
+    host = {k: torch.from_numpy(prob[k]).pin_memory() for k in ("obs_primary", "obs_eliminated", "jp", "jl",
+                                                                   "residual")}
+    dev = {k: v.cuda() for k, v in host.items()}
+    ne = SC.DeviceNormalEquations(P_FULL, L, 6, 3)
+    ws = SC.SchurComplementSolverWorkspace()
+    n, m = P_FULL * 6, L * 3
+    dp = torch.zeros(n, dtype=torch.float64, device="cuda")
+    dl = torch.zeros(m, dtype=torch.float64, device="cuda")
+    mixed = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL, precision="mixed")
+    plain = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL, precision="native")
+    stream = torch.cuda.current_stream()
+
+    def step(opts):
+        ne.accumulate_observations(dev["obs_primary"], dev["obs_eliminated"], dev["jp"], dev["jl"],
+                                   dev["residual"], 1.0)
+        return SC.solve_damped_schur_complement(ne, LAMBDA, opts, ws, dp, dl)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        last = None
+        for _ in range(steps):
+            last = fn()
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, last
+
+    for _ in range(args.warmup):
+        step(mixed)
+        step(plain)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = N.load().pm_kernel_launches()
+    ms_mixed, (_, _, rep_mixed) = timed(lambda: step(mixed), args.steps)
+    launches = (N.load().pm_kernel_launches() - launches0) / args.steps
+    ms_plain, (_, _, rep_plain) = timed(lambda: step(plain), args.steps)
+    clock = clocks.stop()
+
+    # accumulation alone (for the phase table)
+    ms_accum, _ = timed(lambda: ne.accumulate_observations(dev["obs_primary"], dev["obs_eliminated"], dev["jp"],
+                                                           dev["jl"], dev["residual"], 1.0), args.steps)
+    out = {}
+    if rank == 0 and not args.no_extras:
+        out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, mixed, n, m)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    hbm, peak_kind = peaks()
+    # dominant kernel: the Schur assembly (one CTA per block row); algorithmic bytes per launch =
+    # cross blocks read (C x 18 x 8) + eliminated inverses (L x 9 x 8) + y (L x 3 x 8) + primary
+    # blocks (P x 42 x 8) + topology (C x 8 + L x 4) + Schur blocks written (B x 36 x 8) +
+    # RHS + preconditioner (P x 42 x 8)
+    C_, _, _ = ne.counts()
+    _, _, B = ws.dims()
+    assembly_bytes = C_ * 18 * 8 + L * 12 * 8 + P_FULL * 42 * 8 + C_ * 8 + L * 4 + B * 36 * 8 + P_FULL * 42 * 8
+    asm_ms = rep_plain["assembly_ms"]
+    achieved = assembly_bytes / (asm_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": round(ms_mixed, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_mixed, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (FP32 inner PCG, FP64 dots/refinement)", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "observations": nobs, "eliminated_blocks": L, "primary_blocks": P_FULL,
+                   "schur_blocks": B, "cross_blocks": C_, "parallelism": f"replicas x{world} (no exchange step)",
+                   "l2": "inputs larger than L2 (observations 1.9 GB FP64)", "systems_per_step": world},
+        "plain_fp64_ms": round(ms_plain, 4),
+        "mixed_over_plain_speedup": round(ms_plain / ms_mixed, 3),
+        "accumulation_ms": round(ms_accum, 4),
+        "phases_mixed": {k: round(rep_mixed[k], 4) for k in ("pattern_ms", "eliminated_inverse_ms", "assembly_ms",
+                                                            "solve_ms", "back_substitution_ms", "total_ms")},
+        "phases_plain": {k: round(rep_plain[k], 4) for k in ("pattern_ms", "eliminated_inverse_ms", "assembly_ms",
+                                                            "solve_ms", "back_substitution_ms", "total_ms")},
+        "iterations": {"mixed_inner": rep_mixed["iterations"], "mixed_refinements": rep_mixed["refinement_steps"],
+                       "plain": rep_plain["iterations"]},
+        "true_relative_residual": {"mixed": rep_mixed["true_relative_residual"],
+                                   "plain": rep_plain["true_relative_residual"]},
+        "converged": bool(rep_mixed["converged"] and rep_plain["converged"]),
+        "roofline": {"bound": "hbm", "kernel": "assemble_kernel<double,6,3> (+ mirror)", "achieved": round(achieved, 1),
+                     "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
+                     "peak_kind": peak_kind, "algorithmic_bytes_per_launch": assembly_bytes},
+        "gpu_launches": launches,
+        "clocks": clock,
+    }
+    line.update(out)
+    print(json.dumps(line))
+
+
+def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m):
+    out = {}
+    # ---- end to end through the public API with host buffers
+    dp_h = torch.empty(n, dtype=torch.float64).pin_memory()
+    dl_h = torch.empty(m, dtype=torch.float64).pin_memory()
+    stream = torch.cuda.current_stream()
+
+    def e2e_step():
+        for k in ("obs_primary", "obs_eliminated", "jp", "jl", "residual"):
+            dev[k].copy_(host[k], non_blocking=True)
+        ne.accumulate_observations(dev["obs_primary"], dev["obs_eliminated"], dev["jp"], dev["jl"],
+                                   dev["residual"], 1.0)
+        SC.solve_damped_schur_complement(ne, LAMBDA, opts, ws, dp, dl)
+        dp_h.copy_(dp, non_blocking=True)
+        dl_h.copy_(dl, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    h2d = sum(v.numel() * v.element_size() for v in host.values())
+    out["e2e"] = {"value": round(e0.elapsed_time(e1) / args.steps, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
+                  "d2h_bytes_per_step": (n + m) * 8}
+    # ---- SpMV bandwidth: the assembled 6x6 block-CSR Schur matrix and the 128^3 Laplacian CSR
+    hbm, _ = peaks()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    sysd = ws.export()
+    spmv = {}
+    lap = W.laplacian_coo(128, seed=0, dtype=np.float64)
+    for dt, name in ((torch.float64, "f64"), (torch.float32, "f32")):
+        csr = S.coo_to_csr(lap["rows"], lap["cols"], torch.from_numpy(lap["row_indices"]).cuda(),
+                           torch.from_numpy(lap["col_indices"]).cuda(),
+                           torch.from_numpy(lap["values"]).to(dt).cuda())
+        op = S.CsrOperand(csr)
+        x = torch.randn(lap["rows"], dtype=dt, device="cuda")
+        y = torch.empty_like(x)
+        times = []
+        for _ in range(10):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            op.spmv(x, y)
+            b.record(stream)
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+        s = 4 if dt == torch.float32 else 8
+        nn = lap["rows"]
+        byts = csr.nnz * (s + 4) + (nn + 1) * 4 + 2 * nn * s
+        t = statistics.median(times)
+        spmv[f"csr_laplacian128_{name}"] = {"ms": round(t, 4), "GBps": round(byts / (t * 1e-3) / 1e9, 1),
+                                            "frac_of_hbm": round(byts / (t * 1e-3) / 1e9 / hbm, 3),
+                                            "algorithmic_bytes": byts}
+        # COO -> CSR of the same matrix (16.04M triplets)
+        ws_coo = S.SparseOpsWorkspace()
+        r_d = torch.from_numpy(lap["row_indices"]).cuda()
+        c_d = torch.from_numpy(lap["col_indices"]).cuda()
+        v_d = torch.from_numpy(lap["values"]).to(dt).cuda()
+        out_csr = S.CSRMatrix.empty(lap["rows"], lap["cols"], csr.nnz, dt)
+        S.coo_to_csr_async(lap["rows"], lap["cols"], r_d, c_d, v_d, out_csr, ws_coo)
+        torch.cuda.synchronize()
+        ws_coo.check_status()
+        ct = []
+        for _ in range(5):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            S.coo_to_csr_async(lap["rows"], lap["cols"], r_d, c_d, v_d, out_csr, ws_coo)
+            b.record(stream)
+            torch.cuda.synchronize()
+            ws_coo.check_status()
+            ct.append(a.elapsed_time(b))
+        trip = len(lap["values"])
+        cbytes = trip * (16 + s) + csr.nnz * (4 + s) + (nn + 1) * 4
+        tc = statistics.median(ct)
+        spmv[f"coo_to_csr_laplacian128_{name}"] = {"ms": round(tc, 4), "GBps": round(cbytes / (tc * 1e-3) / 1e9, 1),
+                                                   "triplets": trip, "algorithmic_bytes": cbytes}
+    out["spmv"] = spmv
+    # ---- CPU baseline: the reference's own CPU library on a bounded sample, scaled
+    try:
+        import oracle
+        if oracle.available("ref"):
+            ms, rep, nobs = reference_sample_ms(seed=0)
+            scale = L_FULL / REF_SAMPLE_L
+            out["cpu_baseline"] = {
+                "value": round(ms * scale, 1), "unit": "ms", "cores": 1, "kind": "reference",
+                "sample": (f"reference CPU library (oracle/_ref) accumulation + solveDampedSchurComplement(Cpu) on "
+                           f"P=4,000, L={REF_SAMPLE_L:,} ({nobs:,} observations), scaled x{scale:.0f}; "
+                           f"{rep['iterations']} PCG iterations; 1 thread of {os.cpu_count()}")}
+    except Exception as exc:  # noqa: BLE001
+        out["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": str(exc)}
+    return out
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -1,0 +1,299 @@
+/*
+ * plamatrix_b200 -- C ABI of the B200 (sm_100a) implementation of PlaMatrix's
+ * Levenberg-Marquardt normal-equation hot path.
+ *
+ * Conventions (shared by every entry point):
+ *   - Every function returns an int status: PM_OK or one of the PM_* codes below, which
+ *     map one-to-one onto the reference's exception classes.  pm_last_error() returns the
+ *     message of the last failure on the calling thread.
+ *   - Pointers named *_d are device pointers; host arrays are named *_h.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Work is enqueued on it;
+ *     functions documented as "synchronous" wait for it before returning.
+ *   - Workspaces are caller-owned, move-only in spirit, not thread-safe, and bound to the
+ *     first stream they are used with until *_close() (the reference's ownership rule).
+ *   - Index arrays that cross this boundary are int64 (the reference's Index) unless
+ *     a function says otherwise.
+ *
+ * Each declaration names the reference interface it replaces (paths inside the reference
+ * project).
+ */
+#ifndef PLAMATRIX_B200_H
+#define PLAMATRIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define PM_API __attribute__((visibility("default")))
+#else
+#define PM_API
+#endif
+
+typedef struct CUstream_st* pm_stream_t; /* identical to cudaStream_t */
+
+enum
+{
+    PM_OK = 0,
+    PM_INVALID_ARGUMENT = 1, /* std::invalid_argument */
+    PM_OUT_OF_RANGE = 2,     /* std::out_of_range */
+    PM_RUNTIME_ERROR = 3,    /* std::runtime_error */
+    PM_LOGIC_ERROR = 4,      /* std::logic_error */
+    PM_OVERFLOW_ERROR = 5,   /* std::overflow_error */
+    PM_CUDA_ERROR = 6        /* CUDA runtime failure (std::runtime_error in the reference) */
+};
+
+/* Message of the last non-zero status returned on this thread. */
+PM_API const char* pm_last_error(void);
+/* ABI version of this library. */
+PM_API int pm_version(void);
+/* Number of kernels this library has launched in the process so far. */
+PM_API long long pm_kernel_launches(void);
+
+/* =========================================================================== workspaces
+ * Replaces SparseOpsWorkspace (include/plamatrix/sparse/sparse_ops.h:13-77): grow-only,
+ * stream-bound temporary storage plus the deferred COO status. */
+typedef struct pm_sparse_workspace pm_sparse_workspace;
+PM_API int pm_sparse_workspace_create(pm_sparse_workspace** out);
+/* Frees the workspace (stream-ordered on its bound stream). */
+PM_API void pm_sparse_workspace_destroy(pm_sparse_workspace* workspace);
+/* closeAsyncAllocation (sparse_ops.h:26): release storage, unbind the stream. */
+PM_API int pm_sparse_workspace_close(pm_sparse_workspace* workspace);
+PM_API size_t pm_sparse_workspace_capacity(const pm_sparse_workspace* workspace);
+
+/* =========================================================================== COO -> CSR
+ * Deterministic, bit-exact with the reference CPU conversion
+ * (src/sparse/sparse_ops_cpu.cpp:24-134): entries sorted by (row, col) with ties kept in
+ * input order; duplicates combined by taking the first value and adding the rest in input
+ * order.  Inputs: `count` triplets (int64 rows/cols, scalar values) on the device; limits
+ * of the reference GPU path (src/sparse/coo_to_csr.cu:78-104): count and rows < 2^31,
+ * cols <= 2^32-1.  Coordinate and value errors are deferred to pm_coo_status().
+ */
+/* First half of the synchronous cooToCsr (src/sparse/coo_to_csr.cu:536-561): enqueue the
+ * sort and the duplicate-combined count; after a stream sync pm_coo_status() returns the
+ * nnz to allocate, and pm_coo_to_csr_fill_*() writes the CSR from the same sorted state. */
+PM_API int pm_coo_to_csr_count_f32(pm_sparse_workspace* workspace, pm_stream_t stream, int64_t rows, int64_t cols,
+                            int64_t count, const int64_t* row_indices_d, const int64_t* col_indices_d,
+                            const float* values_d);
+PM_API int pm_coo_to_csr_count_f64(pm_sparse_workspace* workspace, pm_stream_t stream, int64_t rows, int64_t cols,
+                            int64_t count, const int64_t* row_indices_d, const int64_t* col_indices_d,
+                            const double* values_d);
+PM_API int pm_coo_to_csr_fill_f32(pm_sparse_workspace* workspace, pm_stream_t stream, int64_t nnz,
+                           int64_t* row_offsets_d, int64_t* col_indices_out_d, float* values_out_d);
+PM_API int pm_coo_to_csr_fill_f64(pm_sparse_workspace* workspace, pm_stream_t stream, int64_t nnz,
+                           int64_t* row_offsets_d, int64_t* col_indices_out_d, double* values_out_d);
+/* cooToCsrAsync (include/plamatrix/sparse/sparse_ops.h:108-120, src/sparse/coo_to_csr.cu:563-576):
+ * full conversion into preallocated output holding exactly `nnz` entries; no host sync.
+ * Synchronize the stream, then call pm_coo_status() before consuming the output. */
+PM_API int pm_coo_to_csr_async_f32(pm_sparse_workspace* workspace, pm_stream_t stream, int64_t rows, int64_t cols,
+                            int64_t count, const int64_t* row_indices_d, const int64_t* col_indices_d,
+                            const float* values_d, int64_t nnz, int64_t* row_offsets_d,
+                            int64_t* col_indices_out_d, float* values_out_d);
+PM_API int pm_coo_to_csr_async_f64(pm_sparse_workspace* workspace, pm_stream_t stream, int64_t rows, int64_t cols,
+                            int64_t count, const int64_t* row_indices_d, const int64_t* col_indices_d,
+                            const double* values_d, int64_t nnz, int64_t* row_offsets_d,
+                            int64_t* col_indices_out_d, double* values_out_d);
+/* SparseOpsWorkspace::checkStatus (src/sparse/coo_to_csr.cu:300-365, 531-534): reads the
+ * deferred status of the last conversion.  Returns PM_LOGIC_ERROR if the stream has not
+ * finished, PM_OUT_OF_RANGE for a coordinate outside the matrix (lowest offending offset),
+ * PM_INVALID_ARGUMENT for a non-finite value or combined sum, PM_RUNTIME_ERROR for an
+ * output nnz that differs from the duplicate-combined nnz.  `nnz_out` (may be NULL)
+ * receives the duplicate-combined nnz. */
+PM_API int pm_coo_status(pm_sparse_workspace* workspace, const char* operation, int64_t* nnz_out);
+
+/* =========================================================================== CSR matrices
+ * A validated CSR operand for the device SpMV and solvers.  Replaces the structure checks
+ * of CSRMatrix<GPU>::validateStructure (include/plamatrix/sparse/csr_matrix.h:197-240) and
+ * the cached cuSPARSE descriptors of SparseOpsWorkspace (src/sparse/sparse_ops.cu:192-231):
+ * the int64 structure is validated once and kept as a compact int32 copy; the values
+ * stay in the caller's array, which must outlive the handle.  Synchronous. */
+typedef struct pm_csr pm_csr;
+PM_API int pm_csr_create_f32(pm_stream_t stream, int64_t rows, int64_t cols, int64_t nnz, const int64_t* row_offsets_d,
+                      const int64_t* col_indices_d, const float* values_d, pm_csr** out);
+PM_API int pm_csr_create_f64(pm_stream_t stream, int64_t rows, int64_t cols, int64_t nnz, const int64_t* row_offsets_d,
+                      const int64_t* col_indices_d, const double* values_d, pm_csr** out);
+PM_API void pm_csr_destroy(pm_csr* matrix);
+/* Point the handle at new values with the same structure (e.g. the next LM iteration). */
+PM_API int pm_csr_set_values(pm_csr* matrix, const void* values_d);
+
+/* spmvAsync (include/plamatrix/sparse/sparse_ops.h:158-165, src/sparse/sparse_ops.cu:687-740):
+ * y = A x on `stream`, hand-written kernel (no cuSPARSE). */
+PM_API int pm_csr_spmv_f32(const pm_csr* matrix, pm_stream_t stream, const float* x_d, float* y_d);
+PM_API int pm_csr_spmv_f64(const pm_csr* matrix, pm_stream_t stream, const double* x_d, double* y_d);
+
+/* =========================================================================== CG / PCG
+ * Replaces cg / pcg / blockPcg on the GPU (include/plamatrix/sparse/iterative_solver.h:297-329,
+ * src/sparse/iterative_solver.cu:262-402).  Dots, alpha and beta are evaluated in FP64 for
+ * both scalar types; convergence is tested on the device (no per-iteration host sync):
+ * tolerance max(absolute, relative * ||r0||) on the recurrence residual, as in the
+ * reference.  Synchronous: returns after the solve (one host read at the end). */
+typedef struct
+{
+    int max_iterations;        /* IterativeSolverOptions::maxIterations (1000) */
+    double relative_tolerance; /* 1e-6, in [0, 1] */
+    double absolute_tolerance; /* 0 */
+    int use_jacobi;            /* useJacobiPreconditioner (1); pcg only */
+    int require_convergence;   /* requireConvergence (0): PM_RUNTIME_ERROR when not converged */
+} pm_solver_options;
+
+typedef struct
+{
+    int converged;
+    int iterations;
+    double initial_residual;
+    double final_residual;
+} pm_solver_report;
+
+/* Replaces IterativeSolverWorkspace<Scalar> (include/plamatrix/sparse/iterative_solver.h:216-251). */
+typedef struct pm_solver_workspace pm_solver_workspace;
+PM_API int pm_solver_workspace_create(pm_solver_workspace** out);
+PM_API void pm_solver_workspace_destroy(pm_solver_workspace* workspace);
+PM_API int pm_solver_workspace_close(pm_solver_workspace* workspace);
+
+PM_API int pm_cg_f32(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix, const float* rhs_d,
+              float* solution_d, const pm_solver_options* options, pm_solver_report* report);
+PM_API int pm_cg_f64(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix, const double* rhs_d,
+              double* solution_d, const pm_solver_options* options, pm_solver_report* report);
+PM_API int pm_pcg_f32(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix, const float* rhs_d,
+               float* solution_d, const pm_solver_options* options, pm_solver_report* report);
+PM_API int pm_pcg_f64(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix, const double* rhs_d,
+               double* solution_d, const pm_solver_options* options, pm_solver_report* report);
+/* blockPcg: caller-supplied row-major inverse diagonal blocks, (rows * block_size) entries. */
+PM_API int pm_block_pcg_f32(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix,
+                     const float* rhs_d, float* solution_d, const float* inverse_blocks_d, int64_t block_size,
+                     const pm_solver_options* options, pm_solver_report* report);
+PM_API int pm_block_pcg_f64(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix,
+                     const double* rhs_d, double* solution_d, const double* inverse_blocks_d, int64_t block_size,
+                     const pm_solver_options* options, pm_solver_report* report);
+
+/* =========================================================================== normal equations
+ * Device-resident state of the reference's BlockNormalEquations<Scalar>
+ * (include/plamatrix/optimization/block_schur.h:196-319, src/optimization/block_normal_equations.cpp):
+ * primary diagonal blocks Hpp (P x bp x bp), eliminated diagonal blocks Hll (L x bl x bl),
+ * gradients, cross blocks W (bp x bl) of every distinct (primary, eliminated) pair grouped by
+ * eliminated block, and upper-triangular primary-primary cross blocks.  value_size selects the
+ * Scalar: 4 (float) or 8 (double). */
+typedef struct pm_normal_equations pm_normal_equations;
+PM_API int pm_ne_create(int64_t primary_count, int64_t eliminated_count, int64_t primary_size,
+                        int64_t eliminated_size, int value_size, pm_normal_equations** out);
+PM_API void pm_ne_destroy(pm_normal_equations* equations);
+/* Counts of the current structure; topology_version changes whenever the structure does. */
+PM_API int pm_ne_counts(const pm_normal_equations* equations, int64_t* cross_count, int64_t* primary_cross_count,
+                        int64_t* topology_version);
+/* Load host state (the reference's accumulated members) onto the device.  Crosses are given
+ * grouped by eliminated block: cross_offsets has L+1 entries, cross k belongs to the eliminated
+ * block whose range holds k, cross_primary[k] is its primary block (the reference's
+ * _eliminatedAdjacency order).  Synchronous. */
+PM_API int pm_ne_upload_f32(pm_normal_equations* equations, pm_stream_t stream, const float* primary_diagonal_h,
+                            const float* eliminated_diagonal_h, const float* primary_gradient_h,
+                            const float* eliminated_gradient_h, int64_t cross_count, const int64_t* cross_offsets_h,
+                            const int64_t* cross_primary_h, const float* cross_values_h, int64_t primary_cross_count,
+                            const int64_t* primary_cross_row_h, const int64_t* primary_cross_col_h,
+                            const float* primary_cross_values_h);
+PM_API int pm_ne_upload_f64(pm_normal_equations* equations, pm_stream_t stream, const double* primary_diagonal_h,
+                            const double* eliminated_diagonal_h, const double* primary_gradient_h,
+                            const double* eliminated_gradient_h, int64_t cross_count, const int64_t* cross_offsets_h,
+                            const int64_t* cross_primary_h, const double* cross_values_h, int64_t primary_cross_count,
+                            const int64_t* primary_cross_row_h, const int64_t* primary_cross_col_h,
+                            const double* primary_cross_values_h);
+/* Copy the device state back to host arrays (any pointer may be NULL).  Synchronous. */
+PM_API int pm_ne_download_f32(const pm_normal_equations* equations, pm_stream_t stream, float* primary_diagonal_h,
+                              float* eliminated_diagonal_h, float* primary_gradient_h, float* eliminated_gradient_h,
+                              int64_t* cross_offsets_h, int64_t* cross_primary_h, float* cross_values_h,
+                              int64_t* primary_cross_row_h, int64_t* primary_cross_col_h,
+                              float* primary_cross_values_h);
+PM_API int pm_ne_download_f64(const pm_normal_equations* equations, pm_stream_t stream, double* primary_diagonal_h,
+                              double* eliminated_diagonal_h, double* primary_gradient_h, double* eliminated_gradient_h,
+                              int64_t* cross_offsets_h, int64_t* cross_primary_h, double* cross_values_h,
+                              int64_t* primary_cross_row_h, int64_t* primary_cross_col_h,
+                              double* primary_cross_values_h);
+/* Huber-weighted accumulation of `count` device-resident observations, each one residual of
+ * size m on one primary and one eliminated block: weight = evaluateHuberLoss(||r||^2, delta)
+ * .weight (include/plamatrix/optimization/robust_loss.h:27-51), then addResidualBlock
+ * (src/optimization/block_normal_equations.cpp:225-312) for every observation.  Jacobians are
+ * row-major (count x m x bp) and (count x m x bl), residuals (count x m).  Replaces the
+ * state: it equals a fresh BlockNormalEquations fed the observations in array order (cross
+ * blocks of an eliminated block ordered by primary index).  The sorting topology is cached
+ * while the index arrays are unchanged. */
+PM_API int pm_ne_accumulate_observations_f32(pm_normal_equations* equations, pm_stream_t stream, int64_t count,
+                                             int64_t residual_size, const int64_t* obs_primary_d,
+                                             const int64_t* obs_eliminated_d, const float* primary_jacobians_d,
+                                             const float* eliminated_jacobians_d, const float* residuals_d,
+                                             float huber_delta);
+PM_API int pm_ne_accumulate_observations_f64(pm_normal_equations* equations, pm_stream_t stream, int64_t count,
+                                             int64_t residual_size, const int64_t* obs_primary_d,
+                                             const int64_t* obs_eliminated_d, const double* primary_jacobians_d,
+                                             const double* eliminated_jacobians_d, const double* residuals_d,
+                                             double huber_delta);
+
+/* =========================================================================== damped Schur solve
+ * Replaces solveDampedSchurComplement (include/plamatrix/optimization/block_schur.h:171-186,
+ * src/optimization/block_schur.cpp:54-459) with SchurComplementSolverWorkspace
+ * (block_schur.h:81-169) as the reusable pattern cache. */
+enum
+{
+    PM_PRECISION_NATIVE = 0, /* assembly, SpMV and PCG vectors in Scalar; dots in FP64 */
+    PM_PRECISION_MIXED = 1   /* double only: FP64 refinement around an FP32 inner PCG */
+};
+
+typedef struct
+{
+    int max_iterations;          /* SchurComplementSolverOptions::maxIterations (100) */
+    double relative_tolerance;   /* 1e-8 */
+    double absolute_tolerance;   /* 1e-12 */
+    double minimum_diagonal;     /* 1e-12 */
+    int use_initial_guess;       /* 0 */
+    int precision;               /* PM_PRECISION_* */
+    int tolerance_rule;          /* 0: abs + rel*||r0|| (Cpu backend), 1: max(abs, rel*||r0||) (blockPcg) */
+    int check_true_residual;     /* compute ||b - S x|| / ||b|| in FP64 after convergence */
+    double inner_relative_tolerance; /* mixed: relative tolerance of each inner FP32 solve (1e-4) */
+    int max_refinements;         /* mixed: outer FP64 refinement steps (8) */
+} pm_schur_options;
+
+typedef struct
+{
+    int converged;
+    int iterations;                /* PCG iterations (inner iterations summed in mixed mode) */
+    double initial_residual_norm;
+    double final_residual_norm;
+    double true_relative_residual; /* -1 when not computed */
+    int pattern_reused;            /* SchurComplementSolverReport::schurPatternReused */
+    int mixed_precision_used;
+    int refinement_steps;
+    double pattern_ms, eliminated_inverse_ms, assembly_ms, solve_ms, back_substitution_ms, total_ms;
+    char message[128];             /* "converged" or the reference's failure message */
+} pm_schur_report;
+
+typedef struct pm_schur_workspace pm_schur_workspace;
+PM_API int pm_schur_workspace_create(pm_schur_workspace** out);
+PM_API void pm_schur_workspace_destroy(pm_schur_workspace* workspace);
+PM_API int pm_schur_workspace_close(pm_schur_workspace* workspace);
+/* SchurComplementSolverWorkspace::patternBuildCount (block_schur.h:121-124). */
+PM_API int64_t pm_schur_pattern_build_count(const pm_schur_workspace* workspace);
+/* Scalar dimension, scalar nnz and 6x6 block count of the last assembled reduced system. */
+PM_API int pm_schur_dims(const pm_schur_workspace* workspace, int64_t* dimension, int64_t* nnz, int64_t* blocks);
+/* Solve for the primary step (P*bp, device) and the eliminated step (L*bl, device).
+ * Synchronous.  Like the reference, SPD failures are returned in report->message with
+ * converged = 0 and PM_OK; invalid arguments return PM_INVALID_ARGUMENT. */
+PM_API int pm_schur_solve_f32(pm_schur_workspace* workspace, pm_stream_t stream, const pm_normal_equations* equations,
+                              float damping, const pm_schur_options* options, float* primary_step_d,
+                              float* eliminated_step_d, pm_schur_report* report);
+PM_API int pm_schur_solve_f64(pm_schur_workspace* workspace, pm_stream_t stream, const pm_normal_equations* equations,
+                              double damping, const pm_schur_options* options, double* primary_step_d,
+                              double* eliminated_step_d, pm_schur_report* report);
+/* The last assembled reduced system in the reference's scalar-CSR layout
+ * (block_schur_sparse_assembly.h:129-153, 262-272): row_offsets (n+1), col_indices and values
+ * (nnz), reduced RHS (n, FP64) and block-Jacobi inverses (P*bp*bp, FP64).  Any may be NULL. */
+PM_API int pm_schur_export_f32(pm_schur_workspace* workspace, pm_stream_t stream, int64_t* row_offsets_d,
+                               int64_t* col_indices_d, float* values_d, double* rhs_d, double* preconditioner_d);
+PM_API int pm_schur_export_f64(pm_schur_workspace* workspace, pm_stream_t stream, int64_t* row_offsets_d,
+                               int64_t* col_indices_d, double* values_d, double* rhs_d, double* preconditioner_d);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLAMATRIX_B200_H */

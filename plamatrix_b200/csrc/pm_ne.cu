@@ -1,0 +1,579 @@
+// Device normal equations: upload/download of the reference's BlockNormalEquations state and
+// the Huber-weighted accumulation of device-resident observations (the caller side of the
+// reference's LM loop: evaluateHuberLoss + addResidualBlock, robust_loss.h:27-51 and
+// block_normal_equations.cpp:136-312).
+//
+// Accumulation order.  For every eliminated block the observations are visited in input
+// order, and so are the observations of every (primary, eliminated) pair; the products
+// `weight * value * jacobian` are evaluated as two rounded multiplies and one rounded add
+// (no fused multiply-add), so the eliminated diagonal blocks, eliminated gradients and cross
+// blocks equal the reference's host accumulation bit for bit.  The primary diagonal blocks
+// and gradients sum ~N/P observations per primary; they are reduced in a fixed
+// (scheduling-independent) tree order instead of the reference's serial order.
+#include "pm_schur.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <sstream>
+#include <vector>
+
+pm_normal_equations::~pm_normal_equations()
+{
+    numeric.release();
+    topology.release();
+    observation_copy.release();
+    if (by_eliminated)
+        pm_sparse_workspace_destroy(by_eliminated);
+    if (by_primary)
+        pm_sparse_workspace_destroy(by_primary);
+}
+
+namespace pm
+{
+namespace
+{
+
+void layout_numeric(pm_normal_equations* ne, cudaStream_t stream)
+{
+    const size_t s = ne->value_size;
+    Carver plan;
+    plan.take<char>(ne->P * ne->bp * ne->bp * s);
+    plan.take<char>(ne->L * ne->bl * ne->bl * s);
+    plan.take<char>(ne->P * ne->bp * s);
+    plan.take<char>(ne->L * ne->bl * s);
+    plan.take<char>(ne->cross_count * ne->bp * ne->bl * s);
+    plan.take<char>(ne->primary_cross_count * ne->bp * ne->bp * s);
+    ne->numeric.ensure(plan.offset + 256, stream, "normal equations");
+    Carver c;
+    c.base = static_cast<char*>(ne->numeric.ptr);
+    ne->primary_diagonal = c.take<char>(ne->P * ne->bp * ne->bp * s);
+    ne->eliminated_diagonal = c.take<char>(ne->L * ne->bl * ne->bl * s);
+    ne->primary_gradient = c.take<char>(ne->P * ne->bp * s);
+    ne->eliminated_gradient = c.take<char>(ne->L * ne->bl * s);
+    ne->cross_values = c.take<char>(ne->cross_count * ne->bp * ne->bl * s);
+    ne->primary_cross_values = c.take<char>(ne->primary_cross_count * ne->bp * ne->bp * s);
+}
+
+void layout_topology(pm_normal_equations* ne, cudaStream_t stream)
+{
+    Carver plan;
+    plan.take<int>(ne->L + 1);
+    plan.take<int>(ne->cross_count + 1);
+    plan.take<int>(ne->cross_count + 1);
+    plan.take<int>(ne->primary_cross_count + 1);
+    plan.take<int>(ne->primary_cross_count + 1);
+    ne->topology.ensure(plan.offset + 256, stream, "normal equations");
+    Carver c;
+    c.base = static_cast<char*>(ne->topology.ptr);
+    ne->cross_offsets = c.take<int>(ne->L + 1);
+    ne->cross_primary = c.take<int>(ne->cross_count + 1);
+    ne->cross_eliminated = c.take<int>(ne->cross_count + 1);
+    ne->primary_cross_row = c.take<int>(ne->primary_cross_count + 1);
+    ne->primary_cross_col = c.take<int>(ne->primary_cross_count + 1);
+}
+
+__global__ void narrow_kernel(const int64_t* __restrict__ in, int* __restrict__ out, int64_t n)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = static_cast<int>(in[i]);
+}
+
+// cross_eliminated[c] = l for the crosses of every eliminated block
+__global__ void cross_owner_kernel(const int* __restrict__ offsets, int64_t L, int* __restrict__ owner)
+{
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < L; l += int64_t(gridDim.x) * blockDim.x)
+        for (int c = offsets[l]; c < offsets[l + 1]; ++c)
+            owner[c] = static_cast<int>(l);
+}
+
+// crosses of the observation path: one per distinct primary of each eliminated bucket,
+// in ascending primary order
+__global__ void observation_crosses_kernel(CooView v, const int* __restrict__ cross_offsets,
+                                           int* __restrict__ cross_primary)
+{
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < v.rows; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        int at = cross_offsets[l];
+        const int b = v.bucket_start[l], e = v.bucket_start[l + 1];
+        for (int q = b; q < e; ++q)
+        {
+            const uint32_t p = static_cast<uint32_t>(v.keys[q] >> 32);
+            if (q == b || p != static_cast<uint32_t>(v.keys[q - 1] >> 32))
+                cross_primary[at++] = static_cast<int>(p);
+        }
+    }
+}
+
+__global__ void compare_kernel(const int64_t* __restrict__ a, const int64_t* __restrict__ b, int64_t n, int* differs)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        if (a[i] != b[i])
+            *differs = 1;
+}
+
+template <typename T>
+__device__ __forceinline__ T huber_weight(const T* r, int m, T delta)
+{
+    T squared = T(0);
+    for (int k = 0; k < m; ++k)
+        squared = add_rn(squared, mul_rn(r[k], r[k]));
+    if (delta == T(0) || squared <= mul_rn(delta, delta))
+        return T(1);
+    return delta / sqrt(squared);
+}
+
+// Per eliminated block: Huber weights, Hll, g_l and the cross blocks W of its distinct primaries.
+template <typename T, int BP, int BL>
+__global__ void __launch_bounds__(128) eliminated_accumulate_kernel(
+    CooView v, int m_rt, int bp_rt, int bl_rt, const T* __restrict__ jp, const T* __restrict__ jl,
+    const T* __restrict__ res, T delta, const int* __restrict__ cross_offsets, T* __restrict__ hll,
+    T* __restrict__ gl, T* __restrict__ w)
+{
+    const int bp = BP > 0 ? BP : bp_rt;
+    const int bl = BL > 0 ? BL : bl_rt;
+    const int m = m_rt;
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < v.rows; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int b = v.bucket_start[l], e = v.bucket_start[l + 1];
+        T* H = hll + l * bl * bl;
+        T* g = gl + l * bl;
+        for (int i = 0; i < bl * bl; ++i)
+            H[i] = T(0);
+        for (int i = 0; i < bl; ++i)
+            g[i] = T(0);
+        // eliminated terms in input order (selection over the bucket, which is sorted by
+        // (primary, input offset)); addResidualBlocks accumulates Hll/g_l per residual in
+        // call order, block_normal_equations.cpp:294-311
+        // (buckets longer than kSelectMax are visited in bucket order instead: deterministic,
+        // but the summation order then differs from the reference's call order)
+        constexpr int kSelectMax = 64;
+        const bool select = e - b <= kSelectMax;
+        uint32_t last = 0;
+        for (int visited = 0; visited < e - b; ++visited)
+        {
+            uint32_t best = 0xffffffffu;
+            if (select)
+            {
+                for (int q = b; q < e; ++q)
+                {
+                    const uint32_t src = static_cast<uint32_t>(v.keys[q]);
+                    if ((visited == 0 || src > last) && src < best)
+                        best = src;
+                }
+            }
+            else
+            {
+                best = static_cast<uint32_t>(v.keys[b + visited]);
+            }
+            last = best;
+            const int64_t i = best;
+            const T* r = res + i * m;
+            const T weight = huber_weight(r, m, delta);
+            const T* J = jl + i * m * bl;
+            for (int row = 0; row < m; ++row)
+                for (int col = 0; col < bl; ++col)
+                {
+                    const T value = J[row * bl + col];
+                    g[col] = add_rn(g[col], mul_rn(mul_rn(weight, value), r[row]));
+                    for (int other = 0; other < bl; ++other)
+                        H[col * bl + other] = add_rn(H[col * bl + other], mul_rn(mul_rn(weight, value), J[row * bl + other]));
+                }
+        }
+        // cross blocks: runs of equal primary, observations in input order inside a run
+        // (block_normal_equations.cpp:268-292)
+        int cross = cross_offsets[l] - 1;
+        for (int q = b; q < e; ++q)
+        {
+            const uint64_t key = v.keys[q];
+            if (q == b || (key >> 32) != (v.keys[q - 1] >> 32))
+            {
+                ++cross;
+                T* W = w + int64_t(cross) * bp * bl;
+                for (int k = 0; k < bp * bl; ++k)
+                    W[k] = T(0);
+            }
+            T* W = w + int64_t(cross) * bp * bl;
+            const int64_t i = static_cast<uint32_t>(key);
+            const T* r = res + i * m;
+            const T weight = huber_weight(r, m, delta);
+            const T* Jp = jp + i * m * bp;
+            const T* Jl = jl + i * m * bl;
+            for (int row = 0; row < m; ++row)
+                for (int pc = 0; pc < bp; ++pc)
+                {
+                    const T pv = Jp[row * bp + pc];
+                    for (int ec = 0; ec < bl; ++ec)
+                        W[pc * bl + ec] = add_rn(W[pc * bl + ec], mul_rn(mul_rn(weight, pv), Jl[row * bl + ec]));
+                }
+        }
+    }
+}
+
+// Per primary block: Hpp and g_p over its observations (input order), reduced in a fixed
+// tree: each thread sums a contiguous slice serially, slices are combined in thread order.
+template <typename T, int BP>
+__global__ void __launch_bounds__(128) primary_accumulate_kernel(CooView v, int m, int bp_rt,
+                                                                 const T* __restrict__ jp, const T* __restrict__ res,
+                                                                 T delta, T* __restrict__ hpp, T* __restrict__ gp)
+{
+    constexpr int MAXB = BP > 0 ? BP : 16;
+    const int bp = BP > 0 ? BP : bp_rt;
+    extern __shared__ unsigned char smem_raw[];
+    T* part = reinterpret_cast<T*>(smem_raw); // [blockDim][bp*bp + bp]
+    const int width = bp * bp + bp;
+    for (int64_t p = blockIdx.x; p < v.rows; p += gridDim.x)
+    {
+        const int b = v.bucket_start[p], e = v.bucket_start[p + 1];
+        const int len = e - b;
+        const int per = (len + blockDim.x - 1) / blockDim.x;
+        const int lo = b + min(len, int(threadIdx.x) * per), hi = b + min(len, int(threadIdx.x + 1) * per);
+        T acc[MAXB * MAXB + MAXB];
+        for (int k = 0; k < width; ++k)
+            acc[k] = T(0);
+        for (int q = lo; q < hi; ++q)
+        {
+            const int64_t i = static_cast<uint32_t>(v.keys[q]);
+            const T* r = res + i * m;
+            const T weight = huber_weight(r, m, delta);
+            const T* J = jp + i * m * bp;
+            for (int row = 0; row < m; ++row)
+                for (int col = 0; col < bp; ++col)
+                {
+                    const T value = J[row * bp + col];
+                    acc[bp * bp + col] = add_rn(acc[bp * bp + col], mul_rn(mul_rn(weight, value), r[row]));
+                    for (int other = 0; other < bp; ++other)
+                        acc[col * bp + other] =
+                            add_rn(acc[col * bp + other], mul_rn(mul_rn(weight, value), J[row * bp + other]));
+                }
+        }
+        for (int k = 0; k < width; ++k)
+            part[threadIdx.x * width + k] = acc[k];
+        __syncthreads();
+        for (int k = threadIdx.x; k < width; k += blockDim.x)
+        {
+            T total = T(0);
+            for (int t = 0; t < blockDim.x; ++t)
+                total = add_rn(total, part[t * width + k]);
+            if (k < bp * bp)
+                hpp[p * bp * bp + k] = total;
+            else
+                gp[p * bp + (k - bp * bp)] = total;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+void ne_upload(pm_normal_equations* ne, cudaStream_t stream, const T* hpp, const T* hll, const T* gp, const T* gl,
+               int64_t C, const int64_t* cross_offsets, const int64_t* cross_primary, const T* cross_values,
+               int64_t PC, const int64_t* pc_row, const int64_t* pc_col, const T* pc_values)
+{
+    if (!ne)
+        fail(PM_INVALID_ARGUMENT, "normal equations handle is null");
+    if (ne->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "normal equations scalar type mismatch");
+    if (C < 0 || PC < 0 || C > INT32_MAX - 1 || PC > INT32_MAX - 1)
+        fail(PM_INVALID_ARGUMENT, "invalid cross block counts");
+    // host-side topology validation (the reference rejects these at accumulation time)
+    if (ne->L > 0 && (!cross_offsets || cross_offsets[0] != 0 || cross_offsets[ne->L] != C))
+        fail(PM_INVALID_ARGUMENT, "cross offsets must start at zero and end at the cross count");
+    for (int64_t l = 0; l < ne->L; ++l)
+        if (cross_offsets[l + 1] < cross_offsets[l])
+            fail(PM_INVALID_ARGUMENT, "cross offsets must be non-decreasing");
+    for (int64_t c = 0; c < C; ++c)
+        if (cross_primary[c] < 0 || cross_primary[c] >= ne->P)
+            fail(PM_OUT_OF_RANGE, "BlockNormalEquations: primary block index out of range");
+    for (int64_t k = 0; k < PC; ++k)
+        if (pc_row[k] < 0 || pc_col[k] >= ne->P || pc_row[k] >= pc_col[k])
+            fail(PM_INVALID_ARGUMENT, "BlockNormalEquations: primary cross blocks must be upper triangular");
+    ne->cross_count = C;
+    ne->primary_cross_count = PC;
+    layout_numeric(ne, stream);
+    layout_topology(ne, stream);
+    const size_t s = sizeof(T);
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (bytes)
+            PM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+    };
+    up(ne->primary_diagonal, hpp, ne->P * ne->bp * ne->bp * s);
+    up(ne->eliminated_diagonal, hll, ne->L * ne->bl * ne->bl * s);
+    up(ne->primary_gradient, gp, ne->P * ne->bp * s);
+    up(ne->eliminated_gradient, gl, ne->L * ne->bl * s);
+    up(ne->cross_values, cross_values, C * ne->bp * ne->bl * s);
+    up(ne->primary_cross_values, pc_values, PC * ne->bp * ne->bp * s);
+    // int64 -> int32 topology through a staging buffer
+    std::vector<int> staging(static_cast<size_t>(std::max<int64_t>({ne->L + 1, C, PC, 1})));
+    auto narrow = [&](int* dst, const int64_t* src, int64_t n) {
+        for (int64_t i = 0; i < n; ++i)
+            staging[i] = static_cast<int>(src[i]);
+        if (n)
+        {
+            PM_CUDA(cudaMemcpyAsync(dst, staging.data(), n * sizeof(int), cudaMemcpyHostToDevice, stream));
+            PM_CUDA(cudaStreamSynchronize(stream));
+        }
+    };
+    if (ne->L > 0)
+        narrow(ne->cross_offsets, cross_offsets, ne->L + 1);
+    else
+        PM_CUDA(cudaMemsetAsync(ne->cross_offsets, 0, sizeof(int), stream));
+    narrow(ne->cross_primary, cross_primary, C);
+    narrow(ne->primary_cross_row, pc_row, PC);
+    narrow(ne->primary_cross_col, pc_col, PC);
+    if (ne->L > 0)
+    {
+        cross_owner_kernel<<<grid_for(ne->L, 256, 4096), 256, 0, stream>>>(ne->cross_offsets, ne->L,
+                                                                           ne->cross_eliminated);
+        PM_LAUNCH_CHECK();
+    }
+    PM_CUDA(cudaStreamSynchronize(stream));
+    ne->observation_topology = false;
+    ne->topology_version += 1;
+}
+
+template <typename T>
+void ne_download(const pm_normal_equations* ne, cudaStream_t stream, T* hpp, T* hll, T* gp, T* gl,
+                 int64_t* cross_offsets, int64_t* cross_primary, T* cross_values, int64_t* pc_row, int64_t* pc_col,
+                 T* pc_values)
+{
+    if (!ne)
+        fail(PM_INVALID_ARGUMENT, "normal equations handle is null");
+    if (ne->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "normal equations scalar type mismatch");
+    const size_t s = sizeof(T);
+    auto down = [&](void* dst, const void* src, size_t bytes) {
+        if (dst && bytes)
+            PM_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+    };
+    down(hpp, ne->primary_diagonal, ne->P * ne->bp * ne->bp * s);
+    down(hll, ne->eliminated_diagonal, ne->L * ne->bl * ne->bl * s);
+    down(gp, ne->primary_gradient, ne->P * ne->bp * s);
+    down(gl, ne->eliminated_gradient, ne->L * ne->bl * s);
+    down(cross_values, ne->cross_values, ne->cross_count * ne->bp * ne->bl * s);
+    down(pc_values, ne->primary_cross_values, ne->primary_cross_count * ne->bp * ne->bp * s);
+    std::vector<int> staging(static_cast<size_t>(std::max<int64_t>({ne->L + 1, ne->cross_count, ne->primary_cross_count, 1})));
+    auto widen = [&](int64_t* dst, const int* src, int64_t n) {
+        if (!dst || n == 0)
+            return;
+        PM_CUDA(cudaMemcpyAsync(staging.data(), src, n * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaStreamSynchronize(stream));
+        for (int64_t i = 0; i < n; ++i)
+            dst[i] = staging[i];
+    };
+    if (ne->L > 0)
+        widen(cross_offsets, ne->cross_offsets, ne->L + 1);
+    else if (cross_offsets)
+        cross_offsets[0] = 0;
+    widen(cross_primary, ne->cross_primary, ne->cross_count);
+    widen(pc_row, ne->primary_cross_row, ne->primary_cross_count);
+    widen(pc_col, ne->primary_cross_col, ne->primary_cross_count);
+    PM_CUDA(cudaStreamSynchronize(stream));
+}
+
+template <typename T>
+void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, int64_t m, const int64_t* obs_primary,
+                   const int64_t* obs_eliminated, const T* jp, const T* jl, const T* res, T delta)
+{
+    if (!ne)
+        fail(PM_INVALID_ARGUMENT, "normal equations handle is null");
+    if (ne->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "normal equations scalar type mismatch");
+    if (count < 0 || m <= 0 || m > 64)
+        fail(PM_INVALID_ARGUMENT, "observation count must be non-negative and residual size in [1, 64]");
+    if (!(delta >= T(0)) || !std::isfinite(static_cast<double>(delta)))
+        fail(PM_INVALID_ARGUMENT, "evaluateHuberLoss: delta must be finite and non-negative");
+    if (count > INT32_MAX - 1)
+        fail(PM_OVERFLOW_ERROR, "observation count exceeds the int32 range of the device path");
+    if (ne->bp > 16 || ne->bl > 16)
+        fail(PM_INVALID_ARGUMENT, "device observation path supports block sizes up to 16");
+    if (count > 0 && (!obs_primary || !obs_eliminated || !jp || !jl || !res))
+        fail(PM_INVALID_ARGUMENT, "observation arrays must be non-null");
+    // ---- topology (cached while the index arrays are unchanged)
+    bool rebuild = !ne->observation_topology || ne->observation_count != count || ne->residual_size != m;
+    int64_t* saved_primary = nullptr;
+    int64_t* saved_eliminated = nullptr;
+    int64_t* zeros = nullptr;
+    int* differs = nullptr;
+    auto carve = [&]() {
+        Carver c;
+        c.base = static_cast<char*>(ne->observation_copy.ptr);
+        saved_primary = c.take<int64_t>(count + 1);
+        saved_eliminated = c.take<int64_t>(count + 1);
+        zeros = c.take<int64_t>(count + 1);
+        differs = c.take<int>(1);
+    };
+    if (!rebuild)
+    {
+        carve();
+        PM_CUDA(cudaMemsetAsync(differs, 0, sizeof(int), stream));
+        compare_kernel<<<grid_for(count, 256, 4096), 256, 0, stream>>>(obs_primary, saved_primary, count, differs);
+        PM_LAUNCH_CHECK();
+        compare_kernel<<<grid_for(count, 256, 4096), 256, 0, stream>>>(obs_eliminated, saved_eliminated, count,
+                                                                         differs);
+        PM_LAUNCH_CHECK();
+        int host_differs = 0;
+        PM_CUDA(cudaMemcpyAsync(&host_differs, differs, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaStreamSynchronize(stream));
+        rebuild = host_differs != 0;
+    }
+    if (rebuild)
+    {
+        Carver plan;
+        plan.take<int64_t>(count + 1);
+        plan.take<int64_t>(count + 1);
+        plan.take<int64_t>(count + 1);
+        plan.take<int>(1);
+        ne->observation_copy.ensure(plan.offset + 256, stream, "normal equations");
+        carve();
+        if (!ne->by_eliminated && pm_sparse_workspace_create(&ne->by_eliminated) != PM_OK)
+            fail(PM_RUNTIME_ERROR, "could not create the observation sort workspace");
+        if (!ne->by_primary && pm_sparse_workspace_create(&ne->by_primary) != PM_OK)
+            fail(PM_RUNTIME_ERROR, "could not create the observation sort workspace");
+        PM_CUDA(cudaMemsetAsync(zeros, 0, (count + 1) * sizeof(int64_t), stream));
+        coo_prepare<float>(ne->by_eliminated, stream, ne->L, ne->P, count, obs_eliminated, obs_primary, nullptr);
+        const int64_t crosses = coo_internal_status(ne->by_eliminated, stream, "accumulate observations");
+        coo_prepare<float>(ne->by_primary, stream, ne->P, 1, count, obs_primary, zeros, nullptr);
+        coo_internal_status(ne->by_primary, stream, "accumulate observations");
+        ne->cross_count = crosses;
+        ne->primary_cross_count = 0;
+        layout_topology(ne, stream);
+        const CooView ve = coo_view(ne->by_eliminated);
+        if (ne->L > 0)
+        {
+            narrow_kernel<<<grid_for(ne->L + 1, 256, 4096), 256, 0, stream>>>(ve.row_offsets, ne->cross_offsets,
+                                                                              ne->L + 1);
+            PM_LAUNCH_CHECK();
+            observation_crosses_kernel<<<grid_for(ne->L, 128, 8192), 128, 0, stream>>>(ve, ne->cross_offsets,
+                                                                                       ne->cross_primary);
+            PM_LAUNCH_CHECK();
+            cross_owner_kernel<<<grid_for(ne->L, 256, 4096), 256, 0, stream>>>(ne->cross_offsets, ne->L,
+                                                                               ne->cross_eliminated);
+            PM_LAUNCH_CHECK();
+        }
+        else
+        {
+            PM_CUDA(cudaMemsetAsync(ne->cross_offsets, 0, sizeof(int), stream));
+        }
+        if (count > 0)
+        {
+            PM_CUDA(cudaMemcpyAsync(saved_primary, obs_primary, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, stream));
+            PM_CUDA(cudaMemcpyAsync(saved_eliminated, obs_eliminated, count * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                                    stream));
+        }
+        ne->observation_count = count;
+        ne->residual_size = m;
+        ne->observation_topology = true;
+        ne->topology_version += 1;
+    }
+    layout_numeric(ne, stream);
+    // ---- numeric accumulation
+    const CooView ve = coo_view(ne->by_eliminated);
+    const CooView vp = coo_view(ne->by_primary);
+    T* hll = static_cast<T*>(ne->eliminated_diagonal);
+    T* gl = static_cast<T*>(ne->eliminated_gradient);
+    T* w = static_cast<T*>(ne->cross_values);
+    T* hpp = static_cast<T*>(ne->primary_diagonal);
+    T* gp = static_cast<T*>(ne->primary_gradient);
+    const int bp = static_cast<int>(ne->bp), bl = static_cast<int>(ne->bl), mm = static_cast<int>(m);
+    if (ne->L > 0)
+    {
+        const unsigned grid = grid_for(ne->L, 128, 1 << 20);
+        if (bp == 6 && bl == 3)
+            eliminated_accumulate_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(ve, mm, bp, bl, jp, jl, res, delta,
+                                                                           ne->cross_offsets, hll, gl, w);
+        else
+            eliminated_accumulate_kernel<T, 0, 0><<<grid, 128, 0, stream>>>(ve, mm, bp, bl, jp, jl, res, delta,
+                                                                           ne->cross_offsets, hll, gl, w);
+        PM_LAUNCH_CHECK();
+    }
+    if (ne->P > 0)
+    {
+        // one slice per thread; the per-thread partials live in shared memory (<= 200 KB)
+        const size_t width_bytes = size_t(bp * bp + bp) * sizeof(T);
+        const int threads = static_cast<int>(std::max<size_t>(32, std::min<size_t>(128, (200u << 10) / width_bytes / 32 * 32)));
+        const size_t smem = size_t(threads) * width_bytes;
+        const unsigned grid = grid_for(ne->P, 1, 1 << 20);
+        if (bp == 6)
+        {
+            PM_CUDA(cudaFuncSetAttribute(primary_accumulate_kernel<T, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+            primary_accumulate_kernel<T, 6><<<grid, threads, smem, stream>>>(vp, mm, bp, jp, res, delta, hpp, gp);
+            PM_LAUNCH_CHECK();
+        }
+        else
+        {
+            PM_CUDA(cudaFuncSetAttribute(primary_accumulate_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem)));
+            primary_accumulate_kernel<T, 0><<<grid, threads, smem, stream>>>(vp, mm, bp, jp, res, delta, hpp, gp);
+            PM_LAUNCH_CHECK();
+        }
+        PM_LAUNCH_CHECK();
+    }
+}
+
+} // namespace
+} // namespace pm
+
+extern "C" {
+
+int pm_ne_create(int64_t P, int64_t L, int64_t bp, int64_t bl, int value_size, pm_normal_equations** out)
+{
+    return pm::guarded([&] {
+        if (!out)
+            pm::fail(PM_INVALID_ARGUMENT, "output handle pointer is null");
+        if (P < 0 || L < 0 || bp <= 0 || bl <= 0)
+            pm::fail(PM_INVALID_ARGUMENT,
+                     "BlockNormalEquations: block counts must be non-negative and block sizes positive");
+        if (value_size != 4 && value_size != 8)
+            pm::fail(PM_INVALID_ARGUMENT, "value size must be 4 (float) or 8 (double)");
+        if (P > INT32_MAX / 64 || L > INT32_MAX - 1)
+            pm::fail(PM_OVERFLOW_ERROR, "block counts exceed the int32 range of the device path");
+        auto* ne = new pm_normal_equations();
+        ne->P = P;
+        ne->L = L;
+        ne->bp = bp;
+        ne->bl = bl;
+        ne->value_size = value_size;
+        *out = ne;
+    });
+}
+
+void pm_ne_destroy(pm_normal_equations* ne) { delete ne; }
+
+int pm_ne_counts(const pm_normal_equations* ne, int64_t* cross_count, int64_t* primary_cross_count,
+                 int64_t* topology_version)
+{
+    return pm::guarded([&] {
+        if (!ne)
+            pm::fail(PM_INVALID_ARGUMENT, "normal equations handle is null");
+        if (cross_count)
+            *cross_count = ne->cross_count;
+        if (primary_cross_count)
+            *primary_cross_count = ne->primary_cross_count;
+        if (topology_version)
+            *topology_version = ne->topology_version;
+    });
+}
+
+#define PM_NE_API(SFX, T)                                                                                          \
+    int pm_ne_upload_##SFX(pm_normal_equations* ne, pm_stream_t s, const T* hpp, const T* hll, const T* gp,          \
+                           const T* gl, int64_t C, const int64_t* co, const int64_t* cp, const T* cv, int64_t PC,   \
+                           const int64_t* pr, const int64_t* pcn, const T* pv)                                     \
+    {                                                                                                               \
+        return pm::guarded([&] { pm::ne_upload<T>(ne, s, hpp, hll, gp, gl, C, co, cp, cv, PC, pr, pcn, pv); });     \
+    }                                                                                                               \
+    int pm_ne_download_##SFX(const pm_normal_equations* ne, pm_stream_t s, T* hpp, T* hll, T* gp, T* gl,            \
+                             int64_t* co, int64_t* cp, T* cv, int64_t* pr, int64_t* pcn, T* pv)                     \
+    {                                                                                                               \
+        return pm::guarded([&] { pm::ne_download<T>(ne, s, hpp, hll, gp, gl, co, cp, cv, pr, pcn, pv); });          \
+    }                                                                                                               \
+    int pm_ne_accumulate_observations_##SFX(pm_normal_equations* ne, pm_stream_t s, int64_t count, int64_t m,       \
+                                            const int64_t* op, const int64_t* ol, const T* jp, const T* jl,         \
+                                            const T* r, T delta)                                                    \
+    {                                                                                                               \
+        return pm::guarded([&] { pm::ne_accumulate<T>(ne, s, count, m, op, ol, jp, jl, r, delta); });               \
+    }
+
+PM_NE_API(f32, float)
+PM_NE_API(f64, double)
+
+} // extern "C"

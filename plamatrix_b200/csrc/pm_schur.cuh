@@ -1,0 +1,105 @@
+// Device-resident two-block normal equations (the state of the reference's
+// BlockNormalEquations, include/plamatrix/optimization/block_schur.h:196-319) and the
+// pieces shared by the accumulation and Schur-solver translation units.
+#pragma once
+
+#include "pm_common.cuh"
+
+struct pm_normal_equations
+{
+    int64_t P = 0, L = 0, bp = 0, bl = 0;
+    int value_size = 8;
+    int64_t cross_count = 0;         // C: distinct (primary, eliminated) pairs
+    int64_t primary_cross_count = 0; // PC: upper-triangular primary-primary blocks
+    // numeric state (Scalar)
+    pm::DeviceBuffer numeric;
+    void* primary_diagonal = nullptr;    // P * bp * bp, row-major blocks
+    void* eliminated_diagonal = nullptr; // L * bl * bl
+    void* primary_gradient = nullptr;    // P * bp
+    void* eliminated_gradient = nullptr; // L * bl
+    void* cross_values = nullptr;        // C * bp * bl, grouped by eliminated block
+    void* primary_cross_values = nullptr; // PC * bp * bp
+    // topology (int32)
+    pm::DeviceBuffer topology;
+    int* cross_offsets = nullptr; // L + 1: crosses of eliminated l are [off[l], off[l+1])
+    int* cross_primary = nullptr; // C
+    int* cross_eliminated = nullptr; // C
+    int* primary_cross_row = nullptr; // PC (row < col)
+    int* primary_cross_col = nullptr; // PC
+    int64_t topology_version = 0;     // bumped whenever the topology arrays change
+    // observation-path topology cache
+    pm_sparse_workspace* by_eliminated = nullptr; // observations bucketed by eliminated block
+    pm_sparse_workspace* by_primary = nullptr;    // observations bucketed by primary block
+    pm::DeviceBuffer observation_copy;            // saved index arrays + zero column
+    int64_t observation_count = -1;
+    int64_t residual_size = 0;
+    bool observation_topology = false;
+    ~pm_normal_equations();
+};
+
+namespace pm
+{
+
+template <typename T>
+__device__ __forceinline__ T mul_rn(T a, T b);
+template <>
+__device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
+template <>
+__device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ T add_rn(T a, T b);
+template <>
+__device__ __forceinline__ float add_rn<float>(float a, float b) { return __fadd_rn(a, b); }
+template <>
+__device__ __forceinline__ double add_rn<double>(double a, double b) { return __dadd_rn(a, b); }
+
+// Cholesky-based SPD inverse in FP64 (the arithmetic of invertPositiveDefiniteInto,
+// src/optimization/block_schur_linear_algebra.h:91-147).  `lower` and `work` are scratch.
+template <int N>
+__device__ __forceinline__ bool spd_inverse(const double* m, int n, double* inv, double* lower, double* work)
+{
+    for (int i = 0; i < n * n; ++i)
+        lower[i] = 0.0;
+    for (int row = 0; row < n; ++row)
+    {
+        for (int col = 0; col <= row; ++col)
+        {
+            double value = m[row * n + col];
+            for (int k = 0; k < col; ++k)
+                value = __dadd_rn(value, -__dmul_rn(lower[row * n + k], lower[col * n + k]));
+            if (row == col)
+            {
+                if (!(value > 0.0) || !isfinite(value))
+                    return false;
+                lower[row * n + col] = sqrt(value);
+            }
+            else
+            {
+                lower[row * n + col] = value / lower[col * n + col];
+            }
+        }
+    }
+    for (int i = 0; i < n * n; ++i)
+        inv[i] = 0.0;
+    for (int col = 0; col < n; ++col)
+    {
+        for (int row = 0; row < n; ++row)
+        {
+            double value = row == col ? 1.0 : 0.0;
+            for (int k = 0; k < row; ++k)
+                value = __dadd_rn(value, -__dmul_rn(lower[row * n + k], work[k]));
+            work[row] = value / lower[row * n + row];
+        }
+        for (int off = 0; off < n; ++off)
+        {
+            const int row = n - 1 - off;
+            double value = work[row];
+            for (int k = row + 1; k < n; ++k)
+                value = __dadd_rn(value, -__dmul_rn(lower[k * n + row], inv[k * n + col]));
+            inv[row * n + col] = value / lower[row * n + row];
+        }
+    }
+    return true;
+}
+
+} // namespace pm

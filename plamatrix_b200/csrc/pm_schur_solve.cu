@@ -1,0 +1,1683 @@
+// Damped Schur-complement solve on the device: the hot path of the reference's
+// solveDampedSchurComplement (src/optimization/block_schur.cpp:54-459) with its reusable
+// Schur pattern (src/optimization/block_schur_sparse_assembly.h:41-260, 472-520).
+//
+// Pipeline (all on one stream, no host round trip except the pattern-cache check and the
+// convergence polls):
+//   1. eliminated blocks: damping H_ii += lambda * max(|H_ii|, minDiag), FP64 Cholesky
+//      inverse, y_l = Hll^-1 g_l                                (one thread per block)
+//   2. pattern (only when the topology changed): per-primary cross lists, block-CSR rows
+//      from shared-memory bitmaps over the block columns, transpose map
+//   3. assembly, one CTA per block row p: S_pq = base_pq - sum_l W_pl Hll^-1 W_ql^T for the
+//      upper blocks (q >= p), the diagonal block and its FP64 Cholesky inverse (block-Jacobi
+//      preconditioner), and the reduced RHS b_p = -g_p + sum_l W_pl y_l.  Crosses are taken in
+//      chunks of 64; each chunk cross marks the upper blocks it touches in per-block 64-bit
+//      masks (integer atomicOr: order independent), then the thread owning a block walks its
+//      mask in cross order and accumulates the 6x6 product in registers.  No float atomics:
+//      the result is bitwise reproducible.  Lower blocks are mirrored afterwards.
+//   4. block-Jacobi PCG on the 6x6 block-CSR (warp per block row SpMV with 128-bit loads,
+//      FP64 dots finished by the last block, alpha/beta/convergence on the device); in mixed
+//      mode an FP64 iterative-refinement loop around an FP32 inner PCG
+//   5. back-substitution dl = Hll^-1 (-g_l - sum W^T dp)                (thread per block)
+#include "pm_schur.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+#include <vector>
+
+namespace pm
+{
+namespace
+{
+constexpr long long kNone = 0x7fffffffffffffffLL;
+constexpr int kRowThreads = 128;
+constexpr int kVecBlock = 256;
+constexpr int kMaxParts = 1024;
+
+struct SchurStatus
+{
+    long long eliminated_bad;
+    long long preconditioner_bad;
+    long long row_too_wide;
+    int pad[2];
+};
+
+struct SolveState // device-side PCG / refinement scalars
+{
+    double rho, alpha, beta, tolerance, initial_squared, residual_squared, rhs_squared;
+    double true_squared;
+    int iterations, max_iterations, done, converged, breakdown, pad;
+    unsigned int ticket[4];
+};
+
+} // namespace
+} // namespace pm
+
+struct pm_schur_workspace
+{
+    pm::DeviceBuffer pattern;
+    pm::DeviceBuffer numeric;
+    pm::DeviceBuffer scratch;
+    pm_sparse_workspace* prim_sort = nullptr;
+    int64_t pattern_builds = 0;
+    const pm_normal_equations* last_ne = nullptr;
+    int64_t last_version = -1;
+    int64_t P = -1, L = -1, bp = -1, bl = -1, C = -1, PC = -1, B = 0;
+    int value_size = 0;
+    bool assembled = false;
+    // pattern (int32)
+    int* prim_offsets = nullptr;
+    int* prim_cross = nullptr;
+    int* block_row_ptr = nullptr;
+    int* block_col = nullptr;
+    int* block_row = nullptr;
+    int* diag_pos = nullptr;
+    int* transpose = nullptr;
+    int* block_pc = nullptr; // per block: primary-cross index k (forward), -(k+2) transposed, -1 none
+    int* saved_offsets = nullptr;
+    int* saved_primary = nullptr;
+    int* saved_pc = nullptr;
+    // numeric
+    double* hinv = nullptr;
+    double* y = nullptr;
+    void* S = nullptr;   // B * bp * bp, Scalar
+    float* S32 = nullptr; // mixed-precision copy
+    double* rhs = nullptr;
+    double* minv = nullptr;
+    float* minv32 = nullptr;
+    pm::SchurStatus* status = nullptr;
+    pm::SolveState* state = nullptr;
+    double* partials = nullptr;
+    pm::SchurStatus* host_status = nullptr; // pinned
+    pm::SolveState* host_state = nullptr;   // pinned
+    cudaEvent_t events[8] = {};
+    cudaEvent_t sync_event = nullptr;
+    ~pm_schur_workspace()
+    {
+        pattern.release();
+        numeric.release();
+        scratch.release();
+        if (prim_sort)
+            pm_sparse_workspace_destroy(prim_sort);
+        if (host_status)
+            cudaFreeHost(host_status);
+        if (host_state)
+            cudaFreeHost(host_state);
+        for (auto& e : events)
+            if (e)
+                cudaEventDestroy(e);
+        if (sync_event)
+            cudaEventDestroy(sync_event);
+    }
+};
+
+namespace pm
+{
+namespace
+{
+
+// ===================================================================== small kernels
+__global__ void status_reset_kernel(SchurStatus* s)
+{
+    s->eliminated_bad = kNone;
+    s->preconditioner_bad = kNone;
+    s->row_too_wide = kNone;
+}
+
+__global__ void widen_int_kernel(const int* __restrict__ in, int64_t* __restrict__ out, int64_t n)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = in[i];
+}
+
+__global__ void iota_kernel(int64_t* __restrict__ out, int64_t n)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = i;
+}
+
+__global__ void keys_to_cross_kernel(const uint64_t* __restrict__ keys, int64_t n, int* __restrict__ out)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = static_cast<int>(keys[i] >> 32);
+}
+
+__global__ void int_compare_kernel(const int* __restrict__ a, const int* __restrict__ b, int64_t n, int* differs)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        if (a[i] != b[i])
+            *differs = 1;
+}
+
+// ===================================================================== 1. eliminated inverses
+template <typename T, int BL>
+__global__ void eliminated_inverse_kernel(int64_t L, int bl_rt, const T* __restrict__ hll, const T* __restrict__ gl,
+                                          double lambda, double min_diag, double* __restrict__ hinv,
+                                          double* __restrict__ y, SchurStatus* status)
+{
+    constexpr int MB = BL > 0 ? BL : 16;
+    const int bl = BL > 0 ? BL : bl_rt;
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < L; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        double m[MB * MB], inv[MB * MB], lower[MB * MB], work[MB];
+        for (int i = 0; i < bl * bl; ++i)
+            m[i] = static_cast<double>(hll[l * bl * bl + i]);
+        for (int d = 0; d < bl; ++d)
+        {
+            double& v = m[d * bl + d];
+            v = __dadd_rn(v, __dmul_rn(lambda, fmax(fabs(v), min_diag)));
+        }
+        if (!spd_inverse<MB>(m, bl, inv, lower, work))
+        {
+            atomicMin(&status->eliminated_bad, static_cast<long long>(l));
+            for (int i = 0; i < bl * bl; ++i)
+                inv[i] = 0.0;
+        }
+        for (int i = 0; i < bl * bl; ++i)
+            hinv[l * bl * bl + i] = inv[i];
+        for (int r = 0; r < bl; ++r)
+        {
+            double s = 0.0;
+            for (int c = 0; c < bl; ++c)
+                s = __dadd_rn(s, __dmul_rn(inv[r * bl + c], static_cast<double>(gl[l * bl + c])));
+            y[l * bl + r] = s;
+        }
+    }
+}
+
+// ===================================================================== 2. pattern
+__device__ __forceinline__ void set_bit(unsigned* bits, int q) { atomicOr(&bits[q >> 5], 1u << (q & 31)); }
+
+// mark every block column of row p in a shared bitmap of P bits
+__device__ void mark_row(int p, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
+                         const int* __restrict__ cross_eliminated, const int* __restrict__ cross_offsets,
+                         const int* __restrict__ cross_primary, const int* __restrict__ pc_row,
+                         const int* __restrict__ pc_col, int64_t PC, unsigned* bits, int words)
+{
+    for (int w = threadIdx.x; w < words; w += blockDim.x)
+        bits[w] = 0u;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        set_bit(bits, p);
+    const int cb = prim_offsets[p], ce = prim_offsets[p + 1];
+    for (int j = cb + threadIdx.x; j < ce; j += blockDim.x)
+    {
+        const int l = cross_eliminated[prim_cross[j]];
+        for (int c = cross_offsets[l]; c < cross_offsets[l + 1]; ++c)
+            set_bit(bits, cross_primary[c]);
+    }
+    for (int64_t k = threadIdx.x; k < PC; k += blockDim.x)
+    {
+        if (pc_row[k] == p)
+            set_bit(bits, pc_col[k]);
+        if (pc_col[k] == p)
+            set_bit(bits, pc_row[k]);
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(256) row_count_kernel(int64_t P, const int* prim_offsets, const int* prim_cross,
+                                                        const int* cross_eliminated, const int* cross_offsets,
+                                                        const int* cross_primary, const int* pc_row, const int* pc_col,
+                                                        int64_t PC, int* __restrict__ row_count)
+{
+    extern __shared__ unsigned bits[];
+    __shared__ int red[256 / 32];
+    const int words = static_cast<int>((P + 31) / 32);
+    for (int64_t p = blockIdx.x; p < P; p += gridDim.x)
+    {
+        mark_row(static_cast<int>(p), prim_offsets, prim_cross, cross_eliminated, cross_offsets, cross_primary, pc_row,
+                 pc_col, PC, bits, words);
+        int local = 0;
+        for (int w = threadIdx.x; w < words; w += blockDim.x)
+            local += __popc(bits[w]);
+        const int total = block_sum<int, 256>(local, red);
+        if (threadIdx.x == 0)
+            row_count[p] = total;
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) row_fill_kernel(int64_t P, const int* prim_offsets, const int* prim_cross,
+                                                       const int* cross_eliminated, const int* cross_offsets,
+                                                       const int* cross_primary, const int* pc_row, const int* pc_col,
+                                                       int64_t PC, const int* __restrict__ row_ptr,
+                                                       int* __restrict__ block_col, int* __restrict__ block_row,
+                                                       int* __restrict__ diag_pos)
+{
+    extern __shared__ unsigned bits[];
+    __shared__ int scan[256 / 32 + 1];
+    const int words = static_cast<int>((P + 31) / 32);
+    for (int64_t p = blockIdx.x; p < P; p += gridDim.x)
+    {
+        mark_row(static_cast<int>(p), prim_offsets, prim_cross, cross_eliminated, cross_offsets, cross_primary, pc_row,
+                 pc_col, PC, bits, words);
+        int carry = row_ptr[p];
+        for (int w0 = 0; w0 < words; w0 += blockDim.x)
+        {
+            const int w = w0 + threadIdx.x;
+            const unsigned word = w < words ? bits[w] : 0u;
+            int total = 0;
+            int at = carry + block_exclusive_scan<int, 256>(__popc(word), scan, total);
+            unsigned rest = word;
+            while (rest)
+            {
+                const int bit = __ffs(rest) - 1;
+                rest &= rest - 1;
+                const int q = w * 32 + bit;
+                block_col[at] = q;
+                block_row[at] = static_cast<int>(p);
+                if (q == p)
+                    diag_pos[p] = at;
+                ++at;
+            }
+            carry += total;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ int find_col(const int* __restrict__ cols, int lo, int hi, int q)
+{
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (cols[mid] < q)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void transpose_kernel(int64_t B, const int* __restrict__ row_ptr, const int* __restrict__ block_col,
+                                 const int* __restrict__ block_row, int* __restrict__ transpose)
+{
+    for (int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < B; b += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int p = block_row[b], q = block_col[b];
+        transpose[b] = find_col(block_col, row_ptr[q], row_ptr[q + 1], p);
+    }
+}
+
+__global__ void block_pc_kernel(int64_t PC, const int* __restrict__ pc_row, const int* __restrict__ pc_col,
+                                const int* __restrict__ row_ptr, const int* __restrict__ block_col,
+                                int* __restrict__ block_pc)
+{
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < PC; k += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int r = pc_row[k], c = pc_col[k];
+        block_pc[find_col(block_col, row_ptr[r], row_ptr[r + 1], c)] = static_cast<int>(k);
+        block_pc[find_col(block_col, row_ptr[c], row_ptr[c + 1], r)] = -static_cast<int>(k) - 2;
+    }
+}
+
+// ===================================================================== 3. assembly
+template <typename T>
+struct AssembleArgs
+{
+    int64_t P;
+    int bp, bl;
+    const int* prim_offsets;
+    const int* prim_cross;
+    const int* cross_eliminated;
+    const int* cross_offsets;
+    const int* cross_primary;
+    const int* block_row_ptr;
+    const int* block_col;
+    const int* diag_pos;
+    const int* block_pc;
+    const T* hpp;
+    const T* gp;
+    const T* w;
+    const T* pcv;
+    const double* hinv;
+    const double* y;
+    double lambda, min_diag;
+    T* S;
+    double* rhs;
+    double* minv;
+    SchurStatus* status;
+};
+
+template <typename T, int BP, int BL, int CH>
+__global__ void __launch_bounds__(kRowThreads) assemble_kernel(AssembleArgs<T> a)
+{
+    using A = T; // accumulation type of the Schur products
+    constexpr int MP = BP > 0 ? BP : 16;
+    constexpr int ML = BL > 0 ? BL : 16;
+    const int bp = BP > 0 ? BP : a.bp;
+    const int bl = BL > 0 ? BL : a.bl;
+    const int bpl = bp * bl, bpp = bp * bp;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    A* t_stage = reinterpret_cast<A*>(smem_raw);               // [CH][bp*bl]
+    A* d_stage = t_stage + CH * bpl;                            // [CH][bp*bp]
+    A* r_stage = d_stage + CH * bpp;                            // [CH][bp]
+    double* diag = reinterpret_cast<double*>(r_stage + CH * bp); // [bp*bp] (FP64 copy of S_pp)
+    unsigned long long* masks = reinterpret_cast<unsigned long long*>(diag + MP * MP); // [kRowThreads]
+    int* c_off = reinterpret_cast<int*>(masks + kRowThreads);   // [CH]
+    int* c_len = c_off + CH;                                    // [CH]
+    const int t = threadIdx.x;
+
+    for (int64_t pp = blockIdx.x; pp < a.P; pp += gridDim.x)
+    {
+        const int p = static_cast<int>(pp);
+        const int row_end = a.block_row_ptr[p + 1];
+        const int dpos = a.diag_pos[p];
+        const int n_up = row_end - dpos; // upper blocks including the diagonal
+        const int cb = a.prim_offsets[p], ce = a.prim_offsets[p + 1];
+        const int groups = max(1, (n_up - 1 + kRowThreads - 1) / kRowThreads);
+        A dacc = A(0), racc = A(0); // thread t < bp*bp: diagonal entry t; thread 64+t (t < bp): rhs entry
+        for (int g = 0; g < groups; ++g)
+        {
+            const int my_u = 1 + g * kRowThreads + t;
+            const bool owner = my_u < n_up;
+            const int my_q = owner ? a.block_col[dpos + my_u] : -1;
+            A acc[MP * MP];
+#pragma unroll
+            for (int k = 0; k < MP * MP; ++k)
+                acc[k] = A(0);
+            for (int c0 = cb; c0 < ce; c0 += CH)
+            {
+                const int nch = min(CH, ce - c0);
+                masks[t] = 0ull;
+                __syncthreads();
+                if (t < nch)
+                {
+                    const int c = a.prim_cross[c0 + t];
+                    const int l = a.cross_eliminated[c];
+                    const int off = a.cross_offsets[l], len = a.cross_offsets[l + 1] - off;
+                    c_off[t] = off;
+                    c_len[t] = len;
+                    const double* hi = a.hinv + int64_t(l) * bl * bl;
+                    const T* W = a.w + int64_t(c) * bpl;
+                    A* Ts = t_stage + t * bpl;
+                    // T = W Hll^-1 (row r of T = Hll^-1 applied to row r of W; Hll^-1 symmetric)
+                    for (int r = 0; r < bp; ++r)
+                        for (int j = 0; j < bl; ++j)
+                        {
+                            A s = A(0);
+                            for (int m = 0; m < bl; ++m)
+                                s += static_cast<A>(hi[j * bl + m]) * static_cast<A>(W[r * bl + m]);
+                            Ts[r * bl + j] = s;
+                        }
+                    if (g == 0)
+                    {
+                        A* Ds = d_stage + t * bpp;
+                        for (int r = 0; r < bp; ++r)
+                            for (int cc = 0; cc < bp; ++cc)
+                            {
+                                A s = A(0);
+                                for (int m = 0; m < bl; ++m)
+                                    s += Ts[r * bl + m] * static_cast<A>(W[cc * bl + m]);
+                                Ds[r * bp + cc] = s;
+                            }
+                        A* Rs = r_stage + t * bp;
+                        const double* yl = a.y + int64_t(l) * bl;
+                        for (int r = 0; r < bp; ++r)
+                        {
+                            A s = A(0);
+                            for (int m = 0; m < bl; ++m)
+                                s += static_cast<A>(W[r * bl + m]) * static_cast<A>(yl[m]);
+                            Rs[r] = s;
+                        }
+                    }
+                    const int lo = dpos + 1 + g * kRowThreads;
+                    const int hi_pos = min(row_end, lo + kRowThreads);
+                    for (int k = 0; k < len; ++k)
+                    {
+                        const int q = a.cross_primary[off + k];
+                        if (q <= p)
+                            continue;
+                        const int u = find_col(a.block_col, dpos + 1, row_end, q);
+                        if (u >= lo && u < hi_pos)
+                            atomicOr(&masks[u - lo], 1ull << t);
+                    }
+                }
+                __syncthreads();
+                if (g == 0)
+                {
+                    if (t < bpp)
+                        for (int i = 0; i < nch; ++i)
+                            dacc += d_stage[i * bpp + t];
+                    if (t >= 64 && t < 64 + bp)
+                        for (int i = 0; i < nch; ++i)
+                            racc += r_stage[i * bp + (t - 64)];
+                }
+                if (owner)
+                {
+                    unsigned long long m = masks[t];
+                    while (m)
+                    {
+                        const int i = __ffsll(static_cast<long long>(m)) - 1;
+                        m &= m - 1;
+                        const int off = c_off[i], len = c_len[i];
+                        int c2 = off;
+                        while (c2 < off + len && a.cross_primary[c2] != my_q)
+                            ++c2;
+                        if (c2 >= off + len)
+                            continue;
+                        const T* W2 = a.w + int64_t(c2) * bpl;
+                        const A* Ts = t_stage + i * bpl;
+                        A w2[MP * ML];
+#pragma unroll
+                        for (int k = 0; k < MP * ML; ++k)
+                            if (k < bpl)
+                                w2[k] = static_cast<A>(W2[k]);
+#pragma unroll
+                        for (int r = 0; r < MP; ++r)
+                        {
+                            if (r >= bp)
+                                break;
+#pragma unroll
+                            for (int cc = 0; cc < MP; ++cc)
+                            {
+                                if (cc >= bp)
+                                    break;
+                                A s = A(0);
+#pragma unroll
+                                for (int mm = 0; mm < ML; ++mm)
+                                {
+                                    if (mm >= bl)
+                                        break;
+                                    s += Ts[r * bl + mm] * w2[cc * bl + mm];
+                                }
+                                acc[r * bp + cc] += s;
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            if (owner)
+            {
+                const int b = dpos + my_u;
+                const int pc = a.block_pc[b];
+                T* out = a.S + int64_t(b) * bpp;
+                for (int r = 0; r < bp; ++r)
+                    for (int cc = 0; cc < bp; ++cc)
+                    {
+                        A base = A(0);
+                        if (pc >= 0)
+                            base = static_cast<A>(a.pcv[int64_t(pc) * bpp + r * bp + cc]);
+                        out[r * bp + cc] = static_cast<T>(base - acc[r * bp + cc]);
+                    }
+            }
+        }
+        // diagonal block, reduced RHS and block-Jacobi inverse
+        if (t < bpp)
+        {
+            const int r = t / bp, cc = t % bp;
+            double base = static_cast<double>(a.hpp[int64_t(p) * bpp + t]);
+            if (r == cc)
+                base = __dadd_rn(base, __dmul_rn(a.lambda, fmax(fabs(base), a.min_diag)));
+            const A value = static_cast<A>(base) - dacc;
+            a.S[int64_t(dpos) * bpp + t] = static_cast<T>(value);
+            diag[t] = static_cast<double>(value);
+        }
+        if (t >= 64 && t < 64 + bp)
+        {
+            const int r = t - 64;
+            a.rhs[int64_t(p) * bp + r] = -static_cast<double>(a.gp[int64_t(p) * bp + r]) + static_cast<double>(racc);
+        }
+        __syncthreads();
+        if (t == 0)
+        {
+            double inv[MP * MP], lower[MP * MP], work[MP];
+            // symmetrise from the lower triangle, as the reference's Cholesky reads it
+            double m[MP * MP];
+            for (int r = 0; r < bp; ++r)
+                for (int cc = 0; cc < bp; ++cc)
+                    m[r * bp + cc] = r >= cc ? diag[r * bp + cc] : diag[cc * bp + r];
+            if (!spd_inverse<MP>(m, bp, inv, lower, work))
+            {
+                atomicMin(&a.status->preconditioner_bad, static_cast<long long>(p));
+                for (int k = 0; k < bpp; ++k)
+                    inv[k] = 0.0;
+            }
+            for (int k = 0; k < bpp; ++k)
+                a.minv[int64_t(p) * bpp + k] = inv[k];
+        }
+        __syncthreads();
+    }
+}
+
+// lower blocks: S[b] = S[transpose(b)]^T
+template <typename T>
+__global__ void mirror_kernel(int64_t B, int bp, const int* __restrict__ block_row, const int* __restrict__ block_col,
+                              const int* __restrict__ transpose, T* __restrict__ S)
+{
+    const int bpp = bp * bp;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < B * bpp; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t b = i / bpp;
+        if (block_col[b] >= block_row[b])
+            continue;
+        const int e = static_cast<int>(i - b * bpp), r = e / bp, c = e % bp;
+        S[i] = S[int64_t(transpose[b]) * bpp + c * bp + r];
+    }
+}
+
+template <typename Tin, typename Tout>
+__global__ void convert_kernel(const Tin* __restrict__ in, Tout* __restrict__ out, int64_t n)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = static_cast<Tout>(in[i]);
+}
+
+// ===================================================================== 4. block PCG
+template <int K, typename Finish>
+__device__ __forceinline__ void finish_reduce(double (&mine)[K], double* partials, unsigned int* ticket, Finish&& fin)
+{
+    __shared__ double red[kVecBlock / 32];
+    __shared__ bool last;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        const double s = block_sum<double, kVecBlock>(mine[k], red);
+        if (threadIdx.x == 0)
+            partials[k * kMaxParts + blockIdx.x] = s;
+    }
+    __threadfence();
+    if (threadIdx.x == 0)
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    double tot[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+            s += __ldcg(partials + k * kMaxParts + b);
+        tot[k] = block_sum<double, kVecBlock>(s, red);
+    }
+    if (threadIdx.x == 0)
+    {
+        *ticket = 0;
+        fin(tot);
+    }
+}
+
+// y_p = sum_b S_b x_col(b) for block row p; lane-strided over the row's blocks, warp reduce
+template <typename V, typename M, int BP>
+__device__ __forceinline__ void bsr_row(const int* __restrict__ row_ptr, const int* __restrict__ block_col,
+                                        const M* __restrict__ S, const V* __restrict__ x, int bp_rt, int64_t p,
+                                        bool valid, int lane, double* y /* [16] */)
+{
+    constexpr int MP = BP > 0 ? BP : 16;
+    const int bp = BP > 0 ? BP : bp_rt;
+    double acc[MP];
+#pragma unroll
+    for (int r = 0; r < MP; ++r)
+        acc[r] = 0.0;
+    if (valid)
+    {
+        const int b0 = row_ptr[p], b1 = row_ptr[p + 1];
+        for (int b = b0 + lane; b < b1; b += 32)
+        {
+            const int q = block_col[b];
+            const M* blk = S + int64_t(b) * bp * bp;
+            V xv[MP];
+#pragma unroll
+            for (int c = 0; c < MP; ++c)
+                if (c < bp)
+                    xv[c] = x[int64_t(q) * bp + c];
+            if constexpr (BP == 6 && sizeof(M) == 4)
+            {
+                const float4* v4 = reinterpret_cast<const float4*>(blk);
+                float m[36];
+#pragma unroll
+                for (int k = 0; k < 9; ++k)
+                {
+                    const float4 f = __ldg(v4 + k);
+                    m[4 * k] = f.x; m[4 * k + 1] = f.y; m[4 * k + 2] = f.z; m[4 * k + 3] = f.w;
+                }
+#pragma unroll
+                for (int r = 0; r < 6; ++r)
+                {
+                    float s = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 6; ++c)
+                        s = fmaf(m[r * 6 + c], static_cast<float>(xv[c]), s);
+                    acc[r] += s;
+                }
+            }
+            else if constexpr (BP == 6 && sizeof(M) == 8)
+            {
+                const double2* v2 = reinterpret_cast<const double2*>(blk);
+#pragma unroll
+                for (int r = 0; r < 6; ++r)
+                {
+                    const double2 a0 = __ldg(v2 + 3 * r), a1 = __ldg(v2 + 3 * r + 1), a2 = __ldg(v2 + 3 * r + 2);
+                    double s = a0.x * static_cast<double>(xv[0]);
+                    s = fma(a0.y, static_cast<double>(xv[1]), s);
+                    s = fma(a1.x, static_cast<double>(xv[2]), s);
+                    s = fma(a1.y, static_cast<double>(xv[3]), s);
+                    s = fma(a2.x, static_cast<double>(xv[4]), s);
+                    s = fma(a2.y, static_cast<double>(xv[5]), s);
+                    acc[r] += s;
+                }
+            }
+            else
+            {
+                for (int r = 0; r < bp; ++r)
+                {
+                    double s = 0.0;
+                    for (int c = 0; c < bp; ++c)
+                        s += static_cast<double>(blk[r * bp + c]) * static_cast<double>(xv[c]);
+                    acc[r] += s;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < MP; ++r)
+    {
+        if (r >= bp)
+            break;
+        double v = acc[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        y[r] = v;
+    }
+}
+
+// plain y = S x (vector type V)
+template <typename V, typename M, int BP>
+__global__ void __launch_bounds__(kVecBlock) bsr_spmv_kernel(int64_t P, int bp, const int* __restrict__ row_ptr,
+                                                             const int* __restrict__ block_col,
+                                                             const M* __restrict__ S, const V* __restrict__ x,
+                                                             V* __restrict__ y)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
+    const int64_t first = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+    const int64_t span = (P + warps - 1) / warps;
+    for (int64_t k = 0; k < span; ++k)
+    {
+        const int64_t p = first + k * warps;
+        double out[16];
+        bsr_row<V, M, BP>(row_ptr, block_col, S, x, bp, p, p < P, lane, out);
+        if (p < P && lane < bp)
+        {
+            double v = 0.0;
+            for (int r = 0; r < bp; ++r)
+                v = lane == r ? out[r] : v;
+            y[p * bp + lane] = static_cast<V>(v);
+        }
+    }
+}
+
+// q = S p and the p.q partial; alpha = rho / p.q (CPU reduced-PCG semantics:
+// block_schur_cpu_solver.h:41-51, non-positive curvature is reported, not thrown)
+template <typename V, typename M, int BP>
+__global__ void __launch_bounds__(kVecBlock) pcg_bsr_kernel(int64_t P, int bp, const int* __restrict__ row_ptr,
+                                                            const int* __restrict__ block_col,
+                                                            const M* __restrict__ S, const V* __restrict__ p_vec,
+                                                            V* __restrict__ q, double* partials, SolveState* st)
+{
+    if (st->done)
+        return;
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
+    const int64_t first = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32;
+    const int64_t span = (P + warps - 1) / warps;
+    double mine[1] = {0.0};
+    for (int64_t k = 0; k < span; ++k)
+    {
+        const int64_t p = first + k * warps;
+        double out[16];
+        bsr_row<V, M, BP>(row_ptr, block_col, S, p_vec, bp, p, p < P, lane, out);
+        if (p < P && lane < bp)
+        {
+            double v = 0.0;
+            for (int r = 0; r < bp; ++r)
+                v = lane == r ? out[r] : v;
+            const V qv = static_cast<V>(v);
+            q[p * bp + lane] = qv;
+            mine[0] += static_cast<double>(p_vec[p * bp + lane]) * static_cast<double>(qv);
+        }
+    }
+    finish_reduce<1>(mine, partials, &st->ticket[1], [&](double (&tot)[1]) {
+        const double den = tot[0];
+        if (!(den > 0.0) || !isfinite(den))
+        {
+            st->breakdown = 1;
+            st->done = 1;
+            st->alpha = 0.0;
+            return;
+        }
+        st->alpha = st->rho / den;
+    });
+}
+
+// x += alpha p; r_out = r_in - alpha q; z = Minv r_out; r.z, r.r; convergence; beta
+template <typename V, typename PM, int BP>
+__global__ void __launch_bounds__(kVecBlock) pcg_block_update_kernel(int64_t P, int bp_rt, V* __restrict__ x,
+                                                                     const V* __restrict__ p_vec,
+                                                                     const V* __restrict__ q, const V* __restrict__ r_in,
+                                                                     V* __restrict__ r_out, V* __restrict__ z,
+                                                                     const PM* __restrict__ minv, double* partials,
+                                                                     SolveState* st)
+{
+    if (st->done)
+        return;
+    constexpr int MP = BP > 0 ? BP : 16;
+    const int bp = BP > 0 ? BP : bp_rt;
+    const double alpha = st->alpha;
+    double mine[2] = {0.0, 0.0};
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+    {
+        double r[MP];
+#pragma unroll
+        for (int k = 0; k < MP; ++k)
+        {
+            if (k >= bp)
+                break;
+            const int64_t i = p * bp + k;
+            x[i] = static_cast<V>(static_cast<double>(x[i]) + alpha * static_cast<double>(p_vec[i]));
+            r[k] = static_cast<double>(static_cast<V>(static_cast<double>(r_in[i]) - alpha * static_cast<double>(q[i])));
+            r_out[i] = static_cast<V>(r[k]);
+            mine[1] += r[k] * r[k];
+        }
+        const PM* m = minv + p * bp * bp;
+#pragma unroll
+        for (int k = 0; k < MP; ++k)
+        {
+            if (k >= bp)
+                break;
+            double s = 0.0;
+#pragma unroll
+            for (int c = 0; c < MP; ++c)
+            {
+                if (c >= bp)
+                    break;
+                s += static_cast<double>(m[k * bp + c]) * r[c];
+            }
+            const V zk = static_cast<V>(s);
+            z[p * bp + k] = zk;
+            mine[0] += r[k] * static_cast<double>(zk);
+        }
+    }
+    finish_reduce<2>(mine, partials, &st->ticket[2], [&](double (&tot)[2]) {
+        st->iterations += 1;
+        st->residual_squared = tot[1];
+        const double norm = sqrt(fmax(0.0, tot[1]));
+        if (!isfinite(tot[1]))
+        {
+            st->breakdown = 1;
+            st->done = 1;
+            return;
+        }
+        if (norm <= st->tolerance)
+        {
+            st->converged = 1;
+            st->done = 1;
+            return;
+        }
+        if (st->iterations >= st->max_iterations)
+        {
+            st->done = 1;
+            return;
+        }
+        st->beta = tot[0] / st->rho;
+        st->rho = tot[0];
+    });
+}
+
+template <typename V>
+__global__ void pcg_block_direction_kernel(int64_t n, const V* __restrict__ z, V* __restrict__ p,
+                                           const SolveState* st)
+{
+    if (st->done)
+        return;
+    const double beta = st->beta;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        p[i] = static_cast<V>(static_cast<double>(z[i]) + beta * static_cast<double>(p[i]));
+}
+
+// r = b - q; z = Minv r; p = z; rho = r.z; ||r||^2.  tol = tolerance rule on ||r0||.
+template <typename V, typename PM, typename B, int BP>
+__global__ void __launch_bounds__(kVecBlock) pcg_block_init_kernel(int64_t P, int bp_rt, const B* __restrict__ b,
+                                                                   const V* __restrict__ q, V* __restrict__ r,
+                                                                   V* __restrict__ z, V* __restrict__ p_vec,
+                                                                   const PM* __restrict__ minv, double rel, double abs_tol,
+                                                                   int rule, int max_iterations, double* partials,
+                                                                   SolveState* st)
+{
+    constexpr int MP = BP > 0 ? BP : 16;
+    const int bp = BP > 0 ? BP : bp_rt;
+    double mine[2] = {0.0, 0.0};
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+    {
+        double rr[MP];
+#pragma unroll
+        for (int k = 0; k < MP; ++k)
+        {
+            if (k >= bp)
+                break;
+            const int64_t i = p * bp + k;
+            rr[k] = static_cast<double>(static_cast<V>(static_cast<double>(b[i]) - static_cast<double>(q[i])));
+            r[i] = static_cast<V>(rr[k]);
+            mine[1] += rr[k] * rr[k];
+        }
+        const PM* m = minv + p * bp * bp;
+#pragma unroll
+        for (int k = 0; k < MP; ++k)
+        {
+            if (k >= bp)
+                break;
+            double s = 0.0;
+            for (int c = 0; c < bp; ++c)
+                s += static_cast<double>(m[k * bp + c]) * rr[c];
+            const V zk = static_cast<V>(s);
+            z[p * bp + k] = zk;
+            p_vec[p * bp + k] = zk;
+            mine[0] += rr[k] * static_cast<double>(zk);
+        }
+    }
+    finish_reduce<2>(mine, partials, &st->ticket[0], [&](double (&tot)[2]) {
+        st->rho = tot[0];
+        st->initial_squared = tot[1];
+        st->residual_squared = tot[1];
+        st->iterations = 0;
+        st->max_iterations = max_iterations;
+        st->done = 0;
+        st->converged = 0;
+        st->breakdown = 0;
+        const double r0 = sqrt(fmax(0.0, tot[1]));
+        st->tolerance = rule == 0 ? abs_tol + rel * r0 : fmax(abs_tol, rel * r0);
+        if (!isfinite(tot[1]))
+        {
+            st->breakdown = 1;
+            st->done = 1;
+        }
+        else if (r0 <= st->tolerance)
+        {
+            st->converged = 1;
+            st->done = 1;
+        }
+    });
+}
+
+// FP64 residual of the refinement loop: r = b - q (q = S64 x), ||r||^2, ||b||^2
+__global__ void __launch_bounds__(kVecBlock) residual_kernel(int64_t n, const double* __restrict__ b,
+                                                             const double* __restrict__ q, double* __restrict__ r,
+                                                             double* partials, SolveState* st)
+{
+    double mine[2] = {0.0, 0.0};
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const double v = b[i] - q[i];
+        if (r)
+            r[i] = v;
+        mine[0] += v * v;
+        mine[1] += b[i] * b[i];
+    }
+    finish_reduce<2>(mine, partials, &st->ticket[3], [&](double (&tot)[2]) {
+        st->true_squared = tot[0];
+        st->rhs_squared = tot[1];
+    });
+}
+
+template <typename V>
+__global__ void axpy_to_double_kernel(int64_t n, const V* __restrict__ d, double* __restrict__ x)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        x[i] += static_cast<double>(d[i]);
+}
+
+// ===================================================================== 5. back-substitution
+template <typename T, int BP, int BL>
+__global__ void backsub_kernel(int64_t L, int bp_rt, int bl_rt, const int* __restrict__ cross_offsets,
+                               const int* __restrict__ cross_primary, const T* __restrict__ w,
+                               const T* __restrict__ gl, const double* __restrict__ hinv, const T* __restrict__ dp,
+                               T* __restrict__ dl)
+{
+    constexpr int ML = BL > 0 ? BL : 16;
+    const int bp = BP > 0 ? BP : bp_rt;
+    const int bl = BL > 0 ? BL : bl_rt;
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < L; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        T point[ML];
+        for (int i = 0; i < bl; ++i)
+            point[i] = -gl[l * bl + i];
+        for (int c = cross_offsets[l]; c < cross_offsets[l + 1]; ++c)
+        {
+            const T* W = w + int64_t(c) * bp * bl;
+            const T* x = dp + int64_t(cross_primary[c]) * bp;
+            for (int col = 0; col < bl; ++col)
+            {
+                T v = T(0);
+                for (int row = 0; row < bp; ++row)
+                    v = add_rn(v, mul_rn(W[row * bl + col], x[row]));
+                point[col] = add_rn(point[col], -v);
+            }
+        }
+        const double* H = hinv + l * bl * bl;
+        for (int r = 0; r < bl; ++r)
+        {
+            double s = 0.0;
+            for (int c = 0; c < bl; ++c)
+                s = __dadd_rn(s, __dmul_rn(H[r * bl + c], static_cast<double>(point[c])));
+            dl[l * bl + r] = static_cast<T>(s);
+        }
+    }
+}
+
+// scalar CSR in the reference layout (valuePosition, block_schur_sparse_assembly.h:262-272)
+template <typename T, typename O>
+__global__ void export_csr_kernel(int64_t B, int bp, int64_t P, const int* __restrict__ row_ptr,
+                                  const int* __restrict__ block_col, const int* __restrict__ block_row,
+                                  const T* __restrict__ S, int64_t* __restrict__ row_offsets,
+                                  int64_t* __restrict__ col_indices, O* __restrict__ values)
+{
+    const int bpp = bp * bp;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < B * bpp; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int64_t b = i / bpp;
+        const int e = static_cast<int>(i - b * bpp), r = e / bp, c = e % bp;
+        const int p = block_row[b];
+        const int64_t first = row_ptr[p];
+        const int64_t slots = row_ptr[p + 1] - first;
+        const int64_t ordinal = b - first;
+        const int64_t row_start = first * bpp + r * slots * bp;
+        const int64_t pos = row_start + ordinal * bp + c;
+        if (ordinal == 0 && c == 0 && row_offsets)
+            row_offsets[int64_t(p) * bp + r] = row_start;
+        if (col_indices)
+            col_indices[pos] = int64_t(block_col[b]) * bp + c;
+        if (values)
+            values[pos] = static_cast<O>(S[i]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && row_offsets)
+        row_offsets[P * bp] = B * bpp;
+}
+
+} // namespace
+} // namespace pm
+
+// ===================================================================== host orchestration
+namespace pm
+{
+namespace
+{
+
+template <typename T>
+void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
+{
+    const int64_t n = ws->P * ws->bp;
+    const int64_t bpp = ws->bp * ws->bp;
+    Carver plan;
+    plan.take<double>(ws->L * ws->bl * ws->bl + 1);
+    plan.take<double>(ws->L * ws->bl + 1);
+    plan.take<T>(ws->B * bpp + 1);
+    plan.take<float>(mixed ? ws->B * bpp + 1 : 1);
+    plan.take<double>(n + 1);
+    plan.take<double>(ws->P * bpp + 1);
+    plan.take<float>(mixed ? ws->P * bpp + 1 : 1);
+    plan.take<SchurStatus>(1);
+    plan.take<SolveState>(1);
+    plan.take<double>(4 * kMaxParts);
+    plan.take<double>(8 * (n + 1)); // PCG / refinement vectors
+    ws->numeric.ensure(plan.offset + 256, stream, "SchurComplementSolverWorkspace");
+    Carver c;
+    c.base = static_cast<char*>(ws->numeric.ptr);
+    ws->hinv = c.take<double>(ws->L * ws->bl * ws->bl + 1);
+    ws->y = c.take<double>(ws->L * ws->bl + 1);
+    ws->S = c.take<T>(ws->B * bpp + 1);
+    ws->S32 = c.take<float>(mixed ? ws->B * bpp + 1 : 1);
+    ws->rhs = c.take<double>(n + 1);
+    ws->minv = c.take<double>(ws->P * bpp + 1);
+    ws->minv32 = c.take<float>(mixed ? ws->P * bpp + 1 : 1);
+    ws->status = c.take<SchurStatus>(1);
+    ws->state = c.take<SolveState>(1);
+    ws->partials = c.take<double>(4 * kMaxParts);
+}
+
+double* vector_area(pm_schur_workspace* ws)
+{
+    Carver c;
+    c.base = reinterpret_cast<char*>(ws->partials + 4 * kMaxParts);
+    return c.take<double>(1); // aligned start of the 8 (n+1)-sized vector slots
+}
+
+void set_smem(const void* fn, size_t bytes)
+{
+    if (bytes > 48 * 1024)
+        PM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+}
+
+bool topology_matches(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
+{
+    if (ws->P != ne->P || ws->L != ne->L || ws->bp != ne->bp || ws->bl != ne->bl || ws->C != ne->cross_count ||
+        ws->PC != ne->primary_cross_count || !ws->saved_offsets)
+        return false;
+    if (ws->last_ne == ne && ws->last_version == ne->topology_version)
+        return true;
+    int* flag = reinterpret_cast<int*>(ws->status) + 7; // pad slot of the status block
+    PM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), stream));
+    int_compare_kernel<<<grid_for(ne->L + 1, 256, 4096), 256, 0, stream>>>(ne->cross_offsets, ws->saved_offsets,
+                                                                            ne->L + 1, flag);
+    PM_LAUNCH_CHECK();
+    int_compare_kernel<<<grid_for(ne->cross_count, 256, 4096), 256, 0, stream>>>(ne->cross_primary, ws->saved_primary,
+                                                                                 ne->cross_count, flag);
+    PM_LAUNCH_CHECK();
+    int_compare_kernel<<<grid_for(ne->primary_cross_count, 256, 4096), 256, 0, stream>>>(
+        ne->primary_cross_row, ws->saved_pc, ne->primary_cross_count, flag);
+    PM_LAUNCH_CHECK();
+    int_compare_kernel<<<grid_for(ne->primary_cross_count, 256, 4096), 256, 0, stream>>>(
+        ne->primary_cross_col, ws->saved_pc + ne->primary_cross_count, ne->primary_cross_count, flag);
+    PM_LAUNCH_CHECK();
+    int differs = 0;
+    PM_CUDA(cudaMemcpyAsync(&differs, flag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaStreamSynchronize(stream));
+    return differs == 0;
+}
+
+void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
+{
+    const int64_t P = ne->P, L = ne->L, C = ne->cross_count, PC = ne->primary_cross_count;
+    const size_t bitmap = size_t((P + 31) / 32) * sizeof(unsigned);
+    if (bitmap > 200 * 1024)
+        fail(PM_OVERFLOW_ERROR, "Schur pattern build supports up to 1,638,400 primary blocks");
+    // fixed-size pattern arrays and scratch
+    Carver plan;
+    plan.take<int>(P + 1);
+    plan.take<int>(C + 1);
+    plan.take<int>(P + 1);
+    plan.take<int>(P + 1);
+    plan.take<int>(P + 1);
+    plan.take<int>(L + 1);
+    plan.take<int>(C + 1);
+    plan.take<int>(2 * PC + 1);
+    plan.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
+    ws->pattern.ensure(plan.offset + 256, stream, "SchurComplementSolverWorkspace");
+    Carver c;
+    c.base = static_cast<char*>(ws->pattern.ptr);
+    ws->prim_offsets = c.take<int>(P + 1);
+    ws->prim_cross = c.take<int>(C + 1);
+    ws->block_row_ptr = c.take<int>(P + 1);
+    int* row_count = c.take<int>(P + 1);
+    ws->diag_pos = c.take<int>(P + 1);
+    ws->saved_offsets = c.take<int>(L + 1);
+    ws->saved_primary = c.take<int>(C + 1);
+    ws->saved_pc = c.take<int>(2 * PC + 1);
+    void* scan_scratch = c.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
+    // per-primary cross lists, ascending eliminated index (crosses are eliminated-major)
+    ws->scratch.ensure(size_t(2 * (C + 1)) * sizeof(int64_t) + 512, stream, "SchurComplementSolverWorkspace");
+    int64_t* primary64 = static_cast<int64_t*>(ws->scratch.ptr);
+    int64_t* ids64 = primary64 + (C + 1);
+    if (!ws->prim_sort && pm_sparse_workspace_create(&ws->prim_sort) != PM_OK)
+        fail(PM_RUNTIME_ERROR, "could not create the pattern sort workspace");
+    if (C > 0)
+    {
+        widen_int_kernel<<<grid_for(C, 256, 4096), 256, 0, stream>>>(ne->cross_primary, primary64, C);
+        PM_LAUNCH_CHECK();
+        iota_kernel<<<grid_for(C, 256, 4096), 256, 0, stream>>>(ids64, C);
+        PM_LAUNCH_CHECK();
+    }
+    coo_prepare<float>(ws->prim_sort, stream, P, C + 1, C, primary64, ids64, nullptr);
+    coo_internal_status(ws->prim_sort, stream, "Schur pattern");
+    const CooView v = coo_view(ws->prim_sort);
+    PM_CUDA(cudaMemcpyAsync(ws->prim_offsets, v.bucket_start, (P + 1) * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    if (C > 0)
+    {
+        keys_to_cross_kernel<<<grid_for(C, 256, 4096), 256, 0, stream>>>(v.keys, C, ws->prim_cross);
+        PM_LAUNCH_CHECK();
+    }
+    // block-CSR rows
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(P, 8 * sm_count())));
+    set_smem(reinterpret_cast<const void*>(row_count_kernel), bitmap);
+    set_smem(reinterpret_cast<const void*>(row_fill_kernel), bitmap);
+    if (P > 0)
+    {
+        row_count_kernel<<<grid, 256, bitmap, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
+                                                        ne->cross_offsets, ne->cross_primary, ne->primary_cross_row,
+                                                        ne->primary_cross_col, PC, row_count);
+        PM_LAUNCH_CHECK();
+    }
+    exclusive_scan<int, int>(row_count, ws->block_row_ptr, P, scan_scratch, stream);
+    int B = 0;
+    PM_CUDA(cudaMemcpyAsync(&B, ws->block_row_ptr + P, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaStreamSynchronize(stream));
+    ws->B = B;
+    // block arrays live behind the fixed part of the scratch buffer's successor allocation
+    Carver bplan;
+    bplan.take<int>(B + 1);
+    bplan.take<int>(B + 1);
+    bplan.take<int>(B + 1);
+    bplan.take<int>(B + 1);
+    const size_t fixed = plan.offset;
+    ws->pattern.ensure(fixed + bplan.offset + 512, stream, "SchurComplementSolverWorkspace");
+    if (ws->pattern.ptr != c.base)
+    {
+        // the pattern buffer moved: re-carve the fixed part (contents are rebuilt below anyway,
+        // except prim lists / row pointers, which are recomputed by re-running this function)
+        return build_pattern(ws, ne, stream);
+    }
+    Carver bc;
+    bc.base = static_cast<char*>(ws->pattern.ptr) + ((fixed + 255) / 256) * 256;
+    ws->block_col = bc.take<int>(B + 1);
+    ws->block_row = bc.take<int>(B + 1);
+    ws->transpose = bc.take<int>(B + 1);
+    ws->block_pc = bc.take<int>(B + 1);
+    if (P > 0)
+    {
+        row_fill_kernel<<<grid, 256, bitmap, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
+                                                       ne->cross_offsets, ne->cross_primary, ne->primary_cross_row,
+                                                       ne->primary_cross_col, PC, ws->block_row_ptr, ws->block_col,
+                                                       ws->block_row, ws->diag_pos);
+        PM_LAUNCH_CHECK();
+        transpose_kernel<<<grid_for(B, 256, 8192), 256, 0, stream>>>(B, ws->block_row_ptr, ws->block_col, ws->block_row,
+                                                                     ws->transpose);
+        PM_LAUNCH_CHECK();
+    }
+    PM_CUDA(cudaMemsetAsync(ws->block_pc, 0xff, size_t(B + 1) * sizeof(int), stream));
+    if (PC > 0)
+    {
+        block_pc_kernel<<<grid_for(PC, 256, 4096), 256, 0, stream>>>(PC, ne->primary_cross_row, ne->primary_cross_col,
+                                                                     ws->block_row_ptr, ws->block_col, ws->block_pc);
+        PM_LAUNCH_CHECK();
+    }
+    PM_CUDA(cudaMemcpyAsync(ws->saved_offsets, ne->cross_offsets, (L + 1) * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    if (C > 0)
+        PM_CUDA(cudaMemcpyAsync(ws->saved_primary, ne->cross_primary, C * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    if (PC > 0)
+    {
+        PM_CUDA(cudaMemcpyAsync(ws->saved_pc, ne->primary_cross_row, PC * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+        PM_CUDA(cudaMemcpyAsync(ws->saved_pc + PC, ne->primary_cross_col, PC * sizeof(int), cudaMemcpyDeviceToDevice,
+                                stream));
+    }
+    ws->P = P;
+    ws->L = L;
+    ws->bp = ne->bp;
+    ws->bl = ne->bl;
+    ws->C = C;
+    ws->PC = PC;
+    ws->pattern_builds += 1;
+}
+
+template <typename T>
+void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, double lambda, double min_diag,
+                     cudaStream_t stream)
+{
+    AssembleArgs<T> a;
+    a.P = ne->P;
+    a.bp = static_cast<int>(ne->bp);
+    a.bl = static_cast<int>(ne->bl);
+    a.prim_offsets = ws->prim_offsets;
+    a.prim_cross = ws->prim_cross;
+    a.cross_eliminated = ne->cross_eliminated;
+    a.cross_offsets = ne->cross_offsets;
+    a.cross_primary = ne->cross_primary;
+    a.block_row_ptr = ws->block_row_ptr;
+    a.block_col = ws->block_col;
+    a.diag_pos = ws->diag_pos;
+    a.block_pc = ws->block_pc;
+    a.hpp = static_cast<const T*>(ne->primary_diagonal);
+    a.gp = static_cast<const T*>(ne->primary_gradient);
+    a.w = static_cast<const T*>(ne->cross_values);
+    a.pcv = static_cast<const T*>(ne->primary_cross_values);
+    a.hinv = ws->hinv;
+    a.y = ws->y;
+    a.lambda = lambda;
+    a.min_diag = min_diag;
+    a.S = static_cast<T*>(ws->S);
+    a.rhs = ws->rhs;
+    a.minv = ws->minv;
+    a.status = ws->status;
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, ne->P));
+    auto smem_for = [&](int ch, int mp) {
+        const int bpl = a.bp * a.bl, bpp = a.bp * a.bp;
+        return size_t(ch) * (bpl + bpp + a.bp) * sizeof(T) + size_t(mp * mp) * sizeof(double) + 64 +
+               kRowThreads * sizeof(unsigned long long) + 2 * ch * sizeof(int) + 64;
+    };
+    if (ne->bp == 6 && ne->bl == 3)
+    {
+        const size_t smem = smem_for(64, 6);
+        set_smem(reinterpret_cast<const void*>(assemble_kernel<T, 6, 3, 64>), smem);
+        assemble_kernel<T, 6, 3, 64><<<grid, kRowThreads, smem, stream>>>(a);
+        PM_LAUNCH_CHECK();
+    }
+    else
+    {
+        if (ne->bp > 16 || ne->bl > 16)
+            fail(PM_INVALID_ARGUMENT, "device Schur solver supports block sizes up to 16");
+        const size_t smem = smem_for(16, 16);
+        set_smem(reinterpret_cast<const void*>(assemble_kernel<T, 0, 0, 16>), smem);
+        assemble_kernel<T, 0, 0, 16><<<grid, kRowThreads, smem, stream>>>(a);
+        PM_LAUNCH_CHECK();
+    }
+    mirror_kernel<T><<<grid_for(ws->B * ne->bp * ne->bp, 256, 65535), 256, 0, stream>>>(
+        ws->B, static_cast<int>(ne->bp), ws->block_row, ws->block_col, ws->transpose, static_cast<T*>(ws->S));
+    PM_LAUNCH_CHECK();
+}
+
+// One preconditioned CG solve on the block-CSR operand (matrix M, vectors V, inverses PM),
+// device-driven; the host polls `done` on a doubling schedule.  Returns the final state.
+template <typename V, typename M, typename PM>
+SolveState block_pcg(pm_schur_workspace* ws, cudaStream_t stream, const M* S, const PM* minv, const double* rhs,
+                     V* x, double rel, double abs_tol, int rule, int max_iterations, V* scratch)
+{
+    const int64_t P = ws->P, n = ws->P * ws->bp;
+    const int bp = static_cast<int>(ws->bp);
+    V* r0 = scratch;
+    V* r1 = r0 + (n + 1);
+    V* z = r1 + (n + 1);
+    V* p = z + (n + 1);
+    V* q = p + (n + 1);
+    const unsigned sgrid = grid_for(P * 32, kVecBlock, kMaxParts);
+    const unsigned ugrid = grid_for(P, kVecBlock, kMaxParts);
+    const unsigned dgrid = grid_for(n, kVecBlock, 4096);
+    const bool six = bp == 6;
+    if (six)
+        bsr_spmv_kernel<V, M, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, x, q);
+    else
+        bsr_spmv_kernel<V, M, 0><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, x, q);
+        PM_LAUNCH_CHECK();
+    if (six)
+        pcg_block_init_kernel<V, PM, double, 6><<<ugrid, kVecBlock, 0, stream>>>(P, bp, rhs, q, r0, z, p, minv, rel,
+                                                                                abs_tol, rule, max_iterations,
+                                                                                ws->partials, ws->state);
+    else
+        pcg_block_init_kernel<V, PM, double, 0><<<ugrid, kVecBlock, 0, stream>>>(P, bp, rhs, q, r0, z, p, minv, rel,
+                                                                                abs_tol, rule, max_iterations,
+                                                                                ws->partials, ws->state);
+    PM_LAUNCH_CHECK();
+    int issued = 0, check_every = 1;
+    V* r_in = r0;
+    V* r_out = r1;
+    while (true)
+    {
+        const int chunk = std::min(check_every, max_iterations - issued);
+        for (int k = 0; k < chunk; ++k)
+        {
+            if (issued > 0)
+                pcg_block_direction_kernel<V><<<dgrid, kVecBlock, 0, stream>>>(n, z, p, ws->state);
+                PM_LAUNCH_CHECK();
+            if (six)
+            {
+                pcg_bsr_kernel<V, M, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, p,
+                                                                         q, ws->partials, ws->state);
+                PM_LAUNCH_CHECK();
+                pcg_block_update_kernel<V, PM, 6><<<ugrid, kVecBlock, 0, stream>>>(P, bp, x, p, q, r_in, r_out, z, minv,
+                                                                                   ws->partials, ws->state);
+                PM_LAUNCH_CHECK();
+            }
+            else
+            {
+                pcg_bsr_kernel<V, M, 0><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, p,
+                                                                         q, ws->partials, ws->state);
+                PM_LAUNCH_CHECK();
+                pcg_block_update_kernel<V, PM, 0><<<ugrid, kVecBlock, 0, stream>>>(P, bp, x, p, q, r_in, r_out, z, minv,
+                                                                                   ws->partials, ws->state);
+                PM_LAUNCH_CHECK();
+            }
+            PM_LAUNCH_CHECK();
+            std::swap(r_in, r_out);
+            ++issued;
+        }
+        PM_CUDA(cudaMemcpyAsync(ws->host_state, ws->state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaEventRecord(ws->sync_event, stream));
+        PM_CUDA(cudaEventSynchronize(ws->sync_event));
+        if (ws->host_state->done || issued >= max_iterations)
+            break;
+        check_every = std::min(check_every * 2, 16);
+    }
+    return *ws->host_state;
+}
+
+// FP64 true residual ||b - S x|| and ||b|| (S in Scalar precision, x FP64)
+template <typename M>
+void true_residual(pm_schur_workspace* ws, cudaStream_t stream, const M* S, const double* x, double* q, double* r,
+                   double& norm, double& rhs_norm)
+{
+    const int64_t P = ws->P, n = P * ws->bp;
+    const int bp = static_cast<int>(ws->bp);
+    const unsigned sgrid = grid_for(P * 32, kVecBlock, kMaxParts);
+    if (bp == 6)
+        bsr_spmv_kernel<double, M, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, x, q);
+    else
+        bsr_spmv_kernel<double, M, 0><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, x, q);
+        PM_LAUNCH_CHECK();
+    residual_kernel<<<grid_for(n, kVecBlock, kMaxParts), kVecBlock, 0, stream>>>(n, ws->rhs, q, r, ws->partials,
+                                                                               ws->state);
+    PM_LAUNCH_CHECK();
+    PM_CUDA(cudaMemcpyAsync(ws->host_state, ws->state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaEventRecord(ws->sync_event, stream));
+    PM_CUDA(cudaEventSynchronize(ws->sync_event));
+    norm = std::sqrt(std::max(0.0, ws->host_state->true_squared));
+    rhs_norm = std::sqrt(std::max(0.0, ws->host_state->rhs_squared));
+}
+
+template <typename T>
+void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_equations* ne, double damping,
+                 const pm_schur_options* o, T* dp, T* dl, pm_schur_report* rep)
+{
+    if (!ws || !ne || !o || !rep)
+        fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: arguments must be non-null");
+    std::memset(rep, 0, sizeof(*rep));
+    rep->true_relative_residual = -1.0;
+    const int64_t P = ne->P, L = ne->L, bp = ne->bp, bl = ne->bl;
+    const int64_t n = P * bp, m = L * bl;
+    if ((n > 0 && !dp) || (m > 0 && !dl) || (dp && static_cast<void*>(dp) == static_cast<void*>(dl)))
+        fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: output vectors must be non-null and distinct");
+    if (!std::isfinite(damping) || damping < 0.0 || o->max_iterations <= 0 || !std::isfinite(o->relative_tolerance) ||
+        o->relative_tolerance < 0.0 || !std::isfinite(o->absolute_tolerance) || o->absolute_tolerance < 0.0 ||
+        !std::isfinite(o->minimum_diagonal) || o->minimum_diagonal <= 0.0)
+        fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: invalid solver options");
+    if (ne->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: scalar type differs from the normal equations");
+    if (bp > 16 || bl > 16)
+        fail(PM_INVALID_ARGUMENT, "device Schur solver supports block sizes up to 16");
+    const bool mixed = o->precision == PM_PRECISION_MIXED && sizeof(T) == 8;
+    if (bp * bp > kRowThreads)
+        fail(PM_INVALID_ARGUMENT, "device Schur solver supports primary block sizes up to 11");
+    ws->numeric.bind(stream, "SchurComplementSolverWorkspace");
+    if (!ws->host_state)
+    {
+        PM_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ws->host_state), sizeof(SolveState)));
+        PM_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ws->host_status), sizeof(SchurStatus)));
+        for (auto& e : ws->events)
+            PM_CUDA(cudaEventCreate(&e));
+        PM_CUDA(cudaEventCreateWithFlags(&ws->sync_event, cudaEventDisableTiming));
+    }
+    if (n > 0 && !o->use_initial_guess)
+        PM_CUDA(cudaMemsetAsync(dp, 0, n * sizeof(T), stream));
+    if (m > 0)
+        PM_CUDA(cudaMemsetAsync(dl, 0, m * sizeof(T), stream));
+    PM_CUDA(cudaEventRecord(ws->events[0], stream));
+    // ---- pattern (checked first: the numeric layout depends on the block count)
+    if (!ws->numeric.ptr || !ws->status)
+    {
+        ws->B = 0;
+        ws->P = P;
+        ws->L = L;
+        ws->bp = bp;
+        ws->bl = bl;
+        numeric_layout<T>(ws, stream, mixed);
+    }
+    const bool reused = ws->pattern_builds > 0 && topology_matches(ws, ne, stream);
+    if (!reused)
+        build_pattern(ws, ne, stream);
+    ws->last_ne = ne;
+    ws->last_version = ne->topology_version;
+    ws->value_size = sizeof(T);
+    rep->pattern_reused = reused;
+    numeric_layout<T>(ws, stream, mixed);
+    PM_CUDA(cudaMemsetAsync(ws->state, 0, sizeof(SolveState), stream));
+    PM_CUDA(cudaEventRecord(ws->events[1], stream));
+    // ---- eliminated inverses
+    status_reset_kernel<<<1, 1, 0, stream>>>(ws->status);
+    PM_LAUNCH_CHECK();
+    if (L > 0)
+    {
+        const unsigned grid = grid_for(L, 128, 1 << 20);
+        if (bl == 3)
+            eliminated_inverse_kernel<T, 3><<<grid, 128, 0, stream>>>(L, 3, static_cast<const T*>(ne->eliminated_diagonal),
+                                                                      static_cast<const T*>(ne->eliminated_gradient),
+                                                                      damping, o->minimum_diagonal, ws->hinv, ws->y,
+                                                                      ws->status);
+        else
+            eliminated_inverse_kernel<T, 0><<<grid, 128, 0, stream>>>(L, static_cast<int>(bl),
+                                                                      static_cast<const T*>(ne->eliminated_diagonal),
+                                                                      static_cast<const T*>(ne->eliminated_gradient),
+                                                                      damping, o->minimum_diagonal, ws->hinv, ws->y,
+                                                                      ws->status);
+        PM_LAUNCH_CHECK();
+    }
+    PM_CUDA(cudaEventRecord(ws->events[2], stream));
+    // ---- assembly + preconditioner + RHS
+    if (P > 0)
+        launch_assembly<T>(ws, ne, damping, o->minimum_diagonal, stream);
+    if (mixed && P > 0)
+    {
+        convert_kernel<T, float><<<grid_for(ws->B * bp * bp, 256, 65535), 256, 0, stream>>>(
+            static_cast<const T*>(ws->S), ws->S32, ws->B * bp * bp);
+        PM_LAUNCH_CHECK();
+        convert_kernel<double, float><<<grid_for(P * bp * bp, 256, 4096), 256, 0, stream>>>(ws->minv, ws->minv32,
+                                                                                            P * bp * bp);
+        PM_LAUNCH_CHECK();
+    }
+    PM_CUDA(cudaEventRecord(ws->events[3], stream));
+    // ---- status of the factorisations (one small read; the reference returns early here)
+    PM_CUDA(cudaMemcpyAsync(ws->host_status, ws->status, sizeof(SchurStatus), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaEventRecord(ws->sync_event, stream));
+    PM_CUDA(cudaEventSynchronize(ws->sync_event));
+    ws->assembled = P > 0;
+    auto timings = [&](int last) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ws->events[0], ws->events[1]);
+        rep->pattern_ms = t;
+        cudaEventElapsedTime(&t, ws->events[1], ws->events[2]);
+        rep->eliminated_inverse_ms = t;
+        cudaEventElapsedTime(&t, ws->events[2], ws->events[3]);
+        rep->assembly_ms = t;
+        if (last >= 4)
+        {
+            cudaEventElapsedTime(&t, ws->events[3], ws->events[4]);
+            rep->solve_ms = t;
+        }
+        if (last >= 5)
+        {
+            cudaEventElapsedTime(&t, ws->events[4], ws->events[5]);
+            rep->back_substitution_ms = t;
+        }
+        cudaEventElapsedTime(&t, ws->events[0], ws->events[last]);
+        rep->total_ms = t;
+    };
+    if (ws->host_status->eliminated_bad != kNone)
+    {
+        timings(3);
+        std::snprintf(rep->message, sizeof(rep->message), "eliminated block is not positive definite");
+        return;
+    }
+    if (ws->host_status->preconditioner_bad != kNone)
+    {
+        timings(3);
+        std::snprintf(rep->message, sizeof(rep->message), "Schur preconditioner block is not positive definite");
+        return;
+    }
+    // ---- PCG
+    double* area = vector_area(ws);
+    SolveState st{};
+    if (n == 0)
+    {
+        rep->converged = 1;
+    }
+    else if (!mixed)
+    {
+        st = block_pcg<T, T, double>(ws, stream, static_cast<const T*>(ws->S), ws->minv, ws->rhs, dp,
+                                     o->relative_tolerance, o->absolute_tolerance, o->tolerance_rule, o->max_iterations,
+                                     reinterpret_cast<T*>(area));
+        rep->converged = st.converged;
+        rep->iterations = st.iterations;
+        rep->initial_residual_norm = std::sqrt(std::max(0.0, st.initial_squared));
+        rep->final_residual_norm = std::sqrt(std::max(0.0, st.residual_squared));
+        if (st.breakdown)
+            std::snprintf(rep->message, sizeof(rep->message), "reduced Schur complement is not positive definite");
+    }
+    else
+    {
+        // FP64 iterative refinement around FP32 inner PCG solves (FP64 dots / alpha / beta)
+        double* x64 = reinterpret_cast<double*>(dp);
+        double* q64 = area;
+        double* r64 = area + (n + 1);
+        float* d32 = reinterpret_cast<float*>(area + 2 * (n + 1));
+        float* inner = d32 + 2 * (n + 1);
+        double norm = 0.0, rhs_norm = 0.0;
+        true_residual<T>(ws, stream, static_cast<const T*>(ws->S), x64, q64, r64, norm, rhs_norm);
+        rep->initial_residual_norm = norm;
+        const double target = o->tolerance_rule == 0 ? o->absolute_tolerance + o->relative_tolerance * norm
+                                                     : std::max(o->absolute_tolerance, o->relative_tolerance * norm);
+        const double inner_rel = o->inner_relative_tolerance > 0.0 ? o->inner_relative_tolerance : 1e-4;
+        int total = 0;
+        const int max_refinements = o->max_refinements > 0 ? o->max_refinements : 8;
+        for (int k = 0; k <= max_refinements; ++k)
+        {
+            rep->final_residual_norm = norm;
+            if (norm <= target)
+            {
+                rep->converged = 1;
+                break;
+            }
+            if (k == max_refinements || total >= o->max_iterations)
+                break;
+            // r64 holds b - S x; solve S32 d = r64 to inner_rel (or to the outer target)
+            PM_CUDA(cudaMemsetAsync(d32, 0, n * sizeof(float), stream));
+            st = block_pcg<float, float, float>(ws, stream, ws->S32, ws->minv32, r64, d32, inner_rel, 0.5 * target, 1,
+                                                o->max_iterations - total, inner);
+            total += st.iterations;
+            rep->refinement_steps += 1;
+            if (st.breakdown)
+            {
+                std::snprintf(rep->message, sizeof(rep->message), "reduced Schur complement is not positive definite");
+                break;
+            }
+            axpy_to_double_kernel<float><<<grid_for(n, 256, 4096), 256, 0, stream>>>(n, d32, x64);
+            PM_LAUNCH_CHECK();
+            true_residual<T>(ws, stream, static_cast<const T*>(ws->S), x64, q64, r64, norm, rhs_norm);
+        }
+        rep->iterations = total;
+        rep->mixed_precision_used = 1;
+        rep->true_relative_residual = rhs_norm > 0 ? rep->final_residual_norm / rhs_norm : 0.0;
+    }
+    PM_CUDA(cudaEventRecord(ws->events[4], stream));
+    if (rep->converged && o->check_true_residual && !mixed && n > 0 && sizeof(T) == 8)
+    {
+        double* q64 = area + 2 * (n + 1);
+        double norm = 0.0, rhs_norm = 0.0;
+        true_residual<T>(ws, stream, static_cast<const T*>(ws->S), reinterpret_cast<const double*>(dp), q64, nullptr,
+                         norm, rhs_norm);
+        rep->true_relative_residual = rhs_norm > 0 ? norm / rhs_norm : 0.0;
+    }
+    if (!rep->converged)
+    {
+        PM_CUDA(cudaEventRecord(ws->events[5], stream));
+        PM_CUDA(cudaEventSynchronize(ws->events[5]));
+        timings(5);
+        if (rep->message[0] == '\0')
+            std::snprintf(rep->message, sizeof(rep->message), "PCG iteration limit reached");
+        return;
+    }
+    // ---- back-substitution
+    if (L > 0)
+    {
+        const unsigned grid = grid_for(L, 128, 1 << 20);
+        if (bp == 6 && bl == 3)
+            backsub_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(L, 6, 3, ne->cross_offsets, ne->cross_primary,
+                                                              static_cast<const T*>(ne->cross_values),
+                                                              static_cast<const T*>(ne->eliminated_gradient), ws->hinv,
+                                                              dp, dl);
+        else
+            backsub_kernel<T, 0, 0><<<grid, 128, 0, stream>>>(L, static_cast<int>(bp), static_cast<int>(bl),
+                                                              ne->cross_offsets, ne->cross_primary,
+                                                              static_cast<const T*>(ne->cross_values),
+                                                              static_cast<const T*>(ne->eliminated_gradient), ws->hinv,
+                                                              dp, dl);
+        PM_LAUNCH_CHECK();
+    }
+    PM_CUDA(cudaEventRecord(ws->events[5], stream));
+    PM_CUDA(cudaEventSynchronize(ws->events[5]));
+    timings(5);
+    std::snprintf(rep->message, sizeof(rep->message), "converged");
+}
+
+template <typename T, typename O>
+void export_system(pm_schur_workspace* ws, cudaStream_t stream, int64_t* ro, int64_t* ci, O* values, double* rhs,
+                   double* minv)
+{
+    if (!ws || !ws->assembled)
+        fail(PM_LOGIC_ERROR, "CUDA Schur values have not been assembled");
+    if (ws->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "export scalar type differs from the assembled system");
+    const int64_t bpp = ws->bp * ws->bp;
+    export_csr_kernel<T, O><<<grid_for(ws->B * bpp, 256, 65535), 256, 0, stream>>>(
+        ws->B, static_cast<int>(ws->bp), ws->P, ws->block_row_ptr, ws->block_col, ws->block_row,
+        static_cast<const T*>(ws->S), ro, ci, values);
+    PM_LAUNCH_CHECK();
+    if (rhs)
+        PM_CUDA(cudaMemcpyAsync(rhs, ws->rhs, ws->P * ws->bp * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    if (minv)
+        PM_CUDA(cudaMemcpyAsync(minv, ws->minv, ws->P * bpp * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+}
+
+} // namespace
+} // namespace pm
+
+extern "C" {
+
+int pm_schur_workspace_create(pm_schur_workspace** out)
+{
+    return pm::guarded([&] {
+        if (!out)
+            pm::fail(PM_INVALID_ARGUMENT, "workspace output pointer is null");
+        *out = new pm_schur_workspace();
+    });
+}
+
+void pm_schur_workspace_destroy(pm_schur_workspace* ws) { delete ws; }
+
+int pm_schur_workspace_close(pm_schur_workspace* ws)
+{
+    return pm::guarded([&] {
+        if (!ws)
+            pm::fail(PM_INVALID_ARGUMENT, "workspace is null");
+        ws->pattern.release();
+        ws->numeric.release();
+        ws->scratch.release();
+        ws->pattern_builds = ws->pattern_builds; // the count survives, the cache does not
+        ws->saved_offsets = nullptr;
+        ws->status = nullptr;
+        ws->assembled = false;
+        ws->last_ne = nullptr;
+        ws->P = -1;
+    });
+}
+
+int64_t pm_schur_pattern_build_count(const pm_schur_workspace* ws) { return ws ? ws->pattern_builds : 0; }
+
+int pm_schur_dims(const pm_schur_workspace* ws, int64_t* dimension, int64_t* nnz, int64_t* blocks)
+{
+    return pm::guarded([&] {
+        if (!ws || !ws->assembled)
+            pm::fail(PM_LOGIC_ERROR, "CUDA Schur values have not been assembled");
+        if (dimension)
+            *dimension = ws->P * ws->bp;
+        if (nnz)
+            *nnz = ws->B * ws->bp * ws->bp;
+        if (blocks)
+            *blocks = ws->B;
+    });
+}
+
+int pm_schur_solve_f32(pm_schur_workspace* ws, pm_stream_t stream, const pm_normal_equations* ne, float damping,
+                       const pm_schur_options* o, float* dp, float* dl, pm_schur_report* rep)
+{
+    return pm::guarded([&] { pm::schur_solve<float>(ws, stream, ne, damping, o, dp, dl, rep); });
+}
+int pm_schur_solve_f64(pm_schur_workspace* ws, pm_stream_t stream, const pm_normal_equations* ne, double damping,
+                       const pm_schur_options* o, double* dp, double* dl, pm_schur_report* rep)
+{
+    return pm::guarded([&] { pm::schur_solve<double>(ws, stream, ne, damping, o, dp, dl, rep); });
+}
+
+int pm_schur_export_f32(pm_schur_workspace* ws, pm_stream_t stream, int64_t* ro, int64_t* ci, float* v, double* rhs,
+                        double* minv)
+{
+    return pm::guarded([&] { pm::export_system<float, float>(ws, stream, ro, ci, v, rhs, minv); });
+}
+int pm_schur_export_f64(pm_schur_workspace* ws, pm_stream_t stream, int64_t* ro, int64_t* ci, double* v, double* rhs,
+                        double* minv)
+{
+    return pm::guarded([&] { pm::export_system<double, double>(ws, stream, ro, ci, v, rhs, minv); });
+}
+
+} // extern "C"

@@ -1,0 +1,775 @@
+// CSR operands, CSR SpMV and CG / PCG / block-PCG for sm_100a.
+//
+// Replaces the reference's cuSPARSE SpMV (src/sparse/sparse_ops.cu:687-740) and its
+// cuBLAS-driven adaptive solver loop (src/sparse/iterative_solver.cu:30-349), which
+// synchronises with the host after every iteration.  Here:
+//   * the int64 CSR structure is validated once and kept as int32 (4 B per index on the
+//     HBM stream instead of 8 B);
+//   * SpMV uses a sub-warp per row (width chosen from the mean row length) with shuffle
+//     reductions;
+//   * one PCG iteration is three kernels (direction update, SpMV fused with the p.q dot,
+//     vector update fused with preconditioner apply and the r.z / r.r dots); every dot is
+//     accumulated in FP64 per block and finished by the last block to arrive, in a fixed
+//     order, which also evaluates alpha / beta, breakdown and convergence on the device;
+//   * the host only polls a device "done" flag on a doubling schedule.
+#include "pm_common.cuh"
+
+#include <cmath>
+#include <limits>
+#include <sstream>
+
+struct pm_csr
+{
+    int value_size = 0;
+    int64_t rows = 0, cols = 0, nnz = 0;
+    int* row_ptr = nullptr; // int32 copy of the validated row offsets
+    int* col_idx = nullptr; // int32 copy of the validated column indices
+    const void* values = nullptr;
+    int threads_per_row = 1;
+};
+
+namespace pm
+{
+
+template <typename T>
+struct Eps;
+template <>
+struct Eps<float>
+{
+    static constexpr double value = 1.1920928955078125e-7;
+};
+template <>
+struct Eps<double>
+{
+    static constexpr double value = 2.2204460492503131e-16;
+};
+
+namespace
+{
+
+constexpr long long kNone = 0x7fffffffffffffffLL;
+constexpr int kReduceBlock = 256;
+constexpr int kMaxReduceBlocks = 1024;
+
+struct CsrCheck
+{
+    long long bad_offsets_row;
+    long long bad_column;
+    long long bad_value;
+    int endpoints_bad;
+};
+
+template <typename T>
+__global__ void validate_csr_kernel(int64_t rows, int64_t cols, int64_t nnz, const int64_t* __restrict__ row_offsets,
+                                    const int64_t* __restrict__ col_indices, const T* __restrict__ values,
+                                    int* __restrict__ row_ptr32, int* __restrict__ col32, CsrCheck* check)
+{
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t == 0 && (row_offsets[0] != 0 || row_offsets[rows] != nnz))
+        check->endpoints_bad = 1;
+    for (int64_t r = t; r < rows; r += stride)
+    {
+        const int64_t b = row_offsets[r], e = row_offsets[r + 1];
+        if (b < 0 || e < b || e > nnz)
+            atomicMin(&check->bad_offsets_row, static_cast<long long>(r));
+        row_ptr32[r] = static_cast<int>(b);
+    }
+    if (t == 0)
+        row_ptr32[rows] = static_cast<int>(nnz);
+    for (int64_t p = t; p < nnz; p += stride)
+    {
+        const int64_t c = col_indices[p];
+        if (c < 0 || c >= cols)
+            atomicMin(&check->bad_column, static_cast<long long>(p));
+        if (!isfinite(static_cast<double>(values[p])))
+            atomicMin(&check->bad_value, static_cast<long long>(p));
+        col32[p] = static_cast<int>(c);
+    }
+}
+
+// y = A x with a TPR-wide sub-warp per row
+template <typename T, int TPR>
+__device__ __forceinline__ T csr_row_dot(const int* __restrict__ rp, const int* __restrict__ ci,
+                                         const T* __restrict__ v, const T* __restrict__ x, int64_t row, bool valid,
+                                         int lane)
+{
+    T sum = T(0);
+    if (valid)
+    {
+        const int b = rp[row], e = rp[row + 1];
+        for (int p = b + lane; p < e; p += TPR)
+            sum += v[p] * __ldg(x + ci[p]);
+    }
+#pragma unroll
+    for (int o = TPR / 2; o > 0; o >>= 1)
+        sum += __shfl_xor_sync(0xffffffffu, sum, o, TPR);
+    return sum;
+}
+
+template <typename T, int TPR>
+__global__ void __launch_bounds__(256) csr_spmv_kernel(int64_t rows, const int* __restrict__ rp,
+                                                       const int* __restrict__ ci, const T* __restrict__ v,
+                                                       const T* __restrict__ x, T* __restrict__ y)
+{
+    const int64_t gid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x / TPR;
+    const int lane = threadIdx.x % TPR;
+    const int64_t first = gid / TPR;
+    const int64_t span = (rows + stride - 1) / stride; // uniform trip count keeps shuffles convergent
+    for (int64_t k = 0; k < span; ++k)
+    {
+        const int64_t row = first + k * stride;
+        const bool valid = row < rows;
+        const T sum = csr_row_dot<T, TPR>(rp, ci, v, x, row, valid, lane);
+        if (valid && lane == 0)
+            y[row] = sum;
+    }
+}
+
+int pick_tpr(int64_t rows, int64_t nnz)
+{
+    const double mean = rows > 0 ? double(nnz) / double(rows) : 1.0;
+    int tpr = 1;
+    while (tpr < 32 && tpr < mean)
+        tpr <<= 1;
+    return tpr;
+}
+
+template <typename T>
+void launch_spmv(const pm_csr* A, const T* x, T* y, cudaStream_t stream)
+{
+    if (A->rows == 0)
+        return;
+    const T* v = static_cast<const T*>(A->values);
+    const int block = 256;
+    const unsigned grid = grid_for(A->rows * A->threads_per_row, block, 65535);
+    switch (A->threads_per_row)
+    {
+    case 1: csr_spmv_kernel<T, 1><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
+    case 2: csr_spmv_kernel<T, 2><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
+    case 4: csr_spmv_kernel<T, 4><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
+    case 8: csr_spmv_kernel<T, 8><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
+    case 16: csr_spmv_kernel<T, 16><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
+    default: csr_spmv_kernel<T, 32><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
+    }
+    PM_LAUNCH_CHECK();
+}
+
+// ------------------------------------------------------------------ PCG state
+struct PcgState
+{
+    double rho;      // r.z of the current direction
+    double alpha;
+    double beta;
+    double tolerance;
+    double initial_squared;
+    double residual_squared;
+    int iterations;
+    int max_iterations;
+    int done;
+    int converged;
+    int breakdown;     // 1: not SPD / non-finite step
+    int nonfinite_init;
+    long long jacobi_bad_row;
+    unsigned int ticket[3];
+    int pad;
+};
+
+// Last block to arrive sums the per-block partials (fixed order) and runs `finish`.
+template <int K, typename Finish>
+__device__ __forceinline__ void reduce_partials(double (&mine)[K], double* partials, unsigned int* ticket,
+                                                Finish&& finish)
+{
+    __shared__ double smem[kReduceBlock / 32];
+    __shared__ bool last;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        const double s = block_sum<double, kReduceBlock>(mine[k], smem);
+        if (threadIdx.x == 0)
+            partials[k * kMaxReduceBlocks + blockIdx.x] = s;
+    }
+    __threadfence();
+    if (threadIdx.x == 0)
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last)
+        return;
+    __threadfence();
+    double totals[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+    {
+        double s = 0.0;
+        for (int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+            s += __ldcg(partials + k * kMaxReduceBlocks + b);
+        totals[k] = block_sum<double, kReduceBlock>(s, smem);
+    }
+    if (threadIdx.x == 0)
+    {
+        *ticket = 0;
+        finish(totals);
+    }
+}
+
+// preconditioned component i of the residual vector `r` (scalar Jacobi, caller blocks, none)
+template <typename T, typename R>
+__device__ __forceinline__ double apply_precond(int mode, int64_t i, R&& residual_at, const T* inv_diag,
+                                                const T* blocks, int64_t bs)
+{
+    if (mode == 1)
+        return static_cast<double>(inv_diag[i]) * residual_at(i);
+    if (mode == 2)
+    {
+        const int64_t blk = i / bs, local = i - blk * bs;
+        const T* row = blocks + blk * bs * bs + local * bs;
+        double z = 0.0;
+        for (int64_t c = 0; c < bs; ++c)
+            z += static_cast<double>(row[c]) * residual_at(blk * bs + c);
+        return z;
+    }
+    return residual_at(i);
+}
+
+// Jacobi inverse: iterative_solver_kernels.cuh:104-131 semantics (sum of diagonal duplicates,
+// 16*eps*rowscale guard); invalid rows are reported (lowest row) instead of NaN markers.
+template <typename T>
+__global__ void jacobi_kernel(int64_t rows, const int* __restrict__ rp, const int* __restrict__ ci,
+                              const T* __restrict__ v, T* __restrict__ inv, PcgState* st)
+{
+    for (int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; r < rows; r += int64_t(gridDim.x) * blockDim.x)
+    {
+        double diag = 0.0, scale = 0.0;
+        bool found = false;
+        for (int p = rp[r]; p < rp[r + 1]; ++p)
+        {
+            const double value = static_cast<double>(v[p]);
+            scale = fmax(scale, fabs(value));
+            if (ci[p] == r)
+            {
+                diag += value;
+                found = true;
+            }
+        }
+        const double threshold = Eps<T>::value * scale * 16.0;
+        const double reciprocal = 1.0 / diag;
+        if (!found || !isfinite(diag) || diag <= threshold || !isfinite(reciprocal))
+        {
+            atomicMin(&st->jacobi_bad_row, static_cast<long long>(r));
+            inv[r] = T(0);
+        }
+        else
+        {
+            inv[r] = static_cast<T>(reciprocal);
+        }
+    }
+}
+
+// r = b - Ax (Ax in q), z = M^-1 r, p = z; rho = r.z, initial ||r||^2
+template <typename T>
+__global__ void __launch_bounds__(kReduceBlock) pcg_init_kernel(int64_t n, const T* __restrict__ b,
+                                                                const T* __restrict__ q, T* __restrict__ r,
+                                                                T* __restrict__ z, T* __restrict__ p, int mode,
+                                                                const T* __restrict__ inv, const T* __restrict__ blocks,
+                                                                int64_t bs, double relative, double absolute,
+                                                                double* partials, PcgState* st)
+{
+    double mine[2] = {0.0, 0.0};
+    auto res = [&](int64_t k) { return static_cast<double>(static_cast<T>(static_cast<double>(b[k]) - static_cast<double>(q[k]))); };
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const double ri = res(i);
+        const T zi = static_cast<T>(apply_precond<T>(mode, i, res, inv, blocks, bs));
+        r[i] = static_cast<T>(ri);
+        z[i] = zi;
+        p[i] = zi;
+        mine[0] += ri * static_cast<double>(zi);
+        mine[1] += ri * ri;
+    }
+    reduce_partials<2>(mine, partials, &st->ticket[0], [&](double (&tot)[2]) {
+        st->rho = tot[0];
+        st->initial_squared = tot[1];
+        st->residual_squared = tot[1];
+        const double initial = sqrt(tot[1]);
+        st->tolerance = fmax(absolute, relative * initial);
+        st->iterations = 0;
+        st->beta = 0.0;
+        if (!isfinite(tot[1]) || tot[1] < 0.0)
+        {
+            st->nonfinite_init = 1;
+            st->done = 1;
+        }
+        else if (initial <= st->tolerance)
+        {
+            st->converged = 1;
+            st->done = 1;
+        }
+        if (st->jacobi_bad_row != kNone)
+            st->done = 1;
+    });
+}
+
+// q = A p, alpha = rho / p.q  (alphaKernel semantics, iterative_solver_kernels.cuh:169-202)
+template <typename T, int TPR>
+__global__ void __launch_bounds__(kReduceBlock) pcg_spmv_kernel(int64_t rows, const int* __restrict__ rp,
+                                                                const int* __restrict__ ci, const T* __restrict__ v,
+                                                                const T* __restrict__ p, T* __restrict__ q,
+                                                                double* partials, PcgState* st)
+{
+    if (st->done)
+        return;
+    double mine[1] = {0.0};
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x / TPR;
+    const int lane = threadIdx.x % TPR;
+    const int64_t first = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / TPR;
+    const int64_t span = (rows + stride - 1) / stride;
+    for (int64_t k = 0; k < span; ++k)
+    {
+        const int64_t row = first + k * stride;
+        const bool valid = row < rows;
+        const T sum = csr_row_dot<T, TPR>(rp, ci, v, p, row, valid, lane);
+        if (valid && lane == 0)
+        {
+            q[row] = sum;
+            mine[0] += static_cast<double>(p[row]) * static_cast<double>(sum);
+        }
+    }
+    reduce_partials<1>(mine, partials, &st->ticket[1], [&](double (&tot)[1]) {
+        const double rho = st->rho, den = tot[0];
+        double alpha = 0.0;
+        if (rho == 0.0 && den == 0.0)
+            alpha = 0.0;
+        else if (isfinite(rho) && isfinite(den) && rho > 0.0 && den > 0.0)
+        {
+            alpha = rho / den;
+            // the step must also be representable in the vector type (the reference forms
+            // alpha in Scalar precision and treats its overflow as breakdown)
+            if (!isfinite(alpha) || !isfinite(static_cast<double>(static_cast<T>(alpha))))
+            {
+                st->breakdown = 1;
+                alpha = 0.0;
+            }
+        }
+        else
+        {
+            st->breakdown = 1;
+        }
+        st->alpha = alpha;
+        if (st->breakdown)
+            st->done = 1;
+    });
+}
+
+// x += alpha p, r -= alpha q, z = M^-1 r; convergence on ||r||, beta = r.z / rho.
+// r is ping-ponged (r_in -> r_out) so block preconditioners read only old values.
+template <typename T>
+__global__ void __launch_bounds__(kReduceBlock) pcg_update_kernel(int64_t n, T* __restrict__ x,
+                                                                  const T* __restrict__ p, const T* __restrict__ q,
+                                                                  const T* __restrict__ r_in, T* __restrict__ r_out,
+                                                                  T* __restrict__ z, int mode,
+                                                                  const T* __restrict__ inv,
+                                                                  const T* __restrict__ blocks, int64_t bs,
+                                                                  double* partials, PcgState* st)
+{
+    if (st->done)
+        return;
+    const double alpha = st->alpha;
+    double mine[2] = {0.0, 0.0};
+    auto res = [&](int64_t k) {
+        return static_cast<double>(static_cast<T>(static_cast<double>(r_in[k]) - alpha * static_cast<double>(q[k])));
+    };
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        x[i] = static_cast<T>(static_cast<double>(x[i]) + alpha * static_cast<double>(p[i]));
+        const double ri = res(i);
+        const T zi = static_cast<T>(apply_precond<T>(mode, i, res, inv, blocks, bs));
+        r_out[i] = static_cast<T>(ri);
+        z[i] = zi;
+        mine[0] += ri * static_cast<double>(zi);
+        mine[1] += ri * ri;
+    }
+    reduce_partials<2>(mine, partials, &st->ticket[2], [&](double (&tot)[2]) {
+        st->iterations += 1;
+        st->residual_squared = tot[1];
+        if (!isfinite(tot[1]) || tot[1] < 0.0)
+        {
+            st->breakdown = 1;
+            st->done = 1;
+            return;
+        }
+        if (sqrt(tot[1]) <= st->tolerance)
+        {
+            st->converged = 1;
+            st->done = 1;
+            return;
+        }
+        if (st->iterations >= st->max_iterations)
+        {
+            st->done = 1;
+            return;
+        }
+        // betaKernel semantics (iterative_solver_kernels.cuh:204-238)
+        const double rho = st->rho, next = tot[0];
+        double beta = 0.0;
+        if (rho == 0.0 && next == 0.0)
+            beta = 0.0;
+        else if (isfinite(rho) && isfinite(next) && rho > 0.0 && next > 0.0)
+        {
+            beta = next / rho;
+            if (!isfinite(beta) || !isfinite(static_cast<double>(static_cast<T>(beta))))
+            {
+                st->breakdown = 1;
+                st->done = 1;
+                beta = 0.0;
+            }
+        }
+        else
+        {
+            st->breakdown = 1;
+            st->done = 1;
+        }
+        st->beta = beta;
+        st->rho = next;
+    });
+}
+
+template <typename T>
+__global__ void pcg_direction_kernel(int64_t n, const T* __restrict__ z, T* __restrict__ p, const PcgState* st)
+{
+    if (st->done)
+        return;
+    const double beta = st->beta;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        p[i] = static_cast<T>(static_cast<double>(z[i]) + beta * static_cast<double>(p[i]));
+}
+
+__global__ void pcg_reset_kernel(PcgState* st, int max_iterations)
+{
+    PcgState s{};
+    s.max_iterations = max_iterations;
+    s.jacobi_bad_row = kNone;
+    *st = s;
+}
+
+} // namespace
+} // namespace pm
+
+struct pm_solver_workspace
+{
+    pm::DeviceBuffer buffer;
+    int* host_done = nullptr; // pinned
+    cudaEvent_t event = nullptr;
+    ~pm_solver_workspace()
+    {
+        buffer.release();
+        if (host_done)
+            cudaFreeHost(host_done);
+        if (event)
+            cudaEventDestroy(event);
+    }
+};
+
+namespace pm
+{
+namespace
+{
+
+template <typename T>
+void csr_create(cudaStream_t stream, int64_t rows, int64_t cols, int64_t nnz, const int64_t* ro, const int64_t* ci,
+                const T* v, pm_csr** out)
+{
+    if (!out)
+        fail(PM_INVALID_ARGUMENT, "CSR output handle pointer is null");
+    if (rows < 0 || cols < 0 || nnz < 0)
+        fail(PM_INVALID_ARGUMENT, "CSRMatrix dimensions must be non-negative");
+    if (nnz > INT32_MAX - 1 || rows > INT32_MAX - 1 || cols > INT32_MAX)
+        fail(PM_OVERFLOW_ERROR, "CSR operand exceeds the int32 index range of the device kernels");
+    if (!ro || (nnz > 0 && (!ci || !v)))
+        fail(PM_INVALID_ARGUMENT, "CSR arrays must be non-null");
+    auto* A = new pm_csr();
+    try
+    {
+        A->value_size = sizeof(T);
+        A->rows = rows;
+        A->cols = cols;
+        A->nnz = nnz;
+        A->values = v;
+        A->threads_per_row = pick_tpr(rows, nnz);
+        PM_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&A->row_ptr), (rows + 1) * sizeof(int), stream));
+        PM_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&A->col_idx), (nnz > 0 ? nnz : 1) * sizeof(int), stream));
+        CsrCheck* check = nullptr;
+        PM_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&check), sizeof(CsrCheck), stream));
+        CsrCheck init{kNone, kNone, kNone, 0};
+        PM_CUDA(cudaMemcpyAsync(check, &init, sizeof(init), cudaMemcpyHostToDevice, stream));
+        validate_csr_kernel<T><<<grid_for(std::max(rows, nnz), 256, 4096), 256, 0, stream>>>(
+            rows, cols, nnz, ro, ci, v, A->row_ptr, A->col_idx, check);
+        PM_LAUNCH_CHECK();
+        CsrCheck result{};
+        PM_CUDA(cudaMemcpyAsync(&result, check, sizeof(result), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaFreeAsync(check, stream));
+        PM_CUDA(cudaStreamSynchronize(stream));
+        if (result.endpoints_bad)
+            fail(PM_INVALID_ARGUMENT, "CSRMatrix row offsets must start at zero and end at nnz");
+        if (result.bad_offsets_row != kNone)
+        {
+            std::ostringstream m;
+            m << "CSRMatrix invalid row offsets at row " << result.bad_offsets_row;
+            fail(PM_INVALID_ARGUMENT, m.str());
+        }
+        if (result.bad_column != kNone)
+        {
+            std::ostringstream m;
+            m << "CSRMatrix column index out of range at position " << result.bad_column;
+            fail(PM_INVALID_ARGUMENT, m.str());
+        }
+        if (result.bad_value != kNone)
+        {
+            std::ostringstream m;
+            m << "CSRMatrix value is not finite at position " << result.bad_value;
+            fail(PM_INVALID_ARGUMENT, m.str());
+        }
+    }
+    catch (...)
+    {
+        cudaStreamSynchronize(stream);
+        cudaFree(A->row_ptr);
+        cudaFree(A->col_idx);
+        delete A;
+        throw;
+    }
+    *out = A;
+}
+
+template <typename T>
+void csr_spmv(const pm_csr* A, cudaStream_t stream, const T* x, T* y)
+{
+    if (!A)
+        fail(PM_INVALID_ARGUMENT, "CSR handle is null");
+    if (A->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "spmv scalar type differs from the CSR operand");
+    if (A->rows > 0 && (!y || (A->cols > 0 && !x)))
+        fail(PM_INVALID_ARGUMENT, "spmv vectors must be non-null");
+    if (x && x == y)
+        fail(PM_INVALID_ARGUMENT, "spmv input and output data must not alias");
+    launch_spmv<T>(A, x, y, stream);
+}
+
+template <typename T>
+void launch_pcg_spmv(const pm_csr* A, const T* p, T* q, double* partials, PcgState* st, unsigned grid,
+                     cudaStream_t stream)
+{
+    const T* v = static_cast<const T*>(A->values);
+    switch (A->threads_per_row)
+    {
+    case 1: pcg_spmv_kernel<T, 1><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
+    case 2: pcg_spmv_kernel<T, 2><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
+    case 4: pcg_spmv_kernel<T, 4><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
+    case 8: pcg_spmv_kernel<T, 8><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
+    case 16: pcg_spmv_kernel<T, 16><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
+    default: pcg_spmv_kernel<T, 32><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
+    }
+    PM_LAUNCH_CHECK();
+}
+
+// mode: 0 = CG, 1 = Jacobi PCG, 2 = caller block inverses
+template <typename T>
+void solve(pm_solver_workspace* ws, cudaStream_t stream, const pm_csr* A, const T* b, T* x, const T* blocks,
+           int64_t bs, const pm_solver_options* o, pm_solver_report* report, int mode)
+{
+    if (!ws || !A || !o || !report)
+        fail(PM_INVALID_ARGUMENT, "solver arguments must be non-null");
+    *report = pm_solver_report{0, 0, 0.0, 0.0};
+    if (o->max_iterations < 0 || !std::isfinite(o->relative_tolerance) || o->relative_tolerance < 0.0 ||
+        o->relative_tolerance > 1.0 || !std::isfinite(o->absolute_tolerance) || o->absolute_tolerance < 0.0)
+        fail(PM_INVALID_ARGUMENT, "invalid CUDA iterative solver options");
+    if (A->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "solver scalar type differs from the CSR operand");
+    if (A->rows != A->cols)
+        fail(PM_INVALID_ARGUMENT, "CUDA iterative solver requires square A and Nx1 rhs/solution");
+    const int64_t n = A->rows;
+    if (n > 0 && (!b || !x))
+        fail(PM_INVALID_ARGUMENT, "solver vectors must be non-null");
+    if (b && b == x)
+        fail(PM_INVALID_ARGUMENT, "CUDA iterative solver rhs and solution must not alias");
+    if (mode == 2)
+    {
+        if (bs <= 0 || n % bs != 0 || !blocks)
+            fail(PM_INVALID_ARGUMENT, "CUDA block PCG requires complete row-major inverse diagonal blocks");
+        if (static_cast<const void*>(blocks) == static_cast<const void*>(b) ||
+            static_cast<const void*>(blocks) == static_cast<const void*>(x))
+            fail(PM_INVALID_ARGUMENT, "CUDA block PCG inverse blocks must not alias rhs or solution");
+    }
+    if (n == 0)
+    {
+        report->converged = 1;
+        return;
+    }
+    Carver plan;
+    plan.take<PcgState>(1);
+    plan.take<double>(3 * kMaxReduceBlocks);
+    for (int k = 0; k < 6; ++k)
+        plan.take<T>(n);
+    ws->buffer.ensure(plan.offset + 256, stream, "IterativeSolverWorkspace");
+    if (!ws->host_done)
+        PM_CUDA(cudaMallocHost(reinterpret_cast<void**>(&ws->host_done), 2 * sizeof(PcgState)));
+    if (!ws->event)
+        PM_CUDA(cudaEventCreateWithFlags(&ws->event, cudaEventDisableTiming));
+    Carver c;
+    c.base = static_cast<char*>(ws->buffer.ptr);
+    PcgState* st = c.take<PcgState>(1);
+    double* partials = c.take<double>(3 * kMaxReduceBlocks);
+    T* r0 = c.take<T>(n);
+    T* r1 = c.take<T>(n);
+    T* z = c.take<T>(n);
+    T* p = c.take<T>(n);
+    T* q = c.take<T>(n);
+    T* inv = c.take<T>(n);
+
+    const unsigned vgrid = grid_for(n, kReduceBlock, kMaxReduceBlocks);
+    const unsigned sgrid = grid_for(n * A->threads_per_row, kReduceBlock, kMaxReduceBlocks);
+    pcg_reset_kernel<<<1, 1, 0, stream>>>(st, o->max_iterations);
+    PM_LAUNCH_CHECK();
+    if (mode == 1)
+    {
+        jacobi_kernel<T><<<grid_for(n, 256, 4096), 256, 0, stream>>>(n, A->row_ptr, A->col_idx,
+                                                                       static_cast<const T*>(A->values), inv, st);
+        PM_LAUNCH_CHECK();
+    }
+    launch_spmv<T>(A, x, q, stream);
+    pcg_init_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, b, q, r0, z, p, mode, inv, blocks, bs,
+                                                            o->relative_tolerance, o->absolute_tolerance, partials, st);
+    PM_LAUNCH_CHECK();
+    int issued = 0;
+    int check_every = 1;
+    T* r_in = r0;
+    T* r_out = r1;
+    PcgState* host = reinterpret_cast<PcgState*>(ws->host_done);
+    bool finished = false;
+    while (!finished)
+    {
+        const int chunk = std::min(check_every, o->max_iterations - issued);
+        for (int k = 0; k < chunk; ++k)
+        {
+            if (issued > 0)
+            {
+                pcg_direction_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, z, p, st);
+                PM_LAUNCH_CHECK();
+            }
+            launch_pcg_spmv<T>(A, p, q, partials + kMaxReduceBlocks * 0, st, sgrid, stream);
+            pcg_update_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, x, p, q, r_in, r_out, z, mode, inv, blocks, bs,
+                                                                      partials + kMaxReduceBlocks * 0, st);
+            PM_LAUNCH_CHECK();
+            std::swap(r_in, r_out);
+            ++issued;
+        }
+        PM_CUDA(cudaMemcpyAsync(host, st, sizeof(PcgState), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaEventRecord(ws->event, stream));
+        PM_CUDA(cudaEventSynchronize(ws->event));
+        finished = host->done || issued >= o->max_iterations;
+        check_every = std::min(check_every * 2, 32);
+    }
+    const PcgState s = *host;
+    if (s.jacobi_bad_row != kNone)
+    {
+        std::ostringstream m;
+        m << "pcg Jacobi diagonal is missing, non-positive, or near zero at row " << s.jacobi_bad_row;
+        fail(PM_RUNTIME_ERROR, m.str());
+    }
+    if (s.nonfinite_init)
+        fail(PM_RUNTIME_ERROR, "CUDA iterative solver initial residual is not finite");
+    report->initial_residual = std::sqrt(s.initial_squared);
+    report->iterations = s.iterations;
+    report->final_residual = std::sqrt(std::max(0.0, s.residual_squared));
+    report->converged = s.converged;
+    if (s.breakdown)
+        fail(PM_RUNTIME_ERROR, "CUDA iterative solver breakdown: matrix is not numerically SPD");
+    if (!s.converged && o->require_convergence)
+    {
+        std::ostringstream m;
+        m << "CUDA iterative solver did not converge in " << s.iterations
+          << " iterations; final residual=" << report->final_residual;
+        fail(PM_RUNTIME_ERROR, m.str());
+    }
+}
+
+} // namespace
+} // namespace pm
+
+extern "C" {
+
+int pm_csr_create_f32(pm_stream_t stream, int64_t rows, int64_t cols, int64_t nnz, const int64_t* ro,
+                      const int64_t* ci, const float* v, pm_csr** out)
+{
+    return pm::guarded([&] { pm::csr_create<float>(stream, rows, cols, nnz, ro, ci, v, out); });
+}
+int pm_csr_create_f64(pm_stream_t stream, int64_t rows, int64_t cols, int64_t nnz, const int64_t* ro,
+                      const int64_t* ci, const double* v, pm_csr** out)
+{
+    return pm::guarded([&] { pm::csr_create<double>(stream, rows, cols, nnz, ro, ci, v, out); });
+}
+void pm_csr_destroy(pm_csr* A)
+{
+    if (A)
+    {
+        cudaFree(A->row_ptr);
+        cudaFree(A->col_idx);
+        delete A;
+    }
+}
+int pm_csr_set_values(pm_csr* A, const void* values)
+{
+    return pm::guarded([&] {
+        if (!A || (A->nnz > 0 && !values))
+            pm::fail(PM_INVALID_ARGUMENT, "CSR handle and values must be non-null");
+        A->values = values;
+    });
+}
+int pm_csr_spmv_f32(const pm_csr* A, pm_stream_t stream, const float* x, float* y)
+{
+    return pm::guarded([&] { pm::csr_spmv<float>(A, stream, x, y); });
+}
+int pm_csr_spmv_f64(const pm_csr* A, pm_stream_t stream, const double* x, double* y)
+{
+    return pm::guarded([&] { pm::csr_spmv<double>(A, stream, x, y); });
+}
+
+int pm_solver_workspace_create(pm_solver_workspace** out)
+{
+    return pm::guarded([&] {
+        if (!out)
+            pm::fail(PM_INVALID_ARGUMENT, "workspace output pointer is null");
+        *out = new pm_solver_workspace();
+    });
+}
+void pm_solver_workspace_destroy(pm_solver_workspace* ws) { delete ws; }
+int pm_solver_workspace_close(pm_solver_workspace* ws)
+{
+    return pm::guarded([&] {
+        if (!ws)
+            pm::fail(PM_INVALID_ARGUMENT, "workspace is null");
+        ws->buffer.release();
+    });
+}
+
+#define PM_SOLVER_API(SFX, T)                                                                                      \
+    int pm_cg_##SFX(pm_solver_workspace* ws, pm_stream_t s, const pm_csr* A, const T* b, T* x,                      \
+                    const pm_solver_options* o, pm_solver_report* r)                                                \
+    {                                                                                                               \
+        return pm::guarded([&] { pm::solve<T>(ws, s, A, b, x, nullptr, 0, o, r, 0); });                            \
+    }                                                                                                               \
+    int pm_pcg_##SFX(pm_solver_workspace* ws, pm_stream_t s, const pm_csr* A, const T* b, T* x,                     \
+                     const pm_solver_options* o, pm_solver_report* r)                                               \
+    {                                                                                                               \
+        return pm::guarded([&] { pm::solve<T>(ws, s, A, b, x, nullptr, 0, o, r, o && o->use_jacobi ? 1 : 0); });  \
+    }                                                                                                               \
+    int pm_block_pcg_##SFX(pm_solver_workspace* ws, pm_stream_t s, const pm_csr* A, const T* b, T* x,               \
+                           const T* blocks, int64_t bs, const pm_solver_options* o, pm_solver_report* r)            \
+    {                                                                                                               \
+        return pm::guarded([&] { pm::solve<T>(ws, s, A, b, x, blocks, bs, o, r, 2); });                            \
+    }
+
+PM_SOLVER_API(f32, float)
+PM_SOLVER_API(f64, double)
+
+} // extern "C"

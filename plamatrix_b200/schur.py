@@ -1,0 +1,230 @@
+"""Python mirror of the reference's optimisation API for the device path
+(include/plamatrix/optimization/block_schur.h): BlockNormalEquations state on the device,
+Huber-weighted accumulation of device observations, solveDampedSchurComplement with a
+reusable SchurComplementSolverWorkspace.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .sparse import _ptr, _stream_handle
+
+vp, i64 = C.c_void_p, C.c_int64
+
+
+class SchurOptions(C.Structure):
+    _fields_ = [("max_iterations", C.c_int), ("relative_tolerance", C.c_double),
+                ("absolute_tolerance", C.c_double), ("minimum_diagonal", C.c_double),
+                ("use_initial_guess", C.c_int), ("precision", C.c_int), ("tolerance_rule", C.c_int),
+                ("check_true_residual", C.c_int), ("inner_relative_tolerance", C.c_double),
+                ("max_refinements", C.c_int)]
+
+
+class SchurReport(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("initial_residual_norm", C.c_double),
+                ("final_residual_norm", C.c_double), ("true_relative_residual", C.c_double),
+                ("pattern_reused", C.c_int), ("mixed_precision_used", C.c_int), ("refinement_steps", C.c_int),
+                ("pattern_ms", C.c_double), ("eliminated_inverse_ms", C.c_double), ("assembly_ms", C.c_double),
+                ("solve_ms", C.c_double), ("back_substitution_ms", C.c_double), ("total_ms", C.c_double),
+                ("message", C.c_char * 128)]
+
+
+for _sfx, _ct in (("f32", C.c_float), ("f64", C.c_double)):
+    N.register(f"pm_ne_upload_{_sfx}", [vp, vp, vp, vp, vp, vp, i64, vp, vp, vp, i64, vp, vp, vp])
+    N.register(f"pm_ne_download_{_sfx}", [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp])
+    N.register(f"pm_ne_accumulate_observations_{_sfx}", [vp, vp, i64, i64, vp, vp, vp, vp, vp, _ct])
+    N.register(f"pm_schur_solve_{_sfx}", [vp, vp, vp, _ct, vp, vp, vp, vp])
+    N.register(f"pm_schur_export_{_sfx}", [vp, vp, vp, vp, vp, vp, vp])
+N.register("pm_ne_create", [i64, i64, i64, i64, C.c_int, vp])
+N.register("pm_ne_destroy", [vp], None)
+N.register("pm_ne_counts", [vp, vp, vp, vp])
+N.register("pm_schur_workspace_create", [vp])
+N.register("pm_schur_workspace_destroy", [vp], None)
+N.register("pm_schur_workspace_close", [vp])
+N.register("pm_schur_pattern_build_count", [vp], C.c_int64)
+N.register("pm_schur_dims", [vp, vp, vp, vp])
+
+PRECISION = {"native": 0, "mixed": 1}
+
+
+@dataclass
+class SchurComplementSolverOptions:
+    """SchurComplementSolverOptions<Scalar> (block_schur.h:31-47) plus device-path knobs."""
+
+    max_iterations: int = 100
+    relative_tolerance: float = 1e-8
+    absolute_tolerance: float = 1e-12
+    minimum_diagonal: float = 1e-12
+    use_initial_guess: bool = False
+    precision: str = "native"
+    tolerance_rule: str = "cpu"      # "cpu": abs + rel*||r0||; "max": max(abs, rel*||r0||)
+    check_true_residual: bool = True
+    inner_relative_tolerance: float = 1e-4
+    max_refinements: int = 8
+
+    def c(self) -> SchurOptions:
+        return SchurOptions(self.max_iterations, self.relative_tolerance, self.absolute_tolerance,
+                            self.minimum_diagonal, int(self.use_initial_guess), PRECISION[self.precision],
+                            0 if self.tolerance_rule == "cpu" else 1, int(self.check_true_residual),
+                            self.inner_relative_tolerance, self.max_refinements)
+
+
+def _dtype_info(dtype):
+    dt = np.dtype(dtype)
+    if dt == np.float32:
+        return "f32", 4, torch.float32, C.c_float
+    if dt == np.float64:
+        return "f64", 8, torch.float64, C.c_double
+    raise N.InvalidArgument(f"unsupported scalar type {dtype}")
+
+
+class DeviceNormalEquations:
+    """Device-resident BlockNormalEquations<Scalar>."""
+
+    def __init__(self, P: int, L: int, bp: int, bl: int, dtype=np.float64):
+        self.sfx, size, self.tdtype, self.ct = _dtype_info(dtype)
+        self.dtype = np.dtype(dtype)
+        self.P, self.L, self.bp, self.bl = P, L, bp, bl
+        h = C.c_void_p()
+        N.call("pm_ne_create", P, L, bp, bl, size, C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        try:
+            if h is not None and N._lib is not None:
+                N._lib.pm_ne_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
+
+    def counts(self):
+        cc, pc, ver = C.c_int64(), C.c_int64(), C.c_int64()
+        N.call("pm_ne_counts", self._h, C.byref(cc), C.byref(pc), C.byref(ver))
+        return cc.value, pc.value, ver.value
+
+    def upload(self, state: dict, stream=None) -> None:
+        """state: the dict layout of oracle.NormalEquations.export() (host numpy arrays)."""
+        dt = self.dtype
+        arr = {k: np.ascontiguousarray(v, dtype=(np.int64 if v.dtype.kind in "iu" else dt)) for k, v in state.items()}
+        C_ = len(arr["cross_primary"])
+        PC = len(arr["primary_cross_row"])
+        hp = lambda a: C.c_void_p(a.ctypes.data) if a.size else None  # noqa: E731
+        N.call(f"pm_ne_upload_{self.sfx}", self._h, _stream_handle(stream), hp(arr["primary_diagonal"]),
+               hp(arr["eliminated_diagonal"]), hp(arr["primary_gradient"]), hp(arr["eliminated_gradient"]), C_,
+               hp(arr["adjacency_offsets"]), hp(arr["cross_primary"]), hp(arr["cross_values"]), PC,
+               hp(arr["primary_cross_row"]), hp(arr["primary_cross_col"]), hp(arr["primary_cross_values"]))
+
+    def download(self, stream=None) -> dict:
+        cc, pc, _ = self.counts()
+        P, L, bp, bl, dt = self.P, self.L, self.bp, self.bl, self.dtype
+        out = {"primary_diagonal": np.zeros((P, bp, bp), dt), "eliminated_diagonal": np.zeros((L, bl, bl), dt),
+               "primary_gradient": np.zeros((P, bp), dt), "eliminated_gradient": np.zeros((L, bl), dt),
+               "adjacency_offsets": np.zeros(L + 1, np.int64), "cross_primary": np.zeros(max(cc, 1), np.int64),
+               "cross_values": np.zeros((max(cc, 1), bp, bl), dt), "primary_cross_row": np.zeros(max(pc, 1), np.int64),
+               "primary_cross_col": np.zeros(max(pc, 1), np.int64),
+               "primary_cross_values": np.zeros((max(pc, 1), bp, bp), dt)}
+        hp = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+        N.call(f"pm_ne_download_{self.sfx}", self._h, _stream_handle(stream), *[hp(out[k]) for k in (
+            "primary_diagonal", "eliminated_diagonal", "primary_gradient", "eliminated_gradient",
+            "adjacency_offsets", "cross_primary", "cross_values", "primary_cross_row", "primary_cross_col",
+            "primary_cross_values")])
+        for k in ("cross_primary", "cross_values"):
+            out[k] = out[k][:cc]
+        for k in ("primary_cross_row", "primary_cross_col", "primary_cross_values"):
+            out[k] = out[k][:pc]
+        return out
+
+    def accumulate_observations(self, obs_primary: torch.Tensor, obs_eliminated: torch.Tensor, jp: torch.Tensor,
+                                jl: torch.Tensor, residual: torch.Tensor, huber_delta: float, stream=None) -> None:
+        count = int(obs_primary.numel())
+        m = int(residual.numel() // max(count, 1)) if count else 1
+        for name, t, dt in (("obs_primary", obs_primary, torch.int64), ("obs_eliminated", obs_eliminated, torch.int64),
+                            ("jp", jp, self.tdtype), ("jl", jl, self.tdtype), ("residual", residual, self.tdtype)):
+            if not t.is_cuda or not t.is_contiguous() or t.dtype != dt:
+                raise N.InvalidArgument(f"{name} must be a contiguous CUDA tensor of dtype {dt}")
+        N.call(f"pm_ne_accumulate_observations_{self.sfx}", self._h, _stream_handle(stream), count, m,
+               _ptr(obs_primary), _ptr(obs_eliminated), _ptr(jp), _ptr(jl), _ptr(residual), self.ct(huber_delta))
+
+
+class SchurComplementSolverWorkspace:
+    """Reusable Schur pattern + device buffers (block_schur.h:81-169)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        N.call("pm_schur_workspace_create", C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def pattern_build_count(self) -> int:
+        return int(N.load().pm_schur_pattern_build_count(self._h))
+
+    def close(self) -> None:
+        N.call("pm_schur_workspace_close", self._h)
+
+    def dims(self):
+        n, nnz, b = C.c_int64(), C.c_int64(), C.c_int64()
+        N.call("pm_schur_dims", self._h, C.byref(n), C.byref(nnz), C.byref(b))
+        return n.value, nnz.value, b.value
+
+    def export(self, dtype=torch.float64, stream=None) -> dict:
+        """Last assembled reduced system in the reference's scalar-CSR layout."""
+        n, nnz, blocks = self.dims()
+        ro = torch.empty(n + 1, dtype=torch.int64, device="cuda")
+        ci = torch.empty(nnz, dtype=torch.int64, device="cuda")
+        v = torch.empty(nnz, dtype=dtype, device="cuda")
+        rhs = torch.empty(n, dtype=torch.float64, device="cuda")
+        bp2 = nnz // max(blocks, 1)
+        P = n // max(int(round(bp2 ** 0.5)), 1) if blocks else 0
+        pre = torch.empty(max(P * bp2, 1), dtype=torch.float64, device="cuda")
+        sfx = "f32" if dtype == torch.float32 else "f64"
+        N.call(f"pm_schur_export_{sfx}", self._h, _stream_handle(stream), _ptr(ro), _ptr(ci), _ptr(v), _ptr(rhs),
+               _ptr(pre))
+        torch.cuda.synchronize()
+        return {"row_offsets": ro, "col_indices": ci, "values": v, "rhs": rhs, "preconditioner": pre}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        try:
+            if h is not None and N._lib is not None:
+                N._lib.pm_schur_workspace_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
+
+
+def solve_damped_schur_complement(equations: DeviceNormalEquations, damping: float,
+                                  options: SchurComplementSolverOptions | None = None,
+                                  workspace: SchurComplementSolverWorkspace | None = None,
+                                  primary_step: torch.Tensor | None = None,
+                                  eliminated_step: torch.Tensor | None = None, stream=None):
+    """solveDampedSchurComplement (block_schur.cpp:54-459) on the device.
+
+    Returns (primary_step, eliminated_step, report dict)."""
+    opts = options or SchurComplementSolverOptions()
+    ws = workspace or SchurComplementSolverWorkspace()
+    n, m = equations.P * equations.bp, equations.L * equations.bl
+    dt = equations.tdtype
+    dp = primary_step if primary_step is not None else torch.zeros(max(n, 1), dtype=dt, device="cuda")
+    dl = eliminated_step if eliminated_step is not None else torch.zeros(max(m, 1), dtype=dt, device="cuda")
+    rep = SchurReport()
+    N.call(f"pm_schur_solve_{equations.sfx}", ws.handle, _stream_handle(stream), equations.handle,
+           equations.ct(damping), C.byref(opts.c()), _ptr(dp), _ptr(dl), C.byref(rep))
+    report = {k: getattr(rep, k) for k, _ in rep._fields_}
+    report["message"] = rep.message.decode()
+    report["converged"] = bool(rep.converged)
+    report["pattern_reused"] = bool(rep.pattern_reused)
+    report["mixed_precision_used"] = bool(rep.mixed_precision_used)
+    return dp[:n], dl[:m], report

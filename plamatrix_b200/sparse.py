@@ -1,0 +1,247 @@
+"""Python mirror of the reference's sparse API for the device path
+(include/plamatrix/sparse/{sparse_ops,iterative_solver}.h): COO -> CSR, SpMV, CG/PCG.
+
+Device arrays are torch CUDA tensors (torch is used for device memory and streams
+only); every computation runs in libplamatrix_b200.so through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _native as N
+
+
+def _stream_handle(stream) -> C.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+def _sfx(dtype: torch.dtype) -> str:
+    if dtype == torch.float32:
+        return "f32"
+    if dtype == torch.float64:
+        return "f64"
+    raise N.InvalidArgument(f"unsupported scalar type {dtype}; expected float32 or float64")
+
+
+def _ptr(t) -> C.c_void_p:
+    return C.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _check_device(name: str, t: torch.Tensor, dtype=None):
+    if not t.is_cuda:
+        raise N.InvalidArgument(f"{name} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise N.InvalidArgument(f"{name} must be contiguous")
+    if dtype is not None and t.dtype != dtype:
+        raise N.InvalidArgument(f"{name} must have dtype {dtype}, got {t.dtype}")
+
+
+class SparseOpsWorkspace:
+    """Grow-only, stream-bound scratch + deferred COO status (sparse_ops.h:13-77)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        N.call("pm_sparse_workspace_create", C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        N.call("pm_sparse_workspace_close", self._h)
+
+    def capacity_bytes(self) -> int:
+        return int(N.load().pm_sparse_workspace_capacity(self._h))
+
+    def check_status(self, operation: str = "cooToCsrAsync") -> int:
+        """checkStatus(): raise the deferred error of the last conversion; return its nnz."""
+        nnz = C.c_int64(0)
+        N.call("pm_coo_status", self._h, operation.encode(), C.byref(nnz))
+        return nnz.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        try:
+            if h is not None and N._lib is not None:
+                N._lib.pm_sparse_workspace_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
+
+
+@dataclass
+class CSRMatrix:
+    """Device CSR with int64 row offsets / column indices (the reference's Index)."""
+
+    rows: int
+    cols: int
+    row_offsets: torch.Tensor
+    col_indices: torch.Tensor
+    values: torch.Tensor
+
+    @property
+    def nnz(self) -> int:
+        return int(self.values.numel())
+
+    @staticmethod
+    def empty(rows: int, cols: int, nnz: int, dtype=torch.float64, device="cuda") -> "CSRMatrix":
+        return CSRMatrix(rows, cols, torch.zeros(rows + 1, dtype=torch.int64, device=device),
+                         torch.empty(nnz, dtype=torch.int64, device=device), torch.empty(nnz, dtype=dtype, device=device))
+
+    def cpu(self):
+        return (self.row_offsets.cpu().numpy(), self.col_indices.cpu().numpy(), self.values.cpu().numpy())
+
+
+def _coo_args(rows, cols, row_indices, col_indices, values):
+    _check_device("row_indices", row_indices, torch.int64)
+    _check_device("col_indices", col_indices, torch.int64)
+    _check_device("values", values)
+    if row_indices.numel() != col_indices.numel() or row_indices.numel() != values.numel():
+        raise N.InvalidArgument("cooToCsr GPU triplet lengths must match")
+    return _sfx(values.dtype), int(values.numel())
+
+
+def coo_to_csr(rows: int, cols: int, row_indices: torch.Tensor, col_indices: torch.Tensor, values: torch.Tensor,
+               workspace: SparseOpsWorkspace | None = None, stream=None) -> CSRMatrix:
+    """Synchronous device cooToCsr (src/sparse/coo_to_csr.cu:536-561): count, sync, allocate, fill."""
+    sfx, count = _coo_args(rows, cols, row_indices, col_indices, values)
+    ws = workspace or SparseOpsWorkspace()
+    s = _stream_handle(stream)
+    N.call(f"pm_coo_to_csr_count_{sfx}", ws.handle, s, rows, cols, count, _ptr(row_indices), _ptr(col_indices),
+           _ptr(values))
+    torch.cuda.synchronize()
+    nnz = ws.check_status("cooToCsr")
+    out = CSRMatrix.empty(rows, cols, nnz, values.dtype, values.device)
+    N.call(f"pm_coo_to_csr_fill_{sfx}", ws.handle, s, nnz, _ptr(out.row_offsets), _ptr(out.col_indices),
+           _ptr(out.values))
+    torch.cuda.synchronize()
+    ws.check_status("cooToCsr")
+    return out
+
+
+def coo_to_csr_async(rows: int, cols: int, row_indices: torch.Tensor, col_indices: torch.Tensor,
+                     values: torch.Tensor, output: CSRMatrix, workspace: SparseOpsWorkspace, stream=None) -> None:
+    """cooToCsrAsync (sparse_ops.h:108-120): enqueue; sync then workspace.check_status()."""
+    sfx, count = _coo_args(rows, cols, row_indices, col_indices, values)
+    if output.rows != rows or output.cols != cols:
+        raise N.PlamatrixError("cooToCsrAsync output dimensions do not match")
+    N.call(f"pm_coo_to_csr_async_{sfx}", workspace.handle, _stream_handle(stream), rows, cols, count,
+           _ptr(row_indices), _ptr(col_indices), _ptr(values), output.nnz, _ptr(output.row_offsets),
+           _ptr(output.col_indices), _ptr(output.values))
+
+
+class CsrOperand:
+    """Validated device CSR operand (int32 structure copy) for SpMV and the solvers."""
+
+    def __init__(self, matrix: CSRMatrix, stream=None):
+        _check_device("values", matrix.values)
+        sfx = _sfx(matrix.values.dtype)
+        h = C.c_void_p()
+        N.call(f"pm_csr_create_{sfx}", _stream_handle(stream), matrix.rows, matrix.cols, matrix.nnz,
+               _ptr(matrix.row_offsets), _ptr(matrix.col_indices), _ptr(matrix.values), C.byref(h))
+        self._h = h
+        self.matrix = matrix
+        self.sfx = sfx
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_values(self, values: torch.Tensor) -> None:
+        N.call("pm_csr_set_values", self._h, _ptr(values))
+        self.matrix = CSRMatrix(self.matrix.rows, self.matrix.cols, self.matrix.row_offsets,
+                                self.matrix.col_indices, values)
+
+    def spmv(self, x: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        if x.numel() != self.matrix.cols:
+            raise N.PlamatrixError(f"spmv dimension mismatch: CSR is {self.matrix.rows}x{self.matrix.cols}, "
+                                   f"x has {x.numel()} rows")
+        y = torch.empty(self.matrix.rows, dtype=x.dtype, device=x.device) if out is None else out
+        if y.numel() != self.matrix.rows:
+            raise N.PlamatrixError("spmv output dimension mismatch")
+        N.call(f"pm_csr_spmv_{self.sfx}", self._h, _stream_handle(stream), _ptr(x), _ptr(y))
+        return y
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        try:
+            if h is not None and N._lib is not None:
+                N._lib.pm_csr_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
+
+
+def spmv(matrix, x: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    op = matrix if isinstance(matrix, CsrOperand) else CsrOperand(matrix, stream)
+    return op.spmv(x, out, stream)
+
+
+@dataclass
+class IterativeSolverOptions:
+    max_iterations: int = 1000
+    relative_tolerance: float = 1e-6
+    absolute_tolerance: float = 0.0
+    use_jacobi_preconditioner: bool = True
+    require_convergence: bool = False
+
+    def c(self) -> N.SolverOptions:
+        return N.SolverOptions(self.max_iterations, self.relative_tolerance, self.absolute_tolerance,
+                               int(self.use_jacobi_preconditioner), int(self.require_convergence))
+
+
+class IterativeSolverWorkspace:
+    def __init__(self):
+        h = C.c_void_p()
+        N.call("pm_solver_workspace_create", C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        N.call("pm_solver_workspace_close", self._h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        try:
+            if h is not None and N._lib is not None:
+                N._lib.pm_solver_workspace_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
+
+
+def _solve(kind: str, matrix, rhs, solution, workspace, options, stream, blocks=None, block_size=0) -> dict:
+    op = matrix if isinstance(matrix, CsrOperand) else CsrOperand(matrix, stream)
+    ws = workspace or IterativeSolverWorkspace()
+    opts = (options or IterativeSolverOptions()).c()
+    rep = N.SolverReport()
+    s = _stream_handle(stream)
+    if kind == "block_pcg":
+        N.call(f"pm_block_pcg_{op.sfx}", ws.handle, s, op.handle, _ptr(rhs), _ptr(solution), _ptr(blocks),
+               block_size, C.byref(opts), C.byref(rep))
+    else:
+        N.call(f"pm_{kind}_{op.sfx}", ws.handle, s, op.handle, _ptr(rhs), _ptr(solution), C.byref(opts),
+               C.byref(rep))
+    return {"converged": bool(rep.converged), "iterations": rep.iterations,
+            "initial_residual": rep.initial_residual, "final_residual": rep.final_residual}
+
+
+def cg(matrix, rhs, solution, workspace=None, options=None, stream=None) -> dict:
+    return _solve("cg", matrix, rhs, solution, workspace, options, stream)
+
+
+def pcg(matrix, rhs, solution, workspace=None, options=None, stream=None) -> dict:
+    return _solve("pcg", matrix, rhs, solution, workspace, options, stream)
+
+
+def block_pcg(matrix, rhs, solution, inverse_blocks, block_size, workspace=None, options=None, stream=None) -> dict:
+    return _solve("block_pcg", matrix, rhs, solution, workspace, options, stream, inverse_blocks, block_size)

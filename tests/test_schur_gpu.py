@@ -1,0 +1,222 @@
+"""Device damped Schur solve against the oracle (pinned to the reference) and the reference's
+known answers: normal-equation accumulation, Schur pattern (bit-exact), values, RHS,
+block-Jacobi PCG, mixed precision, pattern reuse."""
+import numpy as np
+import pytest
+import torch
+
+import known_answers as KA
+from gpu_util import dev, host
+from schur_util import canonical, csr_matvec
+from plamatrix_b200 import _native as N
+from plamatrix_b200 import schur as SC
+from plamatrix_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _oracle_ne(checkers, builder, dtype=np.float64):
+    P, L, bp, bl, residuals = builder()
+    ne = checkers.NormalEquations(P, L, bp, bl, dtype=dtype)
+    for prims, pj, elim, ej, r, w in residuals:
+        ne.add_residual(prims, pj, elim, ej, r, w)
+    return ne
+
+
+def _device_ne(oracle_ne, dtype=np.float64):
+    d = SC.DeviceNormalEquations(oracle_ne.P, oracle_ne.L, oracle_ne.bp, oracle_ne.bl, dtype=dtype)
+    d.upload(oracle_ne.export())
+    return d
+
+
+def _opts(**kw):
+    base = dict(max_iterations=50, relative_tolerance=1e-13, absolute_tolerance=1e-14)
+    base.update(kw)
+    return SC.SchurComplementSolverOptions(**base)
+
+
+@pytest.mark.parametrize("precision", ["native", "mixed"])
+def test_known_answers(checkers, precision):
+    """block_schur_test.cpp:119-158 (synthetic), :77-117 (multi-primary), :482-504 (aggregation)."""
+    ne = _device_ne(_oracle_ne(checkers, KA.synthetic_residuals))
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 0.1, _opts(precision=precision))
+    assert rep["converged"], rep["message"]
+    assert np.allclose(np.concatenate([host(dp), host(dl)]), KA.SYNTHETIC_EXPECTED, atol=1e-10, rtol=0)
+    ne = _device_ne(_oracle_ne(checkers, KA.multi_primary_residuals))
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 0.1, _opts(precision=precision))
+    assert rep["converged"]
+    assert np.allclose(host(dp), KA.MULTI_PRIMARY_EXPECTED["primary"], atol=1e-10, rtol=0)
+    assert np.allclose(host(dl), KA.MULTI_PRIMARY_EXPECTED["eliminated"], atol=1e-10, rtol=0)
+    ne = _device_ne(_oracle_ne(checkers, KA.aggregation_residuals))
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 0.5, SC.SchurComplementSolverOptions(precision=precision))
+    assert rep["converged"]
+    assert np.allclose(host(dp), KA.AGGREGATION_EXPECTED["primary"], atol=1e-12, rtol=0)
+    assert np.allclose(host(dl), KA.AGGREGATION_EXPECTED["eliminated"], atol=1e-12, rtol=0)
+
+
+def test_point_only_float(checkers):
+    """block_schur_test.cpp:531-548."""
+    c = KA.POINT_ONLY
+    o = checkers.NormalEquations(c["P"], c["L"], c["bp"], c["bl"], dtype=np.float32)
+    o.add_residual([], None, 0, [c["jacobian"]], [c["residual"]], 1.0)
+    ne = _device_ne(o, np.float32)
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, c["damping"])
+    assert rep["converged"] and dp.numel() == 0
+    assert host(dl)[0] == pytest.approx(c["eliminated"], abs=1e-6)
+
+
+def test_pattern_reuse_counts(checkers):
+    """block_schur_test.cpp:160-196."""
+    ne = _device_ne(_oracle_ne(checkers, KA.synthetic_residuals))
+    ws = SC.SchurComplementSolverWorkspace()
+    _, _, first = SC.solve_damped_schur_complement(ne, 0.1, _opts(), ws)
+    assert first["converged"] and not first["pattern_reused"] and ws.pattern_build_count() == 1
+    _, _, second = SC.solve_damped_schur_complement(ne, 0.2, _opts(), ws)
+    assert second["converged"] and second["pattern_reused"] and ws.pattern_build_count() == 1
+    # same topology in a different object is still a reuse (signature comparison)
+    ne2 = _device_ne(_oracle_ne(checkers, KA.synthetic_residuals))
+    _, _, third = SC.solve_damped_schur_complement(ne2, 0.2, _opts(), ws)
+    assert third["pattern_reused"] and ws.pattern_build_count() == 1
+    o = checkers.NormalEquations(1, 1, 1, 1)
+    o.add_residual([0], [1.0], 0, [1.0], [-0.5])
+    o.add_residual([0], [1.0], -1, None, [-0.5])
+    changed = _device_ne(o)
+    _, _, fourth = SC.solve_damped_schur_complement(changed, 0.2, _opts(), ws)
+    assert fourth["converged"] and not fourth["pattern_reused"] and ws.pattern_build_count() == 2
+
+
+def test_invalid_options_and_aliasing(checkers):
+    ne = _device_ne(_oracle_ne(checkers, KA.synthetic_residuals))
+    with pytest.raises(N.InvalidArgument):
+        SC.solve_damped_schur_complement(ne, -1.0)
+    with pytest.raises(N.InvalidArgument):
+        SC.solve_damped_schur_complement(ne, 0.1, SC.SchurComplementSolverOptions(minimum_diagonal=0.0))
+    buf = torch.zeros(8, dtype=torch.float64, device="cuda")
+    with pytest.raises(N.InvalidArgument):
+        SC.solve_damped_schur_complement(ne, 0.1, primary_step=buf, eliminated_step=buf)
+
+
+def test_non_spd_eliminated_block_reports_message(checkers):
+    o = checkers.NormalEquations(1, 1, 1, 1)
+    o.add_residual([0], [1.0], -1, None, [1.0])
+    ne = _device_ne(o)  # eliminated block stays zero: damping of zero is zero -> not SPD
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 0.0)
+    assert not rep["converged"] and rep["message"] == "eliminated block is not positive definite"
+
+
+def _device_from_observations(prob, dtype=np.float64):
+    ne = SC.DeviceNormalEquations(prob["P"], prob["L"], prob["bp"], prob["bl"], dtype=dtype)
+    ne.accumulate_observations(dev(prob["obs_primary"]), dev(prob["obs_eliminated"]), dev(prob["jp"]),
+                               dev(prob["jl"]), dev(prob["residual"]), prob["huber_delta"])
+    return ne
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_observation_accumulation_matches_reference(checkers, dtype):
+    """Huber weights + addResidualBlock on the device: eliminated blocks, gradients and cross
+    blocks bit-exact with the reference's accumulation; primary blocks within rounding."""
+    prob = W.small_bundle(seed=21, dtype=dtype)
+    ref = canonical(checkers.normal_equations_from_observations(prob, dtype=dtype).export())
+    got = _device_from_observations(prob, dtype).download()
+    for key in ("eliminated_diagonal", "eliminated_gradient", "adjacency_offsets", "cross_primary", "cross_values"):
+        assert np.array_equal(got[key], ref[key]), key
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    for key in ("primary_diagonal", "primary_gradient"):
+        scale = np.abs(ref[key]).max()
+        assert np.abs(got[key] - ref[key]).max() <= tol * scale, key
+
+
+def test_observation_topology_is_cached_and_rebuilt(checkers):
+    prob = W.small_bundle(seed=3)
+    ne = _device_from_observations(prob)
+    _, _, v1 = ne.counts()
+    ne.accumulate_observations(dev(prob["obs_primary"]), dev(prob["obs_eliminated"]), dev(prob["jp"]),
+                               dev(prob["jl"]), dev(prob["residual"] * 0.5), prob["huber_delta"])
+    assert ne.counts()[2] == v1
+    shuffled = prob["obs_primary"].copy()
+    shuffled[[0, 1]] = shuffled[[1, 0]]
+    ne.accumulate_observations(dev(shuffled), dev(prob["obs_eliminated"]), dev(prob["jp"]), dev(prob["jl"]),
+                               dev(prob["residual"]), prob["huber_delta"])
+    assert ne.counts()[2] == v1 + 1
+
+
+@pytest.mark.parametrize("precision", ["native", "mixed"])
+def test_small_bundle_solve_matches_reference(checkers, precision):
+    """P=20, L=2,000, 8,000 observations, lambda 1e-3, tol 1e-10, <=500 iterations."""
+    prob = W.small_bundle(seed=1)
+    orc = checkers.normal_equations_from_observations(prob)
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=1e-10, max_iterations=500)
+    ne = _device_from_observations(prob)
+    ws = SC.SchurComplementSolverWorkspace()
+    opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-10, precision=precision)
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+    assert rep["converged"] and rep_ref["converged"], rep["message"]
+    if precision == "native":
+        assert abs(rep["iterations"] - rep_ref["iterations"]) <= 1
+    # solutions within 1e-6 relative (FP64)
+    assert np.linalg.norm(host(dp) - dp_ref) <= 1e-6 * np.linalg.norm(dp_ref)
+    assert np.linalg.norm(host(dl) - dl_ref) <= 1e-6 * np.linalg.norm(dl_ref)
+    # reduced system: pattern bit-exact, values / RHS within rounding of the reference assembly
+    ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+    sysd = ws.export()
+    assert np.array_equal(host(sysd["row_offsets"]), ro)
+    assert np.array_equal(host(sysd["col_indices"]), ci)
+    assert np.abs(host(sysd["values"]) - vals).max() <= 1e-12 * np.abs(vals).max()
+    assert np.abs(host(sysd["rhs"]) - rhs).max() <= 1e-12 * np.abs(rhs).max()
+    # FP64 true relative residual of the device step on the reference's reduced system
+    res = rhs - csr_matvec(ro, ci, vals, host(dp))
+    assert np.linalg.norm(res) / np.linalg.norm(rhs) <= 1e-9
+
+
+def test_float_pipeline_matches_reference(checkers):
+    prob = W.small_bundle(seed=5, dtype=np.float32)
+    orc = checkers.normal_equations_from_observations(prob, dtype=np.float32)
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=1e-5, max_iterations=500)
+    ne = _device_from_observations(prob, np.float32)
+    dp, dl, rep = SC.solve_damped_schur_complement(
+        ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-5))
+    assert rep["converged"] and rep_ref["converged"]
+    assert np.linalg.norm(host(dp) - dp_ref) <= 1e-4 * np.linalg.norm(dp_ref)
+    assert np.linalg.norm(host(dl) - dl_ref) <= 1e-4 * np.linalg.norm(dl_ref)
+
+
+def test_windowed_bundle_matches_oracle(checkers):
+    """Large-system generator at 1/10 of the primaries and 1/100 of the eliminated blocks."""
+    prob = W.large_bundle(seed=7, P=400, L=20000)
+    orc = checkers.normal_equations_from_observations(prob)
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=1e-8, max_iterations=200)
+    ne = _device_from_observations(prob)
+    ws = SC.SchurComplementSolverWorkspace()
+    dp, dl, rep = SC.solve_damped_schur_complement(
+        ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=200), ws)
+    assert rep["converged"] and rep_ref["converged"]
+    assert abs(rep["iterations"] - rep_ref["iterations"]) <= 1
+    assert np.linalg.norm(host(dp) - dp_ref) <= 1e-6 * np.linalg.norm(dp_ref)
+    assert np.linalg.norm(host(dl) - dl_ref) <= 1e-6 * np.linalg.norm(dl_ref)
+    ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+    sysd = ws.export()
+    assert np.array_equal(host(sysd["row_offsets"]), ro) and np.array_equal(host(sysd["col_indices"]), ci)
+    assert rep["true_relative_residual"] <= 1e-8 * 1.01
+
+
+def test_repeated_solves_are_bitwise_identical(checkers):
+    prob = W.large_bundle(seed=9, P=300, L=10000)
+    ne = _device_from_observations(prob)
+    ws = SC.SchurComplementSolverWorkspace()
+    a = SC.solve_damped_schur_complement(ne, 1e-3, workspace=ws)
+    b = SC.solve_damped_schur_complement(ne, 1e-3, workspace=ws)
+    ne2 = _device_from_observations(prob)
+    c = SC.solve_damped_schur_complement(ne2, 1e-3)
+    for x, y in ((a, b), (a, c)):
+        assert torch.equal(x[0], y[0]) and torch.equal(x[1], y[1])
+
+
+def test_empty_observations_give_zero_normal_equations():
+    ne = SC.DeviceNormalEquations(3, 4, 6, 3)
+    e = torch.empty(0, dtype=torch.int64, device="cuda")
+    f = torch.empty(0, dtype=torch.float64, device="cuda")
+    ne.accumulate_observations(e, e, f, f, f, 1.0)
+    got = ne.download()
+    assert ne.counts()[0] == 0
+    assert not got["primary_diagonal"].any() and not got["eliminated_diagonal"].any()
+    assert got["adjacency_offsets"].tolist() == [0, 0, 0, 0, 0]

@@ -1,0 +1,131 @@
+"""Device CSR SpMV and CG / PCG / block-PCG against the oracle and the reference's known answers."""
+import numpy as np
+import pytest
+import torch
+
+import known_answers as KA
+from gpu_util import dev, host
+from plamatrix_b200 import _native as N
+from plamatrix_b200 import sparse as S
+from plamatrix_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _csr(checkers, rows, cols, r, c, v, dtype):
+    ro, ci, vv = checkers.coo_to_csr(rows, cols, r, c, np.asarray(v, dtype))
+    return S.CSRMatrix(rows, cols, dev(ro), dev(ci), dev(vv)), (ro, ci, vv)
+
+
+@pytest.mark.parametrize("case", KA.SPMV_CASES)
+def test_spmv_known_answers(checkers, case):
+    A, _ = _csr(checkers, case["rows"], case["cols"], case["r"], case["c"], case["v"], case["dtype"])
+    y = S.spmv(A, dev(np.asarray(case["x"], case["dtype"])))
+    assert host(y).tolist() == case["y"]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("mean", [1, 3, 7, 30, 200])
+def test_spmv_random_against_oracle(checkers, dtype, mean):
+    rng = np.random.default_rng(mean)
+    rows, cols = 3000, 2000
+    n = rows * mean
+    r, c = rng.integers(0, rows, n), rng.integers(0, cols, n)
+    v = rng.standard_normal(n)
+    A, (ro, ci, vv) = _csr(checkers, rows, cols, r, c, v, dtype)
+    x = rng.standard_normal(cols).astype(dtype)
+    y = host(S.spmv(A, dev(x))).astype(np.float64)
+    ref = checkers.csr_spmv(ro, ci, vv.astype(np.float64), x.astype(np.float64))
+    magnitude = checkers.csr_spmv(ro, ci, np.abs(vv.astype(np.float64)), np.abs(x.astype(np.float64)))
+    eps = np.finfo(dtype).eps
+    # any summation order is within (row length) * eps * sum|a_ij x_j|
+    lengths = np.diff(ro).astype(np.float64)
+    assert np.all(np.abs(y - ref) <= (lengths + 1) * eps * magnitude + 1e-300)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_pcg_known_answers(checkers, dtype):
+    tol = 2e-4 if dtype == np.float32 else 1e-10
+    d = KA.DIAGONAL_PCG
+    A, _ = _csr(checkers, 3, 3, d["r"], d["c"], d["v"], dtype)
+    x = torch.zeros(3, dtype=A.values.dtype, device="cuda")
+    rep = S.pcg(A, dev(np.asarray(d["rhs"], dtype)), x)
+    assert rep["converged"] and rep["iterations"] == 1
+    assert np.allclose(host(x), d["solution"], atol=tol)
+    for scale in (1e-3, 1.0, 1e3):
+        r, c, vv = KA.poisson1d(8, scale)
+        A, (ro, ci, v) = _csr(checkers, 8, 8, r, c, vv, dtype)
+        expected = np.arange(1, 9, dtype=dtype)
+        rhs = checkers.csr_spmv(ro, ci, v, expected)
+        opts = S.IterativeSolverOptions(relative_tolerance=1e-5 if dtype == np.float32 else 1e-12)
+        for fn in (S.cg, S.pcg):
+            x = torch.zeros(8, dtype=A.values.dtype, device="cuda")
+            rep = fn(A, dev(rhs), x, options=opts)
+            assert rep["converged"]
+            assert np.all(np.abs(host(x) - expected) <= tol * np.arange(1, 9))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_block_pcg_caller_inverse_one_iteration(checkers, dtype):
+    """iterative_solver_test.cpp:394-424."""
+    b = KA.COUPLED_BLOCK
+    A, (ro, ci, v) = _csr(checkers, 4, 4, b["r"], b["c"], b["v"], dtype)
+    rhs = checkers.csr_spmv(ro, ci, v, np.asarray(b["expected"], dtype))
+    x = torch.zeros(4, dtype=A.values.dtype, device="cuda")
+    opts = S.IterativeSolverOptions(relative_tolerance=1e-5 if dtype == np.float32 else 1e-12)
+    rep = S.block_pcg(A, dev(rhs), x, dev(np.asarray(b["inverse"], dtype)), 2, options=opts)
+    assert rep["converged"] and rep["iterations"] == 1
+    assert np.allclose(host(x), b["expected"], atol=2e-4 if dtype == np.float32 else 1e-10)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_breakdown_leaves_solution_unmodified(checkers, dtype):
+    """iterative_solver_test.cpp:521-560."""
+    A, _ = _csr(checkers, 2, 2, [0, 1], [0, 1], [-1.0, 1.0], dtype)
+    x = torch.zeros(2, dtype=A.values.dtype, device="cuda")
+    with pytest.raises(N.PlamatrixError):
+        S.cg(A, dev(np.ones(2, dtype)), x)
+    assert host(x).tolist() == [0.0, 0.0]
+    tiny = np.finfo(dtype).smallest_subnormal
+    A, _ = _csr(checkers, 1, 1, [0], [0], [tiny], dtype)
+    x = torch.zeros(1, dtype=A.values.dtype, device="cuda")
+    with pytest.raises(N.PlamatrixError):
+        S.cg(A, dev(np.ones(1, dtype)), x)
+    assert host(x).tolist() == [0.0]
+
+
+def test_jacobi_rejects_missing_diagonal(checkers):
+    A, _ = _csr(checkers, 2, 2, [0, 1], [1, 0], [1.0, 1.0], np.float64)
+    with pytest.raises(N.PlamatrixError) as err:
+        S.pcg(A, dev(np.ones(2)), torch.zeros(2, dtype=torch.float64, device="cuda"))
+    assert "Jacobi diagonal" in str(err.value)
+
+
+def test_zero_rhs_and_exact_guess_take_zero_iterations(checkers):
+    r, c, v = KA.poisson1d(4)
+    A, (ro, ci, vv) = _csr(checkers, 4, 4, r, c, v, np.float64)
+    rep = S.cg(A, torch.zeros(4, dtype=torch.float64, device="cuda"), torch.zeros(4, dtype=torch.float64, device="cuda"))
+    assert rep["converged"] and rep["iterations"] == 0 and rep["initial_residual"] == 0.0
+    x = torch.full((4,), 2.0, dtype=torch.float64, device="cuda")
+    rhs = checkers.csr_spmv(ro, ci, vv, np.full(4, 2.0))
+    rep = S.pcg(A, dev(rhs), x)
+    assert rep["converged"] and rep["iterations"] == 0
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_laplacian_pcg_matches_oracle(checkers, dtype):
+    lap = W.laplacian_coo(24, seed=4, dtype=dtype)
+    A, (ro, ci, v) = _csr(checkers, lap["rows"], lap["cols"], lap["row_indices"], lap["col_indices"], lap["values"],
+                          dtype)
+    b = lap["rhs"].astype(dtype)
+    x_ref, rep_ref = checkers.pcg(ro, ci, v, b, relative_tolerance=1e-8)
+    x = torch.zeros(lap["rows"], dtype=A.values.dtype, device="cuda")
+    rep = S.pcg(A, dev(b), x, options=S.IterativeSolverOptions(relative_tolerance=1e-8))
+    assert rep["converged"] and rep_ref["converged"]
+    assert abs(rep["iterations"] - rep_ref["iterations"]) <= (2 if dtype == np.float64 else 8)
+    # true residual of the device solution, in FP64
+    xr = host(x).astype(np.float64)
+    res = b.astype(np.float64) - checkers.csr_spmv(ro, ci, v.astype(np.float64), xr)
+    rel = np.linalg.norm(res) / np.linalg.norm(b.astype(np.float64))
+    assert rel <= (1e-8 * 1.5 if dtype == np.float64 else 1e-6)
+    assert np.allclose(xr, x_ref, rtol=0, atol=(1e-6 if dtype == np.float64 else 1e-3) * np.abs(x_ref).max())
