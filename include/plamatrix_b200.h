@@ -103,6 +103,26 @@ PM_API int pm_coo_to_csr_async_f64(pm_sparse_workspace* workspace, pm_stream_t s
  * output nnz that differs from the duplicate-combined nnz.  `nnz_out` (may be NULL)
  * receives the duplicate-combined nnz. */
 PM_API int pm_coo_status(pm_sparse_workspace* workspace, const char* operation, int64_t* nnz_out);
+/* Allocation-free COO -> CSR (no counterpart in the reference).  For callers that cannot
+ * allocate device memory while they run -- a host application that fixes the device-memory
+ * budget at start-up and owns every allocation, or a latency-critical loop where cudaMalloc
+ * could block or fail mid-run.  Same result as pm_coo_to_csr_async_*; the scratch is one
+ * file-scope device array of 8 MiB that every GPU loading this library holds until exit, so
+ * inputs are limited to 65,536 triplets and 65,536 rows (larger inputs: PM_INVALID_ARGUMENT).
+ * No cudaMalloc / cudaFree or allocating library call is made.  Synchronous: enqueues on
+ * `stream`, waits, and reports coordinate / value errors directly.  The output arrays hold
+ * `capacity` entries (capacity = count always suffices); `nnz_out` (host) receives the
+ * duplicate-combined nnz.  All calls share the scratch array: calls that overlap on a GPU
+ * race, so serialise them.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) and caches it; make that first call before any stream capture. */
+PM_API int pm_coo_to_csr_static_f32(pm_stream_t stream, int64_t rows, int64_t cols, int64_t count,
+                                    const int64_t* row_indices_d, const int64_t* col_indices_d,
+                                    const float* values_d, int64_t capacity, int64_t* row_offsets_d,
+                                    int64_t* col_indices_out_d, float* values_out_d, int64_t* nnz_out);
+PM_API int pm_coo_to_csr_static_f64(pm_stream_t stream, int64_t rows, int64_t cols, int64_t count,
+                                    const int64_t* row_indices_d, const int64_t* col_indices_d,
+                                    const double* values_d, int64_t capacity, int64_t* row_offsets_d,
+                                    int64_t* col_indices_out_d, double* values_out_d, int64_t* nnz_out);
 
 /* =========================================================================== CSR matrices
  * A validated CSR operand for the device SpMV and solvers.  Replaces the structure checks

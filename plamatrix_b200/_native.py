@@ -84,6 +84,8 @@ _SIGNATURES = {
     "pm_coo_to_csr_async_f32": [vp, vp, i64, i64, i64, vp, vp, vp, i64, vp, vp, vp],
     "pm_coo_to_csr_async_f64": [vp, vp, i64, i64, i64, vp, vp, vp, i64, vp, vp, vp],
     "pm_coo_status": [vp, C.c_char_p, vp],
+    "pm_coo_to_csr_static_f32": [vp, i64, i64, i64, vp, vp, vp, i64, vp, vp, vp, vp],
+    "pm_coo_to_csr_static_f64": [vp, i64, i64, i64, vp, vp, vp, i64, vp, vp, vp, vp],
     "pm_csr_create_f32": [vp, i64, i64, i64, vp, vp, vp, vp],
     "pm_csr_create_f64": [vp, i64, i64, i64, vp, vp, vp, vp],
     "pm_csr_destroy": [vp],

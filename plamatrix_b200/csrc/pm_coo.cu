@@ -18,6 +18,7 @@
 
 #include <climits>
 #include <cmath>
+#include <mutex>
 #include <sstream>
 
 namespace pm
@@ -769,6 +770,153 @@ int pm_coo_status(pm_sparse_workspace* ws, const char* operation, int64_t* nnz_o
             pm::fail(PM_RUNTIME_ERROR, m.str());
         }
     });
+}
+
+} // extern "C"
+
+// =========================================================================== allocation-free variant
+// COO -> CSR for callers that must not allocate device memory at call time: for example a
+// host application that hands the library a fixed device-memory budget at start-up and owns
+// every allocation after that, or a latency-critical loop where a cudaMalloc could block or
+// fail in the middle of a run.  The scratch of the conversion (row buckets, sort keys, scan
+// partials, status) lives in one file-scope device array of kStaticScratchBytes, created when
+// the library's device code is loaded on a GPU and held by every GPU that loads the library
+// until the process exits.  Inputs are limited to kStaticMaxTriplets triplets and
+// kStaticMaxRows rows so that the scratch always fits.  All calls share the array: calls
+// that overlap on the GPU (other streams, other host threads, other devices' contexts are
+// separate) race on it, so serialise them.  Each call clears what must start at zero.
+namespace pm
+{
+namespace
+{
+constexpr int64_t kStaticMaxTriplets = 65536;
+constexpr int64_t kStaticMaxRows = 65536;
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;
+} // namespace
+} // namespace pm
+
+static __device__ __align__(256) unsigned char g_static_coo_scratch[pm::kStaticScratchBytes];
+
+namespace pm
+{
+namespace
+{
+
+std::mutex g_static_scratch_mutex;
+void* g_static_scratch_address[64] = {};
+
+// Device address of g_static_coo_scratch for the current device.  The host-side name of the
+// array is only a stand-in, so the address is looked up once per device (with that device
+// current) and cached.  The first call on a device performs this look-up; issue that first
+// call before any stream capture.
+void* static_scratch_address()
+{
+    int device = 0;
+    PM_CUDA(cudaGetDevice(&device));
+    if (device < 0 || device >= 64)
+        fail(PM_RUNTIME_ERROR, "device index out of range for the static scratch table");
+    std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
+    if (!g_static_scratch_address[device])
+    {
+        void* address = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&address, g_static_coo_scratch);
+        if (rc != cudaSuccess || !address)
+            fail(PM_CUDA_ERROR, std::string("cudaGetSymbolAddress(static COO scratch): ") + cudaGetErrorString(rc));
+        g_static_scratch_address[device] = address;
+    }
+    return g_static_scratch_address[device];
+}
+
+// Bytes coo_prepare carves for (rows, count) triplets of type T (same layout, same order).
+template <typename T>
+size_t static_plan_bytes(int64_t rows, int64_t count)
+{
+    const size_t scan_bytes = scan_scratch_bytes(rows + 1, sizeof(int64_t)) + scan_scratch_bytes(rows + 1, sizeof(int));
+    const size_t n = static_cast<size_t>(count > 0 ? count : 1);
+    const size_t R = static_cast<size_t>(rows + 1);
+    Carver plan;
+    plan.take<CooStatus>(1);
+    plan.take<int>(R);
+    plan.take<int>(R + 1);
+    plan.take<int>(n);
+    plan.take<uint64_t>(n);
+    plan.take<T>(n);
+    plan.take<uint64_t>(n);
+    plan.take<T>(n);
+    plan.take<int>(R);
+    plan.take<int>(R);
+    plan.take<int64_t>(R + 1);
+    plan.take<char>(scan_bytes);
+    return plan.offset + 256;
+}
+
+template <typename T>
+void coo_static(cudaStream_t stream, int64_t rows, int64_t cols, int64_t count, const int64_t* ri, const int64_t* ci,
+                const T* v, int64_t capacity, int64_t* ro, int64_t* co, T* vo, int64_t* nnz_out)
+{
+    check_metadata(rows, cols, count);
+    if (count > kStaticMaxTriplets || rows > kStaticMaxRows)
+    {
+        std::ostringstream m;
+        m << "cooToCsr (static scratch): at most " << kStaticMaxTriplets << " triplets and " << kStaticMaxRows
+          << " rows are supported, got " << count << " triplets and " << rows << " rows";
+        fail(PM_INVALID_ARGUMENT, m.str());
+    }
+    require_values(count, v);
+    if (capacity < 0 || !ro || (capacity > 0 && (!co || !vo)))
+        fail(PM_INVALID_ARGUMENT, "cooToCsr (static scratch): output pointers must be non-null");
+    if (v && vo && static_cast<const void*>(v) == static_cast<const void*>(vo))
+        fail(PM_INVALID_ARGUMENT, "cooToCsrAsync values and output must not alias");
+    const size_t need = static_plan_bytes<T>(rows, count);
+    if (need > kStaticScratchBytes)
+        fail(PM_INVALID_ARGUMENT, "cooToCsr (static scratch): scratch plan exceeds the static array");
+    // a workspace whose storage is the static array: it never grows, so nothing is allocated
+    void* const base = static_scratch_address();
+    pm_sparse_workspace ws;
+    ws.buffer.ptr = base;
+    ws.buffer.bytes = kStaticScratchBytes;
+    coo_prepare<T>(&ws, stream, rows, cols, count, ri, ci, v);
+    PM_CUDA(cudaStreamSynchronize(stream));
+    int64_t nnz = 0;
+    int status = pm_coo_status(&ws, "cooToCsr", &nnz);
+    if (status != PM_OK)
+        throw Error(status, pm_last_error());
+    if (nnz > capacity)
+    {
+        std::ostringstream m;
+        m << "cooToCsr (static scratch): output capacity " << capacity << " is below the duplicate-combined nnz "
+          << nnz;
+        fail(PM_RUNTIME_ERROR, m.str());
+    }
+    ws.status_pending = true;
+    coo_fill<T>(&ws, stream, nnz, ro, co, vo, false);
+    PM_CUDA(cudaStreamSynchronize(stream));
+    if (ws.buffer.ptr != base)
+        fail(PM_RUNTIME_ERROR, "cooToCsr (static scratch): scratch storage changed unexpectedly");
+    status = pm_coo_status(&ws, "cooToCsr", nullptr);
+    if (status != PM_OK)
+        throw Error(status, pm_last_error());
+    if (nnz_out)
+        *nnz_out = nnz;
+}
+
+} // namespace
+} // namespace pm
+
+extern "C" {
+
+int pm_coo_to_csr_static_f32(pm_stream_t stream, int64_t rows, int64_t cols, int64_t count, const int64_t* ri,
+                             const int64_t* ci, const float* v, int64_t capacity, int64_t* ro, int64_t* co, float* vo,
+                             int64_t* nnz_out)
+{
+    return pm::guarded([&] { pm::coo_static<float>(stream, rows, cols, count, ri, ci, v, capacity, ro, co, vo, nnz_out); });
+}
+
+int pm_coo_to_csr_static_f64(pm_stream_t stream, int64_t rows, int64_t cols, int64_t count, const int64_t* ri,
+                             const int64_t* ci, const double* v, int64_t capacity, int64_t* ro, int64_t* co, double* vo,
+                             int64_t* nnz_out)
+{
+    return pm::guarded([&] { pm::coo_static<double>(stream, rows, cols, count, ri, ci, v, capacity, ro, co, vo, nnz_out); });
 }
 
 } // extern "C"
