@@ -22,6 +22,7 @@ pm_normal_equations::~pm_normal_equations()
     numeric.release();
     topology.release();
     observation_copy.release();
+    weights.release();
     if (by_eliminated)
         pm_sparse_workspace_destroy(by_eliminated);
     if (by_primary)
@@ -122,16 +123,22 @@ __device__ __forceinline__ T huber_weight(const T* r, int m, T delta)
     return delta / sqrt(squared);
 }
 
-// Per eliminated block: Huber weights, Hll, g_l and the cross blocks W of its distinct primaries.
-template <typename T, int BP, int BL>
-__global__ void __launch_bounds__(128) eliminated_accumulate_kernel(
-    CooView v, int m_rt, int bp_rt, int bl_rt, const T* __restrict__ jp, const T* __restrict__ jl,
-    const T* __restrict__ res, T delta, const int* __restrict__ cross_offsets, T* __restrict__ hll,
-    T* __restrict__ gl, T* __restrict__ w)
+// Huber weight of every observation (one thread each, coalesced residual reads).
+template <typename T>
+__global__ void huber_weights_kernel(int64_t count, int m, const T* __restrict__ res, T delta, T* __restrict__ weight)
 {
-    const int bp = BP > 0 ? BP : bp_rt;
-    const int bl = BL > 0 ? BL : bl_rt;
-    const int m = m_rt;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += int64_t(gridDim.x) * blockDim.x)
+        weight[i] = huber_weight(res + i * m, m, delta);
+}
+
+// Per eliminated block, any block sizes up to 16: the same sums as the fixed-size kernel below,
+// accumulated in place in the output arrays.
+template <typename T>
+__global__ void __launch_bounds__(128) eliminated_accumulate_generic_kernel(
+    CooView v, int m, int bp, int bl, const T* __restrict__ jp, const T* __restrict__ jl, const T* __restrict__ res,
+    const T* __restrict__ weights, const int* __restrict__ cross_offsets, T* __restrict__ hll, T* __restrict__ gl,
+    T* __restrict__ w)
+{
     for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < v.rows; l += int64_t(gridDim.x) * blockDim.x)
     {
         const int b = v.bucket_start[l], e = v.bucket_start[l + 1];
@@ -141,11 +148,6 @@ __global__ void __launch_bounds__(128) eliminated_accumulate_kernel(
             H[i] = T(0);
         for (int i = 0; i < bl; ++i)
             g[i] = T(0);
-        // eliminated terms in input order (selection over the bucket, which is sorted by
-        // (primary, input offset)); addResidualBlocks accumulates Hll/g_l per residual in
-        // call order, block_normal_equations.cpp:294-311
-        // (buckets longer than kSelectMax are visited in bucket order instead: deterministic,
-        // but the summation order then differs from the reference's call order)
         constexpr int kSelectMax = 64;
         const bool select = e - b <= kSelectMax;
         uint32_t last = 0;
@@ -168,19 +170,17 @@ __global__ void __launch_bounds__(128) eliminated_accumulate_kernel(
             last = best;
             const int64_t i = best;
             const T* r = res + i * m;
-            const T weight = huber_weight(r, m, delta);
+            const T weight = weights[i];
             const T* J = jl + i * m * bl;
             for (int row = 0; row < m; ++row)
                 for (int col = 0; col < bl; ++col)
                 {
-                    const T value = J[row * bl + col];
-                    g[col] = add_rn(g[col], mul_rn(mul_rn(weight, value), r[row]));
+                    const T wv = mul_rn(weight, J[row * bl + col]);
+                    g[col] = add_rn(g[col], mul_rn(wv, r[row]));
                     for (int other = 0; other < bl; ++other)
-                        H[col * bl + other] = add_rn(H[col * bl + other], mul_rn(mul_rn(weight, value), J[row * bl + other]));
+                        H[col * bl + other] = add_rn(H[col * bl + other], mul_rn(wv, J[row * bl + other]));
                 }
         }
-        // cross blocks: runs of equal primary, observations in input order inside a run
-        // (block_normal_equations.cpp:268-292)
         int cross = cross_offsets[l] - 1;
         for (int q = b; q < e; ++q)
         {
@@ -194,30 +194,236 @@ __global__ void __launch_bounds__(128) eliminated_accumulate_kernel(
             }
             T* W = w + int64_t(cross) * bp * bl;
             const int64_t i = static_cast<uint32_t>(key);
-            const T* r = res + i * m;
-            const T weight = huber_weight(r, m, delta);
+            const T weight = weights[i];
             const T* Jp = jp + i * m * bp;
             const T* Jl = jl + i * m * bl;
             for (int row = 0; row < m; ++row)
                 for (int pc = 0; pc < bp; ++pc)
                 {
-                    const T pv = Jp[row * bp + pc];
+                    const T wv = mul_rn(weight, Jp[row * bp + pc]);
                     for (int ec = 0; ec < bl; ++ec)
-                        W[pc * bl + ec] = add_rn(W[pc * bl + ec], mul_rn(mul_rn(weight, pv), Jl[row * bl + ec]));
+                        W[pc * bl + ec] = add_rn(W[pc * bl + ec], mul_rn(wv, Jl[row * bl + ec]));
                 }
         }
     }
 }
 
-// Per primary block: Hpp and g_p over its observations (input order), reduced in a fixed
-// tree: each thread sums a contiguous slice serially, slices are combined in thread order.
-template <typename T, int BP>
-__global__ void __launch_bounds__(128) primary_accumulate_kernel(CooView v, int m, int bp_rt,
-                                                                 const T* __restrict__ jp, const T* __restrict__ res,
-                                                                 T delta, T* __restrict__ hpp, T* __restrict__ gp)
+// Per eliminated block (fixed block sizes): Hll, g_l and the cross blocks W of its distinct
+// primaries, accumulated in registers and written once.
+template <typename T, int BP, int BL>
+__global__ void __launch_bounds__(128) eliminated_accumulate_kernel(
+    CooView v, int m_rt, const T* __restrict__ jp, const T* __restrict__ jl,
+    const T* __restrict__ res, const T* __restrict__ weights, const int* __restrict__ cross_offsets,
+    T* __restrict__ hll, T* __restrict__ gl, T* __restrict__ w)
 {
-    constexpr int MAXB = BP > 0 ? BP : 16;
-    const int bp = BP > 0 ? BP : bp_rt;
+    constexpr int MP = BP, ML = BL, bp = BP, bl = BL;
+    const int m = m_rt;
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < v.rows; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int b = v.bucket_start[l], e = v.bucket_start[l + 1];
+        T H[ML * ML], g[ML];
+#pragma unroll
+        for (int i = 0; i < ML * ML; ++i)
+            H[i] = T(0);
+#pragma unroll
+        for (int i = 0; i < ML; ++i)
+            g[i] = T(0);
+        // eliminated terms in input order (selection over the bucket, which is sorted by
+        // (primary, input offset)); addResidualBlocks accumulates Hll/g_l per residual in
+        // call order, block_normal_equations.cpp:294-311.  Buckets longer than kSelectMax are
+        // visited in bucket order instead (deterministic; the sum order then differs).
+        constexpr int kSelectMax = 64;
+        const bool select = e - b <= kSelectMax;
+        uint32_t last = 0;
+        for (int visited = 0; visited < e - b; ++visited)
+        {
+            uint32_t best = 0xffffffffu;
+            if (select)
+            {
+                for (int q = b; q < e; ++q)
+                {
+                    const uint32_t src = static_cast<uint32_t>(v.keys[q]);
+                    if ((visited == 0 || src > last) && src < best)
+                        best = src;
+                }
+            }
+            else
+            {
+                best = static_cast<uint32_t>(v.keys[b + visited]);
+            }
+            last = best;
+            const int64_t i = best;
+            const T* r = res + i * m;
+            const T weight = weights[i];
+            const T* J = jl + i * m * bl;
+            for (int row = 0; row < m; ++row)
+            {
+                const T rr = r[row];
+                T jrow[ML];
+#pragma unroll
+                for (int col = 0; col < ML; ++col)
+                    if (col < bl)
+                        jrow[col] = J[row * bl + col];
+#pragma unroll
+                for (int col = 0; col < ML; ++col)
+                {
+                    if (col >= bl)
+                        break;
+                    const T wv = mul_rn(weight, jrow[col]);
+                    g[col] = add_rn(g[col], mul_rn(wv, rr));
+#pragma unroll
+                    for (int other = 0; other < ML; ++other)
+                    {
+                        if (other >= bl)
+                            break;
+                        H[col * ML + other] = add_rn(H[col * ML + other], mul_rn(wv, jrow[other]));
+                    }
+                }
+            }
+        }
+        T* Hout = hll + l * bl * bl;
+        T* gout = gl + l * bl;
+        for (int col = 0; col < bl; ++col)
+        {
+            gout[col] = g[col];
+            for (int other = 0; other < bl; ++other)
+                Hout[col * bl + other] = H[col * ML + other];
+        }
+        // cross blocks: runs of equal primary, observations in input order inside a run
+        // (block_normal_equations.cpp:268-292)
+        int cross = cross_offsets[l];
+        T W[MP * ML];
+        int q = b;
+        while (q < e)
+        {
+            const uint32_t primary = static_cast<uint32_t>(v.keys[q] >> 32);
+#pragma unroll
+            for (int k = 0; k < MP * ML; ++k)
+                W[k] = T(0);
+            for (; q < e && static_cast<uint32_t>(v.keys[q] >> 32) == primary; ++q)
+            {
+                const int64_t i = static_cast<uint32_t>(v.keys[q]);
+                const T weight = weights[i];
+                const T* Jp = jp + i * m * bp;
+                const T* Jl = jl + i * m * bl;
+                for (int row = 0; row < m; ++row)
+                {
+                    T lrow[ML];
+#pragma unroll
+                    for (int ec = 0; ec < ML; ++ec)
+                        if (ec < bl)
+                            lrow[ec] = Jl[row * bl + ec];
+#pragma unroll
+                    for (int pc = 0; pc < MP; ++pc)
+                    {
+                        if (pc >= bp)
+                            break;
+                        const T wv = mul_rn(weight, Jp[row * bp + pc]);
+#pragma unroll
+                        for (int ec = 0; ec < ML; ++ec)
+                        {
+                            if (ec >= bl)
+                                break;
+                            W[pc * ML + ec] = add_rn(W[pc * ML + ec], mul_rn(wv, lrow[ec]));
+                        }
+                    }
+                }
+            }
+            T* Wout = w + int64_t(cross) * bp * bl;
+            for (int pc = 0; pc < bp; ++pc)
+                for (int ec = 0; ec < bl; ++ec)
+                    Wout[pc * bl + ec] = W[pc * ML + ec];
+            ++cross;
+        }
+    }
+}
+
+// Per primary block (6x6): Hpp and g_p over its observations.  Warp w of the block owns a
+// contiguous slice of the primary's observation list (a multiple of 32 long) and lane j of it the
+// observations lo_w + j, lo_w + j + 32, ...; every lane sums its 42 terms serially, the lanes of a
+// warp are combined by a fixed xor-shuffle tree and the warps in warp order.  The reduction tree
+// depends only on the list length, never on scheduling.
+template <typename T>
+__global__ void __launch_bounds__(128) primary_accumulate6_kernel(CooView v, int m, const T* __restrict__ jp,
+                                                                  const T* __restrict__ res,
+                                                                  const T* __restrict__ weights, T* __restrict__ hpp,
+                                                                  T* __restrict__ gp)
+{
+    constexpr int W = 42; // 36 Hpp entries + 6 gradient entries
+    constexpr int kWarps = 4;
+    __shared__ T part[kWarps][W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t p = blockIdx.x; p < v.rows; p += gridDim.x)
+    {
+        const int b = v.bucket_start[p], e = v.bucket_start[p + 1];
+        const int len = e - b;
+        const int per = ((len + kWarps * 32 - 1) / (kWarps * 32)) * 32;
+        const int lo = b + min(len, warp * per), hi = b + min(len, (warp + 1) * per);
+        T sum[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            sum[k] = T(0);
+        for (int q = lo + lane; q < hi; q += 32)
+        {
+            const int64_t i = static_cast<uint32_t>(v.keys[q]);
+            const T weight = weights[i];
+            const T* r = res + i * m;
+            const T* J = jp + i * m * 6;
+            for (int row = 0; row < m; ++row)
+            {
+                T jrow[6];
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    jrow[c] = J[row * 6 + c];
+                const T rr = r[row];
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                {
+                    const T wv = mul_rn(weight, jrow[c]);
+                    sum[36 + c] = add_rn(sum[36 + c], mul_rn(wv, rr));
+#pragma unroll
+                    for (int o = 0; o < 6; ++o)
+                        sum[c * 6 + o] = add_rn(sum[c * 6 + o], mul_rn(wv, jrow[o]));
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+        {
+            T x = sum[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                x = add_rn(x, __shfl_xor_sync(0xffffffffu, x, o));
+            sum[k] = x;
+        }
+        if (lane == 0)
+        {
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                part[warp][k] = sum[k];
+        }
+        __syncthreads();
+        if (threadIdx.x < W)
+        {
+            T total = T(0);
+            for (int wi = 0; wi < kWarps; ++wi)
+                total = add_rn(total, part[wi][threadIdx.x]);
+            if (threadIdx.x < 36)
+                hpp[p * 36 + threadIdx.x] = total;
+            else
+                gp[p * 6 + (threadIdx.x - 36)] = total;
+        }
+        __syncthreads();
+    }
+}
+
+// Generic block sizes: one thread per contiguous slice, slices combined in thread order.
+template <typename T>
+__global__ void __launch_bounds__(128) primary_accumulate_kernel(CooView v, int m, int bp, const T* __restrict__ jp,
+                                                                 const T* __restrict__ res,
+                                                                 const T* __restrict__ weights, T* __restrict__ hpp,
+                                                                 T* __restrict__ gp)
+{
     extern __shared__ unsigned char smem_raw[];
     T* part = reinterpret_cast<T*>(smem_raw); // [blockDim][bp*bp + bp]
     const int width = bp * bp + bp;
@@ -227,27 +433,24 @@ __global__ void __launch_bounds__(128) primary_accumulate_kernel(CooView v, int 
         const int len = e - b;
         const int per = (len + blockDim.x - 1) / blockDim.x;
         const int lo = b + min(len, int(threadIdx.x) * per), hi = b + min(len, int(threadIdx.x + 1) * per);
-        T acc[MAXB * MAXB + MAXB];
+        T* acc = part + threadIdx.x * width;
         for (int k = 0; k < width; ++k)
             acc[k] = T(0);
         for (int q = lo; q < hi; ++q)
         {
             const int64_t i = static_cast<uint32_t>(v.keys[q]);
             const T* r = res + i * m;
-            const T weight = huber_weight(r, m, delta);
+            const T weight = weights[i];
             const T* J = jp + i * m * bp;
             for (int row = 0; row < m; ++row)
                 for (int col = 0; col < bp; ++col)
                 {
-                    const T value = J[row * bp + col];
-                    acc[bp * bp + col] = add_rn(acc[bp * bp + col], mul_rn(mul_rn(weight, value), r[row]));
+                    const T wv = mul_rn(weight, J[row * bp + col]);
+                    acc[bp * bp + col] = add_rn(acc[bp * bp + col], mul_rn(wv, r[row]));
                     for (int other = 0; other < bp; ++other)
-                        acc[col * bp + other] =
-                            add_rn(acc[col * bp + other], mul_rn(mul_rn(weight, value), J[row * bp + other]));
+                        acc[col * bp + other] = add_rn(acc[col * bp + other], mul_rn(wv, J[row * bp + other]));
                 }
         }
-        for (int k = 0; k < width; ++k)
-            part[threadIdx.x * width + k] = acc[k];
         __syncthreads();
         for (int k = threadIdx.x; k < width; k += blockDim.x)
         {
@@ -327,6 +530,15 @@ void ne_upload(pm_normal_equations* ne, cudaStream_t stream, const T* hpp, const
     }
     PM_CUDA(cudaStreamSynchronize(stream));
     ne->observation_topology = false;
+    bool sorted = true;
+    for (int64_t l = 0; l < ne->L && sorted; ++l)
+        for (int64_t c = cross_offsets[l] + 1; c < cross_offsets[l + 1]; ++c)
+            if (cross_primary[c] <= cross_primary[c - 1])
+            {
+                sorted = false;
+                break;
+            }
+    ne->crosses_sorted = sorted;
     ne->topology_version += 1;
 }
 
@@ -462,6 +674,7 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
         ne->observation_count = count;
         ne->residual_size = m;
         ne->observation_topology = true;
+        ne->crosses_sorted = true; // buckets are sorted by (primary, input offset)
         ne->topology_version += 1;
     }
     layout_numeric(ne, stream);
@@ -474,37 +687,41 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
     T* hpp = static_cast<T*>(ne->primary_diagonal);
     T* gp = static_cast<T*>(ne->primary_gradient);
     const int bp = static_cast<int>(ne->bp), bl = static_cast<int>(ne->bl), mm = static_cast<int>(m);
+    ne->weights.ensure(size_t(count + 1) * sizeof(T) + 256, stream, "normal equations");
+    T* weights = static_cast<T*>(ne->weights.ptr);
+    if (count > 0)
+    {
+        huber_weights_kernel<T><<<grid_for(count, 256, 1 << 20), 256, 0, stream>>>(count, mm, res, delta, weights);
+        PM_LAUNCH_CHECK();
+    }
     if (ne->L > 0)
     {
         const unsigned grid = grid_for(ne->L, 128, 1 << 20);
         if (bp == 6 && bl == 3)
-            eliminated_accumulate_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(ve, mm, bp, bl, jp, jl, res, delta,
+            eliminated_accumulate_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(ve, mm, jp, jl, res, weights,
                                                                            ne->cross_offsets, hll, gl, w);
         else
-            eliminated_accumulate_kernel<T, 0, 0><<<grid, 128, 0, stream>>>(ve, mm, bp, bl, jp, jl, res, delta,
-                                                                           ne->cross_offsets, hll, gl, w);
+            eliminated_accumulate_generic_kernel<T><<<grid, 128, 0, stream>>>(ve, mm, bp, bl, jp, jl, res, weights,
+                                                                             ne->cross_offsets, hll, gl, w);
         PM_LAUNCH_CHECK();
     }
     if (ne->P > 0)
     {
-        // one slice per thread; the per-thread partials live in shared memory (<= 200 KB)
-        const size_t width_bytes = size_t(bp * bp + bp) * sizeof(T);
-        const int threads = static_cast<int>(std::max<size_t>(32, std::min<size_t>(128, (200u << 10) / width_bytes / 32 * 32)));
-        const size_t smem = size_t(threads) * width_bytes;
         const unsigned grid = grid_for(ne->P, 1, 1 << 20);
         if (bp == 6)
         {
-            PM_CUDA(cudaFuncSetAttribute(primary_accumulate_kernel<T, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem)));
-            primary_accumulate_kernel<T, 6><<<grid, threads, smem, stream>>>(vp, mm, bp, jp, res, delta, hpp, gp);
-            PM_LAUNCH_CHECK();
+            primary_accumulate6_kernel<T><<<grid, 128, 0, stream>>>(vp, mm, jp, res, weights, hpp, gp);
         }
         else
         {
-            PM_CUDA(cudaFuncSetAttribute(primary_accumulate_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            // one slice per thread; the per-thread partials live in shared memory (<= 200 KB)
+            const size_t width_bytes = size_t(bp * bp + bp) * sizeof(T);
+            const int threads =
+                static_cast<int>(std::max<size_t>(32, std::min<size_t>(128, (200u << 10) / width_bytes / 32 * 32)));
+            const size_t smem = size_t(threads) * width_bytes;
+            PM_CUDA(cudaFuncSetAttribute(primary_accumulate_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem)));
-            primary_accumulate_kernel<T, 0><<<grid, threads, smem, stream>>>(vp, mm, bp, jp, res, delta, hpp, gp);
-            PM_LAUNCH_CHECK();
+            primary_accumulate_kernel<T><<<grid, threads, smem, stream>>>(vp, mm, bp, jp, res, weights, hpp, gp);
         }
         PM_LAUNCH_CHECK();
     }

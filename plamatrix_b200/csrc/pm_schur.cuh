@@ -27,10 +27,12 @@ struct pm_normal_equations
     int* primary_cross_row = nullptr; // PC (row < col)
     int* primary_cross_col = nullptr; // PC
     int64_t topology_version = 0;     // bumped whenever the topology arrays change
+    bool crosses_sorted = false;      // crosses of every eliminated block in ascending primary order
     // observation-path topology cache
     pm_sparse_workspace* by_eliminated = nullptr; // observations bucketed by eliminated block
     pm_sparse_workspace* by_primary = nullptr;    // observations bucketed by primary block
     pm::DeviceBuffer observation_copy;            // saved index arrays + zero column
+    pm::DeviceBuffer weights;                     // Huber weight of every observation
     int64_t observation_count = -1;
     int64_t residual_size = 0;
     bool observation_topology = false;

@@ -76,6 +76,13 @@ struct pm_schur_workspace
     int* diag_pos = nullptr;
     int* transpose = nullptr;
     int* block_pc = nullptr; // per block: primary-cross index k (forward), -(k+2) transposed, -1 none
+    // 6x3 assembly pair lists (pattern lifetime, own buffer)
+    pm::DeviceBuffer pair_buffer;
+    int64_t U = 0, E = 0;              // upper blocks, cross pairs
+    int2* row_entries = nullptr;       // C: {cross, eliminated} of every primary-list entry
+    int* upper_blocks = nullptr;       // U: block index of every upper block, row-major
+    int* pair_offsets = nullptr;       // B + 1: pairs of block b are [off[b], off[b+1])
+    int4* pairs = nullptr;             // E: {cross of p, cross of q, eliminated, 0}, l ascending per block
     int* saved_offsets = nullptr;
     int* saved_primary = nullptr;
     int* saved_pc = nullptr;
@@ -99,6 +106,7 @@ struct pm_schur_workspace
         pattern.release();
         numeric.release();
         scratch.release();
+        pair_buffer.release();
         if (prim_sort)
             pm_sparse_workspace_destroy(prim_sort);
         if (host_status)
@@ -539,6 +547,303 @@ __global__ void __launch_bounds__(kRowThreads) assemble_kernel(AssembleArgs<T> a
             }
             for (int k = 0; k < bpp; ++k)
                 a.minv[int64_t(p) * bpp + k] = inv[k];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- 6x3 assembly from pair lists
+// The pattern build lists, for every upper block (p, q) of the reduced system, the pairs of
+// crosses (W_lp, W_lq) of the eliminated blocks l that see both p and q, in ascending l.  The
+// numeric assembly is then two flat kernels with no shared-memory staging and no barriers in
+// the main loop: one walks the pair list of each upper block, one the cross list of each row
+// (diagonal block, right-hand side and block-Jacobi inverse).  Every sum runs in a fixed order.
+
+// crosses of row p's list entry j that pair with a later primary: with each eliminated block's
+// crosses sorted by primary these are the entries after the cross itself
+__device__ __forceinline__ void pair_range(int p, int c, int l, const int* __restrict__ cross_offsets, int sorted,
+                                           int& begin, int& end)
+{
+    begin = sorted ? c + 1 : cross_offsets[l];
+    end = cross_offsets[l + 1];
+    (void)p;
+}
+
+__global__ void pair_count_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
+                                  const int* __restrict__ cross_eliminated, const int* __restrict__ cross_offsets,
+                                  const int* __restrict__ cross_primary, int sorted, int* __restrict__ count)
+{
+    for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
+    {
+        const int p = static_cast<int>(pp);
+        for (int j = prim_offsets[p] + threadIdx.x; j < prim_offsets[p + 1]; j += blockDim.x)
+        {
+            const int c = prim_cross[j];
+            const int l = cross_eliminated[c];
+            int b, e;
+            pair_range(p, c, l, cross_offsets, sorted, b, e);
+            int n = 0;
+            if (sorted)
+                n = e - b;
+            else
+                for (int k = b; k < e; ++k)
+                    n += cross_primary[k] > p;
+            count[j] = n;
+        }
+    }
+}
+
+__global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross,
+                                   const int* __restrict__ cross_eliminated, int2* __restrict__ row_entries)
+{
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < C; j += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int c = prim_cross[j];
+        row_entries[j] = make_int2(c, cross_eliminated[c]);
+    }
+}
+
+__global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
+                                 const int* __restrict__ cross_eliminated, const int* __restrict__ cross_offsets,
+                                 const int* __restrict__ cross_primary, int sorted, const int64_t* __restrict__ offset,
+                                 const int* __restrict__ block_row_ptr, const int* __restrict__ block_col,
+                                 const int* __restrict__ diag_pos, int64_t* __restrict__ pair_block,
+                                 int64_t* __restrict__ pair_cross, int* __restrict__ pair_other)
+{
+    for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
+    {
+        const int p = static_cast<int>(pp);
+        const int lo0 = diag_pos[p] + 1, hi0 = block_row_ptr[p + 1];
+        for (int j = prim_offsets[p] + threadIdx.x; j < prim_offsets[p + 1]; j += blockDim.x)
+        {
+            const int c = prim_cross[j];
+            const int l = cross_eliminated[c];
+            int b, e;
+            pair_range(p, c, l, cross_offsets, sorted, b, e);
+            int64_t at = offset[j];
+            for (int k = b; k < e; ++k)
+            {
+                const int q = cross_primary[k];
+                if (q <= p)
+                    continue;
+                int lo = lo0, hi = hi0;
+                while (lo < hi)
+                {
+                    const int mid = (lo + hi) >> 1;
+                    if (block_col[mid] < q)
+                        lo = mid + 1;
+                    else
+                        hi = mid;
+                }
+                pair_block[at] = lo; // the pattern holds (p, q) by construction
+                pair_cross[at] = c;
+                pair_other[at] = k;
+                ++at;
+            }
+        }
+    }
+}
+
+// sorted pair keys (cross of p << 32 | emission index) -> {cross of p, cross of q, eliminated, 0}
+__global__ void pair_gather_kernel(int64_t E, const uint64_t* __restrict__ keys, const int* __restrict__ pair_other,
+                                   const int* __restrict__ cross_eliminated, int4* __restrict__ pairs)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < E; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const uint64_t key = keys[i];
+        const int c = static_cast<int>(key >> 32);
+        pairs[i] = make_int4(c, pair_other[static_cast<uint32_t>(key)], cross_eliminated[c], 0);
+    }
+}
+
+__global__ void upper_count_kernel(int64_t P, const int* __restrict__ block_row_ptr, const int* __restrict__ diag_pos,
+                                   int* __restrict__ count)
+{
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+        count[p] = block_row_ptr[p + 1] - diag_pos[p] - 1;
+}
+
+__global__ void upper_fill_kernel(int64_t P, const int* __restrict__ offset, const int* __restrict__ diag_pos,
+                                  int* __restrict__ upper_blocks)
+{
+    for (int64_t p = blockIdx.x; p < P; p += gridDim.x)
+        for (int i = offset[p] + threadIdx.x; i < offset[p + 1]; i += blockDim.x)
+            upper_blocks[i] = diag_pos[p] + 1 + (i - offset[p]);
+}
+
+// Upper block (p, q), two threads per block (rows 0-2 and 3-5):
+//   S_pq = H_pq - sum_l (W_lp Hll_l^-1) W_lq^T, l ascending, accumulated in FP64 registers.
+template <typename T>
+__global__ void __launch_bounds__(128) assemble_upper6_kernel(int64_t U, const int* __restrict__ upper_blocks,
+                                                              const int* __restrict__ pair_offsets,
+                                                              const int4* __restrict__ pairs, const T* __restrict__ w,
+                                                              const double* __restrict__ hinv,
+                                                              const int* __restrict__ block_pc,
+                                                              const T* __restrict__ pcv, T* __restrict__ S)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < 2 * U; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const int b = upper_blocks[i >> 1];
+        const int half = static_cast<int>(i & 1);
+        const int lo = pair_offsets[b], hi = pair_offsets[b + 1];
+        double acc[3][6];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                acc[r][c] = 0.0;
+        for (int k = lo; k < hi; ++k)
+        {
+            const int4 pr = pairs[k];
+            const T* wp = w + int64_t(pr.x) * 18 + half * 9;
+            const T* wq = w + int64_t(pr.y) * 18;
+            const double* h = hinv + int64_t(pr.z) * 9;
+            double wrow[9], H[9], Wq[18];
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+            {
+                wrow[e] = static_cast<double>(wp[e]);
+                H[e] = h[e];
+            }
+#pragma unroll
+            for (int e = 0; e < 18; ++e)
+                Wq[e] = static_cast<double>(wq[e]);
+#pragma unroll
+            for (int rr = 0; rr < 3; ++rr)
+            {
+                double t[3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j)
+                    t[j] = H[j * 3 + 0] * wrow[rr * 3 + 0] + H[j * 3 + 1] * wrow[rr * 3 + 1] +
+                           H[j * 3 + 2] * wrow[rr * 3 + 2];
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    acc[rr][c] += t[0] * Wq[c * 3] + t[1] * Wq[c * 3 + 1] + t[2] * Wq[c * 3 + 2];
+            }
+        }
+        const int pc = block_pc[b];
+        T* out = S + int64_t(b) * 36;
+#pragma unroll
+        for (int rr = 0; rr < 3; ++rr)
+        {
+            const int r = 3 * half + rr;
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+            {
+                const double base = pc >= 0 ? static_cast<double>(pcv[int64_t(pc) * 36 + r * 6 + c]) : 0.0;
+                out[r * 6 + c] = static_cast<T>(base - acc[rr][c]);
+            }
+        }
+    }
+}
+
+// Row p (one CTA of kDiagThreads): diagonal block, right-hand side and block-Jacobi inverse.
+//   S_pp = Hpp + damping - sum_l W_lp Hll_l^-1 W_lp^T      (lower triangle summed, mirrored)
+//   rhs_p = -g_p + sum_l W_lp y_l,  y_l = Hll_l^-1 g_l
+// Thread t sums the row's crosses t, t + kDiagThreads, ...; warps reduce by a fixed xor tree and
+// are combined in warp order.
+constexpr int kDiagThreads = 128;
+
+template <typename T>
+__global__ void __launch_bounds__(kDiagThreads) assemble_diag6_kernel(
+    int64_t P, const int* __restrict__ prim_offsets, const int2* __restrict__ row_entries, const T* __restrict__ w,
+    const double* __restrict__ hinv, const double* __restrict__ y, const T* __restrict__ hpp, const T* __restrict__ gp,
+    const int* __restrict__ diag_pos, double lambda, double min_diag, T* __restrict__ S, double* __restrict__ rhs,
+    double* __restrict__ minv, SchurStatus* status)
+{
+    constexpr int kSums = 27; // 21 lower-triangle entries + 6 right-hand-side entries
+    constexpr int kWarps = kDiagThreads / 32;
+    __shared__ double part[kWarps][kSums];
+    __shared__ double diag[36];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
+    {
+        const int p = static_cast<int>(pp);
+        double sum[kSums];
+#pragma unroll
+        for (int k = 0; k < kSums; ++k)
+            sum[k] = 0.0;
+        for (int j = prim_offsets[p] + t; j < prim_offsets[p + 1]; j += kDiagThreads)
+        {
+            const int2 e = row_entries[j];
+            const T* wc = w + int64_t(e.x) * 18;
+            const double* h = hinv + int64_t(e.y) * 9;
+            double W[18], H[9];
+#pragma unroll
+            for (int k = 0; k < 18; ++k)
+                W[k] = static_cast<double>(wc[k]);
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                H[k] = h[k];
+            const double y0 = y[int64_t(e.y) * 3], y1 = y[int64_t(e.y) * 3 + 1], y2 = y[int64_t(e.y) * 3 + 2];
+            int k = 0;
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+            {
+                double tr[3];
+#pragma unroll
+                for (int j2 = 0; j2 < 3; ++j2)
+                    tr[j2] = H[j2 * 3 + 0] * W[r * 3 + 0] + H[j2 * 3 + 1] * W[r * 3 + 1] + H[j2 * 3 + 2] * W[r * 3 + 2];
+#pragma unroll
+                for (int c = 0; c <= r; ++c)
+                    sum[k++] += tr[0] * W[c * 3] + tr[1] * W[c * 3 + 1] + tr[2] * W[c * 3 + 2];
+                sum[21 + r] += W[r * 3 + 0] * y0 + W[r * 3 + 1] * y1 + W[r * 3 + 2] * y2;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kSums; ++k)
+        {
+            double x = sum[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                x = __dadd_rn(x, __shfl_xor_sync(0xffffffffu, x, o));
+            sum[k] = x;
+        }
+        if (lane == 0)
+        {
+#pragma unroll
+            for (int k = 0; k < kSums; ++k)
+                part[warp][k] = sum[k];
+        }
+        __syncthreads();
+        const int dpos = diag_pos[p];
+        if (t < 36)
+        {
+            const int r = t / 6, c = t % 6;
+            const int lr = r >= c ? r : c, lc = r >= c ? c : r;
+            const int k = lr * (lr + 1) / 2 + lc;
+            double dacc = 0.0;
+            for (int wi = 0; wi < kWarps; ++wi)
+                dacc = __dadd_rn(dacc, part[wi][k]);
+            double base = static_cast<double>(hpp[int64_t(p) * 36 + t]);
+            if (r == c)
+                base = __dadd_rn(base, __dmul_rn(lambda, fmax(fabs(base), min_diag)));
+            const double value = base - dacc;
+            S[int64_t(dpos) * 36 + t] = static_cast<T>(value);
+            diag[t] = static_cast<double>(static_cast<T>(value));
+        }
+        else if (t < 42)
+        {
+            double racc = 0.0;
+            for (int wi = 0; wi < kWarps; ++wi)
+                racc = __dadd_rn(racc, part[wi][21 + t - 36]);
+            rhs[int64_t(p) * 6 + (t - 36)] = -static_cast<double>(gp[int64_t(p) * 6 + (t - 36)]) + racc;
+        }
+        __syncthreads();
+        if (t == 0)
+        {
+            double m[36], inv[36], lower[36], work[6];
+            for (int r = 0; r < 6; ++r)
+                for (int c = 0; c < 6; ++c)
+                    m[r * 6 + c] = r >= c ? diag[r * 6 + c] : diag[c * 6 + r];
+            if (!spd_inverse<6>(m, 6, inv, lower, work))
+            {
+                atomicMin(&status->preconditioner_bad, static_cast<long long>(p));
+                for (int k = 0; k < 36; ++k)
+                    inv[k] = 0.0;
+            }
+            for (int k = 0; k < 36; ++k)
+                minv[int64_t(p) * 36 + k] = inv[k];
         }
         __syncthreads();
     }
@@ -1081,6 +1386,120 @@ bool topology_matches(pm_schur_workspace* ws, const pm_normal_equations* ne, cud
     return differs == 0;
 }
 
+// Pair lists of the 6x3 assembly: for every upper block (p, q), the crosses (W_lp, W_lq) of the
+// eliminated blocks l seen by both, in ascending l (bucketed and sorted by the COO machinery).
+void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
+{
+    const int64_t P = ne->P, C = ne->cross_count, B = ws->B;
+    const int sorted = ne->crosses_sorted ? 1 : 0;
+    const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(P, 8 * sm_count())));
+    // scratch: pass 1 (pairs per primary-list entry and upper blocks per row, with their scans),
+    // then pass 2 (the emitted pairs); pass 1 is re-run if the scratch has to grow for pass 2
+    Carver s1;
+    s1.take<int>(C + 1);
+    s1.take<int64_t>(C + 2);
+    s1.take<int>(P + 1);
+    s1.take<int>(P + 2);
+    s1.take<char>(scan_scratch_bytes(C + 1, sizeof(int64_t)));
+    s1.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
+    const size_t pass1 = ((s1.offset + 255) / 256) * 256;
+    int* count = nullptr;
+    int64_t* offset = nullptr;
+    int* upper_count = nullptr;
+    int* upper_offset = nullptr;
+    int64_t E = 0;
+    int U = 0;
+    auto run_pass1 = [&]() {
+        Carver c1;
+        c1.base = static_cast<char*>(ws->scratch.ptr);
+        count = c1.take<int>(C + 1);
+        offset = c1.take<int64_t>(C + 2);
+        upper_count = c1.take<int>(P + 1);
+        upper_offset = c1.take<int>(P + 2);
+        void* scan1 = c1.take<char>(scan_scratch_bytes(C + 1, sizeof(int64_t)));
+        void* scan2 = c1.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
+        if (P > 0 && C > 0)
+        {
+            pair_count_kernel<<<grid, 128, 0, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
+                                                        ne->cross_offsets, ne->cross_primary, sorted, count);
+            PM_LAUNCH_CHECK();
+        }
+        exclusive_scan<int, int64_t>(count, offset, C, scan1, stream);
+        if (P > 0)
+        {
+            upper_count_kernel<<<grid_for(P, 256, 4096), 256, 0, stream>>>(P, ws->block_row_ptr, ws->diag_pos,
+                                                                           upper_count);
+            PM_LAUNCH_CHECK();
+        }
+        exclusive_scan<int, int>(upper_count, upper_offset, P, scan2, stream);
+        PM_CUDA(cudaMemcpyAsync(&E, offset + C, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaMemcpyAsync(&U, upper_offset + P, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaStreamSynchronize(stream));
+    };
+    ws->scratch.ensure(pass1 + 512, stream, "SchurComplementSolverWorkspace");
+    run_pass1();
+    if (E > INT32_MAX - 1)
+        fail(PM_OVERFLOW_ERROR, "Schur assembly supports up to 2^31 - 2 cross pairs");
+    Carver s2;
+    s2.take<int64_t>(E + 1);
+    s2.take<int64_t>(E + 1);
+    s2.take<int>(E + 1);
+    void* before = ws->scratch.ptr;
+    ws->scratch.ensure(pass1 + s2.offset + 512, stream, "SchurComplementSolverWorkspace");
+    if (ws->scratch.ptr != before)
+        run_pass1();
+    // pair buffer: row entries (C) | pair offsets (B + 1) | upper blocks (U) | pairs (E)
+    Carver plan;
+    plan.take<int2>(C + 1);
+    plan.take<int>(B + 2);
+    plan.take<int>(U + 1);
+    plan.take<int4>(E + 1);
+    ws->pair_buffer.ensure(plan.offset + 512, stream, "SchurComplementSolverWorkspace");
+    Carver pc;
+    pc.base = static_cast<char*>(ws->pair_buffer.ptr);
+    ws->row_entries = pc.take<int2>(C + 1);
+    ws->pair_offsets = pc.take<int>(B + 2);
+    ws->upper_blocks = pc.take<int>(U + 1);
+    ws->pairs = pc.take<int4>(E + 1);
+    ws->U = U;
+    ws->E = E;
+    if (C > 0)
+    {
+        row_entries_kernel<<<grid_for(C, 256, 1 << 16), 256, 0, stream>>>(C, ws->prim_cross, ne->cross_eliminated,
+                                                                         ws->row_entries);
+        PM_LAUNCH_CHECK();
+    }
+    if (P > 0)
+    {
+        upper_fill_kernel<<<grid, 128, 0, stream>>>(P, upper_offset, ws->diag_pos, ws->upper_blocks);
+        PM_LAUNCH_CHECK();
+    }
+    // pass 2: emit (block, cross of p, cross of q), bucket by block, sort by cross of p
+    Carver c2;
+    c2.base = static_cast<char*>(ws->scratch.ptr) + pass1;
+    int64_t* pair_block = c2.take<int64_t>(E + 1);
+    int64_t* pair_cross = c2.take<int64_t>(E + 1);
+    int* pair_other = c2.take<int>(E + 1);
+    if (P > 0 && E > 0)
+    {
+        pair_emit_kernel<<<grid, 128, 0, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
+                                                   ne->cross_offsets, ne->cross_primary, sorted, offset,
+                                                   ws->block_row_ptr, ws->block_col, ws->diag_pos, pair_block,
+                                                   pair_cross, pair_other);
+        PM_LAUNCH_CHECK();
+    }
+    coo_prepare<float>(ws->prim_sort, stream, B, C + 1, E, pair_block, pair_cross, nullptr);
+    coo_internal_status(ws->prim_sort, stream, "Schur pair lists");
+    const CooView v = coo_view(ws->prim_sort);
+    PM_CUDA(cudaMemcpyAsync(ws->pair_offsets, v.bucket_start, (B + 1) * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    if (E > 0)
+    {
+        pair_gather_kernel<<<grid_for(E, 256, 1 << 16), 256, 0, stream>>>(E, v.keys, pair_other, ne->cross_eliminated,
+                                                                         ws->pairs);
+        PM_LAUNCH_CHECK();
+    }
+}
+
 void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
 {
     const int64_t P = ne->P, L = ne->L, C = ne->cross_count, PC = ne->primary_cross_count;
@@ -1180,6 +1599,8 @@ void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
         PM_LAUNCH_CHECK();
     }
     PM_CUDA(cudaMemsetAsync(ws->block_pc, 0xff, size_t(B + 1) * sizeof(int), stream));
+    if (ne->bp == 6 && ne->bl == 3)
+        build_pairs(ws, ne, stream);
     if (PC > 0)
     {
         block_pc_kernel<<<grid_for(PC, 256, 4096), 256, 0, stream>>>(PC, ne->primary_cross_row, ne->primary_cross_col,
@@ -1241,9 +1662,15 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
     };
     if (ne->bp == 6 && ne->bl == 3)
     {
-        const size_t smem = smem_for(64, 6);
-        set_smem(reinterpret_cast<const void*>(assemble_kernel<T, 6, 3, 64>), smem);
-        assemble_kernel<T, 6, 3, 64><<<grid, kRowThreads, smem, stream>>>(a);
+        if (ws->U > 0)
+        {
+            assemble_upper6_kernel<T><<<grid_for(2 * ws->U, 128, 1 << 20), 128, 0, stream>>>(
+                ws->U, ws->upper_blocks, ws->pair_offsets, ws->pairs, a.w, a.hinv, a.block_pc, a.pcv, a.S);
+            PM_LAUNCH_CHECK();
+        }
+        assemble_diag6_kernel<T><<<grid, kDiagThreads, 0, stream>>>(a.P, a.prim_offsets, ws->row_entries, a.w, a.hinv,
+                                                                    a.y, a.hpp, a.gp, a.diag_pos, a.lambda,
+                                                                    a.min_diag, a.S, a.rhs, a.minv, a.status);
         PM_LAUNCH_CHECK();
     }
     else

@@ -126,6 +126,81 @@ def test_observation_accumulation_matches_reference(checkers, dtype):
         assert np.abs(got[key] - ref[key]).max() <= tol * scale, key
 
 
+def _join(a, b):
+    """Observations of b appended to those of a, b's eliminated blocks numbered after a's."""
+    out = dict(a)
+    out["L"] = a["L"] + b["L"]
+    out["obs_primary"] = np.concatenate([a["obs_primary"], b["obs_primary"]])
+    out["obs_eliminated"] = np.concatenate([a["obs_eliminated"], b["obs_eliminated"] + a["L"]])
+    for k in ("jp", "jl", "residual"):
+        out[k] = np.ascontiguousarray(np.concatenate([a[k], b[k]]))
+    return out
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_generic_block_sizes_match_reference(checkers, dtype):
+    """Block sizes 4 / 2 with 3-row residuals: the generic accumulation and assembly kernels."""
+    prob = W.bundle_problem(24, 1500, per_eliminated=4, residual_size=3, bp=4, bl=2, seed=41, dtype=dtype)
+    orc = checkers.normal_equations_from_observations(prob, dtype=dtype)
+    ref = canonical(orc.export())
+    ne = _device_from_observations(prob, dtype)
+    got = ne.download()
+    for key in ("eliminated_diagonal", "eliminated_gradient", "adjacency_offsets", "cross_primary", "cross_values"):
+        assert np.array_equal(got[key], ref[key]), key
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    for key in ("primary_diagonal", "primary_gradient"):
+        assert np.abs(got[key] - ref[key]).max() <= tol * np.abs(ref[key]).max(), key
+    rtol = 1e-5 if dtype == np.float32 else 1e-10
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=rtol, max_iterations=500)
+    ws = SC.SchurComplementSolverWorkspace()
+    dp, dl, rep = SC.solve_damped_schur_complement(
+        ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=rtol), ws)
+    assert rep["converged"] and rep_ref["converged"], rep["message"]
+    stol = 1e-4 if dtype == np.float32 else 1e-6
+    assert np.linalg.norm(host(dp) - dp_ref) <= stol * np.linalg.norm(dp_ref)
+    assert np.linalg.norm(host(dl) - dl_ref) <= stol * np.linalg.norm(dl_ref)
+    if dtype == np.float64:
+        ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+        sysd = ws.export()
+        assert np.array_equal(host(sysd["row_offsets"]), ro) and np.array_equal(host(sysd["col_indices"]), ci)
+        assert np.abs(host(sysd["values"]) - vals).max() <= 1e-12 * np.abs(vals).max()
+        assert np.abs(host(sysd["rhs"]) - rhs).max() <= 1e-12 * np.abs(rhs).max()
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_hub_point_and_wide_rows_match_reference(checkers, dtype):
+    """Two points seen by all 320 primaries: cross lists longer than the assembly's shared-memory
+    staging area, block rows with 319 upper neighbours (several owner groups per row), and
+    eliminated buckets longer than the input-order selection window."""
+    base = W.bundle_problem(320, 3000, per_eliminated=3, seed=31, dtype=dtype)
+    hub = W.bundle_problem(320, 2, per_eliminated=320, seed=32, dtype=dtype)
+    prob = _join(base, hub)
+    orc = checkers.normal_equations_from_observations(prob, dtype=dtype)
+    ref = canonical(orc.export())
+    ne = _device_from_observations(prob, dtype)
+    got = ne.download()
+    for key in ("adjacency_offsets", "cross_primary", "cross_values"):
+        assert np.array_equal(got[key], ref[key]), key
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    for key in ("eliminated_diagonal", "eliminated_gradient", "primary_diagonal", "primary_gradient"):
+        assert np.abs(got[key] - ref[key]).max() <= tol * np.abs(ref[key]).max(), key
+    rtol = 1e-5 if dtype == np.float32 else 1e-10
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=rtol, max_iterations=1000)
+    ws = SC.SchurComplementSolverWorkspace()
+    dp, dl, rep = SC.solve_damped_schur_complement(
+        ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=1000, relative_tolerance=rtol), ws)
+    assert rep["converged"] and rep_ref["converged"], rep["message"]
+    stol = 1e-4 if dtype == np.float32 else 1e-6
+    assert np.linalg.norm(host(dp) - dp_ref) <= stol * np.linalg.norm(dp_ref)
+    assert np.linalg.norm(host(dl) - dl_ref) <= stol * np.linalg.norm(dl_ref)
+    ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+    sysd = ws.export(torch.float32 if dtype == np.float32 else torch.float64)
+    assert np.array_equal(host(sysd["row_offsets"]), ro) and np.array_equal(host(sysd["col_indices"]), ci)
+    vtol = 1e-5 if dtype == np.float32 else 1e-12
+    assert np.abs(host(sysd["values"]).astype(np.float64) - vals).max() <= vtol * np.abs(vals).max()
+    assert np.abs(host(sysd["rhs"]).astype(np.float64) - rhs).max() <= vtol * np.abs(rhs).max()
+
+
 def test_observation_topology_is_cached_and_rebuilt(checkers):
     prob = W.small_bundle(seed=3)
     ne = _device_from_observations(prob)
