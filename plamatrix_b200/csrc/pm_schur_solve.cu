@@ -41,7 +41,7 @@ struct SchurStatus
     long long eliminated_bad;
     long long preconditioner_bad;
     long long row_too_wide;
-    int pad[2];
+    int pad[2]; // pad[0]: a staged copy of the batched assembly did not complete in time
 };
 
 struct SolveState // device-side PCG / refinement scalars
@@ -76,19 +76,22 @@ struct pm_schur_workspace
     int* diag_pos = nullptr;
     int* transpose = nullptr;
     int* block_pc = nullptr; // per block: primary-cross index k (forward), -(k+2) transposed, -1 none
-    // 6x3 assembly pair lists (pattern lifetime, own buffer)
-    pm::DeviceBuffer pair_buffer;
-    int64_t U = 0, E = 0;              // upper blocks, cross pairs
-    int2* row_entries = nullptr;       // C: {cross, eliminated} of every primary-list entry
-    int* upper_blocks = nullptr;       // U: block index of every upper block, row-major
-    int* pair_offsets = nullptr;       // B + 1: pairs of block b are [off[b], off[b+1])
-    int4* pairs = nullptr;             // E: {cross of p, cross of q, eliminated, 0}, l ascending per block
+    // 6x3 assembly batches (pattern lifetime, own buffer)
+    pm::DeviceBuffer batch_buffer;
+    bool batched = false;          // the batched 6x3 assembly applies to this pattern
+    bool bulk_rows = false;        // batches built for bulk row copies (double values)
+    int64_t E = 0, NB = 0;         // items, batches
+    int2* row_entries = nullptr;   // C: {cross, eliminated} of every primary-list entry
+    int* batch_offset = nullptr;   // P + 1: batches of row p are [off[p], off[p+1])
+    int4* batches = nullptr;       // NB: {first entry, crosses | split, metadata offset, items | ranges << 16}
+    unsigned* meta = nullptr;      // per batch: item words, self rows, copy ranges
     int* saved_offsets = nullptr;
     int* saved_primary = nullptr;
     int* saved_pc = nullptr;
     // numeric
     double* hinv = nullptr;
     double* y = nullptr;
+    int hstride = 0, ystride = 0; // per eliminated block; 12 / 12 (packed [Hll^-1 | y]) for batched 6x3
     void* S = nullptr;   // B * bp * bp, Scalar
     float* S32 = nullptr; // mixed-precision copy
     double* rhs = nullptr;
@@ -106,7 +109,7 @@ struct pm_schur_workspace
         pattern.release();
         numeric.release();
         scratch.release();
-        pair_buffer.release();
+        batch_buffer.release();
         if (prim_sort)
             pm_sparse_workspace_destroy(prim_sort);
         if (host_status)
@@ -132,6 +135,7 @@ __global__ void status_reset_kernel(SchurStatus* s)
     s->eliminated_bad = kNone;
     s->preconditioner_bad = kNone;
     s->row_too_wide = kNone;
+    s->pad[0] = 0;
 }
 
 __global__ void widen_int_kernel(const int* __restrict__ in, int64_t* __restrict__ out, int64_t n)
@@ -162,8 +166,8 @@ __global__ void int_compare_kernel(const int* __restrict__ a, const int* __restr
 // ===================================================================== 1. eliminated inverses
 template <typename T, int BL>
 __global__ void eliminated_inverse_kernel(int64_t L, int bl_rt, const T* __restrict__ hll, const T* __restrict__ gl,
-                                          double lambda, double min_diag, double* __restrict__ hinv,
-                                          double* __restrict__ y, SchurStatus* status)
+                                          double lambda, double min_diag, double* __restrict__ hinv, int hstride,
+                                          double* __restrict__ y, int ystride, SchurStatus* status)
 {
     constexpr int MB = BL > 0 ? BL : 16;
     const int bl = BL > 0 ? BL : bl_rt;
@@ -184,13 +188,13 @@ __global__ void eliminated_inverse_kernel(int64_t L, int bl_rt, const T* __restr
                 inv[i] = 0.0;
         }
         for (int i = 0; i < bl * bl; ++i)
-            hinv[l * bl * bl + i] = inv[i];
+            hinv[l * hstride + i] = inv[i];
         for (int r = 0; r < bl; ++r)
         {
             double s = 0.0;
             for (int c = 0; c < bl; ++c)
                 s = __dadd_rn(s, __dmul_rn(inv[r * bl + c], static_cast<double>(gl[l * bl + c])));
-            y[l * bl + r] = s;
+            y[l * ystride + r] = s;
         }
     }
 }
@@ -552,23 +556,34 @@ __global__ void __launch_bounds__(kRowThreads) assemble_kernel(AssembleArgs<T> a
     }
 }
 
-// ---------------------------------------------------------------- 6x3 assembly from pair lists
-// The pattern build lists, for every upper block (p, q) of the reduced system, the pairs of
-// crosses (W_lp, W_lq) of the eliminated blocks l that see both p and q, in ascending l.  The
-// numeric assembly is then two flat kernels with no shared-memory staging and no barriers in
-// the main loop: one walks the pair list of each upper block, one the cross list of each row
-// (diagonal block, right-hand side and block-Jacobi inverse).  Every sum runs in a fixed order.
+// ---------------------------------------------------------------- 6x3 assembly, batched rows
+// Row p of the reduced system is
+//   S_pp  = Hpp + damping - sum_l W_lp Hll_l^-1 W_lp^T
+//   S_pq  = H_pq          - sum_l W_lp Hll_l^-1 W_lq^T      (q > p, l seeing both p and q)
+//   rhs_p = -g_p          + sum_l W_lp y_l,   y_l = Hll_l^-1 g_l
+// over the crosses (l, p) of row p in ascending l.  Every cross j of the row contributes one
+// "item" per later primary q of its eliminated block (the pair (W_lp, W_lq)).  The pattern
+// build cuts each row's cross list into batches of at most kAsmCross crosses and kAsmItems
+// items, and stores every batch's items sorted by (upper slot, cross).  The numeric kernel
+// runs one CTA per row: the W_lp rows, packed Hll^-1 | y of the batch's crosses and the W_lq
+// rows of its items are copied into shared memory with cp.async, one row per thread (two
+// buffers: batch b+1 is in flight while batch b is consumed; source indices are loaded one
+// batch ahead).  Every thread forms two rows of T = W_lp Hll^-1 per batch and keeps running
+// sums of their diagonal and RHS terms; then owner threads (two per upper block) walk their
+// slot's items.  Two barriers per batch.  Sums run in ascending l within a thread and are
+// reduced in a fixed order: scheduling never changes a result.
+constexpr int kAsmThreads = 256;
+constexpr int kAsmCross = 48;    // crosses per batch
+constexpr int kAsmItems = 112;   // items (staged W_lq rows) per batch
+constexpr int kAsmStages = 3;    // staged batches: owners of b, T of b + 1, copies of b + 2
+constexpr int kAsmSlots = kAsmThreads / 2;     // upper blocks per pass, wide rows (two threads each)
+constexpr int kAsmMidSlots = kAsmThreads / 3;  // upper blocks of a narrow row (three threads each)
+constexpr int kAsmSlotBits = 18;        // item word: slot << 14 | cross << 8 | staged row
+static_assert(kAsmItems <= 256 && kAsmCross <= 64, "item word layout");
+static_assert(kAsmCross + kAsmItems < kAsmThreads, "one staged row per thread, plus the item words");
+static_assert(kAsmCross * 6 <= 2 * kAsmThreads, "two T rows per thread");
 
-// crosses of row p's list entry j that pair with a later primary: with each eliminated block's
-// crosses sorted by primary these are the entries after the cross itself
-__device__ __forceinline__ void pair_range(int p, int c, int l, const int* __restrict__ cross_offsets, int sorted,
-                                           int& begin, int& end)
-{
-    begin = sorted ? c + 1 : cross_offsets[l];
-    end = cross_offsets[l + 1];
-    (void)p;
-}
-
+// items of row-list entry j: one per later primary of its eliminated block
 __global__ void pair_count_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
                                   const int* __restrict__ cross_eliminated, const int* __restrict__ cross_offsets,
                                   const int* __restrict__ cross_primary, int sorted, int* __restrict__ count)
@@ -580,17 +595,22 @@ __global__ void pair_count_kernel(int64_t P, const int* __restrict__ prim_offset
         {
             const int c = prim_cross[j];
             const int l = cross_eliminated[c];
-            int b, e;
-            pair_range(p, c, l, cross_offsets, sorted, b, e);
+            const int e = cross_offsets[l + 1];
             int n = 0;
             if (sorted)
-                n = e - b;
+                n = e - c - 1; // crosses of l are in ascending primary order
             else
-                for (int k = b; k < e; ++k)
+                for (int k = cross_offsets[l]; k < e; ++k)
                     n += cross_primary[k] > p;
             count[j] = n;
         }
     }
+}
+
+__global__ void narrow_offsets_kernel(int64_t n, const int64_t* __restrict__ in, int* __restrict__ out)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        out[i] = static_cast<int>(in[i]);
 }
 
 __global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross,
@@ -603,12 +623,13 @@ __global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross
     }
 }
 
+// items in row-list order: upper slot (block index - diagonal position - 1) and the cross of q
 __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
                                  const int* __restrict__ cross_eliminated, const int* __restrict__ cross_offsets,
                                  const int* __restrict__ cross_primary, int sorted, const int64_t* __restrict__ offset,
                                  const int* __restrict__ block_row_ptr, const int* __restrict__ block_col,
-                                 const int* __restrict__ diag_pos, int64_t* __restrict__ pair_block,
-                                 int64_t* __restrict__ pair_cross, int* __restrict__ pair_other)
+                                 const int* __restrict__ diag_pos, int* __restrict__ item_slot,
+                                 int* __restrict__ item_cross)
 {
     for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
     {
@@ -618,8 +639,7 @@ __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets
         {
             const int c = prim_cross[j];
             const int l = cross_eliminated[c];
-            int b, e;
-            pair_range(p, c, l, cross_offsets, sorted, b, e);
+            const int b = sorted ? c + 1 : cross_offsets[l], e = cross_offsets[l + 1];
             int64_t at = offset[j];
             for (int k = b; k < e; ++k)
             {
@@ -635,217 +655,732 @@ __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets
                     else
                         hi = mid;
                 }
-                pair_block[at] = lo; // the pattern holds (p, q) by construction
-                pair_cross[at] = c;
-                pair_other[at] = k;
+                item_slot[at] = lo - lo0; // the pattern holds (p, q) by construction
+                item_cross[at] = k;
                 ++at;
             }
         }
     }
 }
 
-// sorted pair keys (cross of p << 32 | emission index) -> {cross of p, cross of q, eliminated, 0}
-__global__ void pair_gather_kernel(int64_t E, const uint64_t* __restrict__ keys, const int* __restrict__ pair_other,
-                                   const int* __restrict__ cross_eliminated, int4* __restrict__ pairs)
+// Greedy batches of one row (thread per row).  A cross whose items do not fit an empty batch
+// is split over several single-cross batches; its diagonal term is counted in the first.
+// Batch word w: item count | (1 << 31) when the first cross was started by an earlier batch.
+template <bool Fill>
+__global__ void batch_plan_kernel(int64_t P, const int* __restrict__ prim_offsets, const int64_t* __restrict__ offset,
+                                  int* __restrict__ batch_count, const int* __restrict__ batch_offset,
+                                  int4* __restrict__ batches)
 {
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < E; i += int64_t(gridDim.x) * blockDim.x)
+    for (int64_t pp = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; pp < P; pp += int64_t(gridDim.x) * blockDim.x)
     {
-        const uint64_t key = keys[i];
-        const int c = static_cast<int>(key >> 32);
-        pairs[i] = make_int4(c, pair_other[static_cast<uint32_t>(key)], cross_eliminated[c], 0);
+        const int J0 = prim_offsets[pp], J1 = prim_offsets[pp + 1];
+        int n = 0;
+        int j = J0;
+        int64_t e = offset[J0];
+        while (j < J1)
+        {
+            const int ja = j;
+            const int64_t eb = e;
+            const bool skip = e != offset[j];
+            int nc = 0, ni = 0;
+            bool split = false;
+            while (j < J1 && nc < kAsmCross)
+            {
+                const int64_t rem = offset[j + 1] - e;
+                if (ni + rem <= kAsmItems)
+                {
+                    ni += static_cast<int>(rem);
+                    e = offset[j + 1];
+                    ++j;
+                    ++nc;
+                }
+                else if (nc == 0)
+                {
+                    e += kAsmItems;
+                    ni = kAsmItems;
+                    nc = 1;
+                    split = true;
+                    break;
+                }
+                else
+                {
+                    break;
+                }
+            }
+            if (Fill)
+                batches[batch_offset[pp] + n] = make_int4(ja, split ? ja + 1 : j, static_cast<int>(eb),
+                                                          ni | (skip ? int(0x80000000u) : 0));
+            ++n;
+        }
+        if (!Fill)
+            batch_count[pp] = n;
     }
 }
 
-__global__ void upper_count_kernel(int64_t P, const int* __restrict__ block_row_ptr, const int* __restrict__ diag_pos,
-                                   int* __restrict__ count)
+// Batch metadata.  A batch stages, for each cross i in order, the cross's W_lp row and then
+// the W_lq rows of its items in the batch (rows [R_i, R_i + 1 + n_i)).  Its metadata block
+// (4-word aligned) holds the item words sorted by (slot, cross), the staged self row R_i of
+// every cross, then the copy ranges {first source cross, count | first staged row << 16}.
+// With each eliminated block's crosses sorted by primary, the items of a cross are the crosses
+// right after it, so one range covers a cross and all its items ("contiguous").
+__device__ __forceinline__ int meta_head_words(int ni, int nc) { return (ni + nc + 3) & ~3; }
+
+// items of plan batch d that belong to row-list entry j: [lo, hi)
+__device__ __forceinline__ void cross_items(const int4 d, int j, const int64_t* __restrict__ offset, int64_t& lo,
+                                            int64_t& hi)
 {
-    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
-        count[p] = block_row_ptr[p + 1] - diag_pos[p] - 1;
+    const int64_t eb = d.z, ee = int64_t(d.z) + (d.w & 0x7fffffff);
+    lo = offset[j] > eb ? offset[j] : eb;
+    hi = offset[j + 1] < ee ? offset[j + 1] : ee;
+    if (hi < lo)
+        hi = lo;
 }
 
-__global__ void upper_fill_kernel(int64_t P, const int* __restrict__ offset, const int* __restrict__ diag_pos,
-                                  int* __restrict__ upper_blocks)
+__global__ void batch_meta_size_kernel(int64_t NB, const int4* __restrict__ plan, const int64_t* __restrict__ offset,
+                                       int contiguous, int* __restrict__ words)
 {
-    for (int64_t p = blockIdx.x; p < P; p += gridDim.x)
-        for (int i = offset[p] + threadIdx.x; i < offset[p + 1]; i += blockDim.x)
-            upper_blocks[i] = diag_pos[p] + 1 + (i - offset[p]);
-}
-
-// Upper block (p, q), two threads per block (rows 0-2 and 3-5):
-//   S_pq = H_pq - sum_l (W_lp Hll_l^-1) W_lq^T, l ascending, accumulated in FP64 registers.
-template <typename T>
-__global__ void __launch_bounds__(128) assemble_upper6_kernel(int64_t U, const int* __restrict__ upper_blocks,
-                                                              const int* __restrict__ pair_offsets,
-                                                              const int4* __restrict__ pairs, const T* __restrict__ w,
-                                                              const double* __restrict__ hinv,
-                                                              const int* __restrict__ block_pc,
-                                                              const T* __restrict__ pcv, T* __restrict__ S)
-{
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < 2 * U; i += int64_t(gridDim.x) * blockDim.x)
+    for (int64_t bi = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; bi < NB; bi += int64_t(gridDim.x) * blockDim.x)
     {
-        const int b = upper_blocks[i >> 1];
-        const int half = static_cast<int>(i & 1);
-        const int lo = pair_offsets[b], hi = pair_offsets[b + 1];
-        double acc[3][6];
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int c = 0; c < 6; ++c)
-                acc[r][c] = 0.0;
-        for (int k = lo; k < hi; ++k)
+        const int4 d = plan[bi];
+        const int nc = d.y - d.x, ni = d.w & 0x7fffffff;
+        int nr = 0;
+        for (int i = 0; i < nc; ++i)
         {
-            const int4 pr = pairs[k];
-            const T* wp = w + int64_t(pr.x) * 18 + half * 9;
-            const T* wq = w + int64_t(pr.y) * 18;
-            const double* h = hinv + int64_t(pr.z) * 9;
-            double wrow[9], H[9], Wq[18];
-#pragma unroll
-            for (int e = 0; e < 9; ++e)
+            int64_t lo, hi;
+            cross_items(d, d.x + i, offset, lo, hi);
+            const int n = static_cast<int>(hi - lo);
+            nr += contiguous ? ((n == 0 || lo == offset[d.x + i]) ? 1 : 2) : 1 + n;
+        }
+        words[bi] = meta_head_words(ni, nc) + ((2 * nr + 3) & ~3); // blocks start 16-byte aligned
+    }
+}
+
+// CTA per batch: staged rows, item words (rank sort by (slot, cross)), ranges, descriptor
+// {first entry, cross count | split << 31, metadata offset, item count | range count << 16}.
+__global__ void __launch_bounds__(256) batch_meta_fill_kernel(
+    int64_t NB, const int4* __restrict__ plan, const int64_t* __restrict__ offset, const int* __restrict__ meta_offset,
+    const int* __restrict__ item_slot, const int* __restrict__ item_cross, const int2* __restrict__ row_entries,
+    int contiguous, unsigned* __restrict__ meta, int4* __restrict__ batches)
+{
+    __shared__ unsigned long long key[kAsmItems];
+    __shared__ long long off[kAsmCross + 1];
+    __shared__ int row_start[kAsmCross + 1];
+    __shared__ int range_start[kAsmCross + 1];
+    for (int64_t bi = blockIdx.x; bi < NB; bi += gridDim.x)
+    {
+        const int4 d = plan[bi];
+        const int nc = d.y - d.x, ni = d.w & 0x7fffffff;
+        const int mo = meta_offset[bi];
+        const int head = meta_head_words(ni, nc);
+        for (int i = threadIdx.x; i <= nc; i += blockDim.x)
+            off[i] = offset[d.x + i];
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+            int rows = 0, ranges = 0;
+            for (int i = 0; i < nc; ++i)
             {
-                wrow[e] = static_cast<double>(wp[e]);
-                H[e] = h[e];
+                int64_t lo, hi;
+                cross_items(d, d.x + i, offset, lo, hi);
+                const int n = static_cast<int>(hi - lo);
+                row_start[i] = rows;
+                range_start[i] = ranges;
+                rows += 1 + n;
+                ranges += contiguous ? ((n == 0 || lo == off[i]) ? 1 : 2) : 1 + n;
             }
-#pragma unroll
-            for (int e = 0; e < 18; ++e)
-                Wq[e] = static_cast<double>(wq[e]);
-#pragma unroll
-            for (int rr = 0; rr < 3; ++rr)
+            row_start[nc] = rows;
+            range_start[nc] = ranges;
+            batches[bi] = make_int4(d.x, nc | (d.w & int(0x80000000u)), mo, ni | (ranges << 16));
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < ni; i += blockDim.x)
+        {
+            const int64_t e = int64_t(d.z) + i;
+            int lo = 0, hi = nc; // cross of item e: off[x] <= e < off[x + 1]
+            while (hi - lo > 1)
             {
-                double t[3];
-#pragma unroll
-                for (int j = 0; j < 3; ++j)
-                    t[j] = H[j * 3 + 0] * wrow[rr * 3 + 0] + H[j * 3 + 1] * wrow[rr * 3 + 1] +
-                           H[j * 3 + 2] * wrow[rr * 3 + 2];
-#pragma unroll
-                for (int c = 0; c < 6; ++c)
-                    acc[rr][c] += t[0] * Wq[c * 3] + t[1] * Wq[c * 3 + 1] + t[2] * Wq[c * 3 + 2];
+                const int mid = (lo + hi) >> 1;
+                if (off[mid] <= e)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const int64_t first = off[lo] > int64_t(d.z) ? off[lo] : int64_t(d.z);
+            const unsigned row = static_cast<unsigned>(row_start[lo] + 1 + (e - first));
+            key[i] = (static_cast<unsigned long long>(item_slot[e]) << 32) | (static_cast<unsigned>(lo) << 8) | row;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < ni; i += blockDim.x)
+        {
+            const unsigned long long k = key[i];
+            int rank = 0;
+            for (int x = 0; x < ni; ++x)
+                rank += key[x] < k;
+            const unsigned slot = static_cast<unsigned>(k >> 32);
+            meta[int64_t(mo) + rank] = (slot << 14) | static_cast<unsigned>(k & 0x3fffu);
+        }
+        for (int i = threadIdx.x; i < nc; i += blockDim.x)
+        {
+            meta[int64_t(mo) + ni + i] = static_cast<unsigned>(row_start[i]);
+            int64_t lo, hi;
+            cross_items(d, d.x + i, offset, lo, hi);
+            const int n = static_cast<int>(hi - lo);
+            const int c = row_entries[d.x + i].x;
+            unsigned* r = meta + int64_t(mo) + head + 2 * range_start[i];
+            const unsigned row = static_cast<unsigned>(row_start[i]);
+            if (contiguous && (n == 0 || lo == off[i]))
+            {
+                r[0] = static_cast<unsigned>(c);
+                r[1] = static_cast<unsigned>(1 + n) | (row << 16);
+            }
+            else if (contiguous)
+            {
+                r[0] = static_cast<unsigned>(c);
+                r[1] = 1u | (row << 16);
+                r[2] = static_cast<unsigned>(item_cross[lo]);
+                r[3] = static_cast<unsigned>(n) | ((row + 1) << 16);
+            }
+            else
+            {
+                r[0] = static_cast<unsigned>(c);
+                r[1] = 1u | (row << 16);
+                for (int k = 0; k < n; ++k)
+                {
+                    r[2 + 2 * k] = static_cast<unsigned>(item_cross[lo + k]);
+                    r[3 + 2 * k] = 1u | ((row + 1 + k) << 16);
+                }
             }
         }
-        const int pc = block_pc[b];
-        T* out = S + int64_t(b) * 36;
+        for (int i = ni + nc + threadIdx.x; i < head; i += blockDim.x)
+            meta[int64_t(mo) + i] = 0u;
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+// a row of 18 scalars: 9 copies of 16 bytes (double) or 8 bytes (float)
+template <typename T>
+__device__ __forceinline__ void cp_row18(T* dst, const T* src)
+{
 #pragma unroll
-        for (int rr = 0; rr < 3; ++rr)
+    for (int piece = 0; piece < 9; ++piece)
+    {
+        if constexpr (sizeof(T) == 8)
+            cp_async16(dst + 2 * piece, src + 2 * piece);
+        else
+            cp_async8(dst + 2 * piece, src + 2 * piece);
+    }
+}
+
+// bulk (TMA) copy global -> shared, completion counted in bytes on an mbarrier
+__device__ __forceinline__ unsigned smem_addr(const void* p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(ok)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// bounded wait (about a second of SM clock); false when the phase did not complete
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+    const long long start = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - start > 2000000000ll)
+            return false;
+    return true;
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+
+template <typename T>
+struct __align__(16) AsmBuffer
+{
+    T rows[kAsmCross + kAsmItems][18]; // per cross: W_lp, then the W_lq of its items
+    double hy[kAsmCross][12];          // Hll^-1 (9) | y (3) of the batch's crosses
+    unsigned meta[kAsmCross + kAsmItems + 4]; // item words, then the self row of every cross
+};
+
+template <typename T>
+struct AsmShared
+{
+    union
+    {
+        AsmBuffer<T> buf[kAsmStages];
+        double dpart[kAsmThreads][14]; // end of row: per-thread diagonal / RHS partial sums
+    };
+    __align__(16) double t[2][kAsmCross][20]; // T = W_lp Hll^-1 of two batches, row r at [3r, 3r + 3)
+    double dseg[27][8];
+    unsigned long long bar[kAsmStages]; // one mbarrier per stage
+};
+
+__device__ __forceinline__ int desc_crosses(const int4 d) { return d.y & 0x7fffffff; }
+__device__ __forceinline__ int desc_items(const int4 d) { return d.w & 0xffff; }
+__device__ __forceinline__ int desc_ranges(const int4 d) { return (d.w >> 16) & 0xffff; }
+
+// bytes that land by bulk copy (metadata head, and the rows when they are doubles)
+template <typename T>
+__device__ __forceinline__ unsigned batch_bytes(const int4 d)
+{
+    const int nc = desc_crosses(d), ni = desc_items(d);
+    unsigned bytes = static_cast<unsigned>(meta_head_words(ni, nc)) * 4u;
+    if constexpr (sizeof(T) == 8)
+        bytes += static_cast<unsigned>(nc + ni) * 144u;
+    return bytes;
+}
+
+__device__ __forceinline__ void cp_async_mbar_arrive(unsigned long long* bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// per-thread source indices of one batch, loaded one batch ahead
+struct StageIndex
+{
+    int2 range; // {first source cross, count | first staged row << 16} (threads < range count)
+    int l0, l1; // eliminated blocks of the Hll^-1 | y pieces t and t + kAsmThreads
+};
+
+__device__ __forceinline__ StageIndex asm_index(const int4 d, const int2* __restrict__ row_entries,
+                                                const unsigned* __restrict__ meta)
+{
+    const int t = threadIdx.x;
+    const int nc = desc_crosses(d), ni = desc_items(d), nr = desc_ranges(d);
+    StageIndex x;
+    x.range = make_int2(0, 0);
+    x.l0 = x.l1 = 0;
+    if (t < nr)
+    {
+        const unsigned* r = meta + int64_t(d.z) + meta_head_words(ni, nc) + 2 * t;
+        x.range = make_int2(static_cast<int>(r[0]), static_cast<int>(r[1]));
+    }
+    if (t < nc * 6)
+        x.l0 = row_entries[d.x + t / 6].y;
+    if (t + kAsmThreads < nc * 6)
+        x.l1 = row_entries[d.x + (t + kAsmThreads) / 6].y;
+    return x;
+}
+
+// Issue one batch into a stage: the metadata head and (double) the row ranges by bulk copy,
+// the packed Hll^-1 | y rows (and float rows) by cp.async; the stage's mbarrier counts the
+// bulk bytes (armed by thread 0) and one cp.async arrival per thread.
+template <typename T>
+__device__ __forceinline__ void asm_issue(AsmBuffer<T>& b, unsigned long long* bar, const int4 d, const StageIndex& x,
+                                          const T* __restrict__ w, const double* __restrict__ hy,
+                                          const unsigned* __restrict__ meta)
+{
+    const int t = threadIdx.x;
+    const int nc = desc_crosses(d), ni = desc_items(d), nr = desc_ranges(d);
+    if (t == kAsmThreads - 1)
+        bulk_copy(&b.meta[0], meta + int64_t(d.z), static_cast<unsigned>(meta_head_words(ni, nc)) * 4u, bar);
+    if (t < nr)
+    {
+        const int src = x.range.x, count = x.range.y & 0xffff, row = (x.range.y >> 16) & 0xffff;
+        if constexpr (sizeof(T) == 8)
         {
-            const int r = 3 * half + rr;
+            bulk_copy(&b.rows[row][0], w + int64_t(src) * 18, static_cast<unsigned>(count) * 144u, bar);
+        }
+        else
+        {
+            for (int k = 0; k < count; ++k)
+                cp_row18(&b.rows[row + k][0], w + int64_t(src + k) * 18);
+        }
+    }
+    if (t < nc * 6)
+    {
+        const int i = t / 6, piece = t - (t / 6) * 6;
+        cp_async16(&b.hy[i][2 * piece], hy + int64_t(x.l0) * 12 + 2 * piece);
+    }
+    if (t + kAsmThreads < nc * 6)
+    {
+        const int k = t + kAsmThreads;
+        const int i = k / 6, piece = k - (k / 6) * 6;
+        cp_async16(&b.hy[i][2 * piece], hy + int64_t(x.l1) * 12 + 2 * piece);
+    }
+    cp_async_mbar_arrive(bar);
+}
+
+// slot's items in a batch: item words sorted by slot (word >> 14)
+__device__ __forceinline__ int item_lower_bound(const unsigned* item, int n, int slot)
+{
+    int lo = 0, hi = n;
+    while (lo < hi)
+    {
+        const int mid = (lo + hi) >> 1;
+        if (static_cast<int>(item[mid] >> 14) < slot)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_row18(const T* src, double* q)
+{
+    if constexpr (sizeof(T) == 8)
+    {
+        const double2* s2 = reinterpret_cast<const double2*>(src);
 #pragma unroll
-            for (int c = 0; c < 6; ++c)
-            {
-                const double base = pc >= 0 ? static_cast<double>(pcv[int64_t(pc) * 36 + r * 6 + c]) : 0.0;
-                out[r * 6 + c] = static_cast<T>(base - acc[rr][c]);
-            }
+        for (int e = 0; e < 9; ++e)
+        {
+            const double2 v = s2[e];
+            q[2 * e] = v.x;
+            q[2 * e + 1] = v.y;
+        }
+    }
+    else
+    {
+        const float2* s2 = reinterpret_cast<const float2*>(src);
+#pragma unroll
+        for (int e = 0; e < 9; ++e)
+        {
+            const float2 v = s2[e];
+            q[2 * e] = v.x;
+            q[2 * e + 1] = v.y;
         }
     }
 }
 
-// Row p (one CTA of kDiagThreads): diagonal block, right-hand side and block-Jacobi inverse.
-//   S_pp = Hpp + damping - sum_l W_lp Hll_l^-1 W_lp^T      (lower triangle summed, mirrored)
-//   rhs_p = -g_p + sum_l W_lp y_l,  y_l = Hll_l^-1 g_l
-// Thread t sums the row's crosses t, t + kDiagThreads, ...; warps reduce by a fixed xor tree and
-// are combined in warp order.
-constexpr int kDiagThreads = 128;
+// T rows of one staged batch (thread items k = t and t + kAsmThreads: cross k / 6, row
+// k % 6), with the diagonal / RHS terms of the crosses whose diagonal belongs to the batch.
+template <typename T>
+__device__ __forceinline__ void asm_t_phase(const AsmBuffer<T>& b, double (*tout)[20], const int4 d, bool diag,
+                                            double* d1, double* d2)
+{
+    const int t = threadIdx.x;
+    const int nc = desc_crosses(d), ni = desc_items(d);
+    const int i0 = d.y < 0 ? 1 : 0; // first cross's diagonal term counted by an earlier batch
+#pragma unroll
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        const int k = t + pass * kAsmThreads;
+        const int i = k / 6, r = k - (k / 6) * 6;
+        if (i >= nc)
+            continue;
+        const T* wr = &b.rows[b.meta[ni + i]][0];
+        const double* h = &b.hy[i][0];
+        const double w0 = static_cast<double>(wr[r * 3]), w1 = static_cast<double>(wr[r * 3 + 1]),
+                     w2 = static_cast<double>(wr[r * 3 + 2]);
+        double tr[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+            tr[j] = h[j * 3 + 0] * w0 + h[j * 3 + 1] * w1 + h[j * 3 + 2] * w2;
+        tout[i][r * 3] = tr[0];
+        tout[i][r * 3 + 1] = tr[1];
+        tout[i][r * 3 + 2] = tr[2];
+        if (diag && i >= i0)
+        {
+            double* dd = pass == 0 ? d1 : d2;
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                if (c <= r)
+                    dd[c] += tr[0] * static_cast<double>(wr[c * 3]) + tr[1] * static_cast<double>(wr[c * 3 + 1]) +
+                             tr[2] * static_cast<double>(wr[c * 3 + 2]);
+            dd[6] += w0 * h[9] + w1 * h[10] + w2 * h[11];
+        }
+    }
+}
+
+// Owner work of one staged batch: the slot's items, ROWS consecutive block rows from rbase.
+template <typename T, int ROWS>
+__device__ __forceinline__ void asm_owner(const AsmBuffer<T>& b, const double (*tin)[20], const unsigned* item, int ni,
+                                          int slot, int rbase, double (*acc)[6])
+{
+    for (int k = item_lower_bound(item, ni, slot); k < ni; ++k)
+    {
+        const unsigned word = item[k];
+        if (static_cast<int>(word >> 14) != slot)
+            break;
+        const double* tr = &tin[(word >> 8) & 63][rbase * 3];
+        double q[18], tv[3 * ROWS];
+        load_row18<T>(b.rows[word & 255], q);
+#pragma unroll
+        for (int e = 0; e < 3 * ROWS; ++e)
+            tv[e] = tr[e];
+#pragma unroll
+        for (int rr = 0; rr < ROWS; ++rr)
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                acc[rr][c] += tv[rr * 3] * q[c * 3] + tv[rr * 3 + 1] * q[c * 3 + 1] + tv[rr * 3 + 2] * q[c * 3 + 2];
+    }
+}
+
+// wait for a stage: thread 0 polls its mbarrier (bounded) and arms the stage about to be
+// issued, the CTA votes in the barrier, then every thread observes the completed phase
+// itself.  Returns false after a timeout.
+__device__ __forceinline__ bool asm_sync(unsigned long long* bar, unsigned& parity, bool wait_stage,
+                                         unsigned long long* arm, unsigned arm_bytes)
+{
+    bool ok = true;
+    if (threadIdx.x == 0)
+    {
+        if (wait_stage)
+            ok = mbar_wait(bar, parity);
+        if (arm)
+            mbar_expect_tx(arm, arm_bytes);
+    }
+    if (__syncthreads_or(!ok))
+        return false;
+    if (wait_stage)
+    {
+        if (threadIdx.x != 0)
+            mbar_wait(bar, parity); // complete: returns at once
+        parity ^= 1u;
+    }
+    return true;
+}
 
 template <typename T>
-__global__ void __launch_bounds__(kDiagThreads) assemble_diag6_kernel(
-    int64_t P, const int* __restrict__ prim_offsets, const int2* __restrict__ row_entries, const T* __restrict__ w,
-    const double* __restrict__ hinv, const double* __restrict__ y, const T* __restrict__ hpp, const T* __restrict__ gp,
-    const int* __restrict__ diag_pos, double lambda, double min_diag, T* __restrict__ S, double* __restrict__ rhs,
-    double* __restrict__ minv, SchurStatus* status)
+__global__ void __launch_bounds__(kAsmThreads, 2) assemble_rows6_kernel(
+    int64_t P, const int* __restrict__ batch_offset, const int4* __restrict__ batches,
+    const int2* __restrict__ row_entries, const unsigned* __restrict__ meta, const T* __restrict__ w,
+    const double* __restrict__ hy, const int* __restrict__ block_row_ptr, const int* __restrict__ diag_pos,
+    const int* __restrict__ block_pc, const T* __restrict__ hpp, const T* __restrict__ gp, const T* __restrict__ pcv,
+    double lambda, double min_diag, T* __restrict__ S, double* __restrict__ rhs, SchurStatus* status)
 {
-    constexpr int kSums = 27; // 21 lower-triangle entries + 6 right-hand-side entries
-    constexpr int kWarps = kDiagThreads / 32;
-    __shared__ double part[kWarps][kSums];
-    __shared__ double diag[36];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    AsmShared<T>& sh = *reinterpret_cast<AsmShared<T>*>(smem_raw);
+    const int t = threadIdx.x;
+    if (t == 0)
+    {
+        for (int st = 0; st < kAsmStages; ++st)
+            mbar_init(&sh.bar[st], 1 + kAsmThreads); // thread 0's arm + one cp.async arrival per thread
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned parity[kAsmStages] = {0u, 0u, 0u};
     for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
     {
         const int p = static_cast<int>(pp);
-        double sum[kSums];
+        const int dpos = diag_pos[p];
+        const int n_up = block_row_ptr[p + 1] - dpos - 1;
+        const int b0 = batch_offset[p], nb = batch_offset[p + 1] - b0;
+        const bool mid = n_up <= kAsmMidSlots;
+        const int groups = mid ? 1 : (n_up + kAsmSlots - 1) / kAsmSlots;
+        // diagonal partial sums of this thread's two T rows: entries (r, c <= r), then the RHS
+        double d1[7], d2[7];
 #pragma unroll
-        for (int k = 0; k < kSums; ++k)
-            sum[k] = 0.0;
-        for (int j = prim_offsets[p] + t; j < prim_offsets[p + 1]; j += kDiagThreads)
+        for (int k = 0; k < 7; ++k)
+            d1[k] = d2[k] = 0.0;
+        for (int g = 0; g < groups; ++g)
         {
-            const int2 e = row_entries[j];
-            const T* wc = w + int64_t(e.x) * 18;
-            const double* h = hinv + int64_t(e.y) * 9;
-            double W[18], H[9];
+            const bool first = g == 0;
+            const int slot = mid ? t / 3 : g * kAsmSlots + (t >> 1);
+            const int rbase = mid ? 2 * (t % 3) : 3 * (t & 1);
+            const bool owner = mid ? (t < 3 * kAsmMidSlots && slot < n_up) : slot < n_up;
+            double acc[3][6];
 #pragma unroll
-            for (int k = 0; k < 18; ++k)
-                W[k] = static_cast<double>(wc[k]);
+            for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int k = 0; k < 9; ++k)
-                H[k] = h[k];
-            const double y0 = y[int64_t(e.y) * 3], y1 = y[int64_t(e.y) * 3 + 1], y2 = y[int64_t(e.y) * 3 + 2];
-            int k = 0;
-#pragma unroll
-            for (int r = 0; r < 6; ++r)
+                for (int c = 0; c < 6; ++c)
+                    acc[r][c] = 0.0;
+            // descriptors: owners of batch k, T of k + 1, copies of k + 2 (indices prefetched)
+            int4 dk = make_int4(0, 0, 0, 0), dk1 = dk, dk2 = dk;
+            StageIndex xk2{};
+            if (nb > 0)
             {
-                double tr[3];
+                dk = batches[b0];
+                const StageIndex x0 = asm_index(dk, row_entries, meta);
+                StageIndex x1{};
+                if (nb > 1)
+                {
+                    dk1 = batches[b0 + 1];
+                    x1 = asm_index(dk1, row_entries, meta);
+                }
+                if (t == 0)
+                {
+                    mbar_expect_tx(&sh.bar[0], batch_bytes<T>(dk));
+                    if (nb > 1)
+                        mbar_expect_tx(&sh.bar[1], batch_bytes<T>(dk1));
+                }
+                fence_proxy_async(); // earlier generic use of the buffers precedes the copies
+                __syncthreads();
+                asm_issue(sh.buf[0], &sh.bar[0], dk, x0, w, hy, meta);
+                if (nb > 1)
+                    asm_issue(sh.buf[1], &sh.bar[1], dk1, x1, w, hy, meta);
+                if (nb > 2)
+                {
+                    dk2 = batches[b0 + 2];
+                    xk2 = asm_index(dk2, row_entries, meta);
+                }
+                if (!asm_sync(&sh.bar[0], parity[0], true, nullptr, 0))
+                {
+                    if (t == 0)
+                        atomicExch(&status->pad[0], 1);
+                    return;
+                }
+                asm_t_phase<T>(sh.buf[0], sh.t[0], dk, first, d1, d2);
+            }
+            for (int k = 0; k < nb; ++k)
+            {
+                const int s0 = k % kAsmStages, s1 = (k + 1) % kAsmStages, s2 = (k + 2) % kAsmStages;
+                // stage s1 (batch k + 1) must be complete; arm stage s2 for batch k + 2
+                const bool has1 = k + 1 < nb, has2 = k + 2 < nb;
+                if (!asm_sync(&sh.bar[s1], parity[s1], has1, has2 ? &sh.bar[s2] : nullptr,
+                              has2 ? batch_bytes<T>(dk2) : 0u))
+                {
+                    if (t == 0)
+                        atomicExch(&status->pad[0], 1);
+                    return;
+                }
+                if (has2)
+                    asm_issue(sh.buf[s2], &sh.bar[s2], dk2, xk2, w, hy, meta);
+                int4 dk3 = make_int4(0, 0, 0, 0);
+                StageIndex xk3{};
+                if (k + 3 < nb)
+                {
+                    dk3 = batches[b0 + k + 3];
+                    xk3 = asm_index(dk3, row_entries, meta);
+                }
+                if (has1)
+                    asm_t_phase<T>(sh.buf[s1], sh.t[(k + 1) & 1], dk1, first, d1, d2);
+                if (owner)
+                {
+                    const unsigned* item = sh.buf[s0].meta;
+                    const int ni = desc_items(dk);
+                    if (mid)
+                        asm_owner<T, 2>(sh.buf[s0], sh.t[k & 1], item, ni, slot, rbase, acc);
+                    else
+                        asm_owner<T, 3>(sh.buf[s0], sh.t[k & 1], item, ni, slot, rbase, acc);
+                }
+                dk = dk1;
+                dk1 = dk2;
+                dk2 = dk3;
+                xk2 = xk3;
+            }
+            __syncthreads(); // buffers free before the next group or the partial sums reuse them
+            if (owner)
+            {
+                const int blk = dpos + 1 + slot;
+                const int pc = block_pc[blk];
+                T* out = S + int64_t(blk) * 36;
+                const int rows = mid ? 2 : 3;
+                for (int rr = 0; rr < rows; ++rr)
+                {
+                    const int r = rbase + rr;
 #pragma unroll
-                for (int j2 = 0; j2 < 3; ++j2)
-                    tr[j2] = H[j2 * 3 + 0] * W[r * 3 + 0] + H[j2 * 3 + 1] * W[r * 3 + 1] + H[j2 * 3 + 2] * W[r * 3 + 2];
-#pragma unroll
-                for (int c = 0; c <= r; ++c)
-                    sum[k++] += tr[0] * W[c * 3] + tr[1] * W[c * 3 + 1] + tr[2] * W[c * 3 + 2];
-                sum[21 + r] += W[r * 3 + 0] * y0 + W[r * 3 + 1] * y1 + W[r * 3 + 2] * y2;
+                    for (int c = 0; c < 6; ++c)
+                    {
+                        const double base = pc >= 0 ? static_cast<double>(pcv[int64_t(pc) * 36 + r * 6 + c]) : 0.0;
+                        out[r * 6 + c] = static_cast<T>(base - acc[rr][c]);
+                    }
+                }
             }
         }
+        // ---- diagonal block and RHS: fixed-order reduction of the per-thread partial sums.
+        // Entry e < 21 is lower-triangle (r, c); e in [21, 27) is RHS row e - 21.
 #pragma unroll
-        for (int k = 0; k < kSums; ++k)
+        for (int k = 0; k < 7; ++k)
         {
-            double x = sum[k];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                x = __dadd_rn(x, __shfl_xor_sync(0xffffffffu, x, o));
-            sum[k] = x;
-        }
-        if (lane == 0)
-        {
-#pragma unroll
-            for (int k = 0; k < kSums; ++k)
-                part[warp][k] = sum[k];
+            sh.dpart[t][k] = d1[k];
+            sh.dpart[t][7 + k] = d2[k];
         }
         __syncthreads();
-        const int dpos = diag_pos[p];
+        if (t < 27 * 8)
+        {
+            const int e = t >> 3, seg = t & 7;
+            int r, c;
+            if (e < 21)
+            {
+                r = 0;
+                while (r * (r + 1) / 2 + r < e)
+                    ++r;
+                c = e - r * (r + 1) / 2;
+            }
+            else
+            {
+                r = e - 21;
+                c = 6;
+            }
+            double v = 0.0;
+            for (int u = seg * 32; u < seg * 32 + 32; ++u)
+            {
+                if (u % 6 == r)
+                    v = __dadd_rn(v, sh.dpart[u][c]);
+                if ((u + kAsmThreads) % 6 == r && (u + kAsmThreads) / 6 < kAsmCross)
+                    v = __dadd_rn(v, sh.dpart[u][7 + c]);
+            }
+            sh.dseg[e][seg] = v;
+        }
+        __syncthreads();
         if (t < 36)
         {
             const int r = t / 6, c = t % 6;
             const int lr = r >= c ? r : c, lc = r >= c ? c : r;
-            const int k = lr * (lr + 1) / 2 + lc;
+            const int e = lr * (lr + 1) / 2 + lc;
             double dacc = 0.0;
-            for (int wi = 0; wi < kWarps; ++wi)
-                dacc = __dadd_rn(dacc, part[wi][k]);
+            for (int seg = 0; seg < 8; ++seg)
+                dacc = __dadd_rn(dacc, sh.dseg[e][seg]);
             double base = static_cast<double>(hpp[int64_t(p) * 36 + t]);
             if (r == c)
                 base = __dadd_rn(base, __dmul_rn(lambda, fmax(fabs(base), min_diag)));
-            const double value = base - dacc;
-            S[int64_t(dpos) * 36 + t] = static_cast<T>(value);
-            diag[t] = static_cast<double>(static_cast<T>(value));
+            S[int64_t(dpos) * 36 + t] = static_cast<T>(base - dacc);
         }
         else if (t < 42)
         {
+            const int r = t - 36;
             double racc = 0.0;
-            for (int wi = 0; wi < kWarps; ++wi)
-                racc = __dadd_rn(racc, part[wi][21 + t - 36]);
-            rhs[int64_t(p) * 6 + (t - 36)] = -static_cast<double>(gp[int64_t(p) * 6 + (t - 36)]) + racc;
+            for (int seg = 0; seg < 8; ++seg)
+                racc = __dadd_rn(racc, sh.dseg[21 + r][seg]);
+            rhs[int64_t(p) * 6 + r] = -static_cast<double>(gp[int64_t(p) * 6 + r]) + racc;
         }
-        __syncthreads();
-        if (t == 0)
+        __syncthreads(); // partial sums (aliasing the buffers) consumed before the next row stages
+    }
+}
+
+// Block-Jacobi preconditioner of the assembled system: FP64 inverse of every diagonal block
+// (symmetrised from its lower triangle), thread per block row.
+template <typename T, int BP>
+__global__ void diag_inverse_kernel(int64_t P, const int* __restrict__ diag_pos, const T* __restrict__ S,
+                                    double* __restrict__ minv, SchurStatus* status)
+{
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+    {
+        const T* d = S + int64_t(diag_pos[p]) * BP * BP;
+        double m[BP * BP], inv[BP * BP], lower[BP * BP], work[BP];
+        for (int r = 0; r < BP; ++r)
+            for (int c = 0; c < BP; ++c)
+                m[r * BP + c] = static_cast<double>(r >= c ? d[r * BP + c] : d[c * BP + r]);
+        if (!spd_inverse<BP>(m, BP, inv, lower, work))
         {
-            double m[36], inv[36], lower[36], work[6];
-            for (int r = 0; r < 6; ++r)
-                for (int c = 0; c < 6; ++c)
-                    m[r * 6 + c] = r >= c ? diag[r * 6 + c] : diag[c * 6 + r];
-            if (!spd_inverse<6>(m, 6, inv, lower, work))
-            {
-                atomicMin(&status->preconditioner_bad, static_cast<long long>(p));
-                for (int k = 0; k < 36; ++k)
-                    inv[k] = 0.0;
-            }
-            for (int k = 0; k < 36; ++k)
-                minv[int64_t(p) * 36 + k] = inv[k];
+            atomicMin(&status->preconditioner_bad, static_cast<long long>(p));
+            for (int k = 0; k < BP * BP; ++k)
+                inv[k] = 0.0;
         }
-        __syncthreads();
+        for (int k = 0; k < BP * BP; ++k)
+            minv[p * BP * BP + k] = inv[k];
     }
 }
 
@@ -1242,8 +1777,8 @@ __global__ void axpy_to_double_kernel(int64_t n, const V* __restrict__ d, double
 template <typename T, int BP, int BL>
 __global__ void backsub_kernel(int64_t L, int bp_rt, int bl_rt, const int* __restrict__ cross_offsets,
                                const int* __restrict__ cross_primary, const T* __restrict__ w,
-                               const T* __restrict__ gl, const double* __restrict__ hinv, const T* __restrict__ dp,
-                               T* __restrict__ dl)
+                               const T* __restrict__ gl, const double* __restrict__ hinv, int hstride,
+                               const T* __restrict__ dp, T* __restrict__ dl)
 {
     constexpr int ML = BL > 0 ? BL : 16;
     const int bp = BP > 0 ? BP : bp_rt;
@@ -1265,7 +1800,7 @@ __global__ void backsub_kernel(int64_t L, int bp_rt, int bl_rt, const int* __res
                 point[col] = add_rn(point[col], -v);
             }
         }
-        const double* H = hinv + l * bl * bl;
+        const double* H = hinv + l * hstride;
         for (int r = 0; r < bl; ++r)
         {
             double s = 0.0;
@@ -1319,9 +1854,12 @@ void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
 {
     const int64_t n = ws->P * ws->bp;
     const int64_t bpp = ws->bp * ws->bp;
+    // batched 6x3 assembly: Hll^-1 and y packed per eliminated block in 96 bytes (16-byte copies)
+    ws->hstride = ws->batched ? 12 : static_cast<int>(ws->bl * ws->bl);
+    ws->ystride = ws->batched ? 12 : static_cast<int>(ws->bl);
     Carver plan;
-    plan.take<double>(ws->L * ws->bl * ws->bl + 1);
-    plan.take<double>(ws->L * ws->bl + 1);
+    plan.take<double>(ws->L * ws->hstride + 1);
+    plan.take<double>(ws->batched ? 1 : ws->L * ws->bl + 1);
     plan.take<T>(ws->B * bpp + 1);
     plan.take<float>(mixed ? ws->B * bpp + 1 : 1);
     plan.take<double>(n + 1);
@@ -1334,8 +1872,10 @@ void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
     ws->numeric.ensure(plan.offset + 256, stream, "SchurComplementSolverWorkspace");
     Carver c;
     c.base = static_cast<char*>(ws->numeric.ptr);
-    ws->hinv = c.take<double>(ws->L * ws->bl * ws->bl + 1);
-    ws->y = c.take<double>(ws->L * ws->bl + 1);
+    ws->hinv = c.take<double>(ws->L * ws->hstride + 1);
+    ws->y = c.take<double>(ws->batched ? 1 : ws->L * ws->bl + 1);
+    if (ws->batched)
+        ws->y = ws->hinv + 9;
     ws->S = c.take<T>(ws->B * bpp + 1);
     ws->S32 = c.take<float>(mixed ? ws->B * bpp + 1 : 1);
     ws->rhs = c.take<double>(n + 1);
@@ -1386,15 +1926,16 @@ bool topology_matches(pm_schur_workspace* ws, const pm_normal_equations* ne, cud
     return differs == 0;
 }
 
-// Pair lists of the 6x3 assembly: for every upper block (p, q), the crosses (W_lp, W_lq) of the
-// eliminated blocks l seen by both, in ascending l (bucketed and sorted by the COO machinery).
-void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
+// Batches of the 6x3 assembly (see assemble_rows6_kernel).
+void build_batches(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream, bool bulk_rows)
 {
-    const int64_t P = ne->P, C = ne->cross_count, B = ws->B;
+    const int64_t P = ne->P, C = ne->cross_count;
+    ws->batched = false;
+    if (P > (int64_t(1) << kAsmSlotBits))
+        return; // slot numbers would not fit the item word: the generic assembly runs instead
     const int sorted = ne->crosses_sorted ? 1 : 0;
+    const int contiguous = sorted && bulk_rows ? 1 : 0;
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(P, 8 * sm_count())));
-    // scratch: pass 1 (pairs per primary-list entry and upper blocks per row, with their scans),
-    // then pass 2 (the emitted pairs); pass 1 is re-run if the scratch has to grow for pass 2
     Carver s1;
     s1.take<int>(C + 1);
     s1.take<int64_t>(C + 2);
@@ -1403,19 +1944,18 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     s1.take<char>(scan_scratch_bytes(C + 1, sizeof(int64_t)));
     s1.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
     const size_t pass1 = ((s1.offset + 255) / 256) * 256;
-    int* count = nullptr;
     int64_t* offset = nullptr;
-    int* upper_count = nullptr;
-    int* upper_offset = nullptr;
+    int* bofs = nullptr;
     int64_t E = 0;
-    int U = 0;
+    int NB = 0;
+    // pass 1: items per row-list entry, batches per row (re-run when the scratch moves)
     auto run_pass1 = [&]() {
         Carver c1;
         c1.base = static_cast<char*>(ws->scratch.ptr);
-        count = c1.take<int>(C + 1);
+        int* count = c1.take<int>(C + 1);
         offset = c1.take<int64_t>(C + 2);
-        upper_count = c1.take<int>(P + 1);
-        upper_offset = c1.take<int>(P + 2);
+        int* bcount = c1.take<int>(P + 1);
+        bofs = c1.take<int>(P + 2);
         void* scan1 = c1.take<char>(scan_scratch_bytes(C + 1, sizeof(int64_t)));
         void* scan2 = c1.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
         if (P > 0 && C > 0)
@@ -1427,80 +1967,109 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
         exclusive_scan<int, int64_t>(count, offset, C, scan1, stream);
         if (P > 0)
         {
-            upper_count_kernel<<<grid_for(P, 256, 4096), 256, 0, stream>>>(P, ws->block_row_ptr, ws->diag_pos,
-                                                                           upper_count);
+            batch_plan_kernel<false><<<grid_for(P, 128, 4096), 128, 0, stream>>>(P, ws->prim_offsets, offset, bcount,
+                                                                                nullptr, nullptr);
             PM_LAUNCH_CHECK();
         }
-        exclusive_scan<int, int>(upper_count, upper_offset, P, scan2, stream);
+        exclusive_scan<int, int>(bcount, bofs, P, scan2, stream);
         PM_CUDA(cudaMemcpyAsync(&E, offset + C, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
-        PM_CUDA(cudaMemcpyAsync(&U, upper_offset + P, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaMemcpyAsync(&NB, bofs + P, sizeof(int), cudaMemcpyDeviceToHost, stream));
         PM_CUDA(cudaStreamSynchronize(stream));
     };
     ws->scratch.ensure(pass1 + 512, stream, "SchurComplementSolverWorkspace");
     run_pass1();
     if (E > INT32_MAX - 1)
         fail(PM_OVERFLOW_ERROR, "Schur assembly supports up to 2^31 - 2 cross pairs");
+    // pass 2 scratch: items (slot, cross of q), plan descriptors, metadata sizes and offsets
     Carver s2;
-    s2.take<int64_t>(E + 1);
-    s2.take<int64_t>(E + 1);
     s2.take<int>(E + 1);
+    s2.take<int>(E + 1);
+    s2.take<int4>(NB + 1);
+    s2.take<int>(NB + 1);
+    s2.take<int64_t>(NB + 2);
+    s2.take<int>(NB + 1);
+    s2.take<char>(scan_scratch_bytes(NB + 1, sizeof(int64_t)));
     void* before = ws->scratch.ptr;
     ws->scratch.ensure(pass1 + s2.offset + 512, stream, "SchurComplementSolverWorkspace");
     if (ws->scratch.ptr != before)
         run_pass1();
-    // pair buffer: row entries (C) | pair offsets (B + 1) | upper blocks (U) | pairs (E)
-    Carver plan;
-    plan.take<int2>(C + 1);
-    plan.take<int>(B + 2);
-    plan.take<int>(U + 1);
-    plan.take<int4>(E + 1);
-    ws->pair_buffer.ensure(plan.offset + 512, stream, "SchurComplementSolverWorkspace");
-    Carver pc;
-    pc.base = static_cast<char*>(ws->pair_buffer.ptr);
-    ws->row_entries = pc.take<int2>(C + 1);
-    ws->pair_offsets = pc.take<int>(B + 2);
-    ws->upper_blocks = pc.take<int>(U + 1);
-    ws->pairs = pc.take<int4>(E + 1);
-    ws->U = U;
+    Carver c2;
+    c2.base = static_cast<char*>(ws->scratch.ptr) + pass1;
+    int* item_slot = c2.take<int>(E + 1);
+    int* item_cross = c2.take<int>(E + 1);
+    int4* plan = c2.take<int4>(NB + 1);
+    int* words = c2.take<int>(NB + 1);
+    int64_t* meta_offset64 = c2.take<int64_t>(NB + 2);
+    int* meta_offset = c2.take<int>(NB + 1);
+    void* scan3 = c2.take<char>(scan_scratch_bytes(NB + 1, sizeof(int64_t)));
+    // row entries first: the metadata refers to them
+    Carver fixed;
+    fixed.take<int2>(C + 1);
+    fixed.take<int>(P + 2);
+    fixed.take<int4>(NB + 1);
+    if (P > 0)
+    {
+        batch_plan_kernel<true><<<grid_for(P, 128, 4096), 128, 0, stream>>>(P, ws->prim_offsets, offset, nullptr,
+                                                                           bofs, plan);
+        PM_LAUNCH_CHECK();
+    }
+    if (P > 0 && E > 0)
+    {
+        pair_emit_kernel<<<grid, 128, 0, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
+                                                   ne->cross_offsets, ne->cross_primary, sorted, offset,
+                                                   ws->block_row_ptr, ws->block_col, ws->diag_pos, item_slot,
+                                                   item_cross);
+        PM_LAUNCH_CHECK();
+    }
+    if (NB > 0)
+    {
+        batch_meta_size_kernel<<<grid_for(NB, 128, 1 << 16), 128, 0, stream>>>(NB, plan, offset, contiguous, words);
+        PM_LAUNCH_CHECK();
+    }
+    exclusive_scan<int, int64_t>(words, meta_offset64, NB, scan3, stream);
+    int64_t W = 0;
+    PM_CUDA(cudaMemcpyAsync(&W, meta_offset64 + NB, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaStreamSynchronize(stream));
+    if (W > INT32_MAX - 16)
+        fail(PM_OVERFLOW_ERROR, "Schur assembly metadata exceeds 2^31 words");
+    if (NB > 0)
+    {
+        narrow_offsets_kernel<<<grid_for(NB, 256, 1 << 16), 256, 0, stream>>>(NB, meta_offset64, meta_offset);
+        PM_LAUNCH_CHECK();
+    }
+    // persistent: row entries (C) | batch offsets (P + 1) | batches (NB) | metadata (W)
+    Carver plan_b;
+    plan_b.take<int2>(C + 1);
+    plan_b.take<int>(P + 2);
+    plan_b.take<int4>(NB + 1);
+    plan_b.take<unsigned>(W + 16);
+    ws->batch_buffer.ensure(plan_b.offset + 512, stream, "SchurComplementSolverWorkspace");
+    Carver bc;
+    bc.base = static_cast<char*>(ws->batch_buffer.ptr);
+    ws->row_entries = bc.take<int2>(C + 1);
+    ws->batch_offset = bc.take<int>(P + 2);
+    ws->batches = bc.take<int4>(NB + 1);
+    ws->meta = bc.take<unsigned>(W + 16);
     ws->E = E;
+    ws->NB = NB;
+    PM_CUDA(cudaMemcpyAsync(ws->batch_offset, bofs, (P + 1) * sizeof(int), cudaMemcpyDeviceToDevice, stream));
     if (C > 0)
     {
         row_entries_kernel<<<grid_for(C, 256, 1 << 16), 256, 0, stream>>>(C, ws->prim_cross, ne->cross_eliminated,
                                                                          ws->row_entries);
         PM_LAUNCH_CHECK();
     }
-    if (P > 0)
+    if (NB > 0)
     {
-        upper_fill_kernel<<<grid, 128, 0, stream>>>(P, upper_offset, ws->diag_pos, ws->upper_blocks);
+        batch_meta_fill_kernel<<<grid_for(NB, 1, 1 << 16), 256, 0, stream>>>(
+            NB, plan, offset, meta_offset, item_slot, item_cross, ws->row_entries, contiguous, ws->meta, ws->batches);
         PM_LAUNCH_CHECK();
     }
-    // pass 2: emit (block, cross of p, cross of q), bucket by block, sort by cross of p
-    Carver c2;
-    c2.base = static_cast<char*>(ws->scratch.ptr) + pass1;
-    int64_t* pair_block = c2.take<int64_t>(E + 1);
-    int64_t* pair_cross = c2.take<int64_t>(E + 1);
-    int* pair_other = c2.take<int>(E + 1);
-    if (P > 0 && E > 0)
-    {
-        pair_emit_kernel<<<grid, 128, 0, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
-                                                   ne->cross_offsets, ne->cross_primary, sorted, offset,
-                                                   ws->block_row_ptr, ws->block_col, ws->diag_pos, pair_block,
-                                                   pair_cross, pair_other);
-        PM_LAUNCH_CHECK();
-    }
-    coo_prepare<float>(ws->prim_sort, stream, B, C + 1, E, pair_block, pair_cross, nullptr);
-    coo_internal_status(ws->prim_sort, stream, "Schur pair lists");
-    const CooView v = coo_view(ws->prim_sort);
-    PM_CUDA(cudaMemcpyAsync(ws->pair_offsets, v.bucket_start, (B + 1) * sizeof(int), cudaMemcpyDeviceToDevice, stream));
-    if (E > 0)
-    {
-        pair_gather_kernel<<<grid_for(E, 256, 1 << 16), 256, 0, stream>>>(E, v.keys, pair_other, ne->cross_eliminated,
-                                                                         ws->pairs);
-        PM_LAUNCH_CHECK();
-    }
+    ws->batched = true;
+    ws->bulk_rows = bulk_rows;
 }
 
-void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
+void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream, bool bulk_rows)
 {
     const int64_t P = ne->P, L = ne->L, C = ne->cross_count, PC = ne->primary_cross_count;
     const size_t bitmap = size_t((P + 31) / 32) * sizeof(unsigned);
@@ -1579,7 +2148,7 @@ void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
     {
         // the pattern buffer moved: re-carve the fixed part (contents are rebuilt below anyway,
         // except prim lists / row pointers, which are recomputed by re-running this function)
-        return build_pattern(ws, ne, stream);
+        return build_pattern(ws, ne, stream, bulk_rows);
     }
     Carver bc;
     bc.base = static_cast<char*>(ws->pattern.ptr) + ((fixed + 255) / 256) * 256;
@@ -1599,8 +2168,9 @@ void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
         PM_LAUNCH_CHECK();
     }
     PM_CUDA(cudaMemsetAsync(ws->block_pc, 0xff, size_t(B + 1) * sizeof(int), stream));
+    ws->batched = false;
     if (ne->bp == 6 && ne->bl == 3)
-        build_pairs(ws, ne, stream);
+        build_batches(ws, ne, stream, bulk_rows);
     if (PC > 0)
     {
         block_pc_kernel<<<grid_for(PC, 256, 4096), 256, 0, stream>>>(PC, ne->primary_cross_row, ne->primary_cross_col,
@@ -1660,17 +2230,17 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
         return size_t(ch) * (bpl + bpp + a.bp) * sizeof(T) + size_t(mp * mp) * sizeof(double) + 64 +
                kRowThreads * sizeof(unsigned long long) + 2 * ch * sizeof(int) + 64;
     };
-    if (ne->bp == 6 && ne->bl == 3)
+    if (ws->batched)
     {
-        if (ws->U > 0)
-        {
-            assemble_upper6_kernel<T><<<grid_for(2 * ws->U, 128, 1 << 20), 128, 0, stream>>>(
-                ws->U, ws->upper_blocks, ws->pair_offsets, ws->pairs, a.w, a.hinv, a.block_pc, a.pcv, a.S);
-            PM_LAUNCH_CHECK();
-        }
-        assemble_diag6_kernel<T><<<grid, kDiagThreads, 0, stream>>>(a.P, a.prim_offsets, ws->row_entries, a.w, a.hinv,
-                                                                    a.y, a.hpp, a.gp, a.diag_pos, a.lambda,
-                                                                    a.min_diag, a.S, a.rhs, a.minv, a.status);
+        const size_t smem = sizeof(AsmShared<T>);
+        set_smem(reinterpret_cast<const void*>(assemble_rows6_kernel<T>), smem);
+        assemble_rows6_kernel<T><<<grid, kAsmThreads, smem, stream>>>(
+            a.P, ws->batch_offset, ws->batches, ws->row_entries, ws->meta, a.w, ws->hinv,
+            a.block_row_ptr, a.diag_pos, a.block_pc, a.hpp, a.gp, a.pcv, a.lambda, a.min_diag, a.S, a.rhs,
+            a.status);
+        PM_LAUNCH_CHECK();
+        diag_inverse_kernel<T, 6><<<grid_for(a.P, 64, 1 << 16), 64, 0, stream>>>(a.P, a.diag_pos, a.S, a.minv,
+                                                                                 a.status);
         PM_LAUNCH_CHECK();
     }
     else
@@ -1832,8 +2402,11 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         numeric_layout<T>(ws, stream, mixed);
     }
     const bool reused = ws->pattern_builds > 0 && topology_matches(ws, ne, stream);
+    constexpr bool kBulkRows = sizeof(T) == 8; // float rows (72 bytes) cannot go by bulk copy
     if (!reused)
-        build_pattern(ws, ne, stream);
+        build_pattern(ws, ne, stream, kBulkRows);
+    else if (ws->batched && ws->bulk_rows != kBulkRows)
+        build_batches(ws, ne, stream, kBulkRows);
     ws->last_ne = ne;
     ws->last_version = ne->topology_version;
     ws->value_size = sizeof(T);
@@ -1850,14 +2423,14 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         if (bl == 3)
             eliminated_inverse_kernel<T, 3><<<grid, 128, 0, stream>>>(L, 3, static_cast<const T*>(ne->eliminated_diagonal),
                                                                       static_cast<const T*>(ne->eliminated_gradient),
-                                                                      damping, o->minimum_diagonal, ws->hinv, ws->y,
-                                                                      ws->status);
+                                                                      damping, o->minimum_diagonal, ws->hinv,
+                                                                      ws->hstride, ws->y, ws->ystride, ws->status);
         else
             eliminated_inverse_kernel<T, 0><<<grid, 128, 0, stream>>>(L, static_cast<int>(bl),
                                                                       static_cast<const T*>(ne->eliminated_diagonal),
                                                                       static_cast<const T*>(ne->eliminated_gradient),
-                                                                      damping, o->minimum_diagonal, ws->hinv, ws->y,
-                                                                      ws->status);
+                                                                      damping, o->minimum_diagonal, ws->hinv,
+                                                                      ws->hstride, ws->y, ws->ystride, ws->status);
         PM_LAUNCH_CHECK();
     }
     PM_CUDA(cudaEventRecord(ws->events[2], stream));
@@ -1900,6 +2473,8 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         cudaEventElapsedTime(&t, ws->events[0], ws->events[last]);
         rep->total_ms = t;
     };
+    if (ws->host_status->pad[0] != 0)
+        fail(PM_RUNTIME_ERROR, "Schur assembly: a shared-memory copy did not complete within its time limit");
     if (ws->host_status->eliminated_bad != kNone)
     {
         timings(3);
@@ -2002,13 +2577,13 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             backsub_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(L, 6, 3, ne->cross_offsets, ne->cross_primary,
                                                               static_cast<const T*>(ne->cross_values),
                                                               static_cast<const T*>(ne->eliminated_gradient), ws->hinv,
-                                                              dp, dl);
+                                                              ws->hstride, dp, dl);
         else
             backsub_kernel<T, 0, 0><<<grid, 128, 0, stream>>>(L, static_cast<int>(bp), static_cast<int>(bl),
                                                               ne->cross_offsets, ne->cross_primary,
                                                               static_cast<const T*>(ne->cross_values),
                                                               static_cast<const T*>(ne->eliminated_gradient), ws->hinv,
-                                                              dp, dl);
+                                                              ws->hstride, dp, dl);
         PM_LAUNCH_CHECK();
     }
     PM_CUDA(cudaEventRecord(ws->events[5], stream));
