@@ -27,6 +27,9 @@ pm_normal_equations::~pm_normal_equations()
         pm_sparse_workspace_destroy(by_eliminated);
     if (by_primary)
         pm_sparse_workspace_destroy(by_primary);
+    if (by_eliminated_order)
+        pm_sparse_workspace_destroy(by_eliminated_order);
+    cross_runs.release();
 }
 
 namespace pm
@@ -89,8 +92,9 @@ __global__ void cross_owner_kernel(const int* __restrict__ offsets, int64_t L, i
 
 // crosses of the observation path: one per distinct primary of each eliminated bucket,
 // in ascending primary order
+// in ascending primary order; cross_run[c] is the bucket position of the cross's first observation
 __global__ void observation_crosses_kernel(CooView v, const int* __restrict__ cross_offsets,
-                                           int* __restrict__ cross_primary)
+                                           int* __restrict__ cross_primary, int* __restrict__ cross_run)
 {
     for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < v.rows; l += int64_t(gridDim.x) * blockDim.x)
     {
@@ -100,8 +104,13 @@ __global__ void observation_crosses_kernel(CooView v, const int* __restrict__ cr
         {
             const uint32_t p = static_cast<uint32_t>(v.keys[q] >> 32);
             if (q == b || p != static_cast<uint32_t>(v.keys[q - 1] >> 32))
+            {
+                cross_run[at] = q;
                 cross_primary[at++] = static_cast<int>(p);
+            }
         }
+        if (l == v.rows - 1)
+            cross_run[at] = e;
     }
 }
 
@@ -208,133 +217,99 @@ __global__ void __launch_bounds__(128) eliminated_accumulate_generic_kernel(
     }
 }
 
-// Per eliminated block (fixed block sizes): Hll, g_l and the cross blocks W of its distinct
-// primaries, accumulated in registers and written once.
-template <typename T, int BP, int BL>
-__global__ void __launch_bounds__(128) eliminated_accumulate_kernel(
-    CooView v, int m_rt, const T* __restrict__ jp, const T* __restrict__ jl,
-    const T* __restrict__ res, const T* __restrict__ weights, const int* __restrict__ cross_offsets,
-    T* __restrict__ hll, T* __restrict__ gl, T* __restrict__ w)
+// Eliminated block (3x3), thread per block: Hll and g_l over its observations in input order
+// (addResidualBlocks accumulates per residual in call order, block_normal_equations.cpp:294-311).
+// The bucket of l in `v` lists the observation indices in ascending order.
+template <typename T>
+__global__ void __launch_bounds__(128) eliminated_diagonal3_kernel(CooView v, int m, const T* __restrict__ jl,
+                                                                   const T* __restrict__ res,
+                                                                   const T* __restrict__ weights, T* __restrict__ hll,
+                                                                   T* __restrict__ gl)
 {
-    constexpr int MP = BP, ML = BL, bp = BP, bl = BL;
-    const int m = m_rt;
     for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < v.rows; l += int64_t(gridDim.x) * blockDim.x)
     {
         const int b = v.bucket_start[l], e = v.bucket_start[l + 1];
-        T H[ML * ML], g[ML];
+        T H[9], g[3];
 #pragma unroll
-        for (int i = 0; i < ML * ML; ++i)
-            H[i] = T(0);
+        for (int k = 0; k < 9; ++k)
+            H[k] = T(0);
 #pragma unroll
-        for (int i = 0; i < ML; ++i)
-            g[i] = T(0);
-        // eliminated terms in input order (selection over the bucket, which is sorted by
-        // (primary, input offset)); addResidualBlocks accumulates Hll/g_l per residual in
-        // call order, block_normal_equations.cpp:294-311.  Buckets longer than kSelectMax are
-        // visited in bucket order instead (deterministic; the sum order then differs).
-        constexpr int kSelectMax = 64;
-        const bool select = e - b <= kSelectMax;
-        uint32_t last = 0;
-        for (int visited = 0; visited < e - b; ++visited)
+        for (int k = 0; k < 3; ++k)
+            g[k] = T(0);
+        for (int q = b; q < e; ++q)
         {
-            uint32_t best = 0xffffffffu;
-            if (select)
-            {
-                for (int q = b; q < e; ++q)
-                {
-                    const uint32_t src = static_cast<uint32_t>(v.keys[q]);
-                    if ((visited == 0 || src > last) && src < best)
-                        best = src;
-                }
-            }
-            else
-            {
-                best = static_cast<uint32_t>(v.keys[b + visited]);
-            }
-            last = best;
-            const int64_t i = best;
-            const T* r = res + i * m;
+            const int64_t i = static_cast<uint32_t>(v.keys[q]);
             const T weight = weights[i];
-            const T* J = jl + i * m * bl;
+            const T* J = jl + i * m * 3;
+            const T* r = res + i * m;
             for (int row = 0; row < m; ++row)
             {
                 const T rr = r[row];
-                T jrow[ML];
+                const T j0 = J[row * 3], j1 = J[row * 3 + 1], j2 = J[row * 3 + 2];
+                const T jrow[3] = {j0, j1, j2};
 #pragma unroll
-                for (int col = 0; col < ML; ++col)
-                    if (col < bl)
-                        jrow[col] = J[row * bl + col];
-#pragma unroll
-                for (int col = 0; col < ML; ++col)
+                for (int col = 0; col < 3; ++col)
                 {
-                    if (col >= bl)
-                        break;
                     const T wv = mul_rn(weight, jrow[col]);
                     g[col] = add_rn(g[col], mul_rn(wv, rr));
 #pragma unroll
-                    for (int other = 0; other < ML; ++other)
-                    {
-                        if (other >= bl)
-                            break;
-                        H[col * ML + other] = add_rn(H[col * ML + other], mul_rn(wv, jrow[other]));
-                    }
+                    for (int other = 0; other < 3; ++other)
+                        H[col * 3 + other] = add_rn(H[col * 3 + other], mul_rn(wv, jrow[other]));
                 }
             }
         }
-        T* Hout = hll + l * bl * bl;
-        T* gout = gl + l * bl;
-        for (int col = 0; col < bl; ++col)
-        {
-            gout[col] = g[col];
-            for (int other = 0; other < bl; ++other)
-                Hout[col * bl + other] = H[col * ML + other];
-        }
-        // cross blocks: runs of equal primary, observations in input order inside a run
-        // (block_normal_equations.cpp:268-292)
-        int cross = cross_offsets[l];
-        T W[MP * ML];
-        int q = b;
-        while (q < e)
-        {
-            const uint32_t primary = static_cast<uint32_t>(v.keys[q] >> 32);
 #pragma unroll
-            for (int k = 0; k < MP * ML; ++k)
-                W[k] = T(0);
-            for (; q < e && static_cast<uint32_t>(v.keys[q] >> 32) == primary; ++q)
+        for (int k = 0; k < 9; ++k)
+            hll[l * 9 + k] = H[k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            gl[l * 3 + k] = g[k];
+    }
+}
+
+// Cross block (6x3), thread per cross: W = sum over the cross's observations (a run of equal
+// primary in its eliminated bucket, input order) of w Jp^T Jl (block_normal_equations.cpp:268-292).
+template <typename T>
+__global__ void __launch_bounds__(128) cross_accumulate63_kernel(int64_t C, const uint64_t* __restrict__ keys,
+                                                                 const int* __restrict__ cross_run, int m,
+                                                                 const T* __restrict__ jp, const T* __restrict__ jl,
+                                                                 const T* __restrict__ weights, T* __restrict__ w)
+{
+    for (int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < C; c += int64_t(gridDim.x) * blockDim.x)
+    {
+        T W[18];
+#pragma unroll
+        for (int k = 0; k < 18; ++k)
+            W[k] = T(0);
+        for (int q = cross_run[c]; q < cross_run[c + 1]; ++q)
+        {
+            const int64_t i = static_cast<uint32_t>(keys[q]);
+            const T weight = weights[i];
+            const T* Jp = jp + i * m * 6;
+            const T* Jl = jl + i * m * 3;
+            for (int row = 0; row < m; ++row)
             {
-                const int64_t i = static_cast<uint32_t>(v.keys[q]);
-                const T weight = weights[i];
-                const T* Jp = jp + i * m * bp;
-                const T* Jl = jl + i * m * bl;
-                for (int row = 0; row < m; ++row)
+                T prow[6], lrow[3];
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+                    prow[k] = Jp[row * 6 + k];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    lrow[k] = Jl[row * 3 + k];
+#pragma unroll
+                for (int pc = 0; pc < 6; ++pc)
                 {
-                    T lrow[ML];
+                    const T wv = mul_rn(weight, prow[pc]);
 #pragma unroll
-                    for (int ec = 0; ec < ML; ++ec)
-                        if (ec < bl)
-                            lrow[ec] = Jl[row * bl + ec];
-#pragma unroll
-                    for (int pc = 0; pc < MP; ++pc)
-                    {
-                        if (pc >= bp)
-                            break;
-                        const T wv = mul_rn(weight, Jp[row * bp + pc]);
-#pragma unroll
-                        for (int ec = 0; ec < ML; ++ec)
-                        {
-                            if (ec >= bl)
-                                break;
-                            W[pc * ML + ec] = add_rn(W[pc * ML + ec], mul_rn(wv, lrow[ec]));
-                        }
-                    }
+                    for (int ec = 0; ec < 3; ++ec)
+                        W[pc * 3 + ec] = add_rn(W[pc * 3 + ec], mul_rn(wv, lrow[ec]));
                 }
             }
-            T* Wout = w + int64_t(cross) * bp * bl;
-            for (int pc = 0; pc < bp; ++pc)
-                for (int ec = 0; ec < bl; ++ec)
-                    Wout[pc * bl + ec] = W[pc * ML + ec];
-            ++cross;
         }
+        T* out = w + c * 18;
+#pragma unroll
+        for (int k = 0; k < 18; ++k)
+            out[k] = W[k];
     }
 }
 
@@ -645,17 +620,22 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
         const int64_t crosses = coo_internal_status(ne->by_eliminated, stream, "accumulate observations");
         coo_prepare<float>(ne->by_primary, stream, ne->P, 1, count, obs_primary, zeros, nullptr);
         coo_internal_status(ne->by_primary, stream, "accumulate observations");
+        if (!ne->by_eliminated_order && pm_sparse_workspace_create(&ne->by_eliminated_order) != PM_OK)
+            fail(PM_RUNTIME_ERROR, "could not create the observation sort workspace");
+        coo_prepare<float>(ne->by_eliminated_order, stream, ne->L, 1, count, obs_eliminated, zeros, nullptr);
+        coo_internal_status(ne->by_eliminated_order, stream, "accumulate observations");
         ne->cross_count = crosses;
         ne->primary_cross_count = 0;
         layout_topology(ne, stream);
+        ne->cross_runs.ensure(size_t(crosses + 1) * sizeof(int) + 256, stream, "normal equations");
         const CooView ve = coo_view(ne->by_eliminated);
         if (ne->L > 0)
         {
             narrow_kernel<<<grid_for(ne->L + 1, 256, 4096), 256, 0, stream>>>(ve.row_offsets, ne->cross_offsets,
                                                                               ne->L + 1);
             PM_LAUNCH_CHECK();
-            observation_crosses_kernel<<<grid_for(ne->L, 128, 8192), 128, 0, stream>>>(ve, ne->cross_offsets,
-                                                                                       ne->cross_primary);
+            observation_crosses_kernel<<<grid_for(ne->L, 128, 8192), 128, 0, stream>>>(
+                ve, ne->cross_offsets, ne->cross_primary, static_cast<int*>(ne->cross_runs.ptr));
             PM_LAUNCH_CHECK();
             cross_owner_kernel<<<grid_for(ne->L, 256, 4096), 256, 0, stream>>>(ne->cross_offsets, ne->L,
                                                                                ne->cross_eliminated);
@@ -698,12 +678,23 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
     {
         const unsigned grid = grid_for(ne->L, 128, 1 << 20);
         if (bp == 6 && bl == 3)
-            eliminated_accumulate_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(ve, mm, jp, jl, res, weights,
-                                                                           ne->cross_offsets, hll, gl, w);
+        {
+            const CooView vo = coo_view(ne->by_eliminated_order);
+            eliminated_diagonal3_kernel<T><<<grid, 128, 0, stream>>>(vo, mm, jl, res, weights, hll, gl);
+            PM_LAUNCH_CHECK();
+            if (ne->cross_count > 0)
+            {
+                cross_accumulate63_kernel<T><<<grid_for(ne->cross_count, 128, 1 << 20), 128, 0, stream>>>(
+                    ne->cross_count, ve.keys, static_cast<const int*>(ne->cross_runs.ptr), mm, jp, jl, weights, w);
+                PM_LAUNCH_CHECK();
+            }
+        }
         else
+        {
             eliminated_accumulate_generic_kernel<T><<<grid, 128, 0, stream>>>(ve, mm, bp, bl, jp, jl, res, weights,
                                                                              ne->cross_offsets, hll, gl, w);
-        PM_LAUNCH_CHECK();
+            PM_LAUNCH_CHECK();
+        }
     }
     if (ne->P > 0)
     {

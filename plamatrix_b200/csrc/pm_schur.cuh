@@ -31,6 +31,8 @@ struct pm_normal_equations
     // observation-path topology cache
     pm_sparse_workspace* by_eliminated = nullptr; // observations bucketed by eliminated block
     pm_sparse_workspace* by_primary = nullptr;    // observations bucketed by primary block
+    pm_sparse_workspace* by_eliminated_order = nullptr; // observations bucketed by eliminated block, input order
+    pm::DeviceBuffer cross_runs;                  // C + 1: first by_eliminated position of every cross
     pm::DeviceBuffer observation_copy;            // saved index arrays + zero column
     pm::DeviceBuffer weights;                     // Huber weight of every observation
     int64_t observation_count = -1;
