@@ -857,17 +857,6 @@ __global__ void __launch_bounds__(256) batch_meta_fill_kernel(
     }
 }
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src)
-{
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src)
-{
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
-}
-
 // a row of 18 scalars: 9 copies of 16 bytes (double) or 8 bytes (float)
 template <typename T>
 __device__ __forceinline__ void cp_row18(T* dst, const T* src)
@@ -882,47 +871,7 @@ __device__ __forceinline__ void cp_row18(T* dst, const T* src)
     }
 }
 
-// bulk (TMA) copy global -> shared, completion counted in bytes on an mbarrier
-__device__ __forceinline__ unsigned smem_addr(const void* p)
-{
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                 : "=r"(ok)
-                 : "r"(smem_addr(bar)), "r"(parity)
-                 : "memory");
-    return ok != 0;
-}
-// bounded wait (about a second of SM clock); false when the phase did not complete
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
-{
-    const long long start = clock64();
-    while (!mbar_try_wait(bar, parity))
-        if (clock64() - start > 2000000000ll)
-            return false;
-    return true;
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+
 
 template <typename T>
 struct __align__(16) AsmBuffer
@@ -960,10 +909,7 @@ __device__ __forceinline__ unsigned batch_bytes(const int4 d)
     return bytes;
 }
 
-__device__ __forceinline__ void cp_async_mbar_arrive(unsigned long long* bar)
-{
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
-}
+
 
 // per-thread source indices of one batch, loaded one batch ahead
 struct StageIndex

@@ -107,6 +107,75 @@ __device__ __forceinline__ T csr_row_dot(const int* __restrict__ rp, const int* 
     return sum;
 }
 
+// Short rows (mean <= 8 nonzeros): a warp owns 32 consecutive rows.  Their nonzeros form one
+// contiguous range, loaded coalesced in pieces of kStreamCap (values, columns, then the x
+// gathers, all in flight together); products are staged in shared memory and lane i sums
+// row i's products in column order.  The sum order is the row's storage order.
+constexpr int kStreamCap = 256; // staged products per warp
+constexpr int kStreamUnroll = kStreamCap / 32;
+
+template <typename T>
+__device__ __forceinline__ T csr_stream_rows(int64_t r0, int64_t rows, const int* __restrict__ rp,
+                                             const int* __restrict__ ci, const T* __restrict__ v,
+                                             const T* __restrict__ x, T* __restrict__ stage)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t row = r0 + lane;
+    const bool valid = row < rows;
+    const int my_begin = valid ? rp[row] : 0;
+    const int my_end = valid ? rp[row + 1] : 0;
+    const int last = static_cast<int>(rows - 1 - r0 < 31 ? rows - 1 - r0 : 31);
+    const int cb = __shfl_sync(0xffffffffu, my_begin, 0);
+    const int ce = __shfl_sync(0xffffffffu, my_end, last);
+    T sum = T(0);
+    for (int base = cb; base < ce; base += kStreamCap)
+    {
+        const int n = ce - base < kStreamCap ? ce - base : kStreamCap;
+        int col[kStreamUnroll];
+        T val[kStreamUnroll];
+#pragma unroll
+        for (int u = 0; u < kStreamUnroll; ++u)
+        {
+            const int k = u * 32 + lane;
+            if (k < n)
+            {
+                col[u] = __ldcs(ci + base + k);
+                val[u] = __ldcs(v + base + k);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kStreamUnroll; ++u)
+        {
+            const int k = u * 32 + lane;
+            if (k < n)
+                stage[k] = val[u] * __ldg(x + col[u]);
+        }
+        __syncwarp();
+        const int lo = my_begin > base ? my_begin : base;
+        const int hi = my_end < base + n ? my_end : base + n;
+        for (int k = lo; k < hi; ++k)
+            sum += stage[k - base];
+        __syncwarp();
+    }
+    return sum;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) csr_stream_kernel(int64_t rows, const int* __restrict__ rp,
+                                                         const int* __restrict__ ci, const T* __restrict__ v,
+                                                         const T* __restrict__ x, T* __restrict__ y)
+{
+    __shared__ T stage[8][kStreamCap];
+    const int warp = threadIdx.x >> 5;
+    const int64_t warps = int64_t(gridDim.x) * 8;
+    for (int64_t wrow = (int64_t(blockIdx.x) * 8 + warp) * 32; wrow < rows; wrow += warps * 32)
+    {
+        const T sum = csr_stream_rows<T>(wrow, rows, rp, ci, v, x, stage[warp]);
+        if (wrow + (threadIdx.x & 31) < rows)
+            y[wrow + (threadIdx.x & 31)] = sum;
+    }
+}
+
 template <typename T, int TPR>
 __global__ void __launch_bounds__(256) csr_spmv_kernel(int64_t rows, const int* __restrict__ rp,
                                                        const int* __restrict__ ci, const T* __restrict__ v,
@@ -143,6 +212,13 @@ void launch_spmv(const pm_csr* A, const T* x, T* y, cudaStream_t stream)
         return;
     const T* v = static_cast<const T*>(A->values);
     const int block = 256;
+    if (A->threads_per_row <= 8)
+    {
+        csr_stream_kernel<T><<<grid_for(A->rows, 256, 1 << 20), 256, 0, stream>>>(A->rows, A->row_ptr, A->col_idx,
+                                                                                    v, x, y);
+        PM_LAUNCH_CHECK();
+        return;
+    }
     const unsigned grid = grid_for(A->rows * A->threads_per_row, block, 65535);
     switch (A->threads_per_row)
     {
@@ -310,6 +386,34 @@ __global__ void __launch_bounds__(kReduceBlock) pcg_init_kernel(int64_t n, const
     });
 }
 
+// alpha = rho / p.q on the last block (alphaKernel semantics, iterative_solver_kernels.cuh:169-202)
+template <typename T>
+__device__ __forceinline__ void pcg_alpha(PcgState* st, double den, T)
+{
+    const double rho = st->rho;
+    double alpha = 0.0;
+    if (rho == 0.0 && den == 0.0)
+        alpha = 0.0;
+    else if (isfinite(rho) && isfinite(den) && rho > 0.0 && den > 0.0)
+    {
+        alpha = rho / den;
+        // the step must also be representable in the vector type (the reference forms
+        // alpha in Scalar precision and treats its overflow as breakdown)
+        if (!isfinite(alpha) || !isfinite(static_cast<double>(static_cast<T>(alpha))))
+        {
+            st->breakdown = 1;
+            alpha = 0.0;
+        }
+    }
+    else
+    {
+        st->breakdown = 1;
+    }
+    st->alpha = alpha;
+    if (st->breakdown)
+        st->done = 1;
+}
+
 // q = A p, alpha = rho / p.q  (alphaKernel semantics, iterative_solver_kernels.cuh:169-202)
 template <typename T, int TPR>
 __global__ void __launch_bounds__(kReduceBlock) pcg_spmv_kernel(int64_t rows, const int* __restrict__ rp,
@@ -335,30 +439,34 @@ __global__ void __launch_bounds__(kReduceBlock) pcg_spmv_kernel(int64_t rows, co
             mine[0] += static_cast<double>(p[row]) * static_cast<double>(sum);
         }
     }
-    reduce_partials<1>(mine, partials, &st->ticket[1], [&](double (&tot)[1]) {
-        const double rho = st->rho, den = tot[0];
-        double alpha = 0.0;
-        if (rho == 0.0 && den == 0.0)
-            alpha = 0.0;
-        else if (isfinite(rho) && isfinite(den) && rho > 0.0 && den > 0.0)
+    reduce_partials<1>(mine, partials, &st->ticket[1], [&](double (&tot)[1]) { pcg_alpha(st, tot[0], T(0)); });
+}
+
+// q = A p with the short-row stream layout, alpha = rho / p.q
+template <typename T>
+__global__ void __launch_bounds__(kReduceBlock) pcg_stream_spmv_kernel(int64_t rows, const int* __restrict__ rp,
+                                                                       const int* __restrict__ ci,
+                                                                       const T* __restrict__ v,
+                                                                       const T* __restrict__ p, T* __restrict__ q,
+                                                                       double* partials, PcgState* st)
+{
+    if (st->done)
+        return;
+    __shared__ T stage[kReduceBlock / 32][kStreamCap];
+    double mine[1] = {0.0};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * (kReduceBlock / 32);
+    for (int64_t wrow = (int64_t(blockIdx.x) * (kReduceBlock / 32) + warp) * 32; wrow < rows; wrow += warps * 32)
+    {
+        const T sum = csr_stream_rows<T>(wrow, rows, rp, ci, v, p, stage[warp]);
+        const int64_t row = wrow + lane;
+        if (row < rows)
         {
-            alpha = rho / den;
-            // the step must also be representable in the vector type (the reference forms
-            // alpha in Scalar precision and treats its overflow as breakdown)
-            if (!isfinite(alpha) || !isfinite(static_cast<double>(static_cast<T>(alpha))))
-            {
-                st->breakdown = 1;
-                alpha = 0.0;
-            }
+            q[row] = sum;
+            mine[0] += static_cast<double>(p[row]) * static_cast<double>(sum);
         }
-        else
-        {
-            st->breakdown = 1;
-        }
-        st->alpha = alpha;
-        if (st->breakdown)
-            st->done = 1;
-    });
+    }
+    reduce_partials<1>(mine, partials, &st->ticket[1], [&](double (&tot)[1]) { pcg_alpha(st, tot[0], T(0)); });
 }
 
 // x += alpha p, r -= alpha q, z = M^-1 r; convergence on ||r||, beta = r.z / rho.
@@ -560,6 +668,13 @@ void launch_pcg_spmv(const pm_csr* A, const T* p, T* q, double* partials, PcgSta
                      cudaStream_t stream)
 {
     const T* v = static_cast<const T*>(A->values);
+    if (A->threads_per_row <= 8)
+    {
+        pcg_stream_spmv_kernel<T><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q,
+                                                                     partials, st);
+        PM_LAUNCH_CHECK();
+        return;
+    }
     switch (A->threads_per_row)
     {
     case 1: pcg_spmv_kernel<T, 1><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
@@ -627,7 +742,8 @@ void solve(pm_solver_workspace* ws, cudaStream_t stream, const pm_csr* A, const 
     T* inv = c.take<T>(n);
 
     const unsigned vgrid = grid_for(n, kReduceBlock, kMaxReduceBlocks);
-    const unsigned sgrid = grid_for(n * A->threads_per_row, kReduceBlock, kMaxReduceBlocks);
+    const unsigned sgrid = A->threads_per_row <= 8 ? grid_for(n, kReduceBlock, kMaxReduceBlocks)
+                                                   : grid_for(n * A->threads_per_row, kReduceBlock, kMaxReduceBlocks);
     pcg_reset_kernel<<<1, 1, 0, stream>>>(st, o->max_iterations);
     PM_LAUNCH_CHECK();
     if (mode == 1)
