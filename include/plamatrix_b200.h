@@ -271,6 +271,12 @@ typedef struct
     int check_true_residual;     /* compute ||b - S x|| / ||b|| in FP64 after convergence */
     double inner_relative_tolerance; /* mixed: relative tolerance of each inner FP32 solve (1e-4) */
     int max_refinements;         /* mixed: outer FP64 refinement steps (8) */
+    /* No counterpart in the reference: a learned correction of the block-Jacobi blocks
+     * (pm_mlp_*), NULL for plain block Jacobi.  When its PCG has not reduced the residual by
+     * half over `stagnation_window` iterations (or has not converged), the solve falls back to
+     * plain block Jacobi from the iterate it reached. */
+    const struct pm_mlp* learned;
+    int stagnation_window;       /* 25 */
 } pm_schur_options;
 
 typedef struct
@@ -285,6 +291,9 @@ typedef struct
     int refinement_steps;
     double pattern_ms, eliminated_inverse_ms, assembly_ms, solve_ms, back_substitution_ms, total_ms;
     char message[128];             /* "converged" or the reference's failure message */
+    int learned_used;              /* the learned correction preconditioned (part of) the solve */
+    int learned_fallback;          /* it stagnated and plain block Jacobi finished the solve */
+    int learned_iterations;        /* PCG iterations run with the learned correction */
 } pm_schur_report;
 
 typedef struct pm_schur_workspace pm_schur_workspace;
@@ -311,6 +320,32 @@ PM_API int pm_schur_export_f32(pm_schur_workspace* workspace, pm_stream_t stream
                                int64_t* col_indices_d, float* values_d, double* rhs_d, double* preconditioner_d);
 PM_API int pm_schur_export_f64(pm_schur_workspace* workspace, pm_stream_t stream, int64_t* row_offsets_d,
                                int64_t* col_indices_d, double* values_d, double* rhs_d, double* preconditioner_d);
+
+/* =========================================================================== learned block Jacobi
+ * No counterpart in the reference.  A per-block-row network (25 -> 128 -> 128 -> 21, GELU, BF16
+ * operands and FP32 accumulation on the tensor cores) reads each 6x6 diagonal block of the
+ * reduced system and statistics of its row's off-diagonal block norms, and corrects the
+ * Cholesky factor L of the block:  L'_ii = L_ii softplus(o_ii) / ln 2,  L'_ij = L_ij + o_ij L_jj.
+ * The preconditioner block is (L' L'^T)^-1, SPD by construction; a zero network is plain block
+ * Jacobi.  Training minimises sum_p ||L'L'^T x_p - b_p||^2 / ||b||^2 over solved systems (x, b)
+ * with Adam on FP32 master weights.  Parameters are one FP32 vector: W1 (25x128), b1 (128),
+ * W2 (128x128), b2 (128), W3 (128x21), b3 (21), weights input-major. */
+typedef struct pm_mlp pm_mlp;
+PM_API int64_t pm_mlp_param_count(void);
+/* Xavier-uniform hidden layers from `seed`, zero output layer (starts as block Jacobi). */
+PM_API int pm_mlp_create(uint64_t seed, pm_mlp** out);
+PM_API void pm_mlp_destroy(pm_mlp* mlp);
+PM_API int pm_mlp_get_params(const pm_mlp* mlp, float* host_params);
+PM_API int pm_mlp_set_params(pm_mlp* mlp, const float* host_params);
+/* Forward pass on the system last assembled in `workspace` (6x6 blocks); keeps features and
+ * outputs for pm_mlp_inspect.  Synchronous. */
+PM_API int pm_mlp_forward(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stream_t stream);
+/* Loss and parameter gradients for that system with solution x and right-hand side b (device,
+ * FP64, n = 6P); with `learning_rate` > 0 one Adam step follows.  Synchronous. */
+PM_API int pm_mlp_train_step(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stream_t stream, const double* x_d,
+                             const double* b_d, double learning_rate, double* loss);
+/* Host copies of the last features (P x 25), outputs (P x 21) and gradients; any may be NULL. */
+PM_API int pm_mlp_inspect(const pm_mlp* mlp, int64_t* rows, float* features, float* outputs, float* gradients);
 
 #ifdef __cplusplus
 }

@@ -298,3 +298,71 @@ def normal_equations_from_observations(problem: dict, dtype=np.float64, impl: st
     ne.add_observations(problem["obs_primary"], problem["obs_eliminated"], problem["jp"], problem["jl"],
                         problem["residual"], problem["huber_delta"])
     return ne
+
+
+# ---------------------------------------------------------------- learned block-Jacobi correction
+MLP_IN, MLP_HIDDEN, MLP_OUT = 25, 128, 21
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def mlp_param_count() -> int:
+    fn = lib("orc").orc_mlp_param_count
+    fn.restype = C.c_int64
+    return int(fn())
+
+
+def mlp_features(block_row_ptr, block_col, blocks) -> np.ndarray:
+    """25 features per block row of a 6x6 block-CSR matrix (blocks: B x 36, row-major)."""
+    ro = np.ascontiguousarray(block_row_ptr, np.int64)
+    bc = np.ascontiguousarray(block_col, np.int64)
+    bl = _f64(blocks).reshape(-1, 36)
+    P = len(ro) - 1
+    out = np.zeros((max(P, 1), MLP_IN))
+    _check("orc", lib("orc").orc_mlp_features(C.c_int64(P), _ptr(ro), _ptr(bc), _ptr(bl), _ptr(out)))
+    return out[:P]
+
+
+def mlp_forward(features, params, bf16: bool = False) -> dict:
+    f = _f64(features).reshape(-1, MLP_IN)
+    w = _f64(params)
+    P = f.shape[0]
+    cache = {k: np.zeros((max(P, 1), MLP_HIDDEN)) for k in ("z1", "h1", "z2", "h2")}
+    out = np.zeros((max(P, 1), MLP_OUT))
+    _check("orc", lib("orc").orc_mlp_forward(C.c_int64(P), _ptr(f), _ptr(w), C.c_int(int(bf16)), _ptr(cache["z1"]),
+                                             _ptr(cache["h1"]), _ptr(cache["z2"]), _ptr(cache["h2"]), _ptr(out)))
+    cache = {k: v[:P] for k, v in cache.items()}
+    cache["out"] = out[:P]
+    return cache
+
+
+def mlp_loss_grad(diag_blocks, out, x, b):
+    d = _f64(diag_blocks).reshape(-1, 36)
+    o = _f64(out).reshape(-1, MLP_OUT)
+    P = d.shape[0]
+    loss = C.c_double(0.0)
+    dout = np.zeros((max(P, 1), MLP_OUT))
+    _check("orc", lib("orc").orc_mlp_loss_grad(C.c_int64(P), _ptr(d), _ptr(o), _ptr(_f64(x)), _ptr(_f64(b)),
+                                               C.byref(loss), _ptr(dout)))
+    return loss.value, dout[:P]
+
+
+def mlp_backward(features, params, cache: dict, dout, bf16: bool = False) -> np.ndarray:
+    f = _f64(features).reshape(-1, MLP_IN)
+    P = f.shape[0]
+    grads = np.zeros(mlp_param_count())
+    _check("orc", lib("orc").orc_mlp_backward(C.c_int64(P), _ptr(f), _ptr(_f64(params)), C.c_int(int(bf16)),
+                                              _ptr(_f64(cache["z1"])), _ptr(_f64(cache["h1"])),
+                                              _ptr(_f64(cache["z2"])), _ptr(_f64(cache["h2"])),
+                                              _ptr(_f64(dout)), _ptr(grads)))
+    return grads
+
+
+def mlp_preconditioner(diag_blocks, out) -> np.ndarray:
+    d = _f64(diag_blocks).reshape(-1, 36)
+    P = d.shape[0]
+    minv = np.zeros((max(P, 1), 36))
+    _check("orc", lib("orc").orc_mlp_preconditioner(C.c_int64(P), _ptr(d), _ptr(_f64(out)), _ptr(minv)))
+    return minv[:P]

@@ -199,6 +199,24 @@ int orc_schur_system_f64(const orc_ne_f64* ne, double damping, double minimum_di
                          int64_t* row_offsets, int64_t* col_indices, double* values, double* rhs,
                          double* preconditioner_inverse);
 
+/* ---------------------------------------------------------------- learned correction
+ * No counterpart in the reference: the FP64 restatement of the device MLP that corrects the
+ * block-Jacobi preconditioner (definitions in oracle/mlp.c).  Parameters are one flat vector:
+ * W1 (25x128) b1 (128) W2 (128x128) b2 (128) W3 (128x21) b3 (21), weights input-major. */
+#define ORC_MLP_IN 25
+#define ORC_MLP_HIDDEN 128
+#define ORC_MLP_OUT 21
+int64_t orc_mlp_param_count(void);
+int orc_mlp_features(int64_t P, const int64_t* block_row_ptr, const int64_t* block_col, const double* blocks,
+                     double* features);
+int orc_mlp_forward(int64_t P, const double* features, const double* params, int bf16_operands, double* z1,
+                    double* h1, double* z2, double* h2, double* out);
+int orc_mlp_loss_grad(int64_t P, const double* diag_blocks, const double* out, const double* x, const double* b,
+                      double* loss, double* dout);
+int orc_mlp_backward(int64_t P, const double* features, const double* params, int bf16_operands, const double* z1,
+                     const double* h1, const double* z2, const double* h2, const double* dout, double* grads);
+int orc_mlp_preconditioner(int64_t P, const double* diag_blocks, const double* out, double* minv);
+
 #ifdef __cplusplus
 }
 #endif

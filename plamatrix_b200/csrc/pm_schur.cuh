@@ -106,4 +106,21 @@ __device__ __forceinline__ bool spd_inverse(const double* m, int n, double* inv,
     return true;
 }
 
+// What the learned block-Jacobi correction reads from / writes into a Schur workspace.
+struct SchurView
+{
+    int64_t P = 0, B = 0;
+    int value_size = 0;
+    bool mixed = false;             // minv32 must be refreshed too
+    const int* block_row_ptr = nullptr;
+    const int* block_col = nullptr;
+    const int* diag_pos = nullptr;
+    const void* S = nullptr;        // B x 36 values (value_size bytes each)
+    double* minv = nullptr;         // P x 36 preconditioner blocks (FP64)
+    float* minv32 = nullptr;        // P x 36, mixed precision only
+};
+SchurView schur_view(pm_schur_workspace* ws, bool mixed);
+// features -> network -> (L'L'^T)^-1 of every diagonal block into v.minv (and v.minv32)
+void mlp_apply(const pm_mlp* mlp, const SchurView& v, cudaStream_t stream);
+
 } // namespace pm

@@ -50,6 +50,9 @@ struct SolveState // device-side PCG / refinement scalars
     double true_squared;
     int iterations, max_iterations, done, converged, breakdown, pad;
     unsigned int ticket[4];
+    // stagnation watch: every `window` iterations the residual norm must have halved
+    double window_squared;
+    int window, window_start, stagnated, pad2;
 };
 
 } // namespace
@@ -1612,6 +1615,17 @@ __global__ void __launch_bounds__(kVecBlock) pcg_block_update_kernel(int64_t P, 
             st->done = 1;
             return;
         }
+        if (st->window > 0 && st->iterations - st->window_start >= st->window)
+        {
+            if (tot[1] > 0.25 * st->window_squared) // the norm did not halve over the window
+            {
+                st->stagnated = 1;
+                st->done = 1;
+                return;
+            }
+            st->window_start = st->iterations;
+            st->window_squared = tot[1];
+        }
         st->beta = tot[0] / st->rho;
         st->rho = tot[0];
     });
@@ -1634,8 +1648,8 @@ __global__ void __launch_bounds__(kVecBlock) pcg_block_init_kernel(int64_t P, in
                                                                    const V* __restrict__ q, V* __restrict__ r,
                                                                    V* __restrict__ z, V* __restrict__ p_vec,
                                                                    const PM* __restrict__ minv, double rel, double abs_tol,
-                                                                   int rule, int max_iterations, double* partials,
-                                                                   SolveState* st)
+                                                                   int rule, int max_iterations, int window,
+                                                                   double* partials, SolveState* st)
 {
     constexpr int MP = BP > 0 ? BP : 16;
     const int bp = BP > 0 ? BP : bp_rt;
@@ -1677,6 +1691,10 @@ __global__ void __launch_bounds__(kVecBlock) pcg_block_init_kernel(int64_t P, in
         st->done = 0;
         st->converged = 0;
         st->breakdown = 0;
+        st->window = window;
+        st->window_start = 0;
+        st->window_squared = tot[1];
+        st->stagnated = 0;
         const double r0 = sqrt(fmax(0.0, tot[1]));
         st->tolerance = rule == 0 ? abs_tol + rel * r0 : fmax(abs_tol, rel * r0);
         if (!isfinite(tot[1]))
@@ -2203,11 +2221,34 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
     PM_LAUNCH_CHECK();
 }
 
+} // namespace
+
+SchurView schur_view(pm_schur_workspace* ws, bool mixed)
+{
+    SchurView v;
+    if (!ws || !ws->assembled || ws->bp != 6)
+        return v;
+    v.P = ws->P;
+    v.B = ws->B;
+    v.value_size = ws->value_size;
+    v.mixed = mixed;
+    v.block_row_ptr = ws->block_row_ptr;
+    v.block_col = ws->block_col;
+    v.diag_pos = ws->diag_pos;
+    v.S = ws->S;
+    v.minv = ws->minv;
+    v.minv32 = ws->minv32;
+    return v;
+}
+
+namespace
+{
+
 // One preconditioned CG solve on the block-CSR operand (matrix M, vectors V, inverses PM),
 // device-driven; the host polls `done` on a doubling schedule.  Returns the final state.
 template <typename V, typename M, typename PM>
 SolveState block_pcg(pm_schur_workspace* ws, cudaStream_t stream, const M* S, const PM* minv, const double* rhs,
-                     V* x, double rel, double abs_tol, int rule, int max_iterations, V* scratch)
+                     V* x, double rel, double abs_tol, int rule, int max_iterations, V* scratch, int window = 0)
 {
     const int64_t P = ws->P, n = ws->P * ws->bp;
     const int bp = static_cast<int>(ws->bp);
@@ -2227,11 +2268,11 @@ SolveState block_pcg(pm_schur_workspace* ws, cudaStream_t stream, const M* S, co
         PM_LAUNCH_CHECK();
     if (six)
         pcg_block_init_kernel<V, PM, double, 6><<<ugrid, kVecBlock, 0, stream>>>(P, bp, rhs, q, r0, z, p, minv, rel,
-                                                                                abs_tol, rule, max_iterations,
+                                                                                abs_tol, rule, max_iterations, window,
                                                                                 ws->partials, ws->state);
     else
         pcg_block_init_kernel<V, PM, double, 0><<<ugrid, kVecBlock, 0, stream>>>(P, bp, rhs, q, r0, z, p, minv, rel,
-                                                                                abs_tol, rule, max_iterations,
+                                                                                abs_tol, rule, max_iterations, window,
                                                                                 ws->partials, ws->state);
     PM_LAUNCH_CHECK();
     int issued = 0, check_every = 1;
@@ -2433,6 +2474,36 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         std::snprintf(rep->message, sizeof(rep->message), "Schur preconditioner block is not positive definite");
         return;
     }
+    // ---- learned correction of the block-Jacobi blocks (6x6 only), with plain block Jacobi as
+    // its fallback: when the network's blocks are unusable, or its PCG stagnates
+    bool learned = o->learned && bp == 6 && n > 0;
+    const int window = o->stagnation_window > 0 ? o->stagnation_window : 25;
+    auto restore_block_jacobi = [&]() {
+        diag_inverse_kernel<T, 6><<<grid_for(P, 64, 1 << 16), 64, 0, stream>>>(P, ws->diag_pos,
+                                                                                static_cast<const T*>(ws->S),
+                                                                                ws->minv, ws->status);
+        PM_LAUNCH_CHECK();
+        if (mixed)
+        {
+            convert_kernel<double, float><<<grid_for(P * 36, 256, 4096), 256, 0, stream>>>(ws->minv, ws->minv32,
+                                                                                          P * 36);
+            PM_LAUNCH_CHECK();
+        }
+    };
+    if (learned)
+    {
+        try
+        {
+            mlp_apply(o->learned, schur_view(ws, mixed), stream);
+            rep->learned_used = 1;
+        }
+        catch (const Error&)
+        {
+            restore_block_jacobi();
+            learned = false;
+            rep->learned_fallback = 1;
+        }
+    }
     // ---- PCG
     double* area = vector_area(ws);
     SolveState st{};
@@ -2444,10 +2515,28 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     {
         st = block_pcg<T, T, double>(ws, stream, static_cast<const T*>(ws->S), ws->minv, ws->rhs, dp,
                                      o->relative_tolerance, o->absolute_tolerance, o->tolerance_rule, o->max_iterations,
-                                     reinterpret_cast<T*>(area));
+                                     reinterpret_cast<T*>(area), learned ? window : 0);
+        rep->initial_residual_norm = std::sqrt(std::max(0.0, st.initial_squared));
+        if (learned)
+        {
+            rep->learned_iterations = st.iterations;
+            if (!st.converged)
+            {
+                // plain block Jacobi from the iterate reached (from the start after a breakdown),
+                // to the original tolerance
+                restore_block_jacobi();
+                rep->learned_fallback = 1;
+                if (st.breakdown)
+                    PM_CUDA(cudaMemsetAsync(dp, 0, n * sizeof(T), stream));
+                const int used = st.iterations;
+                const double tol = st.tolerance;
+                st = block_pcg<T, T, double>(ws, stream, static_cast<const T*>(ws->S), ws->minv, ws->rhs, dp, 0.0,
+                                             tol, 1, std::max(0, o->max_iterations - used), reinterpret_cast<T*>(area));
+                st.iterations += used;
+            }
+        }
         rep->converged = st.converged;
         rep->iterations = st.iterations;
-        rep->initial_residual_norm = std::sqrt(std::max(0.0, st.initial_squared));
         rep->final_residual_norm = std::sqrt(std::max(0.0, st.residual_squared));
         if (st.breakdown)
             std::snprintf(rep->message, sizeof(rep->message), "reduced Schur complement is not positive definite");
@@ -2481,9 +2570,23 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             // r64 holds b - S x; solve S32 d = r64 to inner_rel (or to the outer target)
             PM_CUDA(cudaMemsetAsync(d32, 0, n * sizeof(float), stream));
             st = block_pcg<float, float, float>(ws, stream, ws->S32, ws->minv32, r64, d32, inner_rel, 0.5 * target, 1,
-                                                o->max_iterations - total, inner);
+                                                o->max_iterations - total, inner, learned ? window : 0);
             total += st.iterations;
             rep->refinement_steps += 1;
+            if (learned)
+            {
+                rep->learned_iterations += st.iterations;
+                if (!st.converged)
+                {
+                    // plain block Jacobi for the rest of the refinement; a step that broke down
+                    // or stagnated is discarded
+                    restore_block_jacobi();
+                    rep->learned_fallback = 1;
+                    learned = false;
+                    if (st.breakdown || st.stagnated)
+                        continue;
+                }
+            }
             if (st.breakdown)
             {
                 std::snprintf(rep->message, sizeof(rep->message), "reduced Schur complement is not positive definite");

@@ -22,7 +22,7 @@ class SchurOptions(C.Structure):
                 ("absolute_tolerance", C.c_double), ("minimum_diagonal", C.c_double),
                 ("use_initial_guess", C.c_int), ("precision", C.c_int), ("tolerance_rule", C.c_int),
                 ("check_true_residual", C.c_int), ("inner_relative_tolerance", C.c_double),
-                ("max_refinements", C.c_int)]
+                ("max_refinements", C.c_int), ("learned", C.c_void_p), ("stagnation_window", C.c_int)]
 
 
 class SchurReport(C.Structure):
@@ -31,7 +31,8 @@ class SchurReport(C.Structure):
                 ("pattern_reused", C.c_int), ("mixed_precision_used", C.c_int), ("refinement_steps", C.c_int),
                 ("pattern_ms", C.c_double), ("eliminated_inverse_ms", C.c_double), ("assembly_ms", C.c_double),
                 ("solve_ms", C.c_double), ("back_substitution_ms", C.c_double), ("total_ms", C.c_double),
-                ("message", C.c_char * 128)]
+                ("message", C.c_char * 128), ("learned_used", C.c_int), ("learned_fallback", C.c_int),
+                ("learned_iterations", C.c_int)]
 
 
 for _sfx, _ct in (("f32", C.c_float), ("f64", C.c_double)):
@@ -66,12 +67,15 @@ class SchurComplementSolverOptions:
     check_true_residual: bool = True
     inner_relative_tolerance: float = 1e-4
     max_refinements: int = 8
+    learned: "LearnedPreconditioner | None" = None  # no counterpart in the reference
+    stagnation_window: int = 25
 
     def c(self) -> SchurOptions:
         return SchurOptions(self.max_iterations, self.relative_tolerance, self.absolute_tolerance,
                             self.minimum_diagonal, int(self.use_initial_guess), PRECISION[self.precision],
                             0 if self.tolerance_rule == "cpu" else 1, int(self.check_true_residual),
-                            self.inner_relative_tolerance, self.max_refinements)
+                            self.inner_relative_tolerance, self.max_refinements,
+                            self.learned.handle if self.learned is not None else None, self.stagnation_window)
 
 
 def _dtype_info(dtype):
@@ -227,4 +231,84 @@ def solve_damped_schur_complement(equations: DeviceNormalEquations, damping: flo
     report["converged"] = bool(rep.converged)
     report["pattern_reused"] = bool(rep.pattern_reused)
     report["mixed_precision_used"] = bool(rep.mixed_precision_used)
+    report["learned_used"] = bool(rep.learned_used)
+    report["learned_fallback"] = bool(rep.learned_fallback)
     return dp[:n], dl[:m], report
+
+
+# ---------------------------------------------------------------- learned block Jacobi
+N.register("pm_mlp_param_count", [], C.c_int64)
+N.register("pm_mlp_create", [C.c_uint64, vp])
+N.register("pm_mlp_destroy", [vp], None)
+N.register("pm_mlp_get_params", [vp, vp])
+N.register("pm_mlp_set_params", [vp, vp])
+N.register("pm_mlp_forward", [vp, vp, vp])
+N.register("pm_mlp_train_step", [vp, vp, vp, vp, vp, C.c_double, vp])
+N.register("pm_mlp_inspect", [vp, vp, vp, vp, vp])
+
+
+class LearnedPreconditioner:
+    """Per-block-row network correcting the block-Jacobi Cholesky factors of the reduced system
+    (no counterpart in the reference; see pm_mlp_* in include/plamatrix_b200.h).  Pass it as
+    SchurComplementSolverOptions(learned=...); train it on solved systems with train_step."""
+
+    IN, HIDDEN, OUT = 25, 128, 21
+
+    def __init__(self, seed: int = 0):
+        h = C.c_void_p()
+        N.call("pm_mlp_create", C.c_uint64(seed), C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    @staticmethod
+    def param_count() -> int:
+        return int(N.load().pm_mlp_param_count())
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.param_count(), np.float32)
+        N.call("pm_mlp_get_params", self._h, C.c_void_p(out.ctypes.data))
+        return out
+
+    def set_params(self, params: np.ndarray) -> None:
+        a = np.ascontiguousarray(params, np.float32)
+        if a.size != self.param_count():
+            raise N.InvalidArgument("parameter vector has the wrong length")
+        N.call("pm_mlp_set_params", self._h, C.c_void_p(a.ctypes.data))
+
+    def forward(self, workspace: "SchurComplementSolverWorkspace", stream=None) -> dict:
+        N.call("pm_mlp_forward", self._h, workspace.handle, _stream_handle(stream))
+        return self.inspect()
+
+    def train_step(self, workspace: "SchurComplementSolverWorkspace", x: torch.Tensor, b: torch.Tensor,
+                   learning_rate: float = 1e-3, stream=None) -> float:
+        """Loss of the last assembled system in `workspace` for its solution x and right-hand side
+        b (device FP64, n = 6P); with learning_rate > 0 one Adam step follows."""
+        if x.dtype != torch.float64 or b.dtype != torch.float64 or not (x.is_cuda and b.is_cuda):
+            raise N.InvalidArgument("x and b must be float64 CUDA tensors")
+        loss = C.c_double(0.0)
+        N.call("pm_mlp_train_step", self._h, workspace.handle, _stream_handle(stream), _ptr(x), _ptr(b),
+               C.c_double(learning_rate), C.byref(loss))
+        return loss.value
+
+    def inspect(self) -> dict:
+        rows = C.c_int64(0)
+        N.call("pm_mlp_inspect", self._h, C.byref(rows), None, None, None)
+        P = rows.value
+        feats = np.zeros((max(P, 1), self.IN), np.float32)
+        outs = np.zeros((max(P, 1), self.OUT), np.float32)
+        grads = np.zeros(self.param_count(), np.float32)
+        N.call("pm_mlp_inspect", self._h, C.byref(rows), C.c_void_p(feats.ctypes.data),
+               C.c_void_p(outs.ctypes.data), C.c_void_p(grads.ctypes.data))
+        return {"features": feats[:P], "outputs": outs[:P], "gradients": grads}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        try:
+            if h is not None and N._lib is not None:
+                N._lib.pm_mlp_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
