@@ -321,6 +321,33 @@ PM_API int pm_schur_export_f32(pm_schur_workspace* workspace, pm_stream_t stream
 PM_API int pm_schur_export_f64(pm_schur_workspace* workspace, pm_stream_t stream, int64_t* row_offsets_d,
                                int64_t* col_indices_d, double* values_d, double* rhs_d, double* preconditioner_d);
 
+/* =========================================================================== batched solves
+ * No counterpart in the reference: many independent LM systems solved together.  The caller
+ * accumulates them into one normal-equation object (system s owns the primary blocks
+ * [offsets[s], offsets[s+1]) and its own eliminated blocks; no observation couples two
+ * systems).  Pattern, assembly, eliminated inverses and back-substitution run once over the
+ * union; the block-Jacobi (or learned, options->learned) PCG keeps per-system dots, alpha,
+ * beta and convergence on the device, with its iteration captured in a CUDA graph that is
+ * replayed until no system is active.  Every system converges to its own tolerance
+ * (options->relative_tolerance of its own initial residual).  A system whose learned PCG
+ * stagnates restarts from its iterate with plain block Jacobi.  FP64 vectors and dots. */
+typedef struct
+{
+    int converged;
+    int iterations;
+    int learned_fallback;
+    int breakdown;
+    double initial_residual_norm;
+    double final_residual_norm;
+    double time_ms; /* device time from the start of the batched PCG to this system's convergence, -1 if not */
+} pm_batched_system_report;
+PM_API int pm_schur_batched_solve_f64(pm_schur_workspace* workspace, pm_stream_t stream,
+                                      const pm_normal_equations* equations, double damping,
+                                      const pm_schur_options* options, int64_t systems,
+                                      const int64_t* system_primary_offsets, double* primary_step_d,
+                                      double* eliminated_step_d, pm_schur_report* report,
+                                      pm_batched_system_report* per_system);
+
 /* =========================================================================== learned block Jacobi
  * No counterpart in the reference.  A per-block-row network (25 -> 128 -> 128 -> 21, GELU, BF16
  * operands and FP32 accumulation on the tensor cores) reads each 6x6 diagonal block of the

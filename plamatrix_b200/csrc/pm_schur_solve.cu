@@ -107,6 +107,8 @@ struct pm_schur_workspace
     pm::SolveState* host_state = nullptr;   // pinned
     cudaEvent_t events[8] = {};
     cudaEvent_t sync_event = nullptr;
+    cudaStream_t graph_stream = nullptr; // batched PCG: graphs are captured and replayed here
+    cudaEvent_t graph_events[2] = {};
     ~pm_schur_workspace()
     {
         pattern.release();
@@ -124,6 +126,11 @@ struct pm_schur_workspace
                 cudaEventDestroy(e);
         if (sync_event)
             cudaEventDestroy(sync_event);
+        for (auto& e : graph_events)
+            if (e)
+                cudaEventDestroy(e);
+        if (graph_stream)
+            cudaStreamDestroy(graph_stream);
     }
 };
 
@@ -2244,6 +2251,297 @@ SchurView schur_view(pm_schur_workspace* ws, bool mixed)
 namespace
 {
 
+// ---------------------------------------------------------------- batched PCG
+// Many independent systems assembled as one block-diagonal union (system s owns the block rows
+// [row0[s], row0[s+1])).  One set of kernels serves every system: per-system dots are summed
+// by one warp per system over its rows in a fixed order, alpha / beta / convergence are
+// per-system device state, converged systems stop updating, and the iteration is captured
+// once in a CUDA graph that the host replays until no system is active.
+struct BatchState
+{
+    double rho, alpha, beta, tol, rr, rr0, window_sq;
+    long long t_start, t_done; // %globaltimer at (re)start and at convergence
+    int active, iterations, converged, breakdown, stagnated, window_start, restart, pad;
+};
+
+__device__ __forceinline__ long long global_ns()
+{
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// q = S v on the rows of systems selected by `want` (active, or restarting); row_dot = v.q
+template <typename M, int Mode> // Mode 0: iteration (active systems), 1: (re)start (restart flag)
+__global__ void __launch_bounds__(kVecBlock) batch_spmv_kernel(int64_t P, const int* __restrict__ row_ptr,
+                                                               const int* __restrict__ block_col, const M* __restrict__ S,
+                                                               const double* __restrict__ v, double* __restrict__ q,
+                                                               double* __restrict__ row_dot,
+                                                               const int* __restrict__ row_sys,
+                                                               const BatchState* __restrict__ bs)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
+    for (int64_t p = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; p < P; p += warps)
+    {
+        const BatchState& st = bs[row_sys[p]];
+        if (!(Mode == 0 ? st.active : st.restart))
+            continue; // warp-uniform
+        double out[16];
+        bsr_row<double, M, 6>(row_ptr, block_col, S, v, 6, p, true, lane, out);
+        double mine = 0.0;
+        if (lane < 6)
+        {
+            double y = 0.0;
+            for (int r = 0; r < 6; ++r)
+                y = lane == r ? out[r] : y;
+            q[p * 6 + lane] = y;
+            mine = v[p * 6 + lane] * y;
+        }
+        for (int o = 4; o > 0; o >>= 1)
+            mine += __shfl_xor_sync(0xffffffffu, mine, o);
+        if (lane == 0)
+            row_dot[p] = mine;
+    }
+}
+
+// sum of a per-row array over a system's rows (warp, fixed order); valid in every lane
+__device__ __forceinline__ double system_sum(const double* __restrict__ row_val, int r0, int r1, int lane)
+{
+    double s = 0.0;
+    for (int p = r0 + lane; p < r1; p += 32)
+        s += row_val[p];
+    for (int o = 16; o > 0; o >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+__global__ void batch_alpha_kernel(int64_t systems, const int* __restrict__ sys_row, const double* __restrict__ row_dot,
+                                   BatchState* __restrict__ bs)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t s = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; s < systems;
+         s += int64_t(gridDim.x) * blockDim.x / 32)
+    {
+        BatchState& st = bs[s];
+        if (!st.active)
+            continue;
+        const double pq = system_sum(row_dot, sys_row[s], sys_row[s + 1], lane);
+        if (lane == 0)
+        {
+            if (!(pq > 0.0) || !isfinite(pq))
+            {
+                st.breakdown = 1;
+                st.active = 0;
+                st.alpha = 0.0;
+            }
+            else
+            {
+                st.alpha = st.rho / pq;
+            }
+        }
+    }
+}
+
+// x += alpha p, r -= alpha q (Mode 0), or r = b - q, x kept (Mode 1, restarting systems);
+// then z = Minv r and the row sums of r.z and r.r (p = z on restart)
+template <int Mode>
+__global__ void batch_update_kernel(int64_t P, const int* __restrict__ row_sys, const BatchState* __restrict__ bs,
+                                    double* __restrict__ x, double* __restrict__ p_vec, const double* __restrict__ q,
+                                    const double* __restrict__ b, double* __restrict__ r, double* __restrict__ z,
+                                    const double* __restrict__ minv, double* __restrict__ row_rz,
+                                    double* __restrict__ row_rr)
+{
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+    {
+        const BatchState& st = bs[row_sys[p]];
+        if (!(Mode == 0 ? st.active : st.restart))
+            continue;
+        double rr[6];
+        if (Mode == 0)
+        {
+            const double a = st.alpha;
+            for (int k = 0; k < 6; ++k)
+            {
+                x[p * 6 + k] += a * p_vec[p * 6 + k];
+                rr[k] = r[p * 6 + k] - a * q[p * 6 + k];
+                r[p * 6 + k] = rr[k];
+            }
+        }
+        else
+        {
+            for (int k = 0; k < 6; ++k)
+            {
+                rr[k] = b[p * 6 + k] - q[p * 6 + k];
+                r[p * 6 + k] = rr[k];
+            }
+        }
+        const double* m = minv + p * 36;
+        double rz = 0.0, r2 = 0.0;
+        for (int k = 0; k < 6; ++k)
+        {
+            double zk = 0.0;
+            for (int c = 0; c < 6; ++c)
+                zk += m[k * 6 + c] * rr[c];
+            z[p * 6 + k] = zk;
+            if (Mode == 1)
+                p_vec[p * 6 + k] = zk;
+            rz += rr[k] * zk;
+            r2 += rr[k] * rr[k];
+        }
+        row_rz[p] = rz;
+        row_rr[p] = r2;
+    }
+}
+
+// Mode 0: one iteration's convergence / stagnation / beta; Mode 1: (re)start of flagged systems
+template <int Mode>
+__global__ void batch_beta_kernel(int64_t systems, const int* __restrict__ sys_row, const double* __restrict__ row_rz,
+                                  const double* __restrict__ row_rr, BatchState* __restrict__ bs, int max_iterations,
+                                  int window, double rel, double abs_tol, int rule, int* __restrict__ active_count)
+{
+    const int lane = threadIdx.x & 31;
+    for (int64_t s = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; s < systems;
+         s += int64_t(gridDim.x) * blockDim.x / 32)
+    {
+        BatchState& st = bs[s];
+        if (!(Mode == 0 ? st.active : st.restart))
+            continue;
+        const double rz = system_sum(row_rz, sys_row[s], sys_row[s + 1], lane);
+        const double r2 = system_sum(row_rr, sys_row[s], sys_row[s + 1], lane);
+        if (lane != 0)
+            continue;
+        const long long now = global_ns();
+        st.rr = r2;
+        if (Mode == 1)
+        {
+            if (st.restart == 1) // first start: tolerance from this residual
+            {
+                st.rr0 = r2;
+                const double r0 = sqrt(fmax(0.0, r2));
+                st.tol = rule == 0 ? abs_tol + rel * r0 : fmax(abs_tol, rel * r0);
+                st.t_start = now;
+                st.iterations = 0;
+            }
+            st.restart = 0;
+            st.rho = rz;
+            st.window_start = st.iterations;
+            st.window_sq = r2;
+            st.stagnated = 0;
+            st.breakdown = 0;
+            const bool done = !(sqrt(fmax(0.0, r2)) > st.tol);
+            st.converged = done && isfinite(r2);
+            st.active = !done && isfinite(r2) && st.iterations < max_iterations;
+            if (done)
+                st.t_done = now;
+            if (!isfinite(r2))
+                st.breakdown = 1;
+        }
+        else
+        {
+            st.iterations += 1;
+            if (!isfinite(r2))
+            {
+                st.breakdown = 1;
+                st.active = 0;
+            }
+            else if (sqrt(r2) <= st.tol)
+            {
+                st.converged = 1;
+                st.active = 0;
+                st.t_done = now;
+            }
+            else if (st.iterations >= max_iterations)
+            {
+                st.active = 0;
+            }
+            else if (window > 0 && st.iterations - st.window_start >= window && r2 > 0.25 * st.window_sq)
+            {
+                st.stagnated = 1;
+                st.active = 0;
+            }
+            else
+            {
+                if (window > 0 && st.iterations - st.window_start >= window)
+                {
+                    st.window_start = st.iterations;
+                    st.window_sq = r2;
+                }
+                st.beta = rz / st.rho;
+                st.rho = rz;
+            }
+        }
+        if (st.active)
+            atomicAdd(active_count, 1);
+    }
+}
+
+__global__ void batch_direction_kernel(int64_t P, const int* __restrict__ row_sys, const BatchState* __restrict__ bs,
+                                       const double* __restrict__ z, double* __restrict__ p_vec)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < P * 6; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        const BatchState& st = bs[row_sys[i / 6]];
+        if (st.active)
+            p_vec[i] = z[i] + st.beta * p_vec[i];
+    }
+}
+
+__global__ void batch_rows_kernel(int64_t systems, const int* __restrict__ sys_row, int* __restrict__ row_sys)
+{
+    for (int64_t s = blockIdx.x; s < systems; s += gridDim.x)
+        for (int p = sys_row[s] + threadIdx.x; p < sys_row[s + 1]; p += blockDim.x)
+            row_sys[p] = static_cast<int>(s);
+}
+
+// every block must couple rows of one system
+__global__ void batch_check_kernel(int64_t P, const int* __restrict__ row_ptr, const int* __restrict__ block_col,
+                                   const int* __restrict__ row_sys, int* __restrict__ bad)
+{
+    for (int64_t p = blockIdx.x; p < P; p += gridDim.x)
+        for (int b = row_ptr[p] + threadIdx.x; b < row_ptr[p + 1]; b += blockDim.x)
+            if (row_sys[block_col[b]] != row_sys[p])
+                atomicExch(bad, 1);
+}
+
+// restore block Jacobi on the rows of stagnated systems and flag them for a restart
+// (a system that broke down restarts from zero)
+template <typename T>
+__global__ void batch_fallback_kernel(int64_t P, const int* __restrict__ row_sys, BatchState* __restrict__ bs,
+                                      const int* __restrict__ diag_pos, const T* __restrict__ S,
+                                      double* __restrict__ minv, double* __restrict__ x)
+{
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+    {
+        const BatchState& st = bs[row_sys[p]];
+        if (!st.stagnated && !st.breakdown)
+            continue;
+        if (st.breakdown)
+            for (int k = 0; k < 6; ++k)
+                x[p * 6 + k] = 0.0;
+        const T* d = S + int64_t(diag_pos[p]) * 36;
+        double m[36], inv[36], lower[36], work[6];
+        for (int r = 0; r < 6; ++r)
+            for (int c = 0; c < 6; ++c)
+                m[r * 6 + c] = static_cast<double>(r >= c ? d[r * 6 + c] : d[c * 6 + r]);
+        if (!spd_inverse<6>(m, 6, inv, lower, work))
+            for (int k = 0; k < 36; ++k)
+                inv[k] = 0.0;
+        for (int k = 0; k < 36; ++k)
+            minv[p * 36 + k] = inv[k];
+    }
+}
+
+__global__ void batch_flag_restart_kernel(int64_t systems, BatchState* __restrict__ bs, int* __restrict__ fallen)
+{
+    for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < systems; s += int64_t(gridDim.x) * blockDim.x)
+        if (bs[s].stagnated || bs[s].breakdown)
+        {
+            bs[s].restart = 2; // keep the tolerance and the iteration count
+            fallen[s] = 1;
+        }
+}
+
 // One preconditioned CG solve on the block-CSR operand (matrix M, vectors V, inverses PM),
 // device-driven; the host polls `done` on a doubling schedule.  Returns the final state.
 template <typename V, typename M, typename PM>
@@ -2341,9 +2639,195 @@ void true_residual(pm_schur_workspace* ws, cudaStream_t stream, const M* S, cons
     rhs_norm = std::sqrt(std::max(0.0, ws->host_state->rhs_squared));
 }
 
+struct BatchSpec
+{
+    int64_t systems = 0;
+    const int64_t* offsets = nullptr;          // host, systems + 1 block-row offsets
+    pm_batched_system_report* out = nullptr;   // host, systems
+};
+
+// Batched block-Jacobi (or learned) PCG of independent systems; x (FP64, device) holds the
+// initial guesses.  Fills the per-system reports and the summary in `rep`.
+template <typename M>
+void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& spec, const pm_schur_options* o,
+                 bool learned, int window, double* x, pm_schur_report* rep)
+{
+    const int64_t P = ws->P, NS = spec.systems;
+    const M* S = static_cast<const M*>(ws->S);
+    Carver plan;
+    plan.take<int>(NS + 1);
+    plan.take<int>(P + 1);
+    plan.take<BatchState>(NS + 1);
+    for (int k = 0; k < 3; ++k)
+        plan.take<double>(P + 1);
+    for (int k = 0; k < 4; ++k)
+        plan.take<double>(6 * P + 1);
+    plan.take<int>(4);
+    plan.take<int>(NS + 1);
+    ws->scratch.ensure(plan.offset + 512, stream, "SchurComplementSolverWorkspace");
+    Carver c;
+    c.base = static_cast<char*>(ws->scratch.ptr);
+    int* sys_row = c.take<int>(NS + 1);
+    int* row_sys = c.take<int>(P + 1);
+    BatchState* bs = c.take<BatchState>(NS + 1);
+    double* row_dot = c.take<double>(P + 1);
+    double* row_rz = c.take<double>(P + 1);
+    double* row_rr = c.take<double>(P + 1);
+    double* r = c.take<double>(6 * P + 1);
+    double* z = c.take<double>(6 * P + 1);
+    double* pv = c.take<double>(6 * P + 1);
+    double* q = c.take<double>(6 * P + 1);
+    int* flags = c.take<int>(4); // [0] active count, [1] coupling check
+    int* fallen = c.take<int>(NS + 1);
+    std::vector<int> rows32(NS + 1);
+    for (int64_t s = 0; s <= NS; ++s)
+        rows32[s] = static_cast<int>(spec.offsets[s]);
+    std::vector<BatchState> init(NS);
+    for (auto& st : init)
+    {
+        std::memset(&st, 0, sizeof(st));
+        st.restart = 1;
+    }
+    PM_CUDA(cudaMemcpyAsync(sys_row, rows32.data(), (NS + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+    PM_CUDA(cudaMemcpyAsync(bs, init.data(), NS * sizeof(BatchState), cudaMemcpyHostToDevice, stream));
+    PM_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(int), stream));
+    PM_CUDA(cudaMemsetAsync(fallen, 0, (NS + 1) * sizeof(int), stream));
+    batch_rows_kernel<<<grid_for(NS, 1, 4096), 128, 0, stream>>>(NS, sys_row, row_sys);
+    PM_LAUNCH_CHECK();
+    batch_check_kernel<<<grid_for(P, 1, 4096), 128, 0, stream>>>(P, ws->block_row_ptr, ws->block_col, row_sys,
+                                                                  flags + 1);
+    PM_LAUNCH_CHECK();
+    int host_flags[4] = {0, 0, 0, 0};
+    PM_CUDA(cudaMemcpyAsync(host_flags, flags, sizeof(host_flags), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaStreamSynchronize(stream));
+    if (host_flags[1])
+        fail(PM_INVALID_ARGUMENT, "batched Schur solve: a Schur block couples two systems");
+    // the iterations run on the workspace's own stream (a caller's legacy default stream
+    // cannot be captured), ordered after and before the caller's stream by events
+    if (!ws->graph_stream)
+    {
+        PM_CUDA(cudaStreamCreateWithFlags(&ws->graph_stream, cudaStreamNonBlocking));
+        for (auto& e : ws->graph_events)
+            PM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const cudaStream_t caller = stream;
+    PM_CUDA(cudaEventRecord(ws->graph_events[0], caller));
+    stream = ws->graph_stream;
+    PM_CUDA(cudaStreamWaitEvent(stream, ws->graph_events[0], 0));
+    const unsigned rgrid = grid_for(P * 32, kVecBlock, 1 << 16);
+    const unsigned pgrid = grid_for(P, 128, 1 << 16);
+    const unsigned sgrid = grid_for(NS * 32, 128, 1 << 16);
+    const double rel = o->relative_tolerance, abs_tol = o->absolute_tolerance;
+    const int rule = o->tolerance_rule, maxit = o->max_iterations;
+    auto start = [&]() {
+        batch_spmv_kernel<M, 1><<<rgrid, kVecBlock, 0, stream>>>(P, ws->block_row_ptr, ws->block_col, S, x, q, row_dot,
+                                                                 row_sys, bs);
+        PM_LAUNCH_CHECK();
+        batch_update_kernel<1><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, x, pv, q, ws->rhs, r, z, ws->minv, row_rz,
+                                                          row_rr);
+        PM_LAUNCH_CHECK();
+        PM_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), stream));
+        batch_beta_kernel<1><<<sgrid, 128, 0, stream>>>(NS, sys_row, row_rz, row_rr, bs, maxit, learned ? window : 0,
+                                                        rel, abs_tol, rule, flags);
+        PM_LAUNCH_CHECK();
+    };
+    // one CUDA graph holds kChunk iterations of every active system
+    constexpr int kChunk = 8;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    PM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kChunk; ++k)
+    {
+        batch_spmv_kernel<M, 0><<<rgrid, kVecBlock, 0, stream>>>(P, ws->block_row_ptr, ws->block_col, S, pv, q, row_dot,
+                                                                 row_sys, bs);
+        batch_alpha_kernel<<<sgrid, 128, 0, stream>>>(NS, sys_row, row_dot, bs);
+        batch_update_kernel<0><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, x, pv, q, ws->rhs, r, z, ws->minv, row_rz,
+                                                          row_rr);
+        cudaMemsetAsync(flags, 0, sizeof(int), stream);
+        batch_beta_kernel<0><<<sgrid, 128, 0, stream>>>(NS, sys_row, row_rz, row_rr, bs, maxit,
+                                                        learned ? window : 0, rel, abs_tol, rule, flags);
+        batch_direction_kernel<<<grid_for(P * 6, 256, 1 << 16), 256, 0, stream>>>(P, row_sys, bs, z, pv);
+        for (int l = 0; l < 5; ++l)
+            count_launch();
+    }
+    const cudaError_t cap = cudaStreamEndCapture(stream, &graph);
+    if (cap != cudaSuccess)
+        fail(PM_CUDA_ERROR, std::string("batched Schur solve: graph capture failed: ") + cudaGetErrorString(cap));
+    PM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    int* host_count = reinterpret_cast<int*>(ws->host_state); // pinned; the state is not used here
+    auto run = [&](int& issued) {
+        while (issued < maxit)
+        {
+            PM_CUDA(cudaGraphLaunch(exec, stream));
+            issued += kChunk;
+            PM_CUDA(cudaMemcpyAsync(host_count, flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            PM_CUDA(cudaEventRecord(ws->sync_event, stream));
+            PM_CUDA(cudaEventSynchronize(ws->sync_event));
+            if (*host_count == 0)
+                break;
+        }
+    };
+    int issued = 0;
+    try
+    {
+        start();
+        run(issued);
+        if (learned)
+        {
+            // systems whose learned PCG stagnated restart from their iterate with block Jacobi
+            batch_fallback_kernel<M><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, ws->diag_pos, S, ws->minv, x);
+            PM_LAUNCH_CHECK();
+            batch_flag_restart_kernel<<<grid_for(NS, 128, 4096), 128, 0, stream>>>(NS, bs, fallen);
+            PM_LAUNCH_CHECK();
+            start();
+            int again = 0;
+            run(again);
+        }
+    }
+    catch (...)
+    {
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        throw;
+    }
+    PM_CUDA(cudaGraphExecDestroy(exec));
+    PM_CUDA(cudaGraphDestroy(graph));
+    std::vector<BatchState> fin(NS);
+    std::vector<int> fell(NS + 1);
+    PM_CUDA(cudaMemcpyAsync(fin.data(), bs, NS * sizeof(BatchState), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaMemcpyAsync(fell.data(), fallen, (NS + 1) * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaStreamSynchronize(stream));
+    PM_CUDA(cudaEventRecord(ws->graph_events[1], stream));
+    PM_CUDA(cudaStreamWaitEvent(caller, ws->graph_events[1], 0));
+    double r0 = 0.0, r1 = 0.0;
+    int all = 1, most = 0;
+    for (int64_t s = 0; s < NS; ++s)
+    {
+        const BatchState& st = fin[s];
+        pm_batched_system_report& out = spec.out[s];
+        out.converged = st.converged;
+        out.iterations = st.iterations;
+        out.learned_fallback = fell[s];
+        out.breakdown = st.breakdown;
+        out.initial_residual_norm = std::sqrt(std::max(0.0, st.rr0));
+        out.final_residual_norm = std::sqrt(std::max(0.0, st.rr));
+        out.time_ms = st.converged ? double(st.t_done - st.t_start) * 1e-6 : -1.0;
+        r0 += st.rr0;
+        r1 += st.rr;
+        all = all && st.converged;
+        most = std::max(most, st.iterations);
+    }
+    rep->converged = all;
+    rep->iterations = most;
+    rep->initial_residual_norm = std::sqrt(std::max(0.0, r0));
+    rep->final_residual_norm = std::sqrt(std::max(0.0, r1));
+    if (!all)
+        std::snprintf(rep->message, sizeof(rep->message), "batched PCG: some systems did not converge");
+}
+
 template <typename T>
 void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_equations* ne, double damping,
-                 const pm_schur_options* o, T* dp, T* dl, pm_schur_report* rep)
+                 const pm_schur_options* o, T* dp, T* dl, pm_schur_report* rep, const BatchSpec* batch = nullptr)
 {
     if (!ws || !ne || !o || !rep)
         fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: arguments must be non-null");
@@ -2361,7 +2845,18 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: scalar type differs from the normal equations");
     if (bp > 16 || bl > 16)
         fail(PM_INVALID_ARGUMENT, "device Schur solver supports block sizes up to 16");
-    const bool mixed = o->precision == PM_PRECISION_MIXED && sizeof(T) == 8;
+    const bool mixed = o->precision == PM_PRECISION_MIXED && sizeof(T) == 8 && !batch;
+    if (batch)
+    {
+        if (sizeof(T) != 8 || bp != 6)
+            fail(PM_INVALID_ARGUMENT, "batched Schur solve: double values and 6x6 primary blocks required");
+        if (batch->systems <= 0 || !batch->offsets || !batch->out || batch->offsets[0] != 0 ||
+            batch->offsets[batch->systems] != P)
+            fail(PM_INVALID_ARGUMENT, "batched Schur solve: system offsets must run from 0 to the block-row count");
+        for (int64_t s = 0; s < batch->systems; ++s)
+            if (batch->offsets[s + 1] < batch->offsets[s])
+                fail(PM_INVALID_ARGUMENT, "batched Schur solve: system offsets must be non-decreasing");
+    }
     if (bp * bp > kRowThreads)
         fail(PM_INVALID_ARGUMENT, "device Schur solver supports primary block sizes up to 11");
     ws->numeric.bind(stream, "SchurComplementSolverWorkspace");
@@ -2510,6 +3005,12 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     if (n == 0)
     {
         rep->converged = 1;
+    }
+    else if (batch)
+    {
+        batched_pcg<T>(ws, stream, *batch, o, learned, window, reinterpret_cast<double*>(dp), rep);
+        for (int64_t s = 0; s < batch->systems; ++s)
+            rep->learned_fallback = rep->learned_fallback || batch->out[s].learned_fallback;
     }
     else if (!mixed)
     {
@@ -2713,6 +3214,19 @@ int pm_schur_solve_f32(pm_schur_workspace* ws, pm_stream_t stream, const pm_norm
                        const pm_schur_options* o, float* dp, float* dl, pm_schur_report* rep)
 {
     return pm::guarded([&] { pm::schur_solve<float>(ws, stream, ne, damping, o, dp, dl, rep); });
+}
+int pm_schur_batched_solve_f64(pm_schur_workspace* ws, pm_stream_t stream, const pm_normal_equations* ne,
+                               double damping, const pm_schur_options* o, int64_t systems,
+                               const int64_t* system_primary_offsets, double* dp, double* dl, pm_schur_report* rep,
+                               pm_batched_system_report* per_system)
+{
+    return pm::guarded([&] {
+        pm::BatchSpec spec;
+        spec.systems = systems;
+        spec.offsets = system_primary_offsets;
+        spec.out = per_system;
+        pm::schur_solve<double>(ws, stream, ne, damping, o, dp, dl, rep, &spec);
+    });
 }
 int pm_schur_solve_f64(pm_schur_workspace* ws, pm_stream_t stream, const pm_normal_equations* ne, double damping,
                        const pm_schur_options* o, double* dp, double* dl, pm_schur_report* rep)

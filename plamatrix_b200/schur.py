@@ -312,3 +312,59 @@ class LearnedPreconditioner:
         except (AttributeError, TypeError):  # interpreter shutdown
             pass
         self._h = None
+
+
+# ---------------------------------------------------------------- batched independent systems
+class BatchedSystemReport(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iterations", C.c_int), ("learned_fallback", C.c_int),
+                ("breakdown", C.c_int), ("initial_residual_norm", C.c_double), ("final_residual_norm", C.c_double),
+                ("time_ms", C.c_double)]
+
+
+N.register("pm_schur_batched_solve_f64", [vp, vp, vp, C.c_double, vp, i64, vp, vp, vp, vp, vp])
+
+
+def pack_observation_systems(problems: list) -> dict:
+    """One union observation problem (block-diagonal) from independent ones: system s gets the
+    primary blocks [primary_offsets[s], primary_offsets[s+1]) and its own eliminated blocks."""
+    P_off = np.cumsum([0] + [p["P"] for p in problems]).astype(np.int64)
+    L_off = np.cumsum([0] + [p["L"] for p in problems]).astype(np.int64)
+    first = problems[0]
+    for p in problems:
+        if (p["bp"], p["bl"], p["m"]) != (first["bp"], first["bl"], first["m"]):
+            raise N.InvalidArgument("batched systems must share block and residual sizes")
+    cat = lambda key: np.ascontiguousarray(np.concatenate([p[key] for p in problems]))  # noqa: E731
+    return {
+        "P": int(P_off[-1]), "L": int(L_off[-1]), "bp": first["bp"], "bl": first["bl"], "m": first["m"],
+        "huber_delta": first["huber_delta"],
+        "obs_primary": np.ascontiguousarray(np.concatenate([p["obs_primary"] + P_off[i] for i, p in enumerate(problems)])),
+        "obs_eliminated": np.ascontiguousarray(
+            np.concatenate([p["obs_eliminated"] + L_off[i] for i, p in enumerate(problems)])),
+        "jp": cat("jp"), "jl": cat("jl"), "residual": cat("residual"),
+        "primary_offsets": P_off, "eliminated_offsets": L_off,
+    }
+
+
+def solve_batched_schur_complement(equations: DeviceNormalEquations, damping: float, primary_offsets,
+                                   options: SchurComplementSolverOptions | None = None,
+                                   workspace: SchurComplementSolverWorkspace | None = None, stream=None):
+    """Independent systems accumulated into one block-diagonal `equations` (double), solved together.
+    Returns (primary_step, eliminated_step, summary report, list of per-system report dicts)."""
+    if equations.dtype != np.float64:
+        raise N.InvalidArgument("batched solves run on double normal equations")
+    opts = options or SchurComplementSolverOptions()
+    ws = workspace or SchurComplementSolverWorkspace()
+    offs = np.ascontiguousarray(primary_offsets, np.int64)
+    systems = len(offs) - 1
+    n, m = equations.P * equations.bp, equations.L * equations.bl
+    dp = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda")
+    dl = torch.zeros(max(m, 1), dtype=torch.float64, device="cuda")
+    rep = SchurReport()
+    per = (BatchedSystemReport * max(systems, 1))()
+    N.call("pm_schur_batched_solve_f64", ws.handle, _stream_handle(stream), equations.handle, C.c_double(damping),
+           C.byref(opts.c()), systems, C.c_void_p(offs.ctypes.data), _ptr(dp), _ptr(dl), C.byref(rep), per)
+    report = {k: getattr(rep, k) for k, _ in rep._fields_}
+    report["message"] = rep.message.decode()
+    report["converged"] = bool(rep.converged)
+    systems_out = [{k: getattr(per[s], k) for k, _ in BatchedSystemReport._fields_} for s in range(systems)]
+    return dp[:n], dl[:m], report, systems_out
