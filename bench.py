@@ -38,6 +38,8 @@ WORKLOAD = ("schur_lm_P4000_L2000000: P=4,000 x 6-dof, L=2,000,000 x 3-dof, 2+Po
             "lambda 1e-3, FP64 true relative residual 1e-8")
 METRIC = "Schur-PCG ms to 1e-8 FP64 rel. residual: learned+mixed vs plain; SpMV HBM GB/s"
 REF_SAMPLE_L = 100_000  # eliminated blocks of the reference CPU sample (5% of the full system)
+LEARN_TRAIN, LEARN_HOLD, LEARN_STEPS = 8, 3, 20
+BATCH_SYSTEMS = 512
 
 
 def parse():
@@ -217,7 +219,27 @@ def run_ours(args):
             ms = float(t.item())
         return ms, last
 
+    # ---- learned block-Jacobi correction: trained on this problem's own LM sequence (device
+    # kernels: features, tensor-core MLP forward/backward, Adam), held-out iterations and an
+    # unseen seed evaluated against plain block Jacobi
+    from plamatrix_b200 import learned as LR
+    net = SC.LearnedPreconditioner(seed=rank)
+    runner = LR.LMRunner({**prob, **{k: dev[k] for k in ("obs_primary", "obs_eliminated", "residual")},
+                          "jp": dev["jp"], "jl": dev["jl"]})
+    seq = list(LR.lm_sequence({"jp": dev["jp"], "jl": dev["jl"]}, LEARN_TRAIN + LEARN_HOLD, seed=rank))
+    t_train = time.perf_counter()
+    hist = LR.train(net, [runner], [seq[:LEARN_TRAIN]], steps_per_system=LEARN_STEPS, tolerance=TOL)
+    t_train = time.perf_counter() - t_train
+    unseen = W.bundle_problem_device(P_FULL, L, per_eliminated="2+poisson4", window=40, seed=1000 + rank)
+    unseen_runner = LR.LMRunner(unseen)
+    unseen_seq = list(LR.lm_sequence(unseen, LEARN_HOLD, seed=1000 + rank))
+    evaluation = LR.evaluate(net, [runner, unseen_runner], [seq[LEARN_TRAIN:], unseen_seq], tolerance=TOL)
+    del unseen_runner, unseen
+    learned_mixed = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL, precision="mixed",
+                                                    learned=net)
+
     for _ in range(args.warmup):
+        step(learned_mixed)
         step(mixed)
         step(plain)
     torch.cuda.synchronize()
@@ -225,8 +247,9 @@ def run_ours(args):
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = N.load().pm_kernel_launches()
-    ms_mixed, (_, _, rep_mixed) = timed(lambda: step(mixed), args.steps)
+    ms_learned, (_, _, rep_learned) = timed(lambda: step(learned_mixed), args.steps)
     launches = (N.load().pm_kernel_launches() - launches0) / args.steps
+    ms_mixed, (_, _, rep_mixed) = timed(lambda: step(mixed), args.steps)
     ms_plain, (_, _, rep_plain) = timed(lambda: step(plain), args.steps)
     clock = clocks.stop()
 
@@ -235,7 +258,7 @@ def run_ours(args):
                                                            dev["jl"], dev["residual"], 1.0), args.steps)
     out = {}
     if rank == 0 and not args.no_extras:
-        out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, mixed, n, m)
+        out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, mixed, n, m, net)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -252,26 +275,47 @@ def run_ours(args):
     assembly_bytes = C_ * 18 * 8 + L * 12 * 8 + P_FULL * 42 * 8 + C_ * 8 + L * 4 + B * 36 * 8 + P_FULL * 42 * 8
     asm_ms = rep_plain["assembly_ms"]
     achieved = assembly_bytes / (asm_ms * 1e-3) / 1e9
+    phases = ("pattern_ms", "eliminated_inverse_ms", "assembly_ms", "solve_ms", "back_substitution_ms", "total_ms")
     line = {
-        "metric": METRIC, "value": round(ms_mixed, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms_mixed, 4), "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (FP32 inner PCG, FP64 dots/refinement)", "data": "synthetic",
+        "metric": METRIC, "value": round(ms_learned, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_learned, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (FP32 inner PCG, FP64 dots/refinement; BF16 tensor-core MLP)",
+        "data": "synthetic",
         "config": {"workload": WORKLOAD, "observations": nobs, "eliminated_blocks": L, "primary_blocks": P_FULL,
                    "schur_blocks": B, "cross_blocks": C_, "parallelism": f"replicas x{world} (no exchange step)",
                    "l2": "inputs larger than L2 (observations 1.9 GB FP64)", "systems_per_step": world},
         "plain_fp64_ms": round(ms_plain, 4),
+        "mixed_ms": round(ms_mixed, 4),
+        "learned_mixed_over_plain_speedup": round(ms_plain / ms_learned, 3),
         "mixed_over_plain_speedup": round(ms_plain / ms_mixed, 3),
         "accumulation_ms": round(ms_accum, 4),
-        "phases_mixed": {k: round(rep_mixed[k], 4) for k in ("pattern_ms", "eliminated_inverse_ms", "assembly_ms",
-                                                            "solve_ms", "back_substitution_ms", "total_ms")},
-        "phases_plain": {k: round(rep_plain[k], 4) for k in ("pattern_ms", "eliminated_inverse_ms", "assembly_ms",
-                                                            "solve_ms", "back_substitution_ms", "total_ms")},
-        "iterations": {"mixed_inner": rep_mixed["iterations"], "mixed_refinements": rep_mixed["refinement_steps"],
+        "phases_learned_mixed": {k: round(rep_learned[k], 4) for k in phases},
+        "phases_mixed": {k: round(rep_mixed[k], 4) for k in phases},
+        "phases_plain": {k: round(rep_plain[k], 4) for k in phases},
+        "iterations": {"learned_mixed_inner": rep_learned["iterations"],
+                       "learned_mixed_refinements": rep_learned["refinement_steps"],
+                       "learned_fallback": bool(rep_learned["learned_fallback"]),
+                       "mixed_inner": rep_mixed["iterations"], "mixed_refinements": rep_mixed["refinement_steps"],
                        "plain": rep_plain["iterations"]},
-        "true_relative_residual": {"mixed": rep_mixed["true_relative_residual"],
+        "true_relative_residual": {"learned_mixed": rep_learned["true_relative_residual"],
+                                   "mixed": rep_mixed["true_relative_residual"],
                                    "plain": rep_plain["true_relative_residual"]},
-        "converged": bool(rep_mixed["converged"] and rep_plain["converged"]),
-        "roofline": {"bound": "hbm", "kernel": "assemble_kernel<double,6,3> (+ mirror)", "achieved": round(achieved, 1),
+        "converged": bool(rep_learned["converged"] and rep_mixed["converged"] and rep_plain["converged"]),
+        "learned": {
+            "protocol": (f"LM sequence of this problem: {LEARN_TRAIN} training iterations (Jacobians x (1 + 0.1 N(0,1)), "
+                         f"lambda x{{0.5,2}} from 1e-3), {LEARN_STEPS} Adam steps each (lr 2e-3); held out: "
+                         f"{LEARN_HOLD} later iterations and {LEARN_HOLD} iterations of an unseen seed"),
+            "train_seconds": round(t_train, 2),
+            "loss_first_last": [round(float(np.mean([h[0] for h in hist])), 6),
+                                round(float(np.mean([h[1] for h in hist])), 6)] if hist else None,
+            "held_out": [{"plain_iterations": r["plain"]["iterations"], "learned_iterations": r["learned"]["iterations"],
+                          "plain_ms": round(r["plain"]["ms"], 3), "learned_mixed_ms": round(r["learned"]["ms"], 3),
+                          "fallback": bool(r["learned"]["fallback"]),
+                          "learned_true_relative_residual": r["learned"]["true_relative_residual"]}
+                         for r in evaluation],
+        },
+        "roofline": {"bound": "hbm", "kernel": "assemble_rows6_kernel<double> (+ block-Jacobi inverse, mirror)",
+                     "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4), "traffic": None,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": assembly_bytes},
         "gpu_launches": launches,
@@ -281,7 +325,7 @@ def run_ours(args):
     print(json.dumps(line))
 
 
-def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m):
+def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=None):
     out = {}
     # ---- end to end through the public API with host buffers
     dp_h = torch.empty(n, dtype=torch.float64).pin_memory()
@@ -362,6 +406,8 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m):
         spmv[f"coo_to_csr_laplacian128_{name}"] = {"ms": round(tc, 4), "GBps": round(cbytes / (tc * 1e-3) / 1e9, 1),
                                                    "triplets": trip, "algorithmic_bytes": cbytes}
     out["spmv"] = spmv
+    # ---- batched uneven systems
+    out["batched"] = batched_leg(torch, SC, W, net)
     # ---- CPU baseline: the reference's own CPU library on a bounded sample, scaled
     try:
         import oracle
@@ -376,6 +422,74 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m):
     except Exception as exc:  # noqa: BLE001
         out["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": str(exc)}
     return out
+
+
+def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
+    """Independent systems P ~ U{8..512}, L ~ U{500..50,000}, 4 uniform distinct primaries per
+    eliminated block: one batched launch sequence (union accumulation, pattern, assembly,
+    graph-replayed per-system PCG, back-substitution) against a plain per-system loop."""
+    rng = np.random.default_rng(12345)
+    sizes = [(int(rng.integers(8, 513)), int(rng.integers(500, 50_001))) for _ in range(systems)]
+    probs = [W.bundle_problem_device(P, L, per_eliminated=4, seed=50_000 + i) for i, (P, L) in enumerate(sizes)]
+    P_off = np.cumsum([0] + [P for P, _ in sizes]).astype(np.int64)
+    L_off = np.cumsum([0] + [L for _, L in sizes]).astype(np.int64)
+    union = {
+        "obs_primary": torch.cat([p["obs_primary"] + int(P_off[i]) for i, p in enumerate(probs)]),
+        "obs_eliminated": torch.cat([p["obs_eliminated"] + int(L_off[i]) for i, p in enumerate(probs)]),
+        "jp": torch.cat([p["jp"] for p in probs]), "jl": torch.cat([p["jl"] for p in probs]),
+        "residual": torch.cat([p["residual"] for p in probs])}
+    opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=TOL)
+    res = {"systems": systems, "observations": int(union["jp"].shape[0]),
+           "config": "P~U{8..512}, L~U{500..50000}, 4 uniform distinct primaries per eliminated block, tol 1e-8"}
+
+    def run_batched(options):
+        ne_u = SC.DeviceNormalEquations(int(P_off[-1]), int(L_off[-1]), 6, 3)
+        ws_u = SC.SchurComplementSolverWorkspace()
+        times = []
+        for k in range(2):  # the first call builds the pattern
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ne_u.accumulate_observations(union["obs_primary"], union["obs_eliminated"], union["jp"], union["jl"],
+                                         union["residual"], 1.0)
+            torch.cuda.synchronize()
+            t_acc = time.perf_counter() - t0
+            _, _, rep, per = SC.solve_batched_schur_complement(ne_u, LAMBDA, P_off, options, ws_u)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        # a system's time to solution: the shared prefix (accumulation, pattern check, eliminated
+        # inverses, assembly), its own PCG time to convergence, the shared back-substitution
+        prefix = t_acc * 1e3 + rep["pattern_ms"] + rep["eliminated_inverse_ms"] + rep["assembly_ms"]
+        pst = [prefix + s["time_ms"] + rep["back_substitution_ms"] for s in per if s["converged"]]
+        return {"seconds": round(times[-1], 4), "systems_per_s": round(systems / times[-1], 1),
+                "converged": sum(int(s["converged"]) for s in per),
+                "fallbacks": sum(int(s["learned_fallback"]) for s in per),
+                "max_iterations": max(s["iterations"] for s in per),
+                "p50_ms": round(float(np.percentile(pst, 50)), 3) if pst else None,
+                "p99_ms": round(float(np.percentile(pst, 99)), 3) if pst else None}
+
+    res["batched_plain"] = run_batched(opts)
+    if net is not None:
+        res["batched_learned"] = run_batched(SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=TOL,
+                                                                             learned=net))
+    # per-system launch loop (each system with its own normal equations and workspace, warmed)
+    per_ms = []
+    t_loop = 0.0
+    for p in probs:
+        ne_s = SC.DeviceNormalEquations(p["P"], p["L"], 6, 3)
+        ws_s = SC.SchurComplementSolverWorkspace()
+        for k in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ne_s.accumulate_observations(p["obs_primary"], p["obs_eliminated"], p["jp"], p["jl"], p["residual"], 1.0)
+            SC.solve_damped_schur_complement(ne_s, LAMBDA, opts, ws_s)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        per_ms.append(dt * 1e3)
+        t_loop += dt
+    res["per_system_loop"] = {"seconds": round(t_loop, 4), "systems_per_s": round(systems / t_loop, 1),
+                              "p50_ms": round(float(np.percentile(per_ms, 50)), 3),
+                              "p99_ms": round(float(np.percentile(per_ms, 99)), 3)}
+    return res
 
 
 if __name__ == "__main__":

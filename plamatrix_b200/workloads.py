@@ -143,3 +143,51 @@ def uneven_batch(count: int = 512, seed: int = 0, dtype=np.float64, p_range=(8, 
         k = min(per_eliminated, P)
         out.append(bundle_problem(P, L, per_eliminated=k, window=min(P, 40), seed=seed * 100003 + s, dtype=dtype))
     return out
+
+
+def bundle_problem_device(P: int, L: int, *, per_eliminated: str | int = 4, window: int | None = None,
+                          residual_size: int = 2, outlier_fraction: float = 0.05, huber_delta: float = 1.0,
+                          seed: int = 0, device="cuda") -> dict:
+    """`bundle_problem` drawn on the device with torch's generator (same distributions and
+    structure, different values): for the large learned-preconditioner and batched workloads,
+    whose host generation would dominate a benchmark run.  Arrays are device tensors."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    if isinstance(per_eliminated, str):
+        assert per_eliminated == "2+poisson4"
+        count = 2 + torch.poisson(torch.full((L,), 4.0, device=device), generator=g).to(torch.int64)
+    else:
+        count = torch.full((L,), int(per_eliminated), dtype=torch.int64, device=device)
+    limit = min(P, window) if window else P
+    count = count.clamp(max=limit)
+    kmax = int(count.max().item()) if L else 0
+    width = window if window else P
+    cols = []
+    step = max(1, (1 << 26) // max(width, 1))
+    for start in range(0, L, step):
+        stop = min(start + step, L)
+        keys = torch.rand((stop - start, width), generator=g, device=device)
+        cols.append(keys.argsort(dim=1)[:, :kmax])
+    picks = torch.cat(cols, 0) if cols else torch.zeros((0, kmax), dtype=torch.int64, device=device)
+    if window:
+        centre = torch.randint(0, P, (L,), generator=g, device=device)
+        table = (centre[:, None] + picks - window // 2) % P
+    else:
+        table = picks
+    mask = torch.arange(kmax, device=device)[None, :] < count[:, None]
+    obs_primary = table[mask]
+    obs_eliminated = torch.arange(L, device=device).repeat_interleave(count)
+    n = obs_primary.numel()
+    jp = torch.randn((n, residual_size, 6), generator=g, device=device, dtype=torch.float64)
+    jl = torch.randn((n, residual_size, 3), generator=g, device=device, dtype=torch.float64)
+    r = torch.randn((n, residual_size), generator=g, device=device, dtype=torch.float64) * 0.5
+    out_mask = torch.rand(n, generator=g, device=device) < outlier_fraction
+    r[out_mask] = torch.randn((int(out_mask.sum().item()), residual_size), generator=g, device=device,
+                              dtype=torch.float64) * 20.0
+    order = torch.randperm(n, generator=g, device=device)
+    return {"P": P, "L": L, "bp": 6, "bl": 3, "m": residual_size, "huber_delta": huber_delta,
+            "obs_primary": obs_primary[order].contiguous(), "obs_eliminated": obs_eliminated[order].contiguous(),
+            "jp": jp[order].contiguous(), "jl": jl[order].contiguous(), "residual": r[order].contiguous(),
+            "seed": seed}
