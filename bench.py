@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--eliminated", type=int, default=L_FULL, help="L (eliminated blocks)")
     ap.add_argument("--no-extras", action="store_true", help="skip SpMV / e2e / CPU-baseline legs")
+    ap.add_argument("--sparse-only", action="store_true", help="only the Laplacian SpMV / COO->CSR leg")
     return ap.parse_args()
 
 
@@ -352,10 +353,30 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=Non
     h2d = sum(v.numel() * v.element_size() for v in host.values())
     out["e2e"] = {"value": round(e0.elapsed_time(e1) / args.steps, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
                   "d2h_bytes_per_step": (n + m) * 8}
-    # ---- SpMV bandwidth: the assembled 6x6 block-CSR Schur matrix and the 128^3 Laplacian CSR
+    out["spmv"] = sparse_leg(torch, S, W, stream)
+    # ---- batched uneven systems
+    out["batched"] = batched_leg(torch, SC, W, net)
+    # ---- CPU baseline: the reference's own CPU library on a bounded sample, scaled
+    try:
+        import oracle
+        if oracle.available("ref"):
+            ms, rep, nobs = reference_sample_ms(seed=0)
+            scale = L_FULL / REF_SAMPLE_L
+            out["cpu_baseline"] = {
+                "value": round(ms * scale, 1), "unit": "ms", "cores": 1, "kind": "reference",
+                "sample": (f"reference CPU library (oracle/_ref) accumulation + solveDampedSchurComplement(Cpu) on "
+                           f"P=4,000, L={REF_SAMPLE_L:,} ({nobs:,} observations), scaled x{scale:.0f}; "
+                           f"{rep['iterations']} PCG iterations; 1 thread of {os.cpu_count()}")}
+    except Exception as exc:  # noqa: BLE001
+        out["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": str(exc)}
+    return out
+
+
+def sparse_leg(torch, S, W, stream):
+    """CSR SpMV and COO -> CSR of the 128^3 Laplacian (16.04M triplets), FP64 and FP32, L2 flushed
+    between timed calls."""
     hbm, _ = peaks()
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-    sysd = ws.export()
     spmv = {}
     lap = W.laplacian_coo(128, seed=0, dtype=np.float64)
     for dt, name in ((torch.float64, "f64"), (torch.float32, "f32")):
@@ -405,23 +426,7 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=Non
         tc = statistics.median(ct)
         spmv[f"coo_to_csr_laplacian128_{name}"] = {"ms": round(tc, 4), "GBps": round(cbytes / (tc * 1e-3) / 1e9, 1),
                                                    "triplets": trip, "algorithmic_bytes": cbytes}
-    out["spmv"] = spmv
-    # ---- batched uneven systems
-    out["batched"] = batched_leg(torch, SC, W, net)
-    # ---- CPU baseline: the reference's own CPU library on a bounded sample, scaled
-    try:
-        import oracle
-        if oracle.available("ref"):
-            ms, rep, nobs = reference_sample_ms(seed=0)
-            scale = L_FULL / REF_SAMPLE_L
-            out["cpu_baseline"] = {
-                "value": round(ms * scale, 1), "unit": "ms", "cores": 1, "kind": "reference",
-                "sample": (f"reference CPU library (oracle/_ref) accumulation + solveDampedSchurComplement(Cpu) on "
-                           f"P=4,000, L={REF_SAMPLE_L:,} ({nobs:,} observations), scaled x{scale:.0f}; "
-                           f"{rep['iterations']} PCG iterations; 1 thread of {os.cpu_count()}")}
-    except Exception as exc:  # noqa: BLE001
-        out["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": str(exc)}
-    return out
+    return spmv
 
 
 def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
@@ -496,5 +501,10 @@ if __name__ == "__main__":
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.sparse_only:
+        import torch
+        from plamatrix_b200 import sparse as S_
+        from plamatrix_b200 import workloads as W_
+        print(json.dumps({"spmv": sparse_leg(torch, S_, W_, torch.cuda.current_stream())}))
     else:
         run_ours(a)

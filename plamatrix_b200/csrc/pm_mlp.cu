@@ -47,7 +47,7 @@ struct pm_mlp
     int64_t rows = 0;        // rows of the last forward pass
     int64_t capacity = 0;
     float *F = nullptr, *Z1 = nullptr, *H1 = nullptr, *Z2 = nullptr, *H2 = nullptr, *O = nullptr, *dO = nullptr,
-          *dH = nullptr, *dZ = nullptr;
+          *dH = nullptr, *dZ = nullptr, *split = nullptr;
     int64_t step = 0;
 };
 
@@ -63,11 +63,17 @@ __device__ __forceinline__ float gelu_grad(float x)
 }
 
 // ---------------------------------------------------------------- features
+// Warp per block row: lanes 0..20 the scaled lower-triangle entries of the diagonal block;
+// lanes stride over the row's off-diagonal blocks (Frobenius norms), then fixed xor-tree
+// reductions of the norm sum, maximum, minimum and count.
 template <typename T>
-__global__ void features_kernel(int64_t P, const int* __restrict__ row_ptr, const int* __restrict__ col,
-                                const int* __restrict__ diag_pos, const T* __restrict__ S, float* __restrict__ F)
+__global__ void __launch_bounds__(128) features_kernel(int64_t P, const int* __restrict__ row_ptr,
+                                                       const int* __restrict__ col, const int* __restrict__ diag_pos,
+                                                       const T* __restrict__ S, float* __restrict__ F)
 {
-    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * (blockDim.x / 32);
+    for (int64_t p = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 32; p < P; p += warps)
     {
         const T* d = S + int64_t(diag_pos[p]) * 36;
         double s = 0.0;
@@ -77,15 +83,18 @@ __global__ void features_kernel(int64_t P, const int* __restrict__ row_ptr, cons
         if (!(s > 0.0))
             s = 1.0;
         float* f = F + p * kInPad;
-        for (int r = 0; r < 6; ++r)
-            for (int c = 0; c <= r; ++c)
-            {
-                const double a = static_cast<double>(d[r * 6 + c]) / s;
-                f[r * (r + 1) / 2 + c] = static_cast<float>((a < 0.0 ? -1.0 : 1.0) * log1p(fabs(a)));
-            }
-        double sum = 0.0, mx = 0.0, mn = 0.0;
+        if (lane < 21)
+        {
+            int r = 0;
+            while (r * (r + 1) / 2 + r < lane)
+                ++r;
+            const int c = lane - r * (r + 1) / 2;
+            const double a = static_cast<double>(d[r * 6 + c]) / s;
+            f[lane] = static_cast<float>((a < 0.0 ? -1.0 : 1.0) * log1p(fabs(a)));
+        }
+        double sum = 0.0, mx = -1.0, mn = 1e300;
         int n = 0;
-        for (int b = row_ptr[p]; b < row_ptr[p + 1]; ++b)
+        for (int b = row_ptr[p] + lane; b < row_ptr[p + 1]; b += 32)
         {
             if (col[b] == p)
                 continue;
@@ -97,16 +106,26 @@ __global__ void features_kernel(int64_t P, const int* __restrict__ row_ptr, cons
             }
             fro = sqrt(fro) / s;
             sum += fro;
-            mx = n == 0 || fro > mx ? fro : mx;
-            mn = n == 0 || fro < mn ? fro : mn;
+            mx = fmax(mx, fro);
+            mn = fmin(mn, fro);
             ++n;
         }
-        f[21] = n ? static_cast<float>(log1p(sum / n)) : 0.0f;
-        f[22] = n ? static_cast<float>(log1p(mx)) : 0.0f;
-        f[23] = n ? static_cast<float>(log1p(mn)) : 0.0f;
-        f[24] = static_cast<float>(log1p(static_cast<double>(n)) / 4.0);
-        for (int k = kIn; k < kInPad; ++k)
-            f[k] = 0.0f;
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            n += __shfl_xor_sync(0xffffffffu, n, o);
+        }
+        if (lane == 0)
+        {
+            f[21] = n ? static_cast<float>(log1p(sum / n)) : 0.0f;
+            f[22] = n ? static_cast<float>(log1p(mx)) : 0.0f;
+            f[23] = n ? static_cast<float>(log1p(mn)) : 0.0f;
+            f[24] = static_cast<float>(log1p(static_cast<double>(n)) / 4.0);
+        }
+        if (lane >= kIn && lane < kInPad)
+            f[lane] = 0.0f;
     }
 }
 
@@ -119,36 +138,44 @@ constexpr int kTileM = 64, kTileN = 64, kTileK = 32, kTilePad = 8;
 
 __device__ __forceinline__ uint32_t pack2(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
+// With kchunk > 0 the K range is split over blockIdx.z (chunks of kchunk) and every split writes
+// its partial tile to C + blockIdx.z * M * ldc (no bias / activation); reduce_splits_kernel
+// adds the splits in order.
 __global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, const float* __restrict__ A, int64_t sam,
                                                         int64_t sak, const float* __restrict__ B, int64_t sbk,
                                                         int64_t sbn, const float* __restrict__ bias,
-                                                        float* __restrict__ C, int64_t ldc, float* __restrict__ H)
+                                                        float* __restrict__ C, int64_t ldc, float* __restrict__ H,
+                                                        int kchunk)
 {
     __shared__ __align__(16) __nv_bfloat16 As[kTileM][kTileK + kTilePad]; // [m][k]
     __shared__ __align__(16) __nv_bfloat16 Bs[kTileN][kTileK + kTilePad]; // [n][k]
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int g = lane >> 2, tq = lane & 3;
     const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
+    const int kb = kchunk > 0 ? blockIdx.z * kchunk : 0;
+    const int ke = kchunk > 0 ? min(K, kb + kchunk) : K;
+    if (kchunk > 0)
+        C += int64_t(blockIdx.z) * M * ldc;
     float acc[8][4];
 #pragma unroll
     for (int j = 0; j < 8; ++j)
 #pragma unroll
         for (int e = 0; e < 4; ++e)
             acc[j][e] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += kTileK)
+    for (int k0 = kb; k0 < ke; k0 += kTileK)
     {
         for (int i = t; i < kTileM * kTileK; i += 128)
         {
             const int mm = i / kTileK, kk = i - mm * kTileK;
             const int gm = m0 + mm, gk = k0 + kk;
-            const float a = gm < M && gk < K ? A[int64_t(gm) * sam + int64_t(gk) * sak] : 0.0f;
+            const float a = gm < M && gk < ke ? A[int64_t(gm) * sam + int64_t(gk) * sak] : 0.0f;
             As[mm][kk] = __float2bfloat16_rn(a);
         }
         for (int i = t; i < kTileN * kTileK; i += 128)
         {
             const int nn = i / kTileK, kk = i - nn * kTileK;
             const int gn = n0 + nn, gk = k0 + kk;
-            const float b = gn < N && gk < K ? B[int64_t(gk) * sbk + int64_t(gn) * sbn] : 0.0f;
+            const float b = gn < N && gk < ke ? B[int64_t(gk) * sbk + int64_t(gn) * sbn] : 0.0f;
             Bs[nn][kk] = __float2bfloat16_rn(b);
         }
         __syncthreads();
@@ -196,7 +223,40 @@ void gemm(cudaStream_t stream, int M, int N, int K, const float* A, int64_t sam,
     if (M <= 0 || N <= 0)
         return;
     const dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN);
-    gemm_bf16_kernel<<<grid, 128, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, bias, C, ldc, H);
+    gemm_bf16_kernel<<<grid, 128, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, bias, C, ldc, H, 0);
+    PM_LAUNCH_CHECK();
+}
+
+// sum of `splits` partial M x N tiles (compact, split-major) into C (row stride ldc), in order
+__global__ void reduce_splits_kernel(int M, int N, int splits, const float* __restrict__ part, float* __restrict__ C,
+                                     int64_t ldc)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < int64_t(M) * N;
+         i += int64_t(gridDim.x) * blockDim.x)
+    {
+        float s = 0.0f;
+        for (int z = 0; z < splits; ++z)
+            s += part[int64_t(z) * M * N + i];
+        C[(i / N) * ldc + i % N] = s;
+    }
+}
+
+constexpr int kSplitRows = 512; // rows per split of the weight-gradient reductions
+
+int split_count(int64_t K) { return static_cast<int>((K + kSplitRows - 1) / kSplitRows); }
+
+// C = A B with the K (row) dimension split over CTAs; `part` holds split_count(K) * M * N floats
+void gemm_split(cudaStream_t stream, int M, int N, int K, const float* A, int64_t sam, int64_t sak, const float* B,
+                int64_t sbk, int64_t sbn, float* C, int64_t ldc, float* part)
+{
+    if (M <= 0 || N <= 0)
+        return;
+    const int splits = split_count(K);
+    const dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN, splits);
+    gemm_bf16_kernel<<<grid, 128, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, nullptr, part, N, nullptr,
+                                               kSplitRows);
+    PM_LAUNCH_CHECK();
+    reduce_splits_kernel<<<grid_for(int64_t(M) * N, 256, 1024), 256, 0, stream>>>(M, N, splits, part, C, ldc);
     PM_LAUNCH_CHECK();
 }
 
@@ -340,16 +400,28 @@ __global__ void gelu_back_kernel(int64_t n, const float* __restrict__ dH, const 
         dZ[i] = dH[i] * gelu_grad(Z[i]);
 }
 
-// db[c] = sum over rows of G[row][c] (rows in order)
-__global__ void colsum_kernel(int64_t rows, int cols, int64_t ld, const float* __restrict__ G, float* __restrict__ db)
+// partial column sums of G over row chunks of kSplitRows (blockIdx.y), rows in order
+__global__ void colsum_kernel(int64_t rows, int cols, int64_t ld, const float* __restrict__ G,
+                              float* __restrict__ part)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols)
         return;
+    const int64_t r0 = int64_t(blockIdx.y) * kSplitRows;
+    const int64_t r1 = r0 + kSplitRows < rows ? r0 + kSplitRows : rows;
     float s = 0.0f;
-    for (int64_t r = 0; r < rows; ++r)
+    for (int64_t r = r0; r < r1; ++r)
         s += G[r * ld + c];
-    db[c] = s;
+    part[int64_t(blockIdx.y) * cols + c] = s;
+}
+
+void colsum(cudaStream_t stream, int64_t rows, int cols, int64_t ld, const float* G, float* db, float* part)
+{
+    const int splits = split_count(rows);
+    colsum_kernel<<<dim3((cols + 127) / 128, splits), 128, 0, stream>>>(rows, cols, ld, G, part);
+    PM_LAUNCH_CHECK();
+    reduce_splits_kernel<<<1, 128, 0, stream>>>(1, cols, splits, part, db, cols);
+    PM_LAUNCH_CHECK();
 }
 
 __global__ void adam_kernel(int64_t n, float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
@@ -465,6 +537,8 @@ void ensure_rows(pm_mlp* mlp, int64_t P, cudaStream_t stream)
     plan.take<float>(P * kOutPad);
     plan.take<float>(P * kHid);
     plan.take<float>(P * kHid);
+    const int64_t splits = split_count(P);
+    plan.take<float>(splits * kHid * kHid);
     PM_CUDA(cudaMalloc(&mlp->act, plan.offset + 256));
     Carver c;
     c.base = static_cast<char*>(mlp->act);
@@ -477,6 +551,7 @@ void ensure_rows(pm_mlp* mlp, int64_t P, cudaStream_t stream)
     mlp->dO = c.take<float>(P * kOutPad);
     mlp->dH = c.take<float>(P * kHid);
     mlp->dZ = c.take<float>(P * kHid);
+    mlp->split = c.take<float>(splits * kHid * kHid);
     mlp->capacity = P;
 }
 
@@ -487,7 +562,7 @@ void forward(pm_mlp* mlp, const SchurView& v, cudaStream_t stream)
     mlp->rows = P;
     if (P == 0)
         return;
-    const unsigned grid = grid_for(P, 128, 4096);
+    const unsigned grid = grid_for(P * 32, 128, 1 << 16);
     if (v.value_size == 8)
         features_kernel<double><<<grid, 128, 0, stream>>>(P, v.block_row_ptr, v.block_col, v.diag_pos,
                                                           static_cast<const double*>(v.S), mlp->F);
@@ -572,21 +647,19 @@ double train(pm_mlp* mlp, const SchurView& v, cudaStream_t stream, const double*
     // backward (tensor-core GEMMs; the row dimension is the reduction of the weight gradients)
     float* G = mlp->grads;
     const float* W = mlp->params;
-    gemm(stream, kHid, kOut, M, mlp->H2, 1, kHid, mlp->dO, kOutPad, 1, nullptr, G + kOffW3, kOut);
-    colsum_kernel<<<1, 32, 0, stream>>>(P, kOut, kOutPad, mlp->dO, G + kOffB3);
-    PM_LAUNCH_CHECK();
+    float* splits = mlp->split;
+    gemm_split(stream, kHid, kOut, M, mlp->H2, 1, kHid, mlp->dO, kOutPad, 1, G + kOffW3, kOut, splits);
+    colsum(stream, P, kOut, kOutPad, mlp->dO, G + kOffB3, splits);
     gemm(stream, M, kHid, kOut, mlp->dO, kOutPad, 1, W + kOffW3, 1, kOut, nullptr, mlp->dH, kHid);
     gelu_back_kernel<<<grid_for(P * kHid, 256, 4096), 256, 0, stream>>>(P * kHid, mlp->dH, mlp->Z2, mlp->dZ);
     PM_LAUNCH_CHECK();
-    gemm(stream, kHid, kHid, M, mlp->H1, 1, kHid, mlp->dZ, kHid, 1, nullptr, G + kOffW2, kHid);
-    colsum_kernel<<<1, kHid, 0, stream>>>(P, kHid, kHid, mlp->dZ, G + kOffB2);
-    PM_LAUNCH_CHECK();
+    gemm_split(stream, kHid, kHid, M, mlp->H1, 1, kHid, mlp->dZ, kHid, 1, G + kOffW2, kHid, splits);
+    colsum(stream, P, kHid, kHid, mlp->dZ, G + kOffB2, splits);
     gemm(stream, M, kHid, kHid, mlp->dZ, kHid, 1, W + kOffW2, 1, kHid, nullptr, mlp->dH, kHid);
     gelu_back_kernel<<<grid_for(P * kHid, 256, 4096), 256, 0, stream>>>(P * kHid, mlp->dH, mlp->Z1, mlp->dZ);
     PM_LAUNCH_CHECK();
-    gemm(stream, kIn, kHid, M, mlp->F, 1, kInPad, mlp->dZ, kHid, 1, nullptr, G + kOffW1, kHid);
-    colsum_kernel<<<1, kHid, 0, stream>>>(P, kHid, kHid, mlp->dZ, G + kOffB1);
-    PM_LAUNCH_CHECK();
+    gemm_split(stream, kIn, kHid, M, mlp->F, 1, kInPad, mlp->dZ, kHid, 1, G + kOffW1, kHid, splits);
+    colsum(stream, P, kHid, kHid, mlp->dZ, G + kOffB1, splits);
     if (lr > 0.0)
     {
         mlp->step += 1;

@@ -1763,12 +1763,41 @@ __global__ void backsub_kernel(int64_t L, int bp_rt, int bl_rt, const int* __res
         {
             const T* W = w + int64_t(c) * bp * bl;
             const T* x = dp + int64_t(cross_primary[c]) * bp;
-            for (int col = 0; col < bl; ++col)
+            if constexpr (BP == 6 && BL == 3 && sizeof(T) == 8)
             {
-                T v = T(0);
-                for (int row = 0; row < bp; ++row)
-                    v = add_rn(v, mul_rn(W[row * bl + col], x[row]));
-                point[col] = add_rn(point[col], -v);
+                // the cross block as 16-byte loads (the normal-equation buffers are 256-byte aligned
+                // and a block is 144 bytes); the caller's step vector element by element
+                double wv[18], xv[6];
+                const double2* w2 = reinterpret_cast<const double2*>(W);
+#pragma unroll
+                for (int k = 0; k < 9; ++k)
+                {
+                    const double2 a = __ldg(w2 + k);
+                    wv[2 * k] = a.x;
+                    wv[2 * k + 1] = a.y;
+                }
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+                    xv[k] = static_cast<double>(x[k]);
+#pragma unroll
+                for (int col = 0; col < 3; ++col)
+                {
+                    double v = 0.0;
+#pragma unroll
+                    for (int row = 0; row < 6; ++row)
+                        v = __dadd_rn(v, __dmul_rn(wv[row * 3 + col], xv[row]));
+                    point[col] = add_rn(point[col], static_cast<T>(-v));
+                }
+            }
+            else
+            {
+                for (int col = 0; col < bl; ++col)
+                {
+                    T v = T(0);
+                    for (int row = 0; row < bp; ++row)
+                        v = add_rn(v, mul_rn(W[row * bl + col], x[row]));
+                    point[col] = add_rn(point[col], -v);
+                }
             }
         }
         const double* H = hinv + l * hstride;
