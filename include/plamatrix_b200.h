@@ -189,6 +189,32 @@ PM_API int pm_block_pcg_f64(pm_solver_workspace* workspace, pm_stream_t stream, 
                      const double* rhs_d, double* solution_d, const double* inverse_blocks_d, int64_t block_size,
                      const pm_solver_options* options, pm_solver_report* report);
 
+/* Fixed-iteration solves: cgFixedIterationsAsync / pcgFixedIterationsAsync and
+ * finalizeIterativeSolverReport (include/plamatrix/sparse/iterative_solver.h:143-171,
+ * src/sparse/iterative_solver.cu:166-233, 405-474).  Exactly `iterations` CG (Jacobi-PCG) steps
+ * are enqueued on `stream` with no host check; the state records the initial and final
+ * recurrence residuals and an event.  Finalize after the caller has synchronised the stream:
+ * PM_LOGIC_ERROR while the work is still pending or on a destroyed state, PM_RUNTIME_ERROR
+ * for a non-finite residual (breakdown) or, with require_convergence, for a residual above
+ * max(absolute, relative * initial).  The workspace, matrix and vectors must stay alive until
+ * the stream reaches the state's event. */
+typedef struct pm_fixed_state pm_fixed_state;
+PM_API int pm_cg_fixed_iterations_async_f32(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix,
+                                            const float* rhs_d, float* solution_d, int iterations,
+                                            pm_fixed_state** state);
+PM_API int pm_cg_fixed_iterations_async_f64(pm_solver_workspace* workspace, pm_stream_t stream, const pm_csr* matrix,
+                                            const double* rhs_d, double* solution_d, int iterations,
+                                            pm_fixed_state** state);
+PM_API int pm_pcg_fixed_iterations_async_f32(pm_solver_workspace* workspace, pm_stream_t stream,
+                                             const pm_csr* matrix, const float* rhs_d, float* solution_d,
+                                             int iterations, pm_fixed_state** state);
+PM_API int pm_pcg_fixed_iterations_async_f64(pm_solver_workspace* workspace, pm_stream_t stream,
+                                             const pm_csr* matrix, const double* rhs_d, double* solution_d,
+                                             int iterations, pm_fixed_state** state);
+PM_API int pm_fixed_state_finalize(const pm_fixed_state* state, const pm_solver_options* options,
+                                   pm_solver_report* report);
+PM_API void pm_fixed_state_destroy(pm_fixed_state* state);
+
 /* =========================================================================== normal equations
  * Device-resident state of the reference's BlockNormalEquations<Scalar>
  * (include/plamatrix/optimization/block_schur.h:196-319, src/optimization/block_normal_equations.cpp):
@@ -320,6 +346,12 @@ PM_API int pm_schur_export_f32(pm_schur_workspace* workspace, pm_stream_t stream
                                int64_t* col_indices_d, float* values_d, double* rhs_d, double* preconditioner_d);
 PM_API int pm_schur_export_f64(pm_schur_workspace* workspace, pm_stream_t stream, int64_t* row_offsets_d,
                                int64_t* col_indices_d, double* values_d, double* rhs_d, double* preconditioner_d);
+
+/* y = S x on the last assembled reduced system of `workspace` (n = P * bp; x, y device, in the
+ * system's scalar type).  The block-CSR SpMV of the PCG (replaces the spmvAsync call of
+ * solveAcceleratedReducedSchur, block_schur_accelerated.cpp:261-263, iterative_solver.cu:54,99). */
+PM_API int pm_schur_spmv_f32(pm_schur_workspace* workspace, pm_stream_t stream, const float* x_d, float* y_d);
+PM_API int pm_schur_spmv_f64(pm_schur_workspace* workspace, pm_stream_t stream, const double* x_d, double* y_d);
 
 /* =========================================================================== batched solves
  * No counterpart in the reference: many independent LM systems solved together.  The caller

@@ -2854,6 +2854,28 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
         std::snprintf(rep->message, sizeof(rep->message), "batched PCG: some systems did not converge");
 }
 
+// y = S x on the last assembled reduced system (6x6 block CSR, warp per block row)
+template <typename T>
+void schur_spmv(pm_schur_workspace* ws, cudaStream_t stream, const T* x, T* y)
+{
+    if (!ws || !ws->assembled || ws->P <= 0)
+        fail(PM_LOGIC_ERROR, "Schur SpMV: the workspace holds no assembled system");
+    if (ws->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "Schur SpMV: scalar type differs from the assembled system");
+    if (!x || !y || static_cast<const void*>(x) == static_cast<const void*>(y))
+        fail(PM_INVALID_ARGUMENT, "Schur SpMV: vectors must be non-null and distinct");
+    const int64_t P = ws->P;
+    const int bp = static_cast<int>(ws->bp);
+    const unsigned sgrid = grid_for(P * 32, kVecBlock, 1 << 16);
+    if (bp == 6)
+        bsr_spmv_kernel<T, T, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col,
+                                                                  static_cast<const T*>(ws->S), x, y);
+    else
+        bsr_spmv_kernel<T, T, 0><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col,
+                                                                  static_cast<const T*>(ws->S), x, y);
+    PM_LAUNCH_CHECK();
+}
+
 template <typename T>
 void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_equations* ne, double damping,
                  const pm_schur_options* o, T* dp, T* dl, pm_schur_report* rep, const BatchSpec* batch = nullptr)
@@ -3243,6 +3265,14 @@ int pm_schur_solve_f32(pm_schur_workspace* ws, pm_stream_t stream, const pm_norm
                        const pm_schur_options* o, float* dp, float* dl, pm_schur_report* rep)
 {
     return pm::guarded([&] { pm::schur_solve<float>(ws, stream, ne, damping, o, dp, dl, rep); });
+}
+int pm_schur_spmv_f32(pm_schur_workspace* ws, pm_stream_t stream, const float* x, float* y)
+{
+    return pm::guarded([&] { pm::schur_spmv<float>(ws, stream, x, y); });
+}
+int pm_schur_spmv_f64(pm_schur_workspace* ws, pm_stream_t stream, const double* x, double* y)
+{
+    return pm::guarded([&] { pm::schur_spmv<double>(ws, stream, x, y); });
 }
 int pm_schur_batched_solve_f64(pm_schur_workspace* ws, pm_stream_t stream, const pm_normal_equations* ne,
                                double damping, const pm_schur_options* o, int64_t systems,

@@ -560,8 +560,32 @@ __global__ void pcg_reset_kernel(PcgState* st, int max_iterations)
     *st = s;
 }
 
+// initial and final recurrence residuals of a fixed-iteration solve; NaN marks a breakdown
+__global__ void fixed_finish_kernel(const PcgState* st, double* out)
+{
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    const bool bad = st->breakdown || st->nonfinite_init || st->jacobi_bad_row != kNone;
+    out[0] = st->nonfinite_init ? nan : st->initial_squared;
+    out[1] = bad ? nan : st->residual_squared;
+}
+
 } // namespace
 } // namespace pm
+
+struct pm_fixed_state
+{
+    double* residuals = nullptr; // device: initial, final squared residual
+    cudaEvent_t event = nullptr;
+    cudaStream_t stream = nullptr;
+    int submitted = 0;
+    ~pm_fixed_state()
+    {
+        if (event)
+            cudaEventDestroy(event);
+        if (residuals)
+            cudaFree(residuals);
+    }
+};
 
 struct pm_solver_workspace
 {
@@ -809,6 +833,129 @@ void solve(pm_solver_workspace* ws, cudaStream_t stream, const pm_csr* A, const 
     }
 }
 
+// Exactly `iterations` CG (mode 0) or Jacobi-PCG (mode 1) steps with no host check
+// (fixedSolve, src/sparse/iterative_solver.cu:166-233): tolerance 0, so the device state only
+// stops early on an exact zero residual or a breakdown.
+template <typename T>
+pm_fixed_state* fixed_solve(pm_solver_workspace* ws, cudaStream_t stream, const pm_csr* A, const T* b, T* x,
+                            int iterations, int mode)
+{
+    if (!ws || !A)
+        fail(PM_INVALID_ARGUMENT, "solver arguments must be non-null");
+    if (iterations < 0)
+        fail(PM_INVALID_ARGUMENT, "fixed CUDA iterative solver iterations must be non-negative");
+    if (A->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "solver scalar type differs from the CSR operand");
+    if (A->rows != A->cols)
+        fail(PM_INVALID_ARGUMENT, "CUDA iterative solver requires square A and Nx1 rhs/solution");
+    const int64_t n = A->rows;
+    if (n > 0 && (!b || !x))
+        fail(PM_INVALID_ARGUMENT, "solver vectors must be non-null");
+    if (b && b == x)
+        fail(PM_INVALID_ARGUMENT, "CUDA iterative solver rhs and solution must not alias");
+    auto* state = new pm_fixed_state();
+    try
+    {
+        state->stream = stream;
+        state->submitted = iterations;
+        PM_CUDA(cudaMalloc(reinterpret_cast<void**>(&state->residuals), 2 * sizeof(double)));
+        PM_CUDA(cudaEventCreateWithFlags(&state->event, cudaEventDisableTiming));
+        if (n == 0)
+        {
+            PM_CUDA(cudaMemsetAsync(state->residuals, 0, 2 * sizeof(double), stream));
+            PM_CUDA(cudaEventRecord(state->event, stream));
+            return state;
+        }
+        Carver plan;
+        plan.take<PcgState>(1);
+        plan.take<double>(3 * kMaxReduceBlocks);
+        for (int k = 0; k < 6; ++k)
+            plan.take<T>(n);
+        ws->buffer.ensure(plan.offset + 256, stream, "IterativeSolverWorkspace");
+        Carver c;
+        c.base = static_cast<char*>(ws->buffer.ptr);
+        PcgState* st = c.take<PcgState>(1);
+        double* partials = c.take<double>(3 * kMaxReduceBlocks);
+        T* r0 = c.take<T>(n);
+        T* r1 = c.take<T>(n);
+        T* z = c.take<T>(n);
+        T* p = c.take<T>(n);
+        T* q = c.take<T>(n);
+        T* inv = c.take<T>(n);
+        const unsigned vgrid = grid_for(n, kReduceBlock, kMaxReduceBlocks);
+        const unsigned sgrid = A->threads_per_row <= 8 ? grid_for(n, kReduceBlock, kMaxReduceBlocks)
+                                                       : grid_for(n * A->threads_per_row, kReduceBlock, kMaxReduceBlocks);
+        pcg_reset_kernel<<<1, 1, 0, stream>>>(st, iterations);
+        PM_LAUNCH_CHECK();
+        if (mode == 1)
+        {
+            jacobi_kernel<T><<<grid_for(n, 256, 4096), 256, 0, stream>>>(n, A->row_ptr, A->col_idx,
+                                                                           static_cast<const T*>(A->values), inv, st);
+            PM_LAUNCH_CHECK();
+        }
+        launch_spmv<T>(A, x, q, stream);
+        pcg_init_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, b, q, r0, z, p, mode, inv, static_cast<const T*>(nullptr),
+                                                                0, 0.0, 0.0, partials, st);
+        PM_LAUNCH_CHECK();
+        T* r_in = r0;
+        T* r_out = r1;
+        for (int k = 0; k < iterations; ++k)
+        {
+            if (k > 0)
+            {
+                pcg_direction_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, z, p, st);
+                PM_LAUNCH_CHECK();
+            }
+            launch_pcg_spmv<T>(A, p, q, partials, st, sgrid, stream);
+            pcg_update_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, x, p, q, r_in, r_out, z, mode, inv,
+                                                                      static_cast<const T*>(nullptr), 0, partials, st);
+            PM_LAUNCH_CHECK();
+            std::swap(r_in, r_out);
+        }
+        fixed_finish_kernel<<<1, 1, 0, stream>>>(st, state->residuals);
+        PM_LAUNCH_CHECK();
+        PM_CUDA(cudaEventRecord(state->event, stream));
+    }
+    catch (...)
+    {
+        delete state;
+        throw;
+    }
+    return state;
+}
+
+void fixed_finalize(const pm_fixed_state* state, const pm_solver_options* o, pm_solver_report* report)
+{
+    if (!o || !report)
+        fail(PM_INVALID_ARGUMENT, "finalize arguments must be non-null");
+    if (!std::isfinite(o->relative_tolerance) || o->relative_tolerance < 0.0 || o->relative_tolerance > 1.0 ||
+        !std::isfinite(o->absolute_tolerance) || o->absolute_tolerance < 0.0)
+        fail(PM_INVALID_ARGUMENT, "invalid CUDA iterative solver options");
+    if (!state || !state->event)
+        fail(PM_LOGIC_ERROR, "fixed CUDA iterative solver state is empty or closed");
+    const cudaError_t status = cudaEventQuery(state->event);
+    if (status == cudaErrorNotReady)
+        fail(PM_LOGIC_ERROR, "finalizeIterativeSolverReport requires caller stream synchronization");
+    PM_CUDA(status);
+    double host[2] = {0.0, 0.0};
+    PM_CUDA(cudaMemcpy(host, state->residuals, sizeof(host), cudaMemcpyDeviceToHost));
+    if (!std::isfinite(host[0]) || !std::isfinite(host[1]) || host[0] < 0.0 || host[1] < 0.0)
+        fail(PM_RUNTIME_ERROR, "fixed CUDA iterative solver breakdown: residual is not finite");
+    *report = pm_solver_report{0, 0, 0.0, 0.0};
+    report->iterations = state->submitted;
+    report->initial_residual = std::sqrt(host[0]);
+    report->final_residual = std::sqrt(host[1]);
+    const double tolerance = std::max(o->absolute_tolerance, o->relative_tolerance * report->initial_residual);
+    report->converged = report->final_residual <= tolerance;
+    if (!report->converged && o->require_convergence)
+    {
+        std::ostringstream m;
+        m << "fixed CUDA iterative solver did not converge in " << report->iterations
+          << " iterations; final residual=" << report->final_residual;
+        fail(PM_RUNTIME_ERROR, m.str());
+    }
+}
+
 } // namespace
 } // namespace pm
 
@@ -824,6 +971,37 @@ int pm_csr_create_f64(pm_stream_t stream, int64_t rows, int64_t cols, int64_t nn
 {
     return pm::guarded([&] { pm::csr_create<double>(stream, rows, cols, nnz, ro, ci, v, out); });
 }
+#define PM_FIXED(KIND, MODE, SFX, T)                                                                              \
+    int pm_##KIND##_fixed_iterations_async_##SFX(pm_solver_workspace* ws, pm_stream_t s, const pm_csr* A, const T* b, \
+                                                  T* x, int iterations, pm_fixed_state** state)                    \
+    {                                                                                                              \
+        return pm::guarded([&] {                                                                                   \
+            if (!state)                                                                                            \
+                pm::fail(PM_INVALID_ARGUMENT, "fixed solver state pointer is null");                               \
+            *state = pm::fixed_solve<T>(ws, s, A, b, x, iterations, MODE);                                         \
+        });                                                                                                        \
+    }
+PM_FIXED(cg, 0, f32, float)
+PM_FIXED(cg, 0, f64, double)
+PM_FIXED(pcg, 1, f32, float)
+PM_FIXED(pcg, 1, f64, double)
+#undef PM_FIXED
+
+int pm_fixed_state_finalize(const pm_fixed_state* state, const pm_solver_options* o, pm_solver_report* report)
+{
+    return pm::guarded([&] { pm::fixed_finalize(state, o, report); });
+}
+
+void pm_fixed_state_destroy(pm_fixed_state* state)
+{
+    if (state)
+    {
+        if (state->event)
+            cudaEventSynchronize(state->event);
+        delete state;
+    }
+}
+
 void pm_csr_destroy(pm_csr* A)
 {
     if (A)

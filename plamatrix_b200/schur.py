@@ -49,6 +49,8 @@ N.register("pm_schur_workspace_destroy", [vp], None)
 N.register("pm_schur_workspace_close", [vp])
 N.register("pm_schur_pattern_build_count", [vp], C.c_int64)
 N.register("pm_schur_dims", [vp, vp, vp, vp])
+N.register("pm_schur_spmv_f32", [vp, vp, vp, vp])
+N.register("pm_schur_spmv_f64", [vp, vp, vp, vp])
 
 PRECISION = {"native": 0, "mixed": 1}
 
@@ -182,6 +184,13 @@ class SchurComplementSolverWorkspace:
         n, nnz, b = C.c_int64(), C.c_int64(), C.c_int64()
         N.call("pm_schur_dims", self._h, C.byref(n), C.byref(nnz), C.byref(b))
         return n.value, nnz.value, b.value
+
+    def spmv(self, x: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """y = S x on the last assembled reduced system."""
+        sfx = "f32" if x.dtype == torch.float32 else "f64"
+        y = torch.empty_like(x) if out is None else out
+        N.call(f"pm_schur_spmv_{sfx}", self._h, _stream_handle(stream), _ptr(x), _ptr(y))
+        return y
 
     def export(self, dtype=torch.float64, stream=None) -> dict:
         """Last assembled reduced system in the reference's scalar-CSR layout."""

@@ -245,3 +245,61 @@ def pcg(matrix, rhs, solution, workspace=None, options=None, stream=None) -> dic
 
 def block_pcg(matrix, rhs, solution, inverse_blocks, block_size, workspace=None, options=None, stream=None) -> dict:
     return _solve("block_pcg", matrix, rhs, solution, workspace, options, stream, inverse_blocks, block_size)
+
+
+# ---------------------------------------------------------------- fixed-iteration solves
+for _suffix in ("f32", "f64"):
+    for _kind in ("cg", "pcg"):
+        N.register(f"pm_{_kind}_fixed_iterations_async_{_suffix}",
+                   [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p])
+N.register("pm_fixed_state_finalize", [C.c_void_p, C.c_void_p, C.c_void_p])
+N.register("pm_fixed_state_destroy", [C.c_void_p], None)
+
+
+class AsyncIterativeSolverState:
+    """AsyncIterativeSolverState (iterative_solver.h:68-91): the submitted fixed-iteration solve;
+    finalize() after synchronising the stream (finalizeIterativeSolverReport)."""
+
+    def __init__(self, handle, iterations: int):
+        self._h = handle
+        self.submitted_iterations = iterations
+
+    def finalize(self, options: IterativeSolverOptions | None = None) -> dict:
+        opts = (options or IterativeSolverOptions()).c()
+        rep = N.SolverReport()
+        N.call("pm_fixed_state_finalize", self._h, C.byref(opts), C.byref(rep))
+        return {"converged": bool(rep.converged), "iterations": rep.iterations,
+                "initial_residual": rep.initial_residual, "final_residual": rep.final_residual}
+
+    def close(self) -> None:
+        h, self._h = self._h, None
+        if h is not None:
+            N.load().pm_fixed_state_destroy(h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        try:
+            if h is not None and N._lib is not None:
+                N._lib.pm_fixed_state_destroy(h)
+        except (AttributeError, TypeError):  # interpreter shutdown
+            pass
+        self._h = None
+
+
+def _fixed(kind, matrix, rhs, solution, iterations, workspace, stream):
+    op = matrix if isinstance(matrix, CsrOperand) else CsrOperand(matrix, stream)
+    ws = workspace or IterativeSolverWorkspace()
+    h = C.c_void_p()
+    N.call(f"pm_{kind}_fixed_iterations_async_{op.sfx}", ws.handle, _stream_handle(stream), op.handle, _ptr(rhs),
+           _ptr(solution), int(iterations), C.byref(h))
+    st = AsyncIterativeSolverState(h, int(iterations))
+    st._keep = (op, ws)  # the operand and workspace must outlive the submitted work
+    return st
+
+
+def cg_fixed_iterations_async(matrix, rhs, solution, iterations: int, workspace=None, stream=None):
+    return _fixed("cg", matrix, rhs, solution, iterations, workspace, stream)
+
+
+def pcg_fixed_iterations_async(matrix, rhs, solution, iterations: int, workspace=None, stream=None):
+    return _fixed("pcg", matrix, rhs, solution, iterations, workspace, stream)

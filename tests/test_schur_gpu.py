@@ -243,6 +243,32 @@ def test_small_bundle_solve_matches_reference(checkers, precision):
     assert np.linalg.norm(res) / np.linalg.norm(rhs) <= 1e-9
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_reduced_system_spmv_matches_reference(checkers, dtype):
+    """y = S x through the block-CSR SpMV of the assembled system against the reference's
+    scalar CSR of the same reduced system; errors on type mismatch and aliasing."""
+    prob = W.small_bundle(seed=3, dtype=dtype)
+    orc = checkers.normal_equations_from_observations(prob, dtype=dtype)
+    ne = _device_from_observations(prob, dtype)
+    ws = SC.SchurComplementSolverWorkspace()
+    tdt = torch.float32 if dtype == np.float32 else torch.float64
+    with pytest.raises(N.LogicError):
+        ws.spmv(torch.ones(6, dtype=tdt, device="cuda"))
+    SC.solve_damped_schur_complement(ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=5), ws)
+    ro, ci, vals, _ = orc.schur_system(1e-3, with_preconditioner=False)
+    x = np.random.default_rng(0).standard_normal(len(ro) - 1).astype(dtype)
+    y = host(ws.spmv(dev(x)))
+    ref = csr_matvec(ro, ci, vals.astype(np.float64), x.astype(np.float64))
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    assert np.abs(y - ref).max() <= tol * np.abs(ref).max()
+    other = torch.float64 if dtype == np.float32 else torch.float32
+    with pytest.raises(N.InvalidArgument):
+        ws.spmv(torch.ones(len(x), dtype=other, device="cuda"))
+    xd = dev(x)
+    with pytest.raises(N.InvalidArgument):
+        ws.spmv(xd, out=xd)
+
+
 def test_float_pipeline_matches_reference(checkers):
     prob = W.small_bundle(seed=5, dtype=np.float32)
     orc = checkers.normal_equations_from_observations(prob, dtype=np.float32)

@@ -129,3 +129,40 @@ def test_laplacian_pcg_matches_oracle(checkers, dtype):
     rel = np.linalg.norm(res) / np.linalg.norm(b.astype(np.float64))
     assert rel <= (1e-8 * 1.5 if dtype == np.float64 else 1e-6)
     assert np.allclose(xr, x_ref, rtol=0, atol=(1e-6 if dtype == np.float64 else 1e-3) * np.abs(x_ref).max())
+
+
+@pytest.mark.parametrize("kind", ["cg", "pcg"])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_fixed_iterations_match_the_adaptive_solver(checkers, kind, dtype):
+    """cg/pcgFixedIterationsAsync (iterative_solver.h:143-171): k submitted steps give the iterate
+    of the adaptive solver stopped after k iterations; finalize reports the recurrence residuals."""
+    lap = W.laplacian_coo(16, seed=6, dtype=dtype)
+    A, (ro, ci, v) = _csr(checkers, lap["rows"], lap["cols"], lap["row_indices"], lap["col_indices"], lap["values"],
+                          dtype)
+    b = dev(lap["rhs"].astype(dtype))
+    op = S.CsrOperand(A)
+    k = 12
+    x_fixed = torch.zeros(lap["rows"], dtype=A.values.dtype, device="cuda")
+    state = getattr(S, f"{kind}_fixed_iterations_async")(op, b, x_fixed, k)
+    torch.cuda.synchronize()
+    rep = state.finalize(S.IterativeSolverOptions(relative_tolerance=1e-8))
+    x_adapt = torch.zeros_like(x_fixed)
+    ref = getattr(S, kind)(op, b, x_adapt, options=S.IterativeSolverOptions(max_iterations=k, relative_tolerance=1e-30))
+    assert rep["iterations"] == k and ref["iterations"] == k
+    assert torch.equal(x_fixed, x_adapt)
+    assert rep["initial_residual"] == pytest.approx(ref["initial_residual"], rel=1e-12)
+    assert rep["final_residual"] == pytest.approx(ref["final_residual"], rel=1e-12)
+    assert not rep["converged"]
+    with pytest.raises(N.PlamatrixError):
+        state.finalize(S.IterativeSolverOptions(relative_tolerance=1e-8, require_convergence=True))
+    # enough steps converge; zero steps report the initial residual twice
+    x2 = torch.zeros_like(x_fixed)
+    done = getattr(S, f"{kind}_fixed_iterations_async")(op, b, x2, 400)
+    torch.cuda.synchronize()
+    assert done.finalize(S.IterativeSolverOptions(relative_tolerance=1e-5))["converged"]
+    zero = getattr(S, f"{kind}_fixed_iterations_async")(op, b, torch.zeros_like(x_fixed), 0)
+    torch.cuda.synchronize()
+    z = zero.finalize()
+    assert z["iterations"] == 0 and z["initial_residual"] == z["final_residual"]
+    with pytest.raises(N.InvalidArgument):
+        getattr(S, f"{kind}_fixed_iterations_async")(op, b, torch.zeros_like(x_fixed), -1)
