@@ -39,9 +39,9 @@ WORKLOAD = ("schur_lm_P4000_L2000000: P=4,000 x 6-dof, L=2,000,000 x 3-dof, 2+Po
 METRIC = "Schur-PCG ms to 1e-8 FP64 rel. residual: learned+mixed vs plain; SpMV HBM GB/s"
 REF_SAMPLE_L = 100_000  # eliminated blocks of the reference CPU sample (5% of the full system)
 LEARN_TRAIN, LEARN_HOLD, LEARN_STEPS = 8, 3, 20
-# DRAM bytes (read + write) of one full-size launch of the assembly kernel, from an ncu capture
-# of `python bench.py --steps 2 --warmup 1 --no-extras` with dram__bytes_{read,write}.sum
-ASSEMBLY_TRAFFIC_BYTES = 2_858_000_000
+# DRAM bytes (read + write) of one full-size assembly (assemble_diag6 + assemble_upper6), from an
+# ncu capture of `python bench.py --steps 2 --warmup 1 --no-extras` with dram__bytes_{read,write}.sum
+ASSEMBLY_TRAFFIC_BYTES = 5_648_000_000
 BATCH_SYSTEMS = 512
 
 
@@ -318,7 +318,7 @@ def run_ours(args):
                           "learned_true_relative_residual": r["learned"]["true_relative_residual"]}
                          for r in evaluation],
         },
-        "roofline": {"bound": "hbm", "kernel": "assemble_rows6_kernel<double> (+ block-Jacobi inverse, mirror)",
+        "roofline": {"bound": "hbm", "kernel": "assemble_upper6_kernel<double> + assemble_diag6_kernel<double> (+ block-Jacobi inverse, mirror)",
                      "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": ASSEMBLY_TRAFFIC_BYTES if L == L_FULL else None,

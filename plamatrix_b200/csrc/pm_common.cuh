@@ -246,49 +246,12 @@ CooView coo_view(const pm_sparse_workspace* ws);
 int64_t coo_internal_status(pm_sparse_workspace* ws, cudaStream_t stream, const char* operation);
 
 // ---------------------------------------------------------------- async copies
-// bulk (TMA) copy global -> shared, completion counted in bytes on an mbarrier
 __device__ __forceinline__ unsigned smem_addr(const void* p)
 {
     return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                 : "=r"(ok)
-                 : "r"(smem_addr(bar)), "r"(parity)
-                 : "memory");
-    return ok != 0;
-}
-// bounded wait (about a second of SM clock); false when the phase did not complete
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
-{
-    const long long start = clock64();
-    while (!mbar_try_wait(bar, parity))
-        if (clock64() - start > 2000000000ll)
-            return false;
-    return true;
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
-
-// cp.async (LSU path) of 16 / 8 bytes global -> shared
+// cp.async (LSU path) of 16 / 8 bytes global -> shared; completion tracked per thread in
+// commit groups
 __device__ __forceinline__ void cp_async16(void* dst, const void* src)
 {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
@@ -297,10 +260,12 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(dst)), "l"(src) : "memory");
 }
-// the mbarrier receives one arrival once this thread's earlier cp.async copies have landed
-__device__ __forceinline__ void cp_async_mbar_arrive(unsigned long long* bar)
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void cp_async_wait()
 {
-    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 } // namespace pm

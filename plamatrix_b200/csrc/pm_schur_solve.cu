@@ -41,7 +41,7 @@ struct SchurStatus
     long long eliminated_bad;
     long long preconditioner_bad;
     long long row_too_wide;
-    int pad[2]; // pad[0]: a staged copy of the batched assembly did not complete in time
+    int pad[2]; // pad[1]: scratch flag of the topology comparison
 };
 
 struct SolveState // device-side PCG / refinement scalars
@@ -79,22 +79,20 @@ struct pm_schur_workspace
     int* diag_pos = nullptr;
     int* transpose = nullptr;
     int* block_pc = nullptr; // per block: primary-cross index k (forward), -(k+2) transposed, -1 none
-    // 6x3 assembly batches (pattern lifetime, own buffer)
-    pm::DeviceBuffer batch_buffer;
-    bool batched = false;          // the batched 6x3 assembly applies to this pattern
-    bool bulk_rows = false;        // batches built for bulk row copies (double values)
-    int64_t E = 0, NB = 0;         // items, batches
+    // 6x3 assembly cross pairs (pattern lifetime, own buffer)
+    pm::DeviceBuffer pair_buffer;
+    bool paired = false;           // the cross-pair 6x3 assembly applies to this pattern
+    int64_t E = 0;                 // cross pairs
     int2* row_entries = nullptr;   // C: {cross, eliminated} of every primary-list entry
-    int* batch_offset = nullptr;   // P + 1: batches of row p are [off[p], off[p+1])
-    int4* batches = nullptr;       // NB: {first entry, crosses | split, metadata offset, items | ranges << 16}
-    unsigned* meta = nullptr;      // per batch: item words, self rows, copy ranges
+    int64_t* pair_offset = nullptr; // B + 1: pairs of block b are [off[b], off[b+1]) (upper blocks only)
+    int4* pairs = nullptr;         // E: {cross (l, p), cross (l, q), l, 0}, per block in ascending l
     int* saved_offsets = nullptr;
     int* saved_primary = nullptr;
     int* saved_pc = nullptr;
     // numeric
     double* hinv = nullptr;
     double* y = nullptr;
-    int hstride = 0, ystride = 0; // per eliminated block; 12 / 12 (packed [Hll^-1 | y]) for batched 6x3
+    int hstride = 0, ystride = 0; // per eliminated block; 12 / 12 (packed [Hll^-1 | y]) for the 6x3 pairs
     void* S = nullptr;   // B * bp * bp, Scalar
     float* S32 = nullptr; // mixed-precision copy
     double* rhs = nullptr;
@@ -114,7 +112,7 @@ struct pm_schur_workspace
         pattern.release();
         numeric.release();
         scratch.release();
-        batch_buffer.release();
+        pair_buffer.release();
         if (prim_sort)
             pm_sparse_workspace_destroy(prim_sort);
         if (host_status)
@@ -566,32 +564,20 @@ __global__ void __launch_bounds__(kRowThreads) assemble_kernel(AssembleArgs<T> a
     }
 }
 
-// ---------------------------------------------------------------- 6x3 assembly, batched rows
+// ---------------------------------------------------------------- 6x3 assembly over cross pairs
 // Row p of the reduced system is
 //   S_pp  = Hpp + damping - sum_l W_lp Hll_l^-1 W_lp^T
 //   S_pq  = H_pq          - sum_l W_lp Hll_l^-1 W_lq^T      (q > p, l seeing both p and q)
 //   rhs_p = -g_p          + sum_l W_lp y_l,   y_l = Hll_l^-1 g_l
-// over the crosses (l, p) of row p in ascending l.  Every cross j of the row contributes one
-// "item" per later primary q of its eliminated block (the pair (W_lp, W_lq)).  The pattern
-// build cuts each row's cross list into batches of at most kAsmCross crosses and kAsmItems
-// items, and stores every batch's items sorted by (upper slot, cross).  The numeric kernel
-// runs one CTA per row: the W_lp rows, packed Hll^-1 | y of the batch's crosses and the W_lq
-// rows of its items are copied into shared memory with cp.async, one row per thread (two
-// buffers: batch b+1 is in flight while batch b is consumed; source indices are loaded one
-// batch ahead).  Every thread forms two rows of T = W_lp Hll^-1 per batch and keeps running
-// sums of their diagonal and RHS terms; then owner threads (two per upper block) walk their
-// slot's items.  Two barriers per batch.  Sums run in ascending l within a thread and are
-// reduced in a fixed order: scheduling never changes a result.
-constexpr int kAsmThreads = 256;
-constexpr int kAsmCross = 48;    // crosses per batch
-constexpr int kAsmItems = 112;   // items (staged W_lq rows) per batch
-constexpr int kAsmStages = 3;    // staged batches: owners of b, T of b + 1, copies of b + 2
-constexpr int kAsmSlots = kAsmThreads / 2;     // upper blocks per pass, wide rows (two threads each)
-constexpr int kAsmMidSlots = kAsmThreads / 3;  // upper blocks of a narrow row (three threads each)
-constexpr int kAsmSlotBits = 18;        // item word: slot << 14 | cross << 8 | staged row
-static_assert(kAsmItems <= 256 && kAsmCross <= 64, "item word layout");
-static_assert(kAsmCross + kAsmItems < kAsmThreads, "one staged row per thread, plus the item words");
-static_assert(kAsmCross * 6 <= 2 * kAsmThreads, "two T rows per thread");
+// The pattern build lists, for every upper block (p, q), its cross pairs {cross (l, p),
+// cross (l, q), l} in ascending l; the crosses {cross, l} of every row are its row list, also
+// in ascending l.  Two numeric kernels: a CTA per row sums the diagonal block and RHS over the
+// row's crosses, and 16 lanes of a warp per upper block sum its pairs.  Lanes stride over their
+// crosses or pairs, keep their sums in registers (no float atomics) and combine them with fixed
+// shuffle trees.  An upper-block lane holds three of the six rows (8 pair streams x 2 row
+// halves).  Every sum runs in a fixed order: scheduling never changes a result.
+constexpr int kPairLanes = 16;  // lanes per block
+constexpr int kPairStreams = 8; // pair streams of an upper block (two lanes each)
 
 // items of row-list entry j: one per later primary of its eliminated block
 __global__ void pair_count_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
@@ -617,12 +603,6 @@ __global__ void pair_count_kernel(int64_t P, const int* __restrict__ prim_offset
     }
 }
 
-__global__ void narrow_offsets_kernel(int64_t n, const int64_t* __restrict__ in, int* __restrict__ out)
-{
-    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-        out[i] = static_cast<int>(in[i]);
-}
-
 __global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross,
                                    const int* __restrict__ cross_eliminated, int2* __restrict__ row_entries)
 {
@@ -633,13 +613,14 @@ __global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross
     }
 }
 
-// items in row-list order: upper slot (block index - diagonal position - 1) and the cross of q
+// items in row-list order: block index of (p, q) and the cross of q; pairs per block counted
+// with integer atomics (a count does not depend on the order)
 __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
                                  const int* __restrict__ cross_eliminated, const int* __restrict__ cross_offsets,
                                  const int* __restrict__ cross_primary, int sorted, const int64_t* __restrict__ offset,
                                  const int* __restrict__ block_row_ptr, const int* __restrict__ block_col,
-                                 const int* __restrict__ diag_pos, int* __restrict__ item_slot,
-                                 int* __restrict__ item_cross)
+                                 const int* __restrict__ diag_pos, int* __restrict__ item_block,
+                                 int* __restrict__ item_cross, int* __restrict__ block_pairs)
 {
     for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
     {
@@ -665,353 +646,81 @@ __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets
                     else
                         hi = mid;
                 }
-                item_slot[at] = lo - lo0; // the pattern holds (p, q) by construction
+                item_block[at] = lo; // the pattern holds (p, q) by construction
                 item_cross[at] = k;
+                atomicAdd(&block_pairs[lo], 1);
                 ++at;
             }
         }
     }
 }
 
-// Greedy batches of one row (thread per row).  A cross whose items do not fit an empty batch
-// is split over several single-cross batches; its diagonal term is counted in the first.
-// Batch word w: item count | (1 << 31) when the first cross was started by an earlier batch.
-template <bool Fill>
-__global__ void batch_plan_kernel(int64_t P, const int* __restrict__ prim_offsets, const int64_t* __restrict__ offset,
-                                  int* __restrict__ batch_count, const int* __restrict__ batch_offset,
-                                  int4* __restrict__ batches)
+// Stable placement of the items into per-block pair lists, warp per row.  A warp takes 32
+// row-list entries at a time (ascending l); every entry has at most one item per block, so an
+// item's rank in its block is the number of lower lanes with an item there (a lane bitmask per
+// block), after which the block's cursor advances by the mask's population.
+__global__ void pair_place_kernel(int64_t P, const int* __restrict__ prim_offsets, const int64_t* __restrict__ offset,
+                                  const int* __restrict__ item_block, const int* __restrict__ item_cross,
+                                  const int2* __restrict__ row_entries, unsigned* mask, int64_t* cursor,
+                                  int4* __restrict__ pairs)
 {
-    for (int64_t pp = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; pp < P; pp += int64_t(gridDim.x) * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    volatile unsigned* vmask = mask;
+    volatile int64_t* vcursor = cursor;
+    const int64_t warps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t pp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; pp < P; pp += warps)
     {
         const int J0 = prim_offsets[pp], J1 = prim_offsets[pp + 1];
-        int n = 0;
-        int j = J0;
-        int64_t e = offset[J0];
-        while (j < J1)
+        for (int j0 = J0; j0 < J1; j0 += 32)
         {
-            const int ja = j;
-            const int64_t eb = e;
-            const bool skip = e != offset[j];
-            int nc = 0, ni = 0;
-            bool split = false;
-            while (j < J1 && nc < kAsmCross)
+            const int j = j0 + lane;
+            int64_t e0 = 0, e1 = 0;
+            int2 re = make_int2(0, 0);
+            if (j < J1)
             {
-                const int64_t rem = offset[j + 1] - e;
-                if (ni + rem <= kAsmItems)
+                e0 = offset[j];
+                e1 = offset[j + 1];
+                re = row_entries[j];
+            }
+            for (int64_t e = e0; e < e1; ++e)
+                atomicOr(&mask[item_block[e]], 1u << lane);
+            __syncwarp();
+            for (int64_t e = e0; e < e1; ++e)
+            {
+                const int X = item_block[e];
+                const int64_t at = vcursor[X] + __popc(vmask[X] & below);
+                pairs[at] = make_int4(re.x, item_cross[e], re.y, 0);
+            }
+            __syncwarp();
+            for (int64_t e = e0; e < e1; ++e)
+            {
+                const int X = item_block[e];
+                const unsigned m = vmask[X];
+                if (31 - __clz(m) == lane)
                 {
-                    ni += static_cast<int>(rem);
-                    e = offset[j + 1];
-                    ++j;
-                    ++nc;
-                }
-                else if (nc == 0)
-                {
-                    e += kAsmItems;
-                    ni = kAsmItems;
-                    nc = 1;
-                    split = true;
-                    break;
-                }
-                else
-                {
-                    break;
+                    vcursor[X] = vcursor[X] + __popc(m);
+                    vmask[X] = 0u;
                 }
             }
-            if (Fill)
-                batches[batch_offset[pp] + n] = make_int4(ja, split ? ja + 1 : j, static_cast<int>(eb),
-                                                          ni | (skip ? int(0x80000000u) : 0));
-            ++n;
-        }
-        if (!Fill)
-            batch_count[pp] = n;
-    }
-}
-
-// Batch metadata.  A batch stages, for each cross i in order, the cross's W_lp row and then
-// the W_lq rows of its items in the batch (rows [R_i, R_i + 1 + n_i)).  Its metadata block
-// (4-word aligned) holds the item words sorted by (slot, cross), the staged self row R_i of
-// every cross, then the copy ranges {first source cross, count | first staged row << 16}.
-// With each eliminated block's crosses sorted by primary, the items of a cross are the crosses
-// right after it, so one range covers a cross and all its items ("contiguous").
-__device__ __forceinline__ int meta_head_words(int ni, int nc) { return (ni + nc + 3) & ~3; }
-
-// items of plan batch d that belong to row-list entry j: [lo, hi)
-__device__ __forceinline__ void cross_items(const int4 d, int j, const int64_t* __restrict__ offset, int64_t& lo,
-                                            int64_t& hi)
-{
-    const int64_t eb = d.z, ee = int64_t(d.z) + (d.w & 0x7fffffff);
-    lo = offset[j] > eb ? offset[j] : eb;
-    hi = offset[j + 1] < ee ? offset[j + 1] : ee;
-    if (hi < lo)
-        hi = lo;
-}
-
-__global__ void batch_meta_size_kernel(int64_t NB, const int4* __restrict__ plan, const int64_t* __restrict__ offset,
-                                       int contiguous, int* __restrict__ words)
-{
-    for (int64_t bi = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; bi < NB; bi += int64_t(gridDim.x) * blockDim.x)
-    {
-        const int4 d = plan[bi];
-        const int nc = d.y - d.x, ni = d.w & 0x7fffffff;
-        int nr = 0;
-        for (int i = 0; i < nc; ++i)
-        {
-            int64_t lo, hi;
-            cross_items(d, d.x + i, offset, lo, hi);
-            const int n = static_cast<int>(hi - lo);
-            nr += contiguous ? ((n == 0 || lo == offset[d.x + i]) ? 1 : 2) : 1 + n;
-        }
-        words[bi] = meta_head_words(ni, nc) + ((2 * nr + 3) & ~3); // blocks start 16-byte aligned
-    }
-}
-
-// CTA per batch: staged rows, item words (rank sort by (slot, cross)), ranges, descriptor
-// {first entry, cross count | split << 31, metadata offset, item count | range count << 16}.
-__global__ void __launch_bounds__(256) batch_meta_fill_kernel(
-    int64_t NB, const int4* __restrict__ plan, const int64_t* __restrict__ offset, const int* __restrict__ meta_offset,
-    const int* __restrict__ item_slot, const int* __restrict__ item_cross, const int2* __restrict__ row_entries,
-    int contiguous, unsigned* __restrict__ meta, int4* __restrict__ batches)
-{
-    __shared__ unsigned long long key[kAsmItems];
-    __shared__ long long off[kAsmCross + 1];
-    __shared__ int row_start[kAsmCross + 1];
-    __shared__ int range_start[kAsmCross + 1];
-    for (int64_t bi = blockIdx.x; bi < NB; bi += gridDim.x)
-    {
-        const int4 d = plan[bi];
-        const int nc = d.y - d.x, ni = d.w & 0x7fffffff;
-        const int mo = meta_offset[bi];
-        const int head = meta_head_words(ni, nc);
-        for (int i = threadIdx.x; i <= nc; i += blockDim.x)
-            off[i] = offset[d.x + i];
-        __syncthreads();
-        if (threadIdx.x == 0)
-        {
-            int rows = 0, ranges = 0;
-            for (int i = 0; i < nc; ++i)
-            {
-                int64_t lo, hi;
-                cross_items(d, d.x + i, offset, lo, hi);
-                const int n = static_cast<int>(hi - lo);
-                row_start[i] = rows;
-                range_start[i] = ranges;
-                rows += 1 + n;
-                ranges += contiguous ? ((n == 0 || lo == off[i]) ? 1 : 2) : 1 + n;
-            }
-            row_start[nc] = rows;
-            range_start[nc] = ranges;
-            batches[bi] = make_int4(d.x, nc | (d.w & int(0x80000000u)), mo, ni | (ranges << 16));
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < ni; i += blockDim.x)
-        {
-            const int64_t e = int64_t(d.z) + i;
-            int lo = 0, hi = nc; // cross of item e: off[x] <= e < off[x + 1]
-            while (hi - lo > 1)
-            {
-                const int mid = (lo + hi) >> 1;
-                if (off[mid] <= e)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            const int64_t first = off[lo] > int64_t(d.z) ? off[lo] : int64_t(d.z);
-            const unsigned row = static_cast<unsigned>(row_start[lo] + 1 + (e - first));
-            key[i] = (static_cast<unsigned long long>(item_slot[e]) << 32) | (static_cast<unsigned>(lo) << 8) | row;
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < ni; i += blockDim.x)
-        {
-            const unsigned long long k = key[i];
-            int rank = 0;
-            for (int x = 0; x < ni; ++x)
-                rank += key[x] < k;
-            const unsigned slot = static_cast<unsigned>(k >> 32);
-            meta[int64_t(mo) + rank] = (slot << 14) | static_cast<unsigned>(k & 0x3fffu);
-        }
-        for (int i = threadIdx.x; i < nc; i += blockDim.x)
-        {
-            meta[int64_t(mo) + ni + i] = static_cast<unsigned>(row_start[i]);
-            int64_t lo, hi;
-            cross_items(d, d.x + i, offset, lo, hi);
-            const int n = static_cast<int>(hi - lo);
-            const int c = row_entries[d.x + i].x;
-            unsigned* r = meta + int64_t(mo) + head + 2 * range_start[i];
-            const unsigned row = static_cast<unsigned>(row_start[i]);
-            if (contiguous && (n == 0 || lo == off[i]))
-            {
-                r[0] = static_cast<unsigned>(c);
-                r[1] = static_cast<unsigned>(1 + n) | (row << 16);
-            }
-            else if (contiguous)
-            {
-                r[0] = static_cast<unsigned>(c);
-                r[1] = 1u | (row << 16);
-                r[2] = static_cast<unsigned>(item_cross[lo]);
-                r[3] = static_cast<unsigned>(n) | ((row + 1) << 16);
-            }
-            else
-            {
-                r[0] = static_cast<unsigned>(c);
-                r[1] = 1u | (row << 16);
-                for (int k = 0; k < n; ++k)
-                {
-                    r[2 + 2 * k] = static_cast<unsigned>(item_cross[lo + k]);
-                    r[3 + 2 * k] = 1u | ((row + 1 + k) << 16);
-                }
-            }
-        }
-        for (int i = ni + nc + threadIdx.x; i < head; i += blockDim.x)
-            meta[int64_t(mo) + i] = 0u;
-        __syncthreads();
-    }
-}
-
-// a row of 18 scalars: 9 copies of 16 bytes (double) or 8 bytes (float)
-template <typename T>
-__device__ __forceinline__ void cp_row18(T* dst, const T* src)
-{
-#pragma unroll
-    for (int piece = 0; piece < 9; ++piece)
-    {
-        if constexpr (sizeof(T) == 8)
-            cp_async16(dst + 2 * piece, src + 2 * piece);
-        else
-            cp_async8(dst + 2 * piece, src + 2 * piece);
-    }
-}
-
-
-
-template <typename T>
-struct __align__(16) AsmBuffer
-{
-    T rows[kAsmCross + kAsmItems][18]; // per cross: W_lp, then the W_lq of its items
-    double hy[kAsmCross][12];          // Hll^-1 (9) | y (3) of the batch's crosses
-    unsigned meta[kAsmCross + kAsmItems + 4]; // item words, then the self row of every cross
-};
-
-template <typename T>
-struct AsmShared
-{
-    union
-    {
-        AsmBuffer<T> buf[kAsmStages];
-        double dpart[kAsmThreads][14]; // end of row: per-thread diagonal / RHS partial sums
-    };
-    __align__(16) double t[2][kAsmCross][20]; // T = W_lp Hll^-1 of two batches, row r at [3r, 3r + 3)
-    double dseg[27][8];
-    unsigned long long bar[kAsmStages]; // one mbarrier per stage
-};
-
-__device__ __forceinline__ int desc_crosses(const int4 d) { return d.y & 0x7fffffff; }
-__device__ __forceinline__ int desc_items(const int4 d) { return d.w & 0xffff; }
-__device__ __forceinline__ int desc_ranges(const int4 d) { return (d.w >> 16) & 0xffff; }
-
-// bytes that land by bulk copy (metadata head, and the rows when they are doubles)
-template <typename T>
-__device__ __forceinline__ unsigned batch_bytes(const int4 d)
-{
-    const int nc = desc_crosses(d), ni = desc_items(d);
-    unsigned bytes = static_cast<unsigned>(meta_head_words(ni, nc)) * 4u;
-    if constexpr (sizeof(T) == 8)
-        bytes += static_cast<unsigned>(nc + ni) * 144u;
-    return bytes;
-}
-
-
-
-// per-thread source indices of one batch, loaded one batch ahead
-struct StageIndex
-{
-    int2 range; // {first source cross, count | first staged row << 16} (threads < range count)
-    int l0, l1; // eliminated blocks of the Hll^-1 | y pieces t and t + kAsmThreads
-};
-
-__device__ __forceinline__ StageIndex asm_index(const int4 d, const int2* __restrict__ row_entries,
-                                                const unsigned* __restrict__ meta)
-{
-    const int t = threadIdx.x;
-    const int nc = desc_crosses(d), ni = desc_items(d), nr = desc_ranges(d);
-    StageIndex x;
-    x.range = make_int2(0, 0);
-    x.l0 = x.l1 = 0;
-    if (t < nr)
-    {
-        const unsigned* r = meta + int64_t(d.z) + meta_head_words(ni, nc) + 2 * t;
-        x.range = make_int2(static_cast<int>(r[0]), static_cast<int>(r[1]));
-    }
-    if (t < nc * 6)
-        x.l0 = row_entries[d.x + t / 6].y;
-    if (t + kAsmThreads < nc * 6)
-        x.l1 = row_entries[d.x + (t + kAsmThreads) / 6].y;
-    return x;
-}
-
-// Issue one batch into a stage: the metadata head and (double) the row ranges by bulk copy,
-// the packed Hll^-1 | y rows (and float rows) by cp.async; the stage's mbarrier counts the
-// bulk bytes (armed by thread 0) and one cp.async arrival per thread.
-template <typename T>
-__device__ __forceinline__ void asm_issue(AsmBuffer<T>& b, unsigned long long* bar, const int4 d, const StageIndex& x,
-                                          const T* __restrict__ w, const double* __restrict__ hy,
-                                          const unsigned* __restrict__ meta)
-{
-    const int t = threadIdx.x;
-    const int nc = desc_crosses(d), ni = desc_items(d), nr = desc_ranges(d);
-    if (t == kAsmThreads - 1)
-        bulk_copy(&b.meta[0], meta + int64_t(d.z), static_cast<unsigned>(meta_head_words(ni, nc)) * 4u, bar);
-    if (t < nr)
-    {
-        const int src = x.range.x, count = x.range.y & 0xffff, row = (x.range.y >> 16) & 0xffff;
-        if constexpr (sizeof(T) == 8)
-        {
-            bulk_copy(&b.rows[row][0], w + int64_t(src) * 18, static_cast<unsigned>(count) * 144u, bar);
-        }
-        else
-        {
-            for (int k = 0; k < count; ++k)
-                cp_row18(&b.rows[row + k][0], w + int64_t(src + k) * 18);
+            __syncwarp();
         }
     }
-    if (t < nc * 6)
-    {
-        const int i = t / 6, piece = t - (t / 6) * 6;
-        cp_async16(&b.hy[i][2 * piece], hy + int64_t(x.l0) * 12 + 2 * piece);
-    }
-    if (t + kAsmThreads < nc * 6)
-    {
-        const int k = t + kAsmThreads;
-        const int i = k / 6, piece = k - (k / 6) * 6;
-        cp_async16(&b.hy[i][2 * piece], hy + int64_t(x.l1) * 12 + 2 * piece);
-    }
-    cp_async_mbar_arrive(bar);
 }
 
-// slot's items in a batch: item words sorted by slot (word >> 14)
-__device__ __forceinline__ int item_lower_bound(const unsigned* item, int n, int slot)
+// N consecutive scalars from global memory into doubles (16-byte loads for double, 8-byte for
+// float; src aligned to two scalars)
+template <typename T, int N>
+__device__ __forceinline__ void load_pairs(const T* __restrict__ src, double* q)
 {
-    int lo = 0, hi = n;
-    while (lo < hi)
-    {
-        const int mid = (lo + hi) >> 1;
-        if (static_cast<int>(item[mid] >> 14) < slot)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    return lo;
-}
-
-template <typename T>
-__device__ __forceinline__ void load_row18(const T* src, double* q)
-{
+    static_assert(N % 2 == 0, "pairs of scalars");
     if constexpr (sizeof(T) == 8)
     {
         const double2* s2 = reinterpret_cast<const double2*>(src);
 #pragma unroll
-        for (int e = 0; e < 9; ++e)
+        for (int e = 0; e < N / 2; ++e)
         {
-            const double2 v = s2[e];
+            const double2 v = __ldg(s2 + e);
             q[2 * e] = v.x;
             q[2 * e + 1] = v.y;
         }
@@ -1020,299 +729,174 @@ __device__ __forceinline__ void load_row18(const T* src, double* q)
     {
         const float2* s2 = reinterpret_cast<const float2*>(src);
 #pragma unroll
-        for (int e = 0; e < 9; ++e)
+        for (int e = 0; e < N / 2; ++e)
         {
-            const float2 v = s2[e];
+            const float2 v = __ldg(s2 + e);
             q[2 * e] = v.x;
             q[2 * e + 1] = v.y;
         }
     }
 }
 
-// T rows of one staged batch (thread items k = t and t + kAsmThreads: cross k / 6, row
-// k % 6), with the diagonal / RHS terms of the crosses whose diagonal belongs to the batch.
+// Diagonal block and RHS, CTA per row: thread t walks the row's crosses t, t + 256, ... (21
+// lower entries and 6 RHS terms in registers), then a fixed xor tree per warp and the warps'
+// sums in warp order.
+constexpr int kDiagThreads = 256;
 template <typename T>
-__device__ __forceinline__ void asm_t_phase(const AsmBuffer<T>& b, double (*tout)[20], const int4 d, bool diag,
-                                            double* d1, double* d2)
+__global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
+    int64_t P, const int* __restrict__ prim_offsets, const int2* __restrict__ row_entries, const T* __restrict__ w,
+    const double* __restrict__ hy, const T* __restrict__ hpp, const T* __restrict__ gp, double lambda,
+    double min_diag, const int* __restrict__ diag_pos, T* __restrict__ S, double* __restrict__ rhs)
 {
-    const int t = threadIdx.x;
-    const int nc = desc_crosses(d), ni = desc_items(d);
-    const int i0 = d.y < 0 ? 1 : 0; // first cross's diagonal term counted by an earlier batch
-#pragma unroll
-    for (int pass = 0; pass < 2; ++pass)
-    {
-        const int k = t + pass * kAsmThreads;
-        const int i = k / 6, r = k - (k / 6) * 6;
-        if (i >= nc)
-            continue;
-        const T* wr = &b.rows[b.meta[ni + i]][0];
-        const double* h = &b.hy[i][0];
-        const double w0 = static_cast<double>(wr[r * 3]), w1 = static_cast<double>(wr[r * 3 + 1]),
-                     w2 = static_cast<double>(wr[r * 3 + 2]);
-        double tr[3];
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-            tr[j] = h[j * 3 + 0] * w0 + h[j * 3 + 1] * w1 + h[j * 3 + 2] * w2;
-        tout[i][r * 3] = tr[0];
-        tout[i][r * 3 + 1] = tr[1];
-        tout[i][r * 3 + 2] = tr[2];
-        if (diag && i >= i0)
-        {
-            double* dd = pass == 0 ? d1 : d2;
-#pragma unroll
-            for (int c = 0; c < 6; ++c)
-                if (c <= r)
-                    dd[c] += tr[0] * static_cast<double>(wr[c * 3]) + tr[1] * static_cast<double>(wr[c * 3 + 1]) +
-                             tr[2] * static_cast<double>(wr[c * 3 + 2]);
-            dd[6] += w0 * h[9] + w1 * h[10] + w2 * h[11];
-        }
-    }
-}
-
-// Owner work of one staged batch: the slot's items, ROWS consecutive block rows from rbase.
-template <typename T, int ROWS>
-__device__ __forceinline__ void asm_owner(const AsmBuffer<T>& b, const double (*tin)[20], const unsigned* item, int ni,
-                                          int slot, int rbase, double (*acc)[6])
-{
-    for (int k = item_lower_bound(item, ni, slot); k < ni; ++k)
-    {
-        const unsigned word = item[k];
-        if (static_cast<int>(word >> 14) != slot)
-            break;
-        const double* tr = &tin[(word >> 8) & 63][rbase * 3];
-        double q[18], tv[3 * ROWS];
-        load_row18<T>(b.rows[word & 255], q);
-#pragma unroll
-        for (int e = 0; e < 3 * ROWS; ++e)
-            tv[e] = tr[e];
-#pragma unroll
-        for (int rr = 0; rr < ROWS; ++rr)
-#pragma unroll
-            for (int c = 0; c < 6; ++c)
-                acc[rr][c] += tv[rr * 3] * q[c * 3] + tv[rr * 3 + 1] * q[c * 3 + 1] + tv[rr * 3 + 2] * q[c * 3 + 2];
-    }
-}
-
-// wait for a stage: thread 0 polls its mbarrier (bounded) and arms the stage about to be
-// issued, the CTA votes in the barrier, then every thread observes the completed phase
-// itself.  Returns false after a timeout.
-__device__ __forceinline__ bool asm_sync(unsigned long long* bar, unsigned& parity, bool wait_stage,
-                                         unsigned long long* arm, unsigned arm_bytes)
-{
-    bool ok = true;
-    if (threadIdx.x == 0)
-    {
-        if (wait_stage)
-            ok = mbar_wait(bar, parity);
-        if (arm)
-            mbar_expect_tx(arm, arm_bytes);
-    }
-    if (__syncthreads_or(!ok))
-        return false;
-    if (wait_stage)
-    {
-        if (threadIdx.x != 0)
-            mbar_wait(bar, parity); // complete: returns at once
-        parity ^= 1u;
-    }
-    return true;
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kAsmThreads, 2) assemble_rows6_kernel(
-    int64_t P, const int* __restrict__ batch_offset, const int4* __restrict__ batches,
-    const int2* __restrict__ row_entries, const unsigned* __restrict__ meta, const T* __restrict__ w,
-    const double* __restrict__ hy, const int* __restrict__ block_row_ptr, const int* __restrict__ diag_pos,
-    const int* __restrict__ block_pc, const T* __restrict__ hpp, const T* __restrict__ gp, const T* __restrict__ pcv,
-    double lambda, double min_diag, T* __restrict__ S, double* __restrict__ rhs, SchurStatus* status)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    AsmShared<T>& sh = *reinterpret_cast<AsmShared<T>*>(smem_raw);
-    const int t = threadIdx.x;
-    if (t == 0)
-    {
-        for (int st = 0; st < kAsmStages; ++st)
-            mbar_init(&sh.bar[st], 1 + kAsmThreads); // thread 0's arm + one cp.async arrival per thread
-        fence_mbar_init();
-    }
-    __syncthreads();
-    unsigned parity[kAsmStages] = {0u, 0u, 0u};
+    __shared__ double part[kDiagThreads / 32][27];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
     {
         const int p = static_cast<int>(pp);
-        const int dpos = diag_pos[p];
-        const int n_up = block_row_ptr[p + 1] - dpos - 1;
-        const int b0 = batch_offset[p], nb = batch_offset[p + 1] - b0;
-        const bool mid = n_up <= kAsmMidSlots;
-        const int groups = mid ? 1 : (n_up + kAsmSlots - 1) / kAsmSlots;
-        // diagonal partial sums of this thread's two T rows: entries (r, c <= r), then the RHS
-        double d1[7], d2[7];
+        double d[27]; // 21 lower entries (r, c <= r), then the RHS terms
 #pragma unroll
-        for (int k = 0; k < 7; ++k)
-            d1[k] = d2[k] = 0.0;
-        for (int g = 0; g < groups; ++g)
+        for (int e = 0; e < 27; ++e)
+            d[e] = 0.0;
+        const int J1 = prim_offsets[p + 1];
+        for (int j = prim_offsets[p] + t; j < J1; j += kDiagThreads)
         {
-            const bool first = g == 0;
-            const int slot = mid ? t / 3 : g * kAsmSlots + (t >> 1);
-            const int rbase = mid ? 2 * (t % 3) : 3 * (t & 1);
-            const bool owner = mid ? (t < 3 * kAsmMidSlots && slot < n_up) : slot < n_up;
-            double acc[3][6];
+            const int2 re = row_entries[j];
+            double h[12], wv[18];
+            load_pairs<double, 12>(hy + int64_t(re.y) * 12, h);
+            load_pairs<T, 18>(w + int64_t(re.x) * 18, wv);
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+            {
+                const double w0 = wv[3 * r], w1 = wv[3 * r + 1], w2 = wv[3 * r + 2];
+                double tr[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    tr[k] = h[3 * k] * w0 + h[3 * k + 1] * w1 + h[3 * k + 2] * w2;
+#pragma unroll
+                for (int c = 0; c <= r; ++c)
+                    d[r * (r + 1) / 2 + c] += tr[0] * wv[3 * c] + tr[1] * wv[3 * c + 1] + tr[2] * wv[3 * c + 2];
+                d[21 + r] += w0 * h[9] + w1 * h[10] + w2 * h[11];
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < 27; ++e)
+        {
+            const double v = warp_sum(d[e]);
+            if (lane == 0)
+                part[warp][e] = v;
+        }
+        __syncthreads();
+        if (t < 42)
+        {
+            int e, r = 0, c = 0;
+            if (t < 36)
+            {
+                r = t / 6;
+                c = t % 6;
+                const int lr = r >= c ? r : c, lc = r >= c ? c : r;
+                e = lr * (lr + 1) / 2 + lc;
+            }
+            else
+            {
+                e = 21 + (t - 36);
+            }
+            double v = 0.0;
+            for (int k = 0; k < kDiagThreads / 32; ++k)
+                v = __dadd_rn(v, part[k][e]);
+            if (t < 36)
+            {
+                double base = static_cast<double>(hpp[int64_t(p) * 36 + t]);
+                if (r == c)
+                    base = __dadd_rn(base, __dmul_rn(lambda, fmax(fabs(base), min_diag)));
+                S[int64_t(diag_pos[p]) * 36 + t] = static_cast<T>(base - v);
+            }
+            else
+            {
+                rhs[int64_t(p) * 6 + (t - 36)] = -static_cast<double>(gp[int64_t(p) * 6 + (t - 36)]) + v;
+            }
+        }
+        __syncthreads(); // partial sums read before the next row writes them
+    }
+}
+
+// Upper blocks, 16 lanes per block: lane g = 2 s + h walks the block's pairs s, s + 8, ... for
+// rows 3h .. 3h + 2 (the two lanes of a pair load the same Hll^-1 and W_lq rows, which the
+// load unit merges), then a fixed xor tree over the 8 streams.
+constexpr int kUpperThreads = 256;
+__device__ __forceinline__ double stream_sum(double v, unsigned gmask)
+{
+#pragma unroll
+    for (int o = 2; o < kPairLanes; o <<= 1)
+        v += __shfl_xor_sync(gmask, v, o);
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
+    int64_t B, const int64_t* __restrict__ pair_offset, const int4* __restrict__ pairs,
+    const int* __restrict__ block_row, const int* __restrict__ block_col, const int* __restrict__ block_pc,
+    const T* __restrict__ w, const double* __restrict__ hy, const T* __restrict__ pcv, T* __restrict__ S)
+{
+    const int g = threadIdx.x & (kPairLanes - 1);
+    const int s = g >> 1, h = g & 1;
+    const unsigned gmask = 0xffffu << (threadIdx.x & 16);
+    const int64_t groups = int64_t(gridDim.x) * (kUpperThreads / kPairLanes);
+    for (int64_t b = (int64_t(blockIdx.x) * kUpperThreads + threadIdx.x) / kPairLanes; b < B; b += groups)
+    {
+        if (block_col[b] <= block_row[b])
+            continue;
+        double acc[3][6];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                acc[r][c] = 0.0;
+        const int64_t k1 = pair_offset[b + 1];
+        int64_t k = pair_offset[b] + s;
+        int4 next = k < k1 ? pairs[k] : make_int4(0, 0, 0, 0);
+        while (k < k1)
+        {
+            const int4 cur = next;
+            k += kPairStreams;
+            if (k < k1)
+                next = pairs[k];
+            // Hll^-1 (symmetric) and this lane's three rows of W_lp (elements 9h .. 9h + 8,
+            // read as the aligned run 8h .. 8h + 9)
+            double hv[10], a[10], q[18];
+            load_pairs<double, 10>(hy + int64_t(cur.z) * 12, hv);
+            load_pairs<T, 10>(w + int64_t(cur.x) * 18 + 8 * h, a);
+            load_pairs<T, 18>(w + int64_t(cur.y) * 18, q);
+            double tr[3][3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+            {
+                const double w0 = h ? a[3 * r + 1] : a[3 * r], w1 = h ? a[3 * r + 2] : a[3 * r + 1],
+                             w2 = h ? a[3 * r + 3] : a[3 * r + 2];
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk)
+                    tr[r][kk] = hv[3 * kk] * w0 + hv[3 * kk + 1] * w1 + hv[3 * kk + 2] * w2;
+            }
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
                 for (int c = 0; c < 6; ++c)
-                    acc[r][c] = 0.0;
-            // descriptors: owners of batch k, T of k + 1, copies of k + 2 (indices prefetched)
-            int4 dk = make_int4(0, 0, 0, 0), dk1 = dk, dk2 = dk;
-            StageIndex xk2{};
-            if (nb > 0)
-            {
-                dk = batches[b0];
-                const StageIndex x0 = asm_index(dk, row_entries, meta);
-                StageIndex x1{};
-                if (nb > 1)
-                {
-                    dk1 = batches[b0 + 1];
-                    x1 = asm_index(dk1, row_entries, meta);
-                }
-                if (t == 0)
-                {
-                    mbar_expect_tx(&sh.bar[0], batch_bytes<T>(dk));
-                    if (nb > 1)
-                        mbar_expect_tx(&sh.bar[1], batch_bytes<T>(dk1));
-                }
-                fence_proxy_async(); // earlier generic use of the buffers precedes the copies
-                __syncthreads();
-                asm_issue(sh.buf[0], &sh.bar[0], dk, x0, w, hy, meta);
-                if (nb > 1)
-                    asm_issue(sh.buf[1], &sh.bar[1], dk1, x1, w, hy, meta);
-                if (nb > 2)
-                {
-                    dk2 = batches[b0 + 2];
-                    xk2 = asm_index(dk2, row_entries, meta);
-                }
-                if (!asm_sync(&sh.bar[0], parity[0], true, nullptr, 0))
-                {
-                    if (t == 0)
-                        atomicExch(&status->pad[0], 1);
-                    return;
-                }
-                asm_t_phase<T>(sh.buf[0], sh.t[0], dk, first, d1, d2);
-            }
-            for (int k = 0; k < nb; ++k)
-            {
-                const int s0 = k % kAsmStages, s1 = (k + 1) % kAsmStages, s2 = (k + 2) % kAsmStages;
-                // stage s1 (batch k + 1) must be complete; arm stage s2 for batch k + 2
-                const bool has1 = k + 1 < nb, has2 = k + 2 < nb;
-                if (!asm_sync(&sh.bar[s1], parity[s1], has1, has2 ? &sh.bar[s2] : nullptr,
-                              has2 ? batch_bytes<T>(dk2) : 0u))
-                {
-                    if (t == 0)
-                        atomicExch(&status->pad[0], 1);
-                    return;
-                }
-                if (has2)
-                    asm_issue(sh.buf[s2], &sh.bar[s2], dk2, xk2, w, hy, meta);
-                int4 dk3 = make_int4(0, 0, 0, 0);
-                StageIndex xk3{};
-                if (k + 3 < nb)
-                {
-                    dk3 = batches[b0 + k + 3];
-                    xk3 = asm_index(dk3, row_entries, meta);
-                }
-                if (has1)
-                    asm_t_phase<T>(sh.buf[s1], sh.t[(k + 1) & 1], dk1, first, d1, d2);
-                if (owner)
-                {
-                    const unsigned* item = sh.buf[s0].meta;
-                    const int ni = desc_items(dk);
-                    if (mid)
-                        asm_owner<T, 2>(sh.buf[s0], sh.t[k & 1], item, ni, slot, rbase, acc);
-                    else
-                        asm_owner<T, 3>(sh.buf[s0], sh.t[k & 1], item, ni, slot, rbase, acc);
-                }
-                dk = dk1;
-                dk1 = dk2;
-                dk2 = dk3;
-                xk2 = xk3;
-            }
-            __syncthreads(); // buffers free before the next group or the partial sums reuse them
-            if (owner)
-            {
-                const int blk = dpos + 1 + slot;
-                const int pc = block_pc[blk];
-                T* out = S + int64_t(blk) * 36;
-                const int rows = mid ? 2 : 3;
-                for (int rr = 0; rr < rows; ++rr)
-                {
-                    const int r = rbase + rr;
+                    acc[r][c] += tr[r][0] * q[3 * c] + tr[r][1] * q[3 * c + 1] + tr[r][2] * q[3 * c + 2];
+        }
 #pragma unroll
-                    for (int c = 0; c < 6; ++c)
-                    {
-                        const double base = pc >= 0 ? static_cast<double>(pcv[int64_t(pc) * 36 + r * 6 + c]) : 0.0;
-                        out[r * 6 + c] = static_cast<T>(base - acc[rr][c]);
-                    }
-                }
-            }
-        }
-        // ---- diagonal block and RHS: fixed-order reduction of the per-thread partial sums.
-        // Entry e < 21 is lower-triangle (r, c); e in [21, 27) is RHS row e - 21.
+        for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int k = 0; k < 7; ++k)
+            for (int c = 0; c < 6; ++c)
+                acc[r][c] = stream_sum(acc[r][c], gmask);
+        const int pc = block_pc[b];
+        T* out = S + b * 36 + 18 * h;
+#pragma unroll
+        for (int e = 0; e < 18; ++e)
         {
-            sh.dpart[t][k] = d1[k];
-            sh.dpart[t][7 + k] = d2[k];
+            if ((e & (kPairStreams - 1)) != s)
+                continue;
+            const double base = pc >= 0 ? static_cast<double>(pcv[int64_t(pc) * 36 + 18 * h + e]) : 0.0;
+            out[e] = static_cast<T>(base - acc[e / 6][e % 6]);
         }
-        __syncthreads();
-        if (t < 27 * 8)
-        {
-            const int e = t >> 3, seg = t & 7;
-            int r, c;
-            if (e < 21)
-            {
-                r = 0;
-                while (r * (r + 1) / 2 + r < e)
-                    ++r;
-                c = e - r * (r + 1) / 2;
-            }
-            else
-            {
-                r = e - 21;
-                c = 6;
-            }
-            double v = 0.0;
-            for (int u = seg * 32; u < seg * 32 + 32; ++u)
-            {
-                if (u % 6 == r)
-                    v = __dadd_rn(v, sh.dpart[u][c]);
-                if ((u + kAsmThreads) % 6 == r && (u + kAsmThreads) / 6 < kAsmCross)
-                    v = __dadd_rn(v, sh.dpart[u][7 + c]);
-            }
-            sh.dseg[e][seg] = v;
-        }
-        __syncthreads();
-        if (t < 36)
-        {
-            const int r = t / 6, c = t % 6;
-            const int lr = r >= c ? r : c, lc = r >= c ? c : r;
-            const int e = lr * (lr + 1) / 2 + lc;
-            double dacc = 0.0;
-            for (int seg = 0; seg < 8; ++seg)
-                dacc = __dadd_rn(dacc, sh.dseg[e][seg]);
-            double base = static_cast<double>(hpp[int64_t(p) * 36 + t]);
-            if (r == c)
-                base = __dadd_rn(base, __dmul_rn(lambda, fmax(fabs(base), min_diag)));
-            S[int64_t(dpos) * 36 + t] = static_cast<T>(base - dacc);
-        }
-        else if (t < 42)
-        {
-            const int r = t - 36;
-            double racc = 0.0;
-            for (int seg = 0; seg < 8; ++seg)
-                racc = __dadd_rn(racc, sh.dseg[21 + r][seg]);
-            rhs[int64_t(p) * 6 + r] = -static_cast<double>(gp[int64_t(p) * 6 + r]) + racc;
-        }
-        __syncthreads(); // partial sums (aliasing the buffers) consumed before the next row stages
     }
 }
 
@@ -1854,12 +1438,12 @@ void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
 {
     const int64_t n = ws->P * ws->bp;
     const int64_t bpp = ws->bp * ws->bp;
-    // batched 6x3 assembly: Hll^-1 and y packed per eliminated block in 96 bytes (16-byte copies)
-    ws->hstride = ws->batched ? 12 : static_cast<int>(ws->bl * ws->bl);
-    ws->ystride = ws->batched ? 12 : static_cast<int>(ws->bl);
+    // 6x3 cross-pair assembly: Hll^-1 and y packed per eliminated block in 96 bytes (16-byte loads)
+    ws->hstride = ws->paired ? 12 : static_cast<int>(ws->bl * ws->bl);
+    ws->ystride = ws->paired ? 12 : static_cast<int>(ws->bl);
     Carver plan;
     plan.take<double>(ws->L * ws->hstride + 1);
-    plan.take<double>(ws->batched ? 1 : ws->L * ws->bl + 1);
+    plan.take<double>(ws->paired ? 1 : ws->L * ws->bl + 1);
     plan.take<T>(ws->B * bpp + 1);
     plan.take<float>(mixed ? ws->B * bpp + 1 : 1);
     plan.take<double>(n + 1);
@@ -1873,8 +1457,8 @@ void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
     Carver c;
     c.base = static_cast<char*>(ws->numeric.ptr);
     ws->hinv = c.take<double>(ws->L * ws->hstride + 1);
-    ws->y = c.take<double>(ws->batched ? 1 : ws->L * ws->bl + 1);
-    if (ws->batched)
+    ws->y = c.take<double>(ws->paired ? 1 : ws->L * ws->bl + 1);
+    if (ws->paired)
         ws->y = ws->hinv + 9;
     ws->S = c.take<T>(ws->B * bpp + 1);
     ws->S32 = c.take<float>(mixed ? ws->B * bpp + 1 : 1);
@@ -1926,38 +1510,27 @@ bool topology_matches(pm_schur_workspace* ws, const pm_normal_equations* ne, cud
     return differs == 0;
 }
 
-// Batches of the 6x3 assembly (see assemble_rows6_kernel).
-void build_batches(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream, bool bulk_rows)
+// Cross-pair lists of the 6x3 assembly (see assemble_upper6_kernel).
+void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
 {
-    const int64_t P = ne->P, C = ne->cross_count;
-    ws->batched = false;
-    if (P > (int64_t(1) << kAsmSlotBits))
-        return; // slot numbers would not fit the item word: the generic assembly runs instead
+    const int64_t P = ne->P, C = ne->cross_count, B = ws->B;
+    ws->paired = false;
     const int sorted = ne->crosses_sorted ? 1 : 0;
-    const int contiguous = sorted && bulk_rows ? 1 : 0;
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(P, 8 * sm_count())));
     Carver s1;
     s1.take<int>(C + 1);
     s1.take<int64_t>(C + 2);
-    s1.take<int>(P + 1);
-    s1.take<int>(P + 2);
     s1.take<char>(scan_scratch_bytes(C + 1, sizeof(int64_t)));
-    s1.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
     const size_t pass1 = ((s1.offset + 255) / 256) * 256;
     int64_t* offset = nullptr;
-    int* bofs = nullptr;
     int64_t E = 0;
-    int NB = 0;
-    // pass 1: items per row-list entry, batches per row (re-run when the scratch moves)
+    // pass 1: items per row-list entry (re-run when the scratch moves)
     auto run_pass1 = [&]() {
         Carver c1;
         c1.base = static_cast<char*>(ws->scratch.ptr);
         int* count = c1.take<int>(C + 1);
         offset = c1.take<int64_t>(C + 2);
-        int* bcount = c1.take<int>(P + 1);
-        bofs = c1.take<int>(P + 2);
         void* scan1 = c1.take<char>(scan_scratch_bytes(C + 1, sizeof(int64_t)));
-        void* scan2 = c1.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
         if (P > 0 && C > 0)
         {
             pair_count_kernel<<<grid, 128, 0, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
@@ -1965,111 +1538,73 @@ void build_batches(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
             PM_LAUNCH_CHECK();
         }
         exclusive_scan<int, int64_t>(count, offset, C, scan1, stream);
-        if (P > 0)
-        {
-            batch_plan_kernel<false><<<grid_for(P, 128, 4096), 128, 0, stream>>>(P, ws->prim_offsets, offset, bcount,
-                                                                                nullptr, nullptr);
-            PM_LAUNCH_CHECK();
-        }
-        exclusive_scan<int, int>(bcount, bofs, P, scan2, stream);
         PM_CUDA(cudaMemcpyAsync(&E, offset + C, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
-        PM_CUDA(cudaMemcpyAsync(&NB, bofs + P, sizeof(int), cudaMemcpyDeviceToHost, stream));
         PM_CUDA(cudaStreamSynchronize(stream));
     };
     ws->scratch.ensure(pass1 + 512, stream, "SchurComplementSolverWorkspace");
     run_pass1();
-    if (E > INT32_MAX - 1)
-        fail(PM_OVERFLOW_ERROR, "Schur assembly supports up to 2^31 - 2 cross pairs");
-    // pass 2 scratch: items (slot, cross of q), plan descriptors, metadata sizes and offsets
+    // pass 2 scratch: items (block, cross of q), pairs per block, lane masks, cursors
     Carver s2;
     s2.take<int>(E + 1);
     s2.take<int>(E + 1);
-    s2.take<int4>(NB + 1);
-    s2.take<int>(NB + 1);
-    s2.take<int64_t>(NB + 2);
-    s2.take<int>(NB + 1);
-    s2.take<char>(scan_scratch_bytes(NB + 1, sizeof(int64_t)));
+    s2.take<int>(B + 1);
+    s2.take<unsigned>(B + 1);
+    s2.take<int64_t>(B + 1);
+    s2.take<char>(scan_scratch_bytes(B + 1, sizeof(int64_t)));
     void* before = ws->scratch.ptr;
     ws->scratch.ensure(pass1 + s2.offset + 512, stream, "SchurComplementSolverWorkspace");
     if (ws->scratch.ptr != before)
         run_pass1();
     Carver c2;
     c2.base = static_cast<char*>(ws->scratch.ptr) + pass1;
-    int* item_slot = c2.take<int>(E + 1);
+    int* item_block = c2.take<int>(E + 1);
     int* item_cross = c2.take<int>(E + 1);
-    int4* plan = c2.take<int4>(NB + 1);
-    int* words = c2.take<int>(NB + 1);
-    int64_t* meta_offset64 = c2.take<int64_t>(NB + 2);
-    int* meta_offset = c2.take<int>(NB + 1);
-    void* scan3 = c2.take<char>(scan_scratch_bytes(NB + 1, sizeof(int64_t)));
-    // row entries first: the metadata refers to them
-    Carver fixed;
-    fixed.take<int2>(C + 1);
-    fixed.take<int>(P + 2);
-    fixed.take<int4>(NB + 1);
-    if (P > 0)
-    {
-        batch_plan_kernel<true><<<grid_for(P, 128, 4096), 128, 0, stream>>>(P, ws->prim_offsets, offset, nullptr,
-                                                                           bofs, plan);
-        PM_LAUNCH_CHECK();
-    }
+    int* block_pairs = c2.take<int>(B + 1);
+    unsigned* mask = c2.take<unsigned>(B + 1);
+    int64_t* cursor = c2.take<int64_t>(B + 1);
+    void* scan2 = c2.take<char>(scan_scratch_bytes(B + 1, sizeof(int64_t)));
+    // persistent: row entries (C) | pair offsets (B + 1) | pairs (E)
+    Carver plan_b;
+    plan_b.take<int2>(C + 1);
+    plan_b.take<int64_t>(B + 2);
+    plan_b.take<int4>(E + 1);
+    ws->pair_buffer.ensure(plan_b.offset + 512, stream, "SchurComplementSolverWorkspace");
+    Carver bc;
+    bc.base = static_cast<char*>(ws->pair_buffer.ptr);
+    ws->row_entries = bc.take<int2>(C + 1);
+    ws->pair_offset = bc.take<int64_t>(B + 2);
+    ws->pairs = bc.take<int4>(E + 1);
+    ws->E = E;
+    PM_CUDA(cudaMemsetAsync(block_pairs, 0, size_t(B + 1) * sizeof(int), stream));
+    PM_CUDA(cudaMemsetAsync(mask, 0, size_t(B + 1) * sizeof(unsigned), stream));
     if (P > 0 && E > 0)
     {
         pair_emit_kernel<<<grid, 128, 0, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
                                                    ne->cross_offsets, ne->cross_primary, sorted, offset,
-                                                   ws->block_row_ptr, ws->block_col, ws->diag_pos, item_slot,
-                                                   item_cross);
+                                                   ws->block_row_ptr, ws->block_col, ws->diag_pos, item_block,
+                                                   item_cross, block_pairs);
         PM_LAUNCH_CHECK();
     }
-    if (NB > 0)
-    {
-        batch_meta_size_kernel<<<grid_for(NB, 128, 1 << 16), 128, 0, stream>>>(NB, plan, offset, contiguous, words);
-        PM_LAUNCH_CHECK();
-    }
-    exclusive_scan<int, int64_t>(words, meta_offset64, NB, scan3, stream);
-    int64_t W = 0;
-    PM_CUDA(cudaMemcpyAsync(&W, meta_offset64 + NB, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
-    PM_CUDA(cudaStreamSynchronize(stream));
-    if (W > INT32_MAX - 16)
-        fail(PM_OVERFLOW_ERROR, "Schur assembly metadata exceeds 2^31 words");
-    if (NB > 0)
-    {
-        narrow_offsets_kernel<<<grid_for(NB, 256, 1 << 16), 256, 0, stream>>>(NB, meta_offset64, meta_offset);
-        PM_LAUNCH_CHECK();
-    }
-    // persistent: row entries (C) | batch offsets (P + 1) | batches (NB) | metadata (W)
-    Carver plan_b;
-    plan_b.take<int2>(C + 1);
-    plan_b.take<int>(P + 2);
-    plan_b.take<int4>(NB + 1);
-    plan_b.take<unsigned>(W + 16);
-    ws->batch_buffer.ensure(plan_b.offset + 512, stream, "SchurComplementSolverWorkspace");
-    Carver bc;
-    bc.base = static_cast<char*>(ws->batch_buffer.ptr);
-    ws->row_entries = bc.take<int2>(C + 1);
-    ws->batch_offset = bc.take<int>(P + 2);
-    ws->batches = bc.take<int4>(NB + 1);
-    ws->meta = bc.take<unsigned>(W + 16);
-    ws->E = E;
-    ws->NB = NB;
-    PM_CUDA(cudaMemcpyAsync(ws->batch_offset, bofs, (P + 1) * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+    exclusive_scan<int, int64_t>(block_pairs, ws->pair_offset, B, scan2, stream);
+    if (B > 0)
+        PM_CUDA(cudaMemcpyAsync(cursor, ws->pair_offset, size_t(B) * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                                stream));
     if (C > 0)
     {
         row_entries_kernel<<<grid_for(C, 256, 1 << 16), 256, 0, stream>>>(C, ws->prim_cross, ne->cross_eliminated,
                                                                          ws->row_entries);
         PM_LAUNCH_CHECK();
     }
-    if (NB > 0)
+    if (P > 0 && E > 0)
     {
-        batch_meta_fill_kernel<<<grid_for(NB, 1, 1 << 16), 256, 0, stream>>>(
-            NB, plan, offset, meta_offset, item_slot, item_cross, ws->row_entries, contiguous, ws->meta, ws->batches);
+        pair_place_kernel<<<grid_for(P * 32, 256, 1 << 16), 256, 0, stream>>>(
+            P, ws->prim_offsets, offset, item_block, item_cross, ws->row_entries, mask, cursor, ws->pairs);
         PM_LAUNCH_CHECK();
     }
-    ws->batched = true;
-    ws->bulk_rows = bulk_rows;
+    ws->paired = true;
 }
 
-void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream, bool bulk_rows)
+void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStream_t stream)
 {
     const int64_t P = ne->P, L = ne->L, C = ne->cross_count, PC = ne->primary_cross_count;
     const size_t bitmap = size_t((P + 31) / 32) * sizeof(unsigned);
@@ -2148,7 +1683,7 @@ void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
     {
         // the pattern buffer moved: re-carve the fixed part (contents are rebuilt below anyway,
         // except prim lists / row pointers, which are recomputed by re-running this function)
-        return build_pattern(ws, ne, stream, bulk_rows);
+        return build_pattern(ws, ne, stream);
     }
     Carver bc;
     bc.base = static_cast<char*>(ws->pattern.ptr) + ((fixed + 255) / 256) * 256;
@@ -2168,9 +1703,9 @@ void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
         PM_LAUNCH_CHECK();
     }
     PM_CUDA(cudaMemsetAsync(ws->block_pc, 0xff, size_t(B + 1) * sizeof(int), stream));
-    ws->batched = false;
+    ws->paired = false;
     if (ne->bp == 6 && ne->bl == 3)
-        build_batches(ws, ne, stream, bulk_rows);
+        build_pairs(ws, ne, stream);
     if (PC > 0)
     {
         block_pc_kernel<<<grid_for(PC, 256, 4096), 256, 0, stream>>>(PC, ne->primary_cross_row, ne->primary_cross_col,
@@ -2230,15 +1765,19 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
         return size_t(ch) * (bpl + bpp + a.bp) * sizeof(T) + size_t(mp * mp) * sizeof(double) + 64 +
                kRowThreads * sizeof(unsigned long long) + 2 * ch * sizeof(int) + 64;
     };
-    if (ws->batched)
+    if (ws->paired)
     {
-        const size_t smem = sizeof(AsmShared<T>);
-        set_smem(reinterpret_cast<const void*>(assemble_rows6_kernel<T>), smem);
-        assemble_rows6_kernel<T><<<grid, kAsmThreads, smem, stream>>>(
-            a.P, ws->batch_offset, ws->batches, ws->row_entries, ws->meta, a.w, ws->hinv,
-            a.block_row_ptr, a.diag_pos, a.block_pc, a.hpp, a.gp, a.pcv, a.lambda, a.min_diag, a.S, a.rhs,
-            a.status);
+        assemble_diag6_kernel<T><<<grid_for(a.P, 1, 1 << 20), kDiagThreads, 0, stream>>>(
+            a.P, ws->prim_offsets, ws->row_entries, a.w, ws->hinv, a.hpp, a.gp, a.lambda, a.min_diag, a.diag_pos,
+            a.S, a.rhs);
         PM_LAUNCH_CHECK();
+        if (ws->E > 0)
+        {
+            assemble_upper6_kernel<T><<<grid_for(ws->B * kPairLanes, kUpperThreads), kUpperThreads, 0, stream>>>(
+                ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, a.block_pc, a.w, ws->hinv, a.pcv,
+                a.S);
+            PM_LAUNCH_CHECK();
+        }
         diag_inverse_kernel<T, 6><<<grid_for(a.P, 64, 1 << 16), 64, 0, stream>>>(a.P, a.diag_pos, a.S, a.minv,
                                                                                  a.status);
         PM_LAUNCH_CHECK();
@@ -2935,11 +2474,8 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         numeric_layout<T>(ws, stream, mixed);
     }
     const bool reused = ws->pattern_builds > 0 && topology_matches(ws, ne, stream);
-    constexpr bool kBulkRows = sizeof(T) == 8; // float rows (72 bytes) cannot go by bulk copy
     if (!reused)
-        build_pattern(ws, ne, stream, kBulkRows);
-    else if (ws->batched && ws->bulk_rows != kBulkRows)
-        build_batches(ws, ne, stream, kBulkRows);
+        build_pattern(ws, ne, stream);
     ws->last_ne = ne;
     ws->last_version = ne->topology_version;
     ws->value_size = sizeof(T);
@@ -3006,8 +2542,6 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         cudaEventElapsedTime(&t, ws->events[0], ws->events[last]);
         rep->total_ms = t;
     };
-    if (ws->host_status->pad[0] != 0)
-        fail(PM_RUNTIME_ERROR, "Schur assembly: a shared-memory copy did not complete within its time limit");
     if (ws->host_status->eliminated_bad != kNone)
     {
         timings(3);
