@@ -132,6 +132,91 @@ __device__ __forceinline__ T huber_weight(const T* r, int m, T delta)
     return delta / sqrt(squared);
 }
 
+// One residual row's terms, each `weight * value * jacobian` as two rounded multiplies and a
+// rounded add (the reference's host accumulation order).
+template <typename T>
+__device__ __forceinline__ void eliminated3_row(T* H, T* g, T weight, const T* jrow, T rr)
+{
+#pragma unroll
+    for (int col = 0; col < 3; ++col)
+    {
+        const T wv = mul_rn(weight, jrow[col]);
+        g[col] = add_rn(g[col], mul_rn(wv, rr));
+#pragma unroll
+        for (int other = 0; other < 3; ++other)
+            H[col * 3 + other] = add_rn(H[col * 3 + other], mul_rn(wv, jrow[other]));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void cross63_row(T* W, T weight, const T* prow, const T* lrow)
+{
+#pragma unroll
+    for (int pc = 0; pc < 6; ++pc)
+    {
+        const T wv = mul_rn(weight, prow[pc]);
+#pragma unroll
+        for (int ec = 0; ec < 3; ++ec)
+            W[pc * 3 + ec] = add_rn(W[pc * 3 + ec], mul_rn(wv, lrow[ec]));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void primary6_row(T* sum, T weight, const T* jrow, T rr)
+{
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+    {
+        const T wv = mul_rn(weight, jrow[c]);
+        sum[36 + c] = add_rn(sum[36 + c], mul_rn(wv, rr));
+#pragma unroll
+        for (int o = 0; o < 6; ++o)
+            sum[c * 6 + o] = add_rn(sum[c * 6 + o], mul_rn(wv, jrow[o]));
+    }
+}
+
+// N contiguous scalars in pairs (16-byte loads for double, 8-byte for float); p aligned to two
+// scalars
+template <typename T, int N>
+__device__ __forceinline__ void load_vec(const T* __restrict__ p, T* out)
+{
+    static_assert(N % 2 == 0, "pairs of scalars");
+    if constexpr (sizeof(T) == 8)
+    {
+#pragma unroll
+        for (int e = 0; e < N / 2; ++e)
+        {
+            const double2 v = __ldg(reinterpret_cast<const double2*>(p) + e);
+            out[2 * e] = v.x;
+            out[2 * e + 1] = v.y;
+        }
+    }
+    else
+    {
+#pragma unroll
+        for (int e = 0; e < N / 2; ++e)
+        {
+            const float2 v = __ldg(reinterpret_cast<const float2*>(p) + e);
+            out[2 * e] = v.x;
+            out[2 * e + 1] = v.y;
+        }
+    }
+}
+
+template <typename T, int N>
+__device__ __forceinline__ void store_vec(T* __restrict__ p, const T* in)
+{
+    static_assert(N % 2 == 0, "pairs of scalars");
+#pragma unroll
+    for (int e = 0; e < N / 2; ++e)
+    {
+        if constexpr (sizeof(T) == 8)
+            reinterpret_cast<double2*>(p)[e] = make_double2(in[2 * e], in[2 * e + 1]);
+        else
+            reinterpret_cast<float2*>(p)[e] = make_float2(in[2 * e], in[2 * e + 1]);
+    }
+}
+
 // Huber weight of every observation (one thread each, coalesced residual reads).
 template <typename T>
 __global__ void huber_weights_kernel(int64_t count, int m, const T* __restrict__ res, T delta, T* __restrict__ weight)
@@ -243,20 +328,7 @@ __global__ void __launch_bounds__(128) eliminated_diagonal3_kernel(CooView v, in
             const T* J = jl + i * m * 3;
             const T* r = res + i * m;
             for (int row = 0; row < m; ++row)
-            {
-                const T rr = r[row];
-                const T j0 = J[row * 3], j1 = J[row * 3 + 1], j2 = J[row * 3 + 2];
-                const T jrow[3] = {j0, j1, j2};
-#pragma unroll
-                for (int col = 0; col < 3; ++col)
-                {
-                    const T wv = mul_rn(weight, jrow[col]);
-                    g[col] = add_rn(g[col], mul_rn(wv, rr));
-#pragma unroll
-                    for (int other = 0; other < 3; ++other)
-                        H[col * 3 + other] = add_rn(H[col * 3 + other], mul_rn(wv, jrow[other]));
-                }
-            }
+                eliminated3_row(H, g, weight, J + row * 3, r[row]);
         }
 #pragma unroll
         for (int k = 0; k < 9; ++k)
@@ -288,23 +360,7 @@ __global__ void __launch_bounds__(128) cross_accumulate63_kernel(int64_t C, cons
             const T* Jp = jp + i * m * 6;
             const T* Jl = jl + i * m * 3;
             for (int row = 0; row < m; ++row)
-            {
-                T prow[6], lrow[3];
-#pragma unroll
-                for (int k = 0; k < 6; ++k)
-                    prow[k] = Jp[row * 6 + k];
-#pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    lrow[k] = Jl[row * 3 + k];
-#pragma unroll
-                for (int pc = 0; pc < 6; ++pc)
-                {
-                    const T wv = mul_rn(weight, prow[pc]);
-#pragma unroll
-                    for (int ec = 0; ec < 3; ++ec)
-                        W[pc * 3 + ec] = add_rn(W[pc * 3 + ec], mul_rn(wv, lrow[ec]));
-                }
-            }
+                cross63_row(W, weight, Jp + row * 6, Jl + row * 3);
         }
         T* out = w + c * 18;
 #pragma unroll
@@ -313,14 +369,119 @@ __global__ void __launch_bounds__(128) cross_accumulate63_kernel(int64_t C, cons
     }
 }
 
+// Two-row residuals, thread per eliminated block: Hll and g_l over the block's observations in
+// input order (the sums of eliminated_diagonal3_kernel), the Huber weight evaluated inline and
+// rows read in pairs of scalars; the next observation index is loaded one step ahead.
+template <typename T>
+__global__ void __launch_bounds__(128) eliminated3_m2_kernel(CooView vo, const T* __restrict__ jl,
+                                                             const T* __restrict__ res, T delta, T* __restrict__ hll,
+                                                             T* __restrict__ gl)
+{
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < vo.rows; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        T H[9], g[3];
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            H[k] = T(0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            g[k] = T(0);
+        const int e = vo.bucket_start[l + 1];
+        int q = vo.bucket_start[l];
+        uint64_t next = q < e ? vo.keys[q] : 0;
+        for (; q < e; ++q)
+        {
+            const int64_t i = static_cast<uint32_t>(next);
+            if (q + 1 < e)
+                next = vo.keys[q + 1];
+            T r[2], J[6];
+            load_vec<T, 2>(res + i * 2, r);
+            load_vec<T, 6>(jl + i * 6, J);
+            const T weight = huber_weight(r, 2, delta);
+            eliminated3_row(H, g, weight, J, r[0]);
+            eliminated3_row(H, g, weight, J + 3, r[1]);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            hll[l * 9 + k] = H[k];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            gl[l * 3 + k] = g[k];
+    }
+}
+
+// Two-row residuals, thread per cross: W over the cross's observations in input order (the
+// sums of cross_accumulate63_kernel), weight inline, rows read in pairs of scalars.  A warp's
+// 32 consecutive W rows (contiguous in memory) leave through shared memory in coalesced
+// 16-byte stores.  (Reading the observations in input order and scattering single-observation
+// W rows instead measured 1.7x slower: scattered 144-byte writes cost more than the gathers.)
+constexpr int kCrossThreads = 128;
+template <typename T>
+__global__ void __launch_bounds__(kCrossThreads) cross63_m2_kernel(int64_t C, const uint64_t* __restrict__ keys,
+                                                                   const int* __restrict__ cross_run,
+                                                                   const T* __restrict__ jp, const T* __restrict__ jl,
+                                                                   const T* __restrict__ res, T delta,
+                                                                   T* __restrict__ w)
+{
+    __shared__ __align__(16) T stage[kCrossThreads / 32][32 * 18];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t step = int64_t(gridDim.x) * kCrossThreads;
+    for (int64_t base = int64_t(blockIdx.x) * kCrossThreads; base < C; base += step)
+    {
+        const int64_t c = base + threadIdx.x;
+        T W[18];
+#pragma unroll
+        for (int k = 0; k < 18; ++k)
+            W[k] = T(0);
+        if (c < C)
+        {
+            for (int q = cross_run[c]; q < cross_run[c + 1]; ++q)
+            {
+                const int64_t i = static_cast<uint32_t>(keys[q]);
+                T r[2], Jp[12], Jl[6];
+                load_vec<T, 2>(res + i * 2, r);
+                load_vec<T, 12>(jp + i * 12, Jp);
+                load_vec<T, 6>(jl + i * 6, Jl);
+                const T weight = huber_weight(r, 2, delta);
+                cross63_row(W, weight, Jp, Jl);
+                cross63_row(W, weight, Jp + 6, Jl + 3);
+            }
+        }
+        T* st = stage[warp];
+        store_vec<T, 18>(st + lane * 18, W);
+        __syncwarp();
+        // the warp's rows [c0, c0 + n) are contiguous in W
+        const int64_t c0 = base + warp * 32;
+        const int n = c0 < C ? static_cast<int>(C - c0 < 32 ? C - c0 : 32) : 0;
+        constexpr int kPer = 16 / sizeof(T); // scalars per 16-byte piece
+        for (int piece = lane; piece < n * 18 / kPer; piece += 32)
+        {
+            if constexpr (sizeof(T) == 8)
+                reinterpret_cast<double2*>(w + c0 * 18)[piece] = reinterpret_cast<const double2*>(st)[piece];
+            else
+                reinterpret_cast<float4*>(w + c0 * 18)[piece] = reinterpret_cast<const float4*>(st)[piece];
+        }
+        if constexpr (sizeof(T) == 4)
+        {
+            // a float row is 72 bytes: an odd row count leaves one 8-byte tail
+            if (lane == 0 && (n * 18) % kPer != 0)
+                reinterpret_cast<float2*>(w + c0 * 18)[(n * 18) / 2 - 1] =
+                    reinterpret_cast<const float2*>(st)[(n * 18) / 2 - 1];
+        }
+        __syncwarp();
+    }
+}
+
 // Per primary block (6x6): Hpp and g_p over its observations.  Warp w of the block owns a
 // contiguous slice of the primary's observation list (a multiple of 32 long) and lane j of it the
 // observations lo_w + j, lo_w + j + 32, ...; every lane sums its 42 terms serially, the lanes of a
 // warp are combined by a fixed xor-shuffle tree and the warps in warp order.  The reduction tree
 // depends only on the list length, never on scheduling.
-template <typename T>
+// M == 2: two-row residuals read in pairs of scalars, Huber weight evaluated inline (weights
+// unused); M == 0: any residual size m, weights precomputed.
+template <typename T, int M>
 __global__ void __launch_bounds__(128) primary_accumulate6_kernel(CooView v, int m, const T* __restrict__ jp,
-                                                                  const T* __restrict__ res,
+                                                                  const T* __restrict__ res, T delta,
                                                                   const T* __restrict__ weights, T* __restrict__ hpp,
                                                                   T* __restrict__ gp)
 {
@@ -341,25 +502,22 @@ __global__ void __launch_bounds__(128) primary_accumulate6_kernel(CooView v, int
         for (int q = lo + lane; q < hi; q += 32)
         {
             const int64_t i = static_cast<uint32_t>(v.keys[q]);
-            const T weight = weights[i];
-            const T* r = res + i * m;
-            const T* J = jp + i * m * 6;
-            for (int row = 0; row < m; ++row)
+            if constexpr (M == 2)
             {
-                T jrow[6];
-#pragma unroll
-                for (int c = 0; c < 6; ++c)
-                    jrow[c] = J[row * 6 + c];
-                const T rr = r[row];
-#pragma unroll
-                for (int c = 0; c < 6; ++c)
-                {
-                    const T wv = mul_rn(weight, jrow[c]);
-                    sum[36 + c] = add_rn(sum[36 + c], mul_rn(wv, rr));
-#pragma unroll
-                    for (int o = 0; o < 6; ++o)
-                        sum[c * 6 + o] = add_rn(sum[c * 6 + o], mul_rn(wv, jrow[o]));
-                }
+                T r[2], J[12];
+                load_vec<T, 2>(res + i * 2, r);
+                load_vec<T, 12>(jp + i * 12, J);
+                const T weight = huber_weight(r, 2, delta);
+                primary6_row(sum, weight, J, r[0]);
+                primary6_row(sum, weight, J + 6, r[1]);
+            }
+            else
+            {
+                const T weight = weights[i];
+                const T* r = res + i * m;
+                const T* J = jp + i * m * 6;
+                for (int row = 0; row < m; ++row)
+                    primary6_row(sum, weight, J + row * 6, r[row]);
             }
         }
 #pragma unroll
@@ -640,6 +798,7 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
             cross_owner_kernel<<<grid_for(ne->L, 256, 4096), 256, 0, stream>>>(ne->cross_offsets, ne->L,
                                                                                ne->cross_eliminated);
             PM_LAUNCH_CHECK();
+
         }
         else
         {
@@ -667,17 +826,36 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
     T* hpp = static_cast<T*>(ne->primary_diagonal);
     T* gp = static_cast<T*>(ne->primary_gradient);
     const int bp = static_cast<int>(ne->bp), bl = static_cast<int>(ne->bl), mm = static_cast<int>(m);
-    ne->weights.ensure(size_t(count + 1) * sizeof(T) + 256, stream, "normal equations");
-    T* weights = static_cast<T*>(ne->weights.ptr);
-    if (count > 0)
+    // two-row residuals with pair-aligned rows: weights inline, rows read in pairs of scalars
+    const auto paired = [](const void* ptr) { return reinterpret_cast<uintptr_t>(ptr) % (2 * sizeof(T)) == 0; };
+    const bool rows2 = mm == 2 && bp == 6 && bl == 3 && paired(jp) && paired(jl) && paired(res) && paired(w);
+    T* weights = nullptr;
+    if (!rows2)
     {
-        huber_weights_kernel<T><<<grid_for(count, 256, 1 << 20), 256, 0, stream>>>(count, mm, res, delta, weights);
-        PM_LAUNCH_CHECK();
+        ne->weights.ensure(size_t(count + 1) * sizeof(T) + 256, stream, "normal equations");
+        weights = static_cast<T*>(ne->weights.ptr);
+        if (count > 0)
+        {
+            huber_weights_kernel<T><<<grid_for(count, 256, 1 << 20), 256, 0, stream>>>(count, mm, res, delta, weights);
+            PM_LAUNCH_CHECK();
+        }
     }
     if (ne->L > 0)
     {
         const unsigned grid = grid_for(ne->L, 128, 1 << 20);
-        if (bp == 6 && bl == 3)
+        if (rows2)
+        {
+            eliminated3_m2_kernel<T><<<grid, 128, 0, stream>>>(coo_view(ne->by_eliminated_order), jl, res, delta, hll,
+                                                               gl);
+            PM_LAUNCH_CHECK();
+            if (ne->cross_count > 0)
+            {
+                cross63_m2_kernel<T><<<grid_for(ne->cross_count, kCrossThreads, 1 << 20), kCrossThreads, 0, stream>>>(
+                    ne->cross_count, ve.keys, static_cast<const int*>(ne->cross_runs.ptr), jp, jl, res, delta, w);
+                PM_LAUNCH_CHECK();
+            }
+        }
+        else if (bp == 6 && bl == 3)
         {
             const CooView vo = coo_view(ne->by_eliminated_order);
             eliminated_diagonal3_kernel<T><<<grid, 128, 0, stream>>>(vo, mm, jl, res, weights, hll, gl);
@@ -699,9 +877,11 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
     if (ne->P > 0)
     {
         const unsigned grid = grid_for(ne->P, 1, 1 << 20);
-        if (bp == 6)
+        if (rows2)
+            primary_accumulate6_kernel<T, 2><<<grid, 128, 0, stream>>>(vp, mm, jp, res, delta, nullptr, hpp, gp);
+        else if (bp == 6)
         {
-            primary_accumulate6_kernel<T><<<grid, 128, 0, stream>>>(vp, mm, jp, res, weights, hpp, gp);
+            primary_accumulate6_kernel<T, 0><<<grid, 128, 0, stream>>>(vp, mm, jp, res, delta, weights, hpp, gp);
         }
         else
         {

@@ -126,6 +126,46 @@ def test_observation_accumulation_matches_reference(checkers, dtype):
         assert np.abs(got[key] - ref[key]).max() <= tol * scale, key
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_repeated_pairs_and_unaligned_rows_match_reference(checkers, dtype):
+    """Crosses with several observations (the first 600 observations repeated with new values
+    and interleaved) and Jacobian / residual rows that do not start on a 16-byte boundary (the
+    generic path): eliminated, gradient and cross blocks bit-exact."""
+    base = W.small_bundle(seed=23, dtype=dtype)
+    rng = np.random.default_rng(5)
+    k = 600
+    prob = dict(base)
+    prob["obs_primary"] = np.concatenate([base["obs_primary"], base["obs_primary"][:k]])
+    prob["obs_eliminated"] = np.concatenate([base["obs_eliminated"], base["obs_eliminated"][:k]])
+    for key in ("jp", "jl", "residual"):
+        extra = rng.standard_normal(base[key][:k].shape).astype(dtype)
+        prob[key] = np.concatenate([base[key], extra])
+    order = rng.permutation(len(prob["obs_primary"]))
+    for key in ("obs_primary", "obs_eliminated", "jp", "jl", "residual"):
+        prob[key] = np.ascontiguousarray(prob[key][order])
+    ref = canonical(checkers.normal_equations_from_observations(prob, dtype=dtype).export())
+    dne = _device_from_observations(prob, dtype)
+    assert dne.counts()[0] < len(prob["obs_primary"])  # some crosses have several observations
+    got = dne.download()
+    for key in ("eliminated_diagonal", "eliminated_gradient", "adjacency_offsets", "cross_primary", "cross_values"):
+        assert np.array_equal(got[key], ref[key]), key
+
+    def shifted(a):  # same values, device row pointer one scalar past an aligned allocation
+        t = torch.zeros(a.size + 1, dtype=torch.float32 if dtype == np.float32 else torch.float64, device="cuda")
+        t[1:] = torch.as_tensor(a.reshape(-1)).cuda()
+        return t[1:].view(a.shape)
+
+    ne = SC.DeviceNormalEquations(prob["P"], prob["L"], prob["bp"], prob["bl"], dtype=dtype)
+    ne.accumulate_observations(dev(prob["obs_primary"]), dev(prob["obs_eliminated"]), shifted(prob["jp"]),
+                               shifted(prob["jl"]), shifted(prob["residual"]), prob["huber_delta"])
+    got2 = ne.download()
+    for key in ("eliminated_diagonal", "eliminated_gradient", "cross_values"):
+        assert np.array_equal(got2[key], ref[key]), key
+    tol = 1e-5 if dtype == np.float32 else 1e-12
+    for key in ("primary_diagonal", "primary_gradient"):
+        assert np.abs(got2[key] - got[key]).max() <= tol * np.abs(ref[key]).max(), key
+
+
 def _join(a, b):
     """Observations of b appended to those of a, b's eliminated blocks numbered after a's."""
     out = dict(a)
