@@ -260,6 +260,8 @@ def run_ours(args):
     # accumulation alone (for the phase table)
     ms_accum, _ = timed(lambda: ne.accumulate_observations(dev["obs_primary"], dev["obs_eliminated"], dev["jp"],
                                                            dev["jl"], dev["residual"], 1.0), args.steps)
+    # the 6x6 block-CSR SpMV of the PCG on the system the plain step assembled
+    schur_spmv = schur_spmv_leg(torch, ws, n, stream) if rank == 0 else None
     out = {}
     if rank == 0 and not args.no_extras:
         out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, mixed, n, m, net)
@@ -323,6 +325,7 @@ def run_ours(args):
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": ASSEMBLY_TRAFFIC_BYTES if L == L_FULL else None,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": assembly_bytes},
+        "schur_spmv_fp64": schur_spmv,
         "gpu_launches": launches,
         "clocks": clock,
     }
@@ -376,6 +379,46 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=Non
     return out
 
 
+def flushed_ms(torch, fn, flush, stream, reps=10):
+    """Median device time of fn() with L2 flushed before each call (CUDA events on `stream`)."""
+    times = []
+    for _ in range(reps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    return statistics.median(times)
+
+
+def same_size_read_ms(torch, nbytes, flush, stream):
+    """A plain device reduction (torch.sum) over nbytes, L2 flushed: what a streaming kernel of
+    this size reaches on this GPU (the long-copy peak needs GBs in flight)."""
+    ref = torch.ones(max(1, nbytes // 8), dtype=torch.float64, device="cuda")
+    out = torch.empty((), dtype=torch.float64, device="cuda")
+    t = flushed_ms(torch, lambda: torch.sum(ref, dim=(0,), out=out), flush, stream)
+    del ref
+    return t
+
+
+def schur_spmv_leg(torch, ws, n, stream):
+    """y = S x on the assembled 6x6 block-CSR Schur system (FP64), L2 flushed before each call."""
+    hbm, _ = peaks()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    dim, nnz, blocks = ws.dims()
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    t = flushed_ms(torch, lambda: ws.spmv(x, out=y, stream=stream), flush, stream)
+    byts = blocks * 36 * 8 + (n // 6 + 1) * 4 + blocks * 4 + 2 * n * 8
+    tr = same_size_read_ms(torch, byts, flush, stream)
+    return {"ms": round(t, 4), "GBps": round(byts / (t * 1e-3) / 1e9, 1),
+            "frac_of_hbm": round(byts / (t * 1e-3) / 1e9 / hbm, 3),
+            "same_size_read_GBps": round(byts / (tr * 1e-3) / 1e9, 1), "frac_of_same_size_read": round(tr / t, 3),
+            "algorithmic_bytes": byts, "blocks": blocks}
+
+
 def sparse_leg(torch, S, W, stream):
     """CSR SpMV and COO -> CSR of the 128^3 Laplacian (16.04M triplets), FP64 and FP32, L2 flushed
     between timed calls."""
@@ -390,21 +433,15 @@ def sparse_leg(torch, S, W, stream):
         op = S.CsrOperand(csr)
         x = torch.randn(lap["rows"], dtype=dt, device="cuda")
         y = torch.empty_like(x)
-        times = []
-        for _ in range(10):
-            flush.zero_()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            op.spmv(x, y)
-            b.record(stream)
-            torch.cuda.synchronize()
-            times.append(a.elapsed_time(b))
+        t = flushed_ms(torch, lambda: op.spmv(x, y), flush, stream)
         s = 4 if dt == torch.float32 else 8
         nn = lap["rows"]
         byts = csr.nnz * (s + 4) + (nn + 1) * 4 + 2 * nn * s
-        t = statistics.median(times)
+        tr = same_size_read_ms(torch, byts, flush, stream)
         spmv[f"csr_laplacian128_{name}"] = {"ms": round(t, 4), "GBps": round(byts / (t * 1e-3) / 1e9, 1),
                                             "frac_of_hbm": round(byts / (t * 1e-3) / 1e9 / hbm, 3),
+                                            "same_size_read_GBps": round(byts / (tr * 1e-3) / 1e9, 1),
+                                            "frac_of_same_size_read": round(tr / t, 3),
                                             "algorithmic_bytes": byts}
         # COO -> CSR of the same matrix (16.04M triplets)
         ws_coo = S.SparseOpsWorkspace()
