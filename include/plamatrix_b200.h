@@ -144,6 +144,16 @@ PM_API int pm_csr_set_values(pm_csr* matrix, const void* values_d);
 PM_API int pm_csr_spmv_f32(const pm_csr* matrix, pm_stream_t stream, const float* x_d, float* y_d);
 PM_API int pm_csr_spmv_f64(const pm_csr* matrix, pm_stream_t stream, const double* x_d, double* y_d);
 
+/* output = A input for dense matrices in column-major order (leading dimension = rows):
+ * input is input_rows x input_cols (input_rows == A's columns), output is output_rows x
+ * output_cols (A's rows x input_cols).  Replaces spmmAsync (sparse_ops.cu:762-818; the CPU order
+ * of sparse_ops_cpu.cpp:244-270): PM_RUNTIME_ERROR on a dimension mismatch,
+ * PM_INVALID_ARGUMENT when input and output alias; an empty A writes zeros. */
+PM_API int pm_csr_spmm_f32(const pm_csr* matrix, pm_stream_t stream, int64_t input_rows, int64_t input_cols,
+                           const float* input_d, int64_t output_rows, int64_t output_cols, float* output_d);
+PM_API int pm_csr_spmm_f64(const pm_csr* matrix, pm_stream_t stream, int64_t input_rows, int64_t input_cols,
+                           const double* input_d, int64_t output_rows, int64_t output_cols, double* output_d);
+
 /* =========================================================================== CG / PCG
  * Replaces cg / pcg / blockPcg on the GPU (include/plamatrix/sparse/iterative_solver.h:297-329,
  * src/sparse/iterative_solver.cu:262-402).  Dots, alpha and beta are evaluated in FP64 for

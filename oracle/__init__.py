@@ -108,6 +108,18 @@ def csr_spmv(row_offsets, cols, vals, x, impl: str = "orc"):
     return y
 
 
+def csr_spmm(row_offsets, cols, vals, n_cols, B, impl: str = "orc"):
+    """output (rows x k) = CSR x B (n_cols x k); B and output column-major (numpy order="F")."""
+    n = len(row_offsets) - 1
+    B = np.asfortranarray(B, dtype=vals.dtype)
+    k = B.shape[1]
+    out = np.zeros((n, k), dtype=vals.dtype, order="F")
+    fn = getattr(lib(impl), f"{impl}_csr_spmm_{_sfx(vals.dtype)}")
+    _check(impl, fn(C.c_int64(n), C.c_int64(n_cols), _ptr(row_offsets), _ptr(cols), _ptr(vals), C.c_int64(k),
+                    _ptr(B), _ptr(out)))
+    return out
+
+
 class SolverOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_int), ("relative_tolerance", C.c_double),
                 ("absolute_tolerance", C.c_double), ("use_jacobi", C.c_int),

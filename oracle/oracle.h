@@ -56,6 +56,14 @@ int orc_csr_spmv_f32(int64_t rows, int64_t cols, const int64_t* row_offsets, con
 int orc_csr_spmv_f64(int64_t rows, int64_t cols, const int64_t* row_offsets, const int64_t* columns,
                      const double* values, const double* x, double* y);
 
+/* ---------------------------------------------------------------- CSR SpMM
+ * Follows src/sparse/sparse_ops_cpu.cpp:244-270: output (rows x k) = CSR x input (cols x k),
+ * both dense matrices column-major. */
+int orc_csr_spmm_f32(int64_t rows, int64_t cols, const int64_t* row_offsets, const int64_t* columns,
+                     const float* values, int64_t k, const float* input, float* output);
+int orc_csr_spmm_f64(int64_t rows, int64_t cols, const int64_t* row_offsets, const int64_t* columns,
+                     const double* values, int64_t k, const double* input, double* output);
+
 /* ---------------------------------------------------------------- CG / PCG */
 typedef struct
 {

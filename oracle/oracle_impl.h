@@ -105,6 +105,32 @@ int FN(orc_csr_spmv)(int64_t rows, int64_t cols, const int64_t* row_offsets, con
     return ORC_OK;
 }
 
+/* spmm: sparse_ops_cpu.cpp:244-270; dense matrices column-major (leading dimension = rows),
+ * column by column, each row summed from zero in storage order. */
+int FN(orc_csr_spmm)(int64_t rows, int64_t cols, const int64_t* row_offsets, const int64_t* columns,
+                     const S* values, int64_t k, const S* input, S* output)
+{
+    if (input == output && input != NULL)
+    {
+        return orc_fail(ORC_INVALID_ARGUMENT, "spmm input and output data must not alias");
+    }
+    for (int64_t col = 0; col < k; ++col)
+    {
+        const S* b_column = input + col * cols;
+        S* out_column = output + col * rows;
+        for (int64_t row = 0; row < rows; ++row)
+        {
+            S sum = (S)0;
+            for (int64_t position = row_offsets[row]; position < row_offsets[row + 1]; ++position)
+            {
+                sum += values[position] * b_column[columns[position]];
+            }
+            out_column[row] = sum;
+        }
+    }
+    return ORC_OK;
+}
+
 /* ===================================================================== CG / PCG
  * iterative_solver_cpu.cpp:15-284 (validateOptions, validateSystem, jacobiInverse, solve). */
 static double FN(orc_dot64)(int64_t n, const double* a, const double* b)

@@ -123,6 +123,18 @@ int spmvImpl(int64_t n, int64_t cols, const int64_t* rp, const int64_t* ci, cons
     });
 }
 
+template <typename S>
+int spmmImpl(int64_t n, int64_t cols, const int64_t* rp, const int64_t* ci, const S* v, int64_t k, const S* in, S* out)
+{
+    return guarded([&] {
+        auto csr = makeCsr(n, rp, ci, v, cols);
+        plamatrix::DenseMatrix<S, plamatrix::Device::CPU> b(cols, k), c(n, k);
+        std::memcpy(b.data(), in, sizeof(S) * static_cast<size_t>(cols * k));
+        plamatrix::spmm(csr, b, c);
+        std::memcpy(out, c.data(), sizeof(S) * static_cast<size_t>(n * k));
+    });
+}
+
 struct SolverOptionsC
 {
     int max_iterations;
@@ -415,6 +427,16 @@ int ref_csr_spmv_f64(int64_t n, int64_t cols, const int64_t* rp, const int64_t* 
                      const double* x, double* y)
 {
     return spmvImpl(n, cols, rp, ci, v, x, y);
+}
+int ref_csr_spmm_f32(int64_t n, int64_t cols, const int64_t* rp, const int64_t* ci, const float* v, int64_t k,
+                     const float* in, float* out)
+{
+    return spmmImpl(n, cols, rp, ci, v, k, in, out);
+}
+int ref_csr_spmm_f64(int64_t n, int64_t cols, const int64_t* rp, const int64_t* ci, const double* v, int64_t k,
+                     const double* in, double* out)
+{
+    return spmmImpl(n, cols, rp, ci, v, k, in, out);
 }
 int ref_pcg_f32(int64_t n, const int64_t* rp, const int64_t* ci, const float* v, const float* rhs, float* x,
                 const SolverOptionsC* o, int preconditioned, SolverReportC* r)

@@ -687,6 +687,131 @@ void csr_spmv(const pm_csr* A, cudaStream_t stream, const T* x, T* y)
     launch_spmv<T>(A, x, y, stream);
 }
 
+// ------------------------------------------------------------------ SpMM
+// output (rows x k) = A input (cols x k), dense matrices column-major (leading dimension = rows).
+// A warp owns 32 consecutive rows; their nonzero range is staged in shared memory in pieces of
+// kStreamCap (columns, values, coalesced) and lane i forms row i of up to kSpmmCols output
+// columns at a time, each sum from zero in storage order with one rounded multiply and one
+// rounded add per term (the reference CPU spmm, sparse_ops_cpu.cpp:244-270).
+constexpr int kSpmmCols = 8;
+
+template <typename T>
+__device__ __forceinline__ T mul_round(T a, T b)
+{
+    if constexpr (sizeof(T) == 8)
+        return __dmul_rn(a, b);
+    else
+        return __fmul_rn(a, b);
+}
+template <typename T>
+__device__ __forceinline__ T add_round(T a, T b)
+{
+    if constexpr (sizeof(T) == 8)
+        return __dadd_rn(a, b);
+    else
+        return __fadd_rn(a, b);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) csr_spmm_kernel(int64_t rows, int64_t cols, int64_t k,
+                                                       const int* __restrict__ rp, const int* __restrict__ ci,
+                                                       const T* __restrict__ v, const T* __restrict__ in,
+                                                       T* __restrict__ out)
+{
+    __shared__ int scol[8][kStreamCap];
+    __shared__ T sval[8][kStreamCap];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t warps = int64_t(gridDim.x) * 8;
+    for (int64_t wrow = (int64_t(blockIdx.x) * 8 + warp) * 32; wrow < rows; wrow += warps * 32)
+    {
+        const int64_t row = wrow + lane;
+        const bool valid = row < rows;
+        const int my_begin = valid ? rp[row] : 0;
+        const int my_end = valid ? rp[row + 1] : 0;
+        const int last = static_cast<int>(rows - 1 - wrow < 31 ? rows - 1 - wrow : 31);
+        const int cb = __shfl_sync(0xffffffffu, my_begin, 0);
+        const int ce = __shfl_sync(0xffffffffu, my_end, last);
+        for (int64_t j0 = 0; j0 < k; j0 += kSpmmCols)
+        {
+            const int nj = k - j0 < kSpmmCols ? static_cast<int>(k - j0) : kSpmmCols;
+            T sum[kSpmmCols];
+#pragma unroll
+            for (int j = 0; j < kSpmmCols; ++j)
+                sum[j] = T(0);
+            for (int base = cb; base < ce; base += kStreamCap)
+            {
+                const int n = ce - base < kStreamCap ? ce - base : kStreamCap;
+                for (int e = lane; e < n; e += 32)
+                {
+                    scol[warp][e] = __ldg(ci + base + e);
+                    sval[warp][e] = __ldg(v + base + e);
+                }
+                __syncwarp();
+                const int lo = my_begin > base ? my_begin : base;
+                const int hi = my_end < base + n ? my_end : base + n;
+                for (int e = lo; e < hi; ++e)
+                {
+                    const T a = sval[warp][e - base];
+                    const T* b = in + scol[warp][e - base];
+#pragma unroll
+                    for (int j = 0; j < kSpmmCols; ++j)
+                        if (j < nj)
+                            sum[j] = add_round(sum[j], mul_round(a, __ldg(b + (j0 + j) * cols)));
+                }
+                __syncwarp();
+            }
+            if (valid)
+            {
+#pragma unroll
+                for (int j = 0; j < kSpmmCols; ++j)
+                    if (j < nj)
+                        out[(j0 + j) * rows + row] = sum[j];
+            }
+        }
+    }
+}
+
+template <typename T>
+void csr_spmm(const pm_csr* A, cudaStream_t stream, int64_t in_rows, int64_t in_cols, const T* in, int64_t out_rows,
+              int64_t out_cols, T* out)
+{
+    if (!A)
+        fail(PM_INVALID_ARGUMENT, "CSR handle is null");
+    if (A->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "spmm scalar type differs from the CSR operand");
+    if (in_rows < 0 || in_cols < 0 || out_rows < 0 || out_cols < 0)
+        fail(PM_INVALID_ARGUMENT, "spmm dimensions must be non-negative");
+    if (in_rows != A->cols)
+    {
+        std::ostringstream m;
+        m << "spmm GPU dimension mismatch: CSR is " << A->rows << "x" << A->cols << ", input is " << in_rows << "x"
+          << in_cols;
+        fail(PM_RUNTIME_ERROR, m.str());
+    }
+    if (out_rows != A->rows || out_cols != in_cols)
+    {
+        std::ostringstream m;
+        m << "spmm GPU output dimension mismatch: output is " << out_rows << "x" << out_cols << ", expected "
+          << A->rows << "x" << in_cols;
+        fail(PM_RUNTIME_ERROR, m.str());
+    }
+    if (in && in == out)
+        fail(PM_INVALID_ARGUMENT, "spmm GPU input and output data must not alias");
+    if (out_rows * out_cols == 0)
+        return;
+    if (!out || (A->nnz > 0 && !in))
+        fail(PM_INVALID_ARGUMENT, "spmm matrices must be non-null");
+    if (A->nnz == 0)
+    {
+        PM_CUDA(cudaMemsetAsync(out, 0, size_t(out_rows * out_cols) * sizeof(T), stream));
+        return;
+    }
+    csr_spmm_kernel<T><<<grid_for(A->rows, 256, 1 << 20), 256, 0, stream>>>(A->rows, A->cols, in_cols, A->row_ptr,
+                                                                             A->col_idx, static_cast<const T*>(A->values),
+                                                                             in, out);
+    PM_LAUNCH_CHECK();
+}
+
 template <typename T>
 void launch_pcg_spmv(const pm_csr* A, const T* p, T* q, double* partials, PcgState* st, unsigned grid,
                      cudaStream_t stream)
@@ -1026,6 +1151,19 @@ int pm_csr_spmv_f32(const pm_csr* A, pm_stream_t stream, const float* x, float* 
 int pm_csr_spmv_f64(const pm_csr* A, pm_stream_t stream, const double* x, double* y)
 {
     return pm::guarded([&] { pm::csr_spmv<double>(A, stream, x, y); });
+}
+
+int pm_csr_spmm_f32(const pm_csr* A, pm_stream_t stream, int64_t input_rows, int64_t input_cols, const float* input,
+                    int64_t output_rows, int64_t output_cols, float* output)
+{
+    return pm::guarded(
+        [&] { pm::csr_spmm<float>(A, stream, input_rows, input_cols, input, output_rows, output_cols, output); });
+}
+int pm_csr_spmm_f64(const pm_csr* A, pm_stream_t stream, int64_t input_rows, int64_t input_cols, const double* input,
+                    int64_t output_rows, int64_t output_cols, double* output)
+{
+    return pm::guarded(
+        [&] { pm::csr_spmm<double>(A, stream, input_rows, input_cols, input, output_rows, output_cols, output); });
 }
 
 int pm_solver_workspace_create(pm_solver_workspace** out)

@@ -168,6 +168,20 @@ class CsrOperand:
         N.call(f"pm_csr_spmv_{self.sfx}", self._h, _stream_handle(stream), _ptr(x), _ptr(y))
         return y
 
+    def spmm(self, B: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        """out = A B for column-major dense matrices (spmmAsync, sparse_ops.cu:762-818): B is
+        (cols x k) and out (rows x k), each with strides (1, its row count), e.g.
+        `dense_matrix(rows, k)`."""
+        if B.dim() != 2 or out is not None and out.dim() != 2:
+            raise N.InvalidArgument("spmm operands must be 2-D column-major tensors")
+        y = dense_matrix(self.matrix.rows, B.shape[1], B.dtype, B.device) if out is None else out
+        for name, t in (("input", B), ("output", y)):
+            if t.numel() > 0 and t.shape[1] > 1 and t.stride() != (1, t.shape[0]):
+                raise N.InvalidArgument(f"spmm {name} must be column-major (strides (1, rows))")
+        N.call(f"pm_csr_spmm_{self.sfx}", self._h, _stream_handle(stream), B.shape[0], B.shape[1], _ptr(B),
+               y.shape[0], y.shape[1], _ptr(y))
+        return y
+
     def __del__(self):
         h = getattr(self, "_h", None)
         try:
@@ -176,6 +190,16 @@ class CsrOperand:
         except (AttributeError, TypeError):  # interpreter shutdown
             pass
         self._h = None
+
+
+def dense_matrix(rows: int, cols: int, dtype=torch.float64, device="cuda") -> torch.Tensor:
+    """A (rows x cols) column-major device matrix, the reference's DenseMatrix layout."""
+    return torch.empty((cols, rows), dtype=dtype, device=device).t()
+
+
+def spmm(matrix, B: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+    op = matrix if isinstance(matrix, CsrOperand) else CsrOperand(matrix, stream)
+    return op.spmm(B, out, stream)
 
 
 def spmv(matrix, x: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
@@ -253,6 +277,9 @@ for _suffix in ("f32", "f64"):
         N.register(f"pm_{_kind}_fixed_iterations_async_{_suffix}",
                    [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p])
 N.register("pm_fixed_state_finalize", [C.c_void_p, C.c_void_p, C.c_void_p])
+for _suffix in ("f32", "f64"):
+    N.register(f"pm_csr_spmm_{_suffix}", [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64,
+                                          C.c_int64, C.c_void_p])
 N.register("pm_fixed_state_destroy", [C.c_void_p], None)
 
 

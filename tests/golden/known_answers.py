@@ -56,6 +56,19 @@ SPMV_CASES = [
     },
 ]
 
+# dense matrices column-major: "B" and "out" list their columns
+SPMM_CASES = [
+    {   # test/unit/sparse/sparse_ops_test.cpp:196-233 and :704-735 (GPU)
+        "dtype": np.float64, "rows": 3, "cols": 3, "r": [1, 0, 2, 0], "c": [1, 2, 0, 0],
+        "v": [4.0, 2.0, -1.0, 3.0], "B": [[1.0, 2.0, 3.0], [10.0, 20.0, 30.0]],
+        "out": [[9.0, 8.0, -1.0], [90.0, 80.0, -10.0]],
+    },
+    {   # test/unit/sparse/sparse_ops_test.cpp:737-760 (GPU, synchronous spmm)
+        "dtype": np.float32, "rows": 2, "cols": 2, "r": [0, 1], "c": [0, 1], "v": [2.0, 3.0],
+        "B": [[4.0, 5.0], [6.0, 7.0]], "out": [[8.0, 15.0], [12.0, 21.0]],
+    },
+]
+
 # ------------------------------------------------------------------ iterative solvers
 # test/unit/sparse/iterative_solver_test.cpp:103-123: diagonal PCG converges in one iteration
 DIAGONAL_PCG = {"r": [0, 1, 2], "c": [0, 1, 2], "v": [2.0, 4.0, 8.0], "rhs": [2.0, 8.0, 24.0],

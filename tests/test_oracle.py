@@ -55,6 +55,29 @@ def test_spmv_known_answers(checkers, case):
         assert y.tolist() == case["y"]
 
 
+@pytest.mark.parametrize("case", KA.SPMM_CASES)
+def test_spmm_known_answers(checkers, case):
+    for impl in _impls(checkers):
+        ro, ci, v = checkers.coo_to_csr(case["rows"], case["cols"], case["r"], case["c"],
+                                        np.array(case["v"], case["dtype"]), impl=impl)
+        B = np.array(case["B"], case["dtype"]).T
+        out = checkers.csr_spmm(ro, ci, v, case["cols"], B, impl=impl)
+        assert out.T.tolist() == case["out"]
+
+
+def test_spmm_matches_reference_bitwise(checkers):
+    if not checkers.available("ref"):
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(8)
+    for dtype in (np.float32, np.float64):
+        r, c = rng.integers(0, 200, 3000), rng.integers(0, 150, 3000)
+        ro, ci, v = checkers.coo_to_csr(200, 150, r, c, rng.standard_normal(3000).astype(dtype))
+        B = rng.standard_normal((150, 5)).astype(dtype)
+        a = checkers.csr_spmm(ro, ci, v, 150, B, impl="orc")
+        b = checkers.csr_spmm(ro, ci, v, 150, B, impl="ref")
+        assert np.array_equal(np.ascontiguousarray(a).view(np.uint8), np.ascontiguousarray(b).view(np.uint8))
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_pcg_diagonal_and_poisson(checkers, dtype):
     tol = 2e-4 if dtype == np.float32 else 1e-10

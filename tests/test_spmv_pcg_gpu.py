@@ -24,6 +24,60 @@ def test_spmv_known_answers(checkers, case):
     assert host(y).tolist() == case["y"]
 
 
+@pytest.mark.parametrize("case", KA.SPMM_CASES)
+def test_spmm_known_answers(checkers, case):
+    A, _ = _csr(checkers, case["rows"], case["cols"], case["r"], case["c"], case["v"], case["dtype"])
+    tdt = torch.float32 if case["dtype"] == np.float32 else torch.float64
+    B = S.dense_matrix(case["cols"], len(case["B"]), tdt)
+    B.copy_(torch.as_tensor(np.array(case["B"], case["dtype"]).T))
+    out = S.dense_matrix(case["rows"], len(case["B"]), tdt)
+    out.fill_(-100.0)
+    got = S.spmm(A, B, out)
+    assert got.data_ptr() == out.data_ptr()
+    assert host(got.t().contiguous()).tolist() == case["out"]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("mean", [1, 7, 300])
+def test_spmm_random_matches_oracle_bitwise(checkers, dtype, mean):
+    """Row sums in storage order with rounded products: bit-exact with the CPU order, for
+    short rows, long rows (several staged pieces) and 1, 8 and 11 columns."""
+    rng = np.random.default_rng(mean)
+    rows, cols = 700, 500
+    r, c = rng.integers(0, rows, rows * mean), rng.integers(0, cols, rows * mean)
+    A, (ro, ci, vv) = _csr(checkers, rows, cols, r, c, rng.standard_normal(rows * mean), dtype)
+    op = S.CsrOperand(A)
+    tdt = torch.float32 if dtype == np.float32 else torch.float64
+    for k in (1, 8, 11):
+        Bh = rng.standard_normal((cols, k)).astype(dtype)
+        B = S.dense_matrix(cols, k, tdt)
+        B.copy_(torch.as_tensor(Bh))
+        got = host(op.spmm(B).t().contiguous()).T
+        ref = checkers.csr_spmm(ro, ci, vv, cols, Bh)
+        assert np.array_equal(np.ascontiguousarray(got.astype(dtype)).view(np.uint8),
+                              np.ascontiguousarray(ref).view(np.uint8))
+
+
+def test_spmm_errors_and_empty(checkers):
+    A, _ = _csr(checkers, 3, 3, [0, 1], [0, 1], [2.0, 3.0], np.float64)
+    op = S.CsrOperand(A)
+    with pytest.raises(N.PlamatrixError, match="dimension mismatch"):
+        op.spmm(S.dense_matrix(2, 2))
+    with pytest.raises(N.PlamatrixError, match="output dimension mismatch"):
+        op.spmm(S.dense_matrix(3, 2), out=S.dense_matrix(1, 2))
+    B = S.dense_matrix(3, 3)
+    with pytest.raises(N.InvalidArgument):
+        op.spmm(B, out=B)
+    empty, _ = _csr(checkers, 0, 3, [], [], [], np.float64)
+    assert S.spmm(empty, S.dense_matrix(3, 2)).shape == (0, 2)
+    zero, _ = _csr(checkers, 2, 3, [], [], [], np.float64)
+    ones = S.dense_matrix(3, 2)
+    ones.fill_(1.0)
+    out = S.dense_matrix(2, 2)
+    out.fill_(5.0)
+    assert torch.count_nonzero(S.spmm(zero, ones, out)).item() == 0
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 @pytest.mark.parametrize("mean", [1, 3, 7, 30, 200])
 def test_spmv_random_against_oracle(checkers, dtype, mean):
