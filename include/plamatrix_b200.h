@@ -284,6 +284,11 @@ PM_API int pm_ne_accumulate_observations_f64(pm_normal_equations* equations, pm_
                                              const int64_t* obs_eliminated_d, const double* primary_jacobians_d,
                                              const double* eliminated_jacobians_d, const double* residuals_d,
                                              double huber_delta);
+/* Synchronous check of the last accumulation: PM_INVALID_ARGUMENT when an observation's squared
+ * residual norm was not finite, which evaluateHuberLoss rejects (robust_loss.h:31-35);
+ * *first_bad_h receives the first such observation index, or -1.  The accumulation itself
+ * stays asynchronous; pm_schur_solve_* reports the same error from its own status read. */
+PM_API int pm_ne_check_observations(const pm_normal_equations* equations, pm_stream_t stream, int64_t* first_bad_h);
 
 /* =========================================================================== damped Schur solve
  * Replaces solveDampedSchurComplement (include/plamatrix/optimization/block_schur.h:171-186,
@@ -415,6 +420,43 @@ PM_API int pm_mlp_train_step(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stre
                              const double* b_d, double learning_rate, double* loss);
 /* Host copies of the last features (P x 25), outputs (P x 21) and gradients; any may be NULL. */
 PM_API int pm_mlp_inspect(const pm_mlp* mlp, int64_t* rows, float* features, float* outputs, float* gradients);
+
+/* =========================================================================== LM loop (caller side)
+ * Replaces LevenbergMarquardtOptions / LevenbergMarquardtStrategy
+ * (include/plamatrix/optimization/levenberg_marquardt.h:13-95): host state, the damping updated in
+ * the strategy's scalar type (f32 / f64 as the template argument).  create returns
+ * PM_INVALID_ARGUMENT ("LevenbergMarquardtStrategy: invalid damping options") for bounds or
+ * factors the reference rejects; options == NULL takes the defaults. */
+typedef struct
+{
+    double initial_damping; /* 1e-3 */
+    double minimum_damping; /* 1e-12 */
+    double maximum_damping; /* 1e12 */
+    double decrease_factor; /* 0.3, after an accepted step */
+    double increase_factor; /* 10, after a rejected or invalid step */
+} pm_lm_options;
+typedef struct pm_lm_strategy pm_lm_strategy;
+PM_API void pm_lm_options_default(pm_lm_options* options);
+PM_API int pm_lm_strategy_create_f32(const pm_lm_options* options, pm_lm_strategy** out);
+PM_API int pm_lm_strategy_create_f64(const pm_lm_options* options, pm_lm_strategy** out);
+PM_API void pm_lm_strategy_destroy(pm_lm_strategy* strategy);
+PM_API int pm_lm_accept_step(pm_lm_strategy* strategy);
+PM_API int pm_lm_reject_step(pm_lm_strategy* strategy);
+PM_API int pm_lm_strategy_state(const pm_lm_strategy* strategy, double* damping_h, int* accepted_steps_h,
+                                int* rejected_steps_h);
+
+/* Total robust cost sum_i evaluateHuberLoss(|r_i|^2, delta).cost of `count` residuals of size m
+ * (residual_d: count x m, row-major), written to *cost_d (device, FP64) -- the cost an LM loop
+ * compares between trial steps (robust_loss.h:27-51 per residual, summed by the caller in the
+ * reference).  Per-residual costs are exact in the residual's type; the FP64 sum uses a fixed
+ * tree, so results repeat bit for bit.  A residual whose squared norm is not finite makes the
+ * total non-finite (evaluateHuberLoss rejects it; an LM caller rejects the step).  scratch_d
+ * holds PM_HUBER_COST_SCRATCH doubles of caller-owned device memory. */
+#define PM_HUBER_COST_SCRATCH 1024
+PM_API int pm_huber_cost_f32(pm_stream_t stream, int64_t count, int64_t m, const float* residual_d, float delta,
+                             double* scratch_d, double* cost_d);
+PM_API int pm_huber_cost_f64(pm_stream_t stream, int64_t count, int64_t m, const double* residual_d, double delta,
+                             double* scratch_d, double* cost_d);
 
 #ifdef __cplusplus
 }

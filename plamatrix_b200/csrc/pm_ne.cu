@@ -30,6 +30,7 @@ pm_normal_equations::~pm_normal_equations()
     if (by_eliminated_order)
         pm_sparse_workspace_destroy(by_eliminated_order);
     cross_runs.release();
+    observation_status.release();
 }
 
 namespace pm
@@ -122,14 +123,35 @@ __global__ void compare_kernel(const int64_t* __restrict__ a, const int64_t* __r
 }
 
 template <typename T>
-__device__ __forceinline__ T huber_weight(const T* r, int m, T delta)
+__device__ __forceinline__ T squared_norm(const T* r, int m)
 {
     T squared = T(0);
     for (int k = 0; k < m; ++k)
         squared = add_rn(squared, mul_rn(r[k], r[k]));
+    return squared;
+}
+
+template <typename T>
+__device__ __forceinline__ T huber_weight_of(T squared, T delta)
+{
     if (delta == T(0) || squared <= mul_rn(delta, delta))
         return T(1);
     return delta / sqrt(squared);
+}
+
+template <typename T>
+__device__ __forceinline__ T huber_weight(const T* r, int m, T delta)
+{
+    return huber_weight_of(squared_norm(r, m), delta);
+}
+
+// evaluateHuberLoss rejects a squared residual norm that is not finite (robust_loss.h:31-35):
+// the device path records the first such observation for the host to report
+template <typename T>
+__device__ __forceinline__ void note_nonfinite(T squared, int64_t i, long long* first_bad)
+{
+    if (!isfinite(squared))
+        atomicMin(first_bad, static_cast<long long>(i));
 }
 
 // One residual row's terms, each `weight * value * jacobian` as two rounded multiplies and a
@@ -219,10 +241,15 @@ __device__ __forceinline__ void store_vec(T* __restrict__ p, const T* in)
 
 // Huber weight of every observation (one thread each, coalesced residual reads).
 template <typename T>
-__global__ void huber_weights_kernel(int64_t count, int m, const T* __restrict__ res, T delta, T* __restrict__ weight)
+__global__ void huber_weights_kernel(int64_t count, int m, const T* __restrict__ res, T delta, T* __restrict__ weight,
+                                     long long* first_bad)
 {
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += int64_t(gridDim.x) * blockDim.x)
-        weight[i] = huber_weight(res + i * m, m, delta);
+    {
+        const T squared = squared_norm(res + i * m, m);
+        note_nonfinite(squared, i, first_bad);
+        weight[i] = huber_weight_of(squared, delta);
+    }
 }
 
 // Per eliminated block, any block sizes up to 16: the same sums as the fixed-size kernel below,
@@ -375,7 +402,7 @@ __global__ void __launch_bounds__(128) cross_accumulate63_kernel(int64_t C, cons
 template <typename T>
 __global__ void __launch_bounds__(128) eliminated3_m2_kernel(CooView vo, const T* __restrict__ jl,
                                                              const T* __restrict__ res, T delta, T* __restrict__ hll,
-                                                             T* __restrict__ gl)
+                                                             T* __restrict__ gl, long long* first_bad)
 {
     for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < vo.rows; l += int64_t(gridDim.x) * blockDim.x)
     {
@@ -397,7 +424,9 @@ __global__ void __launch_bounds__(128) eliminated3_m2_kernel(CooView vo, const T
             T r[2], J[6];
             load_vec<T, 2>(res + i * 2, r);
             load_vec<T, 6>(jl + i * 6, J);
-            const T weight = huber_weight(r, 2, delta);
+            const T squared = squared_norm(r, 2);
+            note_nonfinite(squared, i, first_bad);
+            const T weight = huber_weight_of(squared, delta);
             eliminated3_row(H, g, weight, J, r[0]);
             eliminated3_row(H, g, weight, J + 3, r[1]);
         }
@@ -610,6 +639,8 @@ void ne_upload(pm_normal_equations* ne, cudaStream_t stream, const T* hpp, const
         fail(PM_INVALID_ARGUMENT, "normal equations scalar type mismatch");
     if (C < 0 || PC < 0 || C > INT32_MAX - 1 || PC > INT32_MAX - 1)
         fail(PM_INVALID_ARGUMENT, "invalid cross block counts");
+    if (ne->observation_status.ptr) // uploaded state carries no observations
+        PM_CUDA(cudaMemsetAsync(ne->observation_status.ptr, 0x7f, sizeof(long long), stream));
     // host-side topology validation (the reference rejects these at accumulation time)
     if (ne->L > 0 && (!cross_offsets || cross_offsets[0] != 0 || cross_offsets[ne->L] != C))
         fail(PM_INVALID_ARGUMENT, "cross offsets must start at zero and end at the cross count");
@@ -826,6 +857,10 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
     T* hpp = static_cast<T*>(ne->primary_diagonal);
     T* gp = static_cast<T*>(ne->primary_gradient);
     const int bp = static_cast<int>(ne->bp), bl = static_cast<int>(ne->bl), mm = static_cast<int>(m);
+    // first observation with a non-finite squared residual norm (none: every byte 0x7f)
+    ne->observation_status.ensure(256, stream, "normal equations");
+    long long* first_bad = static_cast<long long*>(ne->observation_status.ptr);
+    PM_CUDA(cudaMemsetAsync(first_bad, 0x7f, sizeof(long long), stream));
     // two-row residuals with pair-aligned rows: weights inline, rows read in pairs of scalars
     const auto paired = [](const void* ptr) { return reinterpret_cast<uintptr_t>(ptr) % (2 * sizeof(T)) == 0; };
     const bool rows2 = mm == 2 && bp == 6 && bl == 3 && paired(jp) && paired(jl) && paired(res) && paired(w);
@@ -836,7 +871,8 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
         weights = static_cast<T*>(ne->weights.ptr);
         if (count > 0)
         {
-            huber_weights_kernel<T><<<grid_for(count, 256, 1 << 20), 256, 0, stream>>>(count, mm, res, delta, weights);
+            huber_weights_kernel<T><<<grid_for(count, 256, 1 << 20), 256, 0, stream>>>(count, mm, res, delta, weights,
+                                                                                         first_bad);
             PM_LAUNCH_CHECK();
         }
     }
@@ -846,7 +882,7 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
         if (rows2)
         {
             eliminated3_m2_kernel<T><<<grid, 128, 0, stream>>>(coo_view(ne->by_eliminated_order), jl, res, delta, hll,
-                                                               gl);
+                                                               gl, first_bad);
             PM_LAUNCH_CHECK();
             if (ne->cross_count > 0)
             {
@@ -902,6 +938,27 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
 } // namespace pm
 
 extern "C" {
+
+int pm_ne_check_observations(const pm_normal_equations* ne, pm_stream_t stream, int64_t* first_bad)
+{
+    return pm::guarded([&] {
+        if (!ne)
+            pm::fail(PM_INVALID_ARGUMENT, "normal equations handle is null");
+        long long bad = -1;
+        if (ne->observation_status.ptr)
+        {
+            PM_CUDA(cudaMemcpyAsync(&bad, ne->observation_status.ptr, sizeof(long long), cudaMemcpyDeviceToHost, stream));
+            PM_CUDA(cudaStreamSynchronize(stream));
+            if (bad < 0 || bad >= ne->observation_count)
+                bad = -1;
+        }
+        if (first_bad)
+            *first_bad = bad;
+        if (bad >= 0)
+            pm::fail(PM_INVALID_ARGUMENT, "evaluateHuberLoss: squared residual norm must be finite and non-negative "
+                                          "(observation " + std::to_string(bad) + ")");
+    });
+}
 
 int pm_ne_create(int64_t P, int64_t L, int64_t bp, int64_t bl, int value_size, pm_normal_equations** out)
 {

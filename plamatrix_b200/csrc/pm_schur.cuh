@@ -35,6 +35,7 @@ struct pm_normal_equations
     pm::DeviceBuffer cross_runs;                  // C + 1: first by_eliminated position of every cross
     pm::DeviceBuffer observation_copy;            // saved index arrays + zero column
     pm::DeviceBuffer weights;                     // Huber weight of every observation
+    pm::DeviceBuffer observation_status;          // long long: first observation with a non-finite squared norm
     int64_t observation_count = -1;
     int64_t residual_size = 0;
     bool observation_topology = false;

@@ -42,6 +42,7 @@ struct SchurStatus
     long long preconditioner_bad;
     long long row_too_wide;
     int pad[2]; // pad[1]: scratch flag of the topology comparison
+    long long observation_bad; // the normal equations' first observation with a non-finite residual norm
 };
 
 struct SolveState // device-side PCG / refinement scalars
@@ -144,6 +145,7 @@ __global__ void status_reset_kernel(SchurStatus* s)
     s->preconditioner_bad = kNone;
     s->row_too_wide = kNone;
     s->pad[0] = 0;
+    s->observation_bad = kNone;
 }
 
 __global__ void widen_int_kernel(const int* __restrict__ in, int64_t* __restrict__ out, int64_t n)
@@ -2486,6 +2488,9 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     // ---- eliminated inverses
     status_reset_kernel<<<1, 1, 0, stream>>>(ws->status);
     PM_LAUNCH_CHECK();
+    if (ne->observation_status.ptr)
+        PM_CUDA(cudaMemcpyAsync(&ws->status->observation_bad, ne->observation_status.ptr, sizeof(long long),
+                                cudaMemcpyDeviceToDevice, stream));
     if (L > 0)
     {
         const unsigned grid = grid_for(L, 128, 1 << 20);
@@ -2542,6 +2547,14 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         cudaEventElapsedTime(&t, ws->events[0], ws->events[last]);
         rep->total_ms = t;
     };
+    {
+        // the accumulation met a non-finite residual: evaluateHuberLoss throws on it before the
+        // reference reaches the solve (robust_loss.h:31-35)
+        const long long bad = ws->host_status->observation_bad;
+        if (bad >= 0 && bad < ne->observation_count)
+            fail(PM_INVALID_ARGUMENT, "evaluateHuberLoss: squared residual norm must be finite and non-negative "
+                                      "(observation " + std::to_string(bad) + ")");
+    }
     if (ws->host_status->eliminated_bad != kNone)
     {
         timings(3);

@@ -44,6 +44,7 @@ for _sfx, _ct in (("f32", C.c_float), ("f64", C.c_double)):
 N.register("pm_ne_create", [i64, i64, i64, i64, C.c_int, vp])
 N.register("pm_ne_destroy", [vp], None)
 N.register("pm_ne_counts", [vp, vp, vp, vp])
+N.register("pm_ne_check_observations", [vp, vp, vp])
 N.register("pm_schur_workspace_create", [vp])
 N.register("pm_schur_workspace_destroy", [vp], None)
 N.register("pm_schur_workspace_close", [vp])
@@ -149,6 +150,12 @@ class DeviceNormalEquations:
         for k in ("primary_cross_row", "primary_cross_col", "primary_cross_values"):
             out[k] = out[k][:pc]
         return out
+
+    def check_observations(self, stream=None) -> None:
+        """Raise InvalidArgument when the last accumulation met a residual whose squared norm is
+        not finite (evaluateHuberLoss, robust_loss.h:31-35); synchronises the stream."""
+        bad = C.c_int64(-1)
+        N.call("pm_ne_check_observations", self._h, _stream_handle(stream), C.byref(bad))
 
     def accumulate_observations(self, obs_primary: torch.Tensor, obs_eliminated: torch.Tensor, jp: torch.Tensor,
                                 jl: torch.Tensor, residual: torch.Tensor, huber_delta: float, stream=None) -> None:

@@ -166,6 +166,33 @@ def test_repeated_pairs_and_unaligned_rows_match_reference(checkers, dtype):
         assert np.abs(got2[key] - got[key]).max() <= tol * np.abs(ref[key]).max(), key
 
 
+@pytest.mark.parametrize("residual_size", [2, 3])
+def test_nonfinite_residual_is_rejected(residual_size):
+    """A residual whose squared norm is NaN or overflows is rejected as evaluateHuberLoss
+    rejects it: by the explicit check and by the next solve, naming the first such observation;
+    a clean accumulation clears the report."""
+    prob = W.bundle_problem(30, 400, per_eliminated=4, residual_size=residual_size, seed=4)
+    bad = dict(prob)
+    bad["residual"] = prob["residual"].copy()
+    bad["residual"][7, 0] = np.nan
+    bad["residual"][19, -1] = 1e200
+    ne = _device_from_observations(bad)
+    with pytest.raises(N.InvalidArgument, match="observation 7"):
+        ne.check_observations()
+    with pytest.raises(N.InvalidArgument, match="observation 7"):
+        SC.solve_damped_schur_complement(ne, 1e-3)
+    bad["residual"][7, 0] = 0.5
+    ne.accumulate_observations(dev(bad["obs_primary"]), dev(bad["obs_eliminated"]), dev(bad["jp"]), dev(bad["jl"]),
+                               dev(bad["residual"]), bad["huber_delta"])
+    with pytest.raises(N.InvalidArgument, match="observation 19"):
+        ne.check_observations()
+    ne.accumulate_observations(dev(prob["obs_primary"]), dev(prob["obs_eliminated"]), dev(prob["jp"]),
+                               dev(prob["jl"]), dev(prob["residual"]), prob["huber_delta"])
+    ne.check_observations()
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=500))
+    assert rep["converged"]
+
+
 def _join(a, b):
     """Observations of b appended to those of a, b's eliminated blocks numbered after a's."""
     out = dict(a)
