@@ -318,7 +318,19 @@ typedef struct
      * plain block Jacobi from the iterate it reached. */
     const struct pm_mlp* learned;
     int stagnation_window;       /* 25 */
+    /* SchurComplementLinearBackend (block_schur.h:21-27): PM_LINEAR_PCG (block-Jacobi PCG, the
+     * Cpu / Cuda backends) or PM_LINEAR_DENSE (DenseCpu: a dense FP64 Cholesky of the reduced
+     * system on the device, block_schur_dense_solver.h:236-318; up to PM_DENSE_MAX_UNKNOWNS
+     * primary unknowns, single systems only; iterations = 1; messages as the reference's). */
+    int linear_backend;
 } pm_schur_options;
+
+enum
+{
+    PM_LINEAR_PCG = 0,
+    PM_LINEAR_DENSE = 1
+};
+#define PM_DENSE_MAX_UNKNOWNS 16384
 
 typedef struct
 {

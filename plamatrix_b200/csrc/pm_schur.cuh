@@ -121,6 +121,12 @@ struct SchurView
     float* minv32 = nullptr;        // P x 36, mixed precision only
 };
 SchurView schur_view(pm_schur_workspace* ws, bool mixed);
+// dense FP64 Cholesky of the n = P bp reduced system in block CSR: A (n x n scratch) and x (the
+// right-hand side in, the solution out); *status (device) = 0, or 1 + the column of the first
+// pivot that is not positive and finite
+template <typename T>
+void dense_schur_factor_solve(cudaStream_t stream, int64_t P, int bp, const int* row_ptr, const int* block_col,
+                              const T* S, double* A, double* x, int* status);
 // features -> network -> (L'L'^T)^-1 of every diagonal block into v.minv (and v.minv32)
 void mlp_apply(const pm_mlp* mlp, const SchurView& v, cudaStream_t stream);
 

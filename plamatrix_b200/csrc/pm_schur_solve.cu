@@ -22,6 +22,7 @@
 #include "pm_schur.cuh"
 
 #include <algorithm>
+#include <limits>
 #include <cmath>
 #include <cstring>
 #include <sstream>
@@ -64,6 +65,7 @@ struct pm_schur_workspace
     pm::DeviceBuffer pattern;
     pm::DeviceBuffer numeric;
     pm::DeviceBuffer scratch;
+    pm::DeviceBuffer dense; // dense backend: n x n factor and status
     pm_sparse_workspace* prim_sort = nullptr;
     int64_t pattern_builds = 0;
     const pm_normal_equations* last_ne = nullptr;
@@ -113,6 +115,7 @@ struct pm_schur_workspace
         pattern.release();
         numeric.release();
         scratch.release();
+        dense.release();
         pair_buffer.release();
         if (prim_sort)
             pm_sparse_workspace_destroy(prim_sort);
@@ -2437,7 +2440,14 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: scalar type differs from the normal equations");
     if (bp > 16 || bl > 16)
         fail(PM_INVALID_ARGUMENT, "device Schur solver supports block sizes up to 16");
-    const bool mixed = o->precision == PM_PRECISION_MIXED && sizeof(T) == 8 && !batch;
+    if (o->linear_backend != PM_LINEAR_PCG && o->linear_backend != PM_LINEAR_DENSE)
+        fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: unknown linear backend");
+    const bool dense = o->linear_backend == PM_LINEAR_DENSE;
+    if (dense && batch)
+        fail(PM_INVALID_ARGUMENT, "batched Schur solve: the dense backend solves single systems");
+    if (dense && n > PM_DENSE_MAX_UNKNOWNS)
+        fail(PM_INVALID_ARGUMENT, "dense Schur backend supports up to 16,384 primary unknowns");
+    const bool mixed = o->precision == PM_PRECISION_MIXED && sizeof(T) == 8 && !batch && !dense;
     if (batch)
     {
         if (sizeof(T) != 8 || bp != 6)
@@ -2561,7 +2571,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         std::snprintf(rep->message, sizeof(rep->message), "eliminated block is not positive definite");
         return;
     }
-    if (ws->host_status->preconditioner_bad != kNone)
+    if (ws->host_status->preconditioner_bad != kNone && !dense) // DenseCpu builds no preconditioner
     {
         timings(3);
         std::snprintf(rep->message, sizeof(rep->message), "Schur preconditioner block is not positive definite");
@@ -2603,6 +2613,53 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     if (n == 0)
     {
         rep->converged = 1;
+    }
+    else if (dense)
+    {
+        // DenseCpu (block_schur_dense_solver.h:236-318): factor, solve, FP64 residual check
+        Carver plan;
+        plan.take<double>(n * n);
+        plan.take<int>(1);
+        ws->dense.ensure(plan.offset + 256, stream, "SchurComplementSolverWorkspace");
+        Carver c;
+        c.base = static_cast<char*>(ws->dense.ptr);
+        double* A = c.take<double>(n * n);
+        int* dstatus = c.take<int>(1);
+        double* x64 = area;
+        double* q64 = area + (n + 1);
+        double* r64 = area + 2 * (n + 1);
+        PM_CUDA(cudaMemcpyAsync(x64, ws->rhs, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        dense_schur_factor_solve<T>(stream, ws->P, static_cast<int>(bp), ws->block_row_ptr, ws->block_col,
+                                    static_cast<const T*>(ws->S), A, x64, dstatus);
+        int bad = 0;
+        PM_CUDA(cudaMemcpyAsync(&bad, dstatus, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaStreamSynchronize(stream));
+        rep->iterations = 1;
+        if (bad != 0)
+        {
+            std::snprintf(rep->message, sizeof(rep->message), "reduced Schur complement is not positive definite");
+        }
+        else
+        {
+            if constexpr (sizeof(T) == 8)
+                PM_CUDA(cudaMemcpyAsync(dp, x64, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+            else
+            {
+                convert_kernel<double, float><<<grid_for(n, 256, 4096), 256, 0, stream>>>(x64, dp, n);
+                PM_LAUNCH_CHECK();
+            }
+            double norm = 0.0, rhs_norm = 0.0;
+            true_residual<T>(ws, stream, static_cast<const T*>(ws->S), x64, q64, r64, norm, rhs_norm);
+            rep->initial_residual_norm = rhs_norm;
+            rep->final_residual_norm = norm;
+            rep->true_relative_residual = rhs_norm > 0 ? norm / rhs_norm : 0.0;
+            const double eps = std::numeric_limits<T>::epsilon();
+            const double tol = std::max(o->absolute_tolerance + o->relative_tolerance * rhs_norm,
+                                        100.0 * eps * std::max(1.0, rhs_norm));
+            rep->converged = std::isfinite(norm) && norm <= tol;
+            if (!rep->converged)
+                std::snprintf(rep->message, sizeof(rep->message), "dense Cholesky residual exceeds tolerance");
+        }
     }
     else if (batch)
     {

@@ -22,7 +22,8 @@ class SchurOptions(C.Structure):
                 ("absolute_tolerance", C.c_double), ("minimum_diagonal", C.c_double),
                 ("use_initial_guess", C.c_int), ("precision", C.c_int), ("tolerance_rule", C.c_int),
                 ("check_true_residual", C.c_int), ("inner_relative_tolerance", C.c_double),
-                ("max_refinements", C.c_int), ("learned", C.c_void_p), ("stagnation_window", C.c_int)]
+                ("max_refinements", C.c_int), ("learned", C.c_void_p), ("stagnation_window", C.c_int),
+                ("linear_backend", C.c_int)]
 
 
 class SchurReport(C.Structure):
@@ -56,6 +57,10 @@ N.register("pm_schur_spmv_f64", [vp, vp, vp, vp])
 PRECISION = {"native": 0, "mixed": 1}
 
 
+LINEAR_BACKEND = {"pcg": 0, "dense": 1}
+DENSE_MAX_UNKNOWNS = 16384  # PM_DENSE_MAX_UNKNOWNS
+
+
 @dataclass
 class SchurComplementSolverOptions:
     """SchurComplementSolverOptions<Scalar> (block_schur.h:31-47) plus device-path knobs."""
@@ -72,13 +77,15 @@ class SchurComplementSolverOptions:
     max_refinements: int = 8
     learned: "LearnedPreconditioner | None" = None  # no counterpart in the reference
     stagnation_window: int = 25
+    linear_backend: str = "pcg"  # "pcg" (Cpu / Cuda backends) or "dense" (DenseCpu: device Cholesky)
 
     def c(self) -> SchurOptions:
         return SchurOptions(self.max_iterations, self.relative_tolerance, self.absolute_tolerance,
                             self.minimum_diagonal, int(self.use_initial_guess), PRECISION[self.precision],
                             0 if self.tolerance_rule == "cpu" else 1, int(self.check_true_residual),
                             self.inner_relative_tolerance, self.max_refinements,
-                            self.learned.handle if self.learned is not None else None, self.stagnation_window)
+                            self.learned.handle if self.learned is not None else None, self.stagnation_window,
+                            LINEAR_BACKEND[self.linear_backend])
 
 
 def _dtype_info(dtype):

@@ -138,6 +138,22 @@ MULTI_PRIMARY_EXPECTED = {"primary": [-1.345185185185185, -0.512592592592593],
                           "eliminated": [-0.493827160493827]}
 
 
+def coupled_chain_residuals():
+    """DenseCpuSolvesParallelSizeCoupledSystemDeterministically, block_schur_test.cpp:275-331:
+    24 primary blocks of size 6, identity blocks with residuals 0.01 (1 + block + component),
+    and a 1-row residual coupling every block with the next."""
+    P, bp = 24, 6
+    identity = np.eye(bp).reshape(-1).tolist()
+    res = []
+    for b in range(P):
+        res.append(([b], identity, -1, None, [0.01 * (1 + b + c) for c in range(bp)], 1.0))
+    left = [1.0, 0.2, -0.1, 0.3, 0.05, -0.2]
+    right = [-0.8, 0.1, 0.25, -0.2, 0.15, 0.3]
+    for b in range(P - 1):
+        res.append(([b, b + 1], left + right, -1, None, [0.02 * (b + 1)], 1.0))
+    return P, 0, bp, 1, res
+
+
 def aggregation_residuals():
     """AggregatesRepeatedVariablePairsBeforeElimination, block_schur_test.cpp:482-504 (damping 0.5)."""
     return 1, 1, 1, 1, [([0], [1.0, 0.0][:1], 0, [1.0], [1.0], 1.0),

@@ -54,6 +54,75 @@ def test_known_answers(checkers, precision):
     assert np.allclose(host(dl), KA.AGGREGATION_EXPECTED["eliminated"], atol=1e-12, rtol=0)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_dense_backend_known_answers(checkers, dtype):
+    """DenseCpuMatchesDenseDampedNormalEquation (block_schur_test.cpp:268-273): the synthetic and
+    multi-primary systems through the dense backend; one 'iteration'."""
+    tol = 1e-5 if dtype == np.float32 else 1e-10
+    opts = _opts(linear_backend="dense")
+    ne = _device_ne(_oracle_ne(checkers, KA.synthetic_residuals, dtype), dtype)
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 0.1, opts)
+    assert rep["converged"] and rep["iterations"] == 1, rep["message"]
+    assert np.allclose(np.concatenate([host(dp), host(dl)]), KA.SYNTHETIC_EXPECTED, atol=tol, rtol=0)
+    ne = _device_ne(_oracle_ne(checkers, KA.multi_primary_residuals, dtype), dtype)
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 0.1, opts)
+    assert rep["converged"]
+    assert np.allclose(host(dp), KA.MULTI_PRIMARY_EXPECTED["primary"], atol=tol, rtol=0)
+    assert np.allclose(host(dl), KA.MULTI_PRIMARY_EXPECTED["eliminated"], atol=tol, rtol=0)
+
+
+def test_dense_backend_coupled_chain_is_deterministic(checkers):
+    """block_schur_test.cpp:275-331: 24 coupled 6x6 primary blocks, no eliminated blocks; two
+    dense solves agree bit for bit and with the oracle's reduced PCG."""
+    orc = _oracle_ne(checkers, KA.coupled_chain_residuals)
+    ne = _device_ne(orc)
+    opts = SC.SchurComplementSolverOptions(relative_tolerance=1e-12, absolute_tolerance=1e-14,
+                                           linear_backend="dense")
+    a, _, rep1 = SC.solve_damped_schur_complement(ne, 0.01, opts)
+    b, _, rep2 = SC.solve_damped_schur_complement(ne, 0.01, opts)
+    assert rep1["converged"] and rep2["converged"], rep1["message"]
+    assert torch.equal(a, b) and np.all(np.isfinite(host(a)))
+    ref, _, rep_ref = orc.solve(0.01, relative_tolerance=1e-13, max_iterations=500)
+    assert rep_ref["converged"]
+    assert np.linalg.norm(host(a) - ref) <= 1e-9 * np.linalg.norm(ref)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("size", ["small", "windowed"])
+def test_dense_backend_matches_direct_solve(checkers, dtype, size):
+    """Device Cholesky over many panels and tiles (n = 120 and 2,400 primary unknowns) against a
+    direct solve of the reference's reduced system and the oracle's PCG solution."""
+    prob = (W.small_bundle(seed=11, dtype=dtype) if size == "small"
+            else W.large_bundle(seed=7, P=400, L=20000, dtype=dtype))
+    orc = checkers.normal_equations_from_observations(prob, dtype=dtype)
+    ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+    n = len(ro) - 1
+    dense = np.zeros((n, n))
+    dense[np.repeat(np.arange(n), np.diff(ro)), ci] = vals
+    direct = np.linalg.solve(dense, rhs.astype(np.float64))
+    ne = _device_from_observations(prob, dtype)
+    dp, dl, rep = SC.solve_damped_schur_complement(
+        ne, 1e-3, SC.SchurComplementSolverOptions(relative_tolerance=1e-10, linear_backend="dense"))
+    assert rep["converged"] and rep["iterations"] == 1, rep["message"]
+    tol = 1e-4 if dtype == np.float32 else 1e-9
+    assert np.linalg.norm(host(dp).astype(np.float64) - direct) <= tol * np.linalg.norm(direct)
+    assert rep["true_relative_residual"] <= (1e-5 if dtype == np.float32 else 1e-12)
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=1e-10, max_iterations=1000)
+    stol = 1e-4 if dtype == np.float32 else 1e-6
+    assert np.linalg.norm(host(dl).astype(np.float64) - dl_ref) <= stol * np.linalg.norm(dl_ref)
+
+
+def test_dense_backend_rejections(checkers):
+    # a primary block without observations and no damping: a zero pivot
+    o = checkers.NormalEquations(2, 1, 1, 1)
+    o.add_residual([0], [1.0], 0, [2.0], [1.0])
+    dp, dl, rep = SC.solve_damped_schur_complement(_device_ne(o), 0.0, _opts(linear_backend="dense"))
+    assert not rep["converged"] and rep["message"] == "reduced Schur complement is not positive definite"
+    big = SC.DeviceNormalEquations(SC.DENSE_MAX_UNKNOWNS // 6 + 1, 1, 6, 3)
+    with pytest.raises(N.InvalidArgument, match="16,384"):
+        SC.solve_damped_schur_complement(big, 1e-3, _opts(linear_backend="dense"))
+
+
 def test_point_only_float(checkers):
     """block_schur_test.cpp:531-548."""
     c = KA.POINT_ONLY
