@@ -443,6 +443,11 @@ def sparse_leg(torch, S, W, stream):
                                             "same_size_read_GBps": round(byts / (tr * 1e-3) / 1e9, 1),
                                             "frac_of_same_size_read": round(tr / t, 3),
                                             "algorithmic_bytes": byts}
+        # the autotuner's pick for this operand (timed with warm caches), then flushed again
+        chosen = op.autotune(x, y, stream)
+        ta = flushed_ms(torch, lambda: op.spmv(x, y), flush, stream)
+        spmv[f"csr_laplacian128_{name}"]["autotuned"] = {"kernel": S.CsrOperand.KERNELS[chosen], "ms": round(ta, 4),
+                                                         "GBps": round(byts / (ta * 1e-3) / 1e9, 1)}
         # COO -> CSR of the same matrix (16.04M triplets)
         ws_coo = S.SparseOpsWorkspace()
         r_d = torch.from_numpy(lap["row_indices"]).cuda()

@@ -144,6 +144,17 @@ PM_API int pm_csr_set_values(pm_csr* matrix, const void* values_d);
 PM_API int pm_csr_spmv_f32(const pm_csr* matrix, pm_stream_t stream, const float* x_d, float* y_d);
 PM_API int pm_csr_spmv_f64(const pm_csr* matrix, pm_stream_t stream, const double* x_d, double* y_d);
 
+/* No counterpart in the reference (its SpMV is cuSPARSE's): the SpMV shape of an operand.
+ * kernel -1 = heuristic (mean row length), 0 = row-group stream (a warp per 32 rows), 1..32 =
+ * lanes per row.  pm_csr_autotune_* times every shape on this operand with the caller's vectors
+ * and stream (synchronous; overwrites y_d) and keeps the fastest; CG / PCG on the operand use the
+ * same shape.  Shapes order a row's additions differently, so the choice is part of a result's
+ * rounding; pm_csr_set_kernel pins one for reproducibility across processes. */
+PM_API int pm_csr_autotune_f32(pm_csr* matrix, pm_stream_t stream, const float* x_d, float* y_d, int* kernel_h);
+PM_API int pm_csr_autotune_f64(pm_csr* matrix, pm_stream_t stream, const double* x_d, double* y_d, int* kernel_h);
+PM_API int pm_csr_set_kernel(pm_csr* matrix, int kernel);
+PM_API int pm_csr_kernel(const pm_csr* matrix, int* kernel_h, int* heuristic_lanes_h);
+
 /* output = A input for dense matrices in column-major order (leading dimension = rows):
  * input is input_rows x input_cols (input_rows == A's columns), output is output_rows x
  * output_cols (A's rows x input_cols).  Replaces spmmAsync (sparse_ops.cu:762-818; the CPU order

@@ -25,11 +25,16 @@ struct pm_csr
     int* row_ptr = nullptr; // int32 copy of the validated row offsets
     int* col_idx = nullptr; // int32 copy of the validated column indices
     const void* values = nullptr;
-    int threads_per_row = 1;
+    int threads_per_row = 1; // lanes per row of the heuristic
+    int kernel = -1;         // -1: heuristic; 0: row-group stream; 1..32: lanes per row (autotuned or set)
 };
 
 namespace pm
 {
+
+// the SpMV shape of an operand: the row-group stream kernel, or TPR lanes per row
+inline bool use_stream(const pm_csr* A) { return A->kernel == 0 || (A->kernel < 0 && A->threads_per_row <= 8); }
+inline int lanes_per_row(const pm_csr* A) { return A->kernel > 0 ? A->kernel : A->threads_per_row; }
 
 template <typename T>
 struct Eps;
@@ -212,15 +217,15 @@ void launch_spmv(const pm_csr* A, const T* x, T* y, cudaStream_t stream)
         return;
     const T* v = static_cast<const T*>(A->values);
     const int block = 256;
-    if (A->threads_per_row <= 8)
+    if (use_stream(A))
     {
         csr_stream_kernel<T><<<grid_for(A->rows, 256, 1 << 20), 256, 0, stream>>>(A->rows, A->row_ptr, A->col_idx,
                                                                                     v, x, y);
         PM_LAUNCH_CHECK();
         return;
     }
-    const unsigned grid = grid_for(A->rows * A->threads_per_row, block, 65535);
-    switch (A->threads_per_row)
+    const unsigned grid = grid_for(A->rows * lanes_per_row(A), block, 65535);
+    switch (lanes_per_row(A))
     {
     case 1: csr_spmv_kernel<T, 1><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
     case 2: csr_spmv_kernel<T, 2><<<grid, block, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, x, y); break;
@@ -687,6 +692,62 @@ void csr_spmv(const pm_csr* A, cudaStream_t stream, const T* x, T* y)
     launch_spmv<T>(A, x, y, stream);
 }
 
+// ------------------------------------------------------------------ SpMV autotuning
+// Times every SpMV shape (row-group stream; 1, 2, 4, 8, 16, 32 lanes per row) on the operand with
+// the caller's vectors and stream (one warm-up, then `reps` launches each, CUDA events) and keeps
+// the fastest in the handle; the CG / PCG solvers use the same shape.  Shapes differ in the order
+// of a row's additions, so the choice is part of a result's rounding; pm_csr_set_kernel pins one.
+template <typename T>
+int csr_autotune(pm_csr* A, cudaStream_t stream, const T* x, T* y, int reps)
+{
+    if (!A)
+        fail(PM_INVALID_ARGUMENT, "CSR handle is null");
+    if (A->value_size != static_cast<int>(sizeof(T)))
+        fail(PM_INVALID_ARGUMENT, "autotune scalar type differs from the CSR operand");
+    if (A->rows > 0 && (!y || (A->cols > 0 && !x)))
+        fail(PM_INVALID_ARGUMENT, "autotune vectors must be non-null");
+    if (x && x == y)
+        fail(PM_INVALID_ARGUMENT, "spmv input and output data must not alias");
+    if (A->rows == 0 || A->nnz == 0)
+        return A->kernel;
+    const int candidates[] = {0, 1, 2, 4, 8, 16, 32};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PM_CUDA(cudaEventCreate(&e0));
+    PM_CUDA(cudaEventCreate(&e1));
+    int best = A->kernel;
+    float best_ms = 0.f;
+    try
+    {
+        for (const int c : candidates)
+        {
+            A->kernel = c;
+            launch_spmv<T>(A, x, y, stream);
+            PM_CUDA(cudaEventRecord(e0, stream));
+            for (int r = 0; r < reps; ++r)
+                launch_spmv<T>(A, x, y, stream);
+            PM_CUDA(cudaEventRecord(e1, stream));
+            PM_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            PM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (c == candidates[0] || ms < best_ms)
+            {
+                best = c;
+                best_ms = ms;
+            }
+        }
+    }
+    catch (...)
+    {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    A->kernel = best;
+    return best;
+}
+
 // ------------------------------------------------------------------ SpMM
 // output (rows x k) = A input (cols x k), dense matrices column-major (leading dimension = rows).
 // A warp owns 32 consecutive rows; their nonzero range is staged in shared memory in pieces of
@@ -817,14 +878,14 @@ void launch_pcg_spmv(const pm_csr* A, const T* p, T* q, double* partials, PcgSta
                      cudaStream_t stream)
 {
     const T* v = static_cast<const T*>(A->values);
-    if (A->threads_per_row <= 8)
+    if (use_stream(A))
     {
         pcg_stream_spmv_kernel<T><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q,
                                                                      partials, st);
         PM_LAUNCH_CHECK();
         return;
     }
-    switch (A->threads_per_row)
+    switch (lanes_per_row(A))
     {
     case 1: pcg_spmv_kernel<T, 1><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
     case 2: pcg_spmv_kernel<T, 2><<<grid, kReduceBlock, 0, stream>>>(A->rows, A->row_ptr, A->col_idx, v, p, q, partials, st); break;
@@ -891,8 +952,8 @@ void solve(pm_solver_workspace* ws, cudaStream_t stream, const pm_csr* A, const 
     T* inv = c.take<T>(n);
 
     const unsigned vgrid = grid_for(n, kReduceBlock, kMaxReduceBlocks);
-    const unsigned sgrid = A->threads_per_row <= 8 ? grid_for(n, kReduceBlock, kMaxReduceBlocks)
-                                                   : grid_for(n * A->threads_per_row, kReduceBlock, kMaxReduceBlocks);
+    const unsigned sgrid = use_stream(A) ? grid_for(n, kReduceBlock, kMaxReduceBlocks)
+                                                   : grid_for(n * lanes_per_row(A), kReduceBlock, kMaxReduceBlocks);
     pcg_reset_kernel<<<1, 1, 0, stream>>>(st, o->max_iterations);
     PM_LAUNCH_CHECK();
     if (mode == 1)
@@ -1008,8 +1069,8 @@ pm_fixed_state* fixed_solve(pm_solver_workspace* ws, cudaStream_t stream, const 
         T* q = c.take<T>(n);
         T* inv = c.take<T>(n);
         const unsigned vgrid = grid_for(n, kReduceBlock, kMaxReduceBlocks);
-        const unsigned sgrid = A->threads_per_row <= 8 ? grid_for(n, kReduceBlock, kMaxReduceBlocks)
-                                                       : grid_for(n * A->threads_per_row, kReduceBlock, kMaxReduceBlocks);
+        const unsigned sgrid = use_stream(A) ? grid_for(n, kReduceBlock, kMaxReduceBlocks)
+                                                       : grid_for(n * lanes_per_row(A), kReduceBlock, kMaxReduceBlocks);
         pcg_reset_kernel<<<1, 1, 0, stream>>>(st, iterations);
         PM_LAUNCH_CHECK();
         if (mode == 1)
@@ -1164,6 +1225,46 @@ int pm_csr_spmm_f64(const pm_csr* A, pm_stream_t stream, int64_t input_rows, int
 {
     return pm::guarded(
         [&] { pm::csr_spmm<double>(A, stream, input_rows, input_cols, input, output_rows, output_cols, output); });
+}
+
+int pm_csr_autotune_f32(pm_csr* A, pm_stream_t stream, const float* x, float* y, int* kernel)
+{
+    return pm::guarded([&] {
+        const int k = pm::csr_autotune<float>(A, stream, x, y, 5);
+        if (kernel)
+            *kernel = k;
+    });
+}
+int pm_csr_autotune_f64(pm_csr* A, pm_stream_t stream, const double* x, double* y, int* kernel)
+{
+    return pm::guarded([&] {
+        const int k = pm::csr_autotune<double>(A, stream, x, y, 5);
+        if (kernel)
+            *kernel = k;
+    });
+}
+int pm_csr_set_kernel(pm_csr* A, int kernel)
+{
+    return pm::guarded([&] {
+        if (!A)
+            pm::fail(PM_INVALID_ARGUMENT, "CSR handle is null");
+        if (!(kernel == -1 || kernel == 0 || kernel == 1 || kernel == 2 || kernel == 4 || kernel == 8 ||
+              kernel == 16 || kernel == 32))
+            pm::fail(PM_INVALID_ARGUMENT, "SpMV kernel must be -1 (heuristic), 0 (row-group stream) or 1, 2, 4, "
+                                          "8, 16, 32 lanes per row");
+        A->kernel = kernel;
+    });
+}
+int pm_csr_kernel(const pm_csr* A, int* kernel, int* heuristic_lanes)
+{
+    return pm::guarded([&] {
+        if (!A)
+            pm::fail(PM_INVALID_ARGUMENT, "CSR handle is null");
+        if (kernel)
+            *kernel = A->kernel;
+        if (heuristic_lanes)
+            *heuristic_lanes = A->threads_per_row;
+    });
 }
 
 int pm_solver_workspace_create(pm_solver_workspace** out)

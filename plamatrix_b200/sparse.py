@@ -168,6 +168,27 @@ class CsrOperand:
         N.call(f"pm_csr_spmv_{self.sfx}", self._h, _stream_handle(stream), _ptr(x), _ptr(y))
         return y
 
+    KERNELS = {-1: "heuristic", 0: "row-group stream", 1: "1 lane/row", 2: "2 lanes/row", 4: "4 lanes/row",
+               8: "8 lanes/row", 16: "16 lanes/row", 32: "32 lanes/row"}
+
+    def autotune(self, x: torch.Tensor | None = None, y: torch.Tensor | None = None, stream=None) -> int:
+        """Time every SpMV shape on this operand (x, y: the caller's vectors, random ones when
+        omitted; y is overwritten) and keep the fastest; returns its code (see KERNELS)."""
+        dt = self.matrix.values.dtype
+        x = torch.randn(self.matrix.cols, dtype=dt, device="cuda") if x is None else x
+        y = torch.empty(self.matrix.rows, dtype=dt, device="cuda") if y is None else y
+        k = C.c_int(-1)
+        N.call(f"pm_csr_autotune_{self.sfx}", self._h, _stream_handle(stream), _ptr(x), _ptr(y), C.byref(k))
+        return k.value
+
+    def set_kernel(self, kernel: int) -> None:
+        N.call("pm_csr_set_kernel", self._h, int(kernel))
+
+    def kernel(self) -> int:
+        k, h = C.c_int(), C.c_int()
+        N.call("pm_csr_kernel", self._h, C.byref(k), C.byref(h))
+        return k.value
+
     def spmm(self, B: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         """out = A B for column-major dense matrices (spmmAsync, sparse_ops.cu:762-818): B is
         (cols x k) and out (rows x k), each with strides (1, its row count), e.g.
@@ -277,7 +298,10 @@ for _suffix in ("f32", "f64"):
         N.register(f"pm_{_kind}_fixed_iterations_async_{_suffix}",
                    [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p])
 N.register("pm_fixed_state_finalize", [C.c_void_p, C.c_void_p, C.c_void_p])
+N.register("pm_csr_set_kernel", [C.c_void_p, C.c_int])
+N.register("pm_csr_kernel", [C.c_void_p, C.c_void_p, C.c_void_p])
 for _suffix in ("f32", "f64"):
+    N.register(f"pm_csr_autotune_{_suffix}", [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p])
     N.register(f"pm_csr_spmm_{_suffix}", [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_int64,
                                           C.c_int64, C.c_void_p])
 N.register("pm_fixed_state_destroy", [C.c_void_p], None)

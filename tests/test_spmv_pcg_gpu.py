@@ -98,6 +98,32 @@ def test_spmv_random_against_oracle(checkers, dtype, mean):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("mean", [2, 40])
+def test_autotuned_and_pinned_shapes_match_oracle(checkers, dtype, mean):
+    """Every SpMV shape, and the autotuned one, agrees with the oracle within the summation-order
+    bound; the solvers run with the chosen shape."""
+    rng = np.random.default_rng(mean + 100)
+    rows, cols = 4000, 4000
+    n = rows * mean
+    r, c = rng.integers(0, rows, n), rng.integers(0, cols, n)
+    A, (ro, ci, vv) = _csr(checkers, rows, cols, r, c, rng.standard_normal(n), dtype)
+    op = S.CsrOperand(A)
+    assert op.kernel() == -1
+    x = rng.standard_normal(cols).astype(dtype)
+    ref = checkers.csr_spmv(ro, ci, vv.astype(np.float64), x.astype(np.float64))
+    magnitude = checkers.csr_spmv(ro, ci, np.abs(vv.astype(np.float64)), np.abs(x.astype(np.float64)))
+    bound = (np.diff(ro).astype(np.float64) + 1) * np.finfo(dtype).eps * magnitude + 1e-300
+    for k in (0, 1, 2, 4, 8, 16, 32, -1):
+        op.set_kernel(k)
+        assert np.all(np.abs(host(op.spmv(dev(x))).astype(np.float64) - ref) <= bound), k
+    chosen = op.autotune(dev(x), torch.empty(rows, dtype=dev(x).dtype, device="cuda"))
+    assert chosen in S.CsrOperand.KERNELS and chosen >= 0 and op.kernel() == chosen
+    assert np.all(np.abs(host(op.spmv(dev(x))).astype(np.float64) - ref) <= bound)
+    with pytest.raises(N.InvalidArgument):
+        op.set_kernel(3)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_pcg_known_answers(checkers, dtype):
     tol = 2e-4 if dtype == np.float32 else 1e-10
     d = KA.DIAGONAL_PCG
