@@ -2713,6 +2713,10 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         const double inner_rel = o->inner_relative_tolerance > 0.0 ? o->inner_relative_tolerance : 1e-4;
         int total = 0;
         const int max_refinements = o->max_refinements > 0 ? o->max_refinements : 8;
+        // the FP32 pass is guarded (block_schur_accelerated.cpp:160-195): a step that breaks
+        // down or does not reduce the FP64 residual hands the solve to FP64 PCG from the iterate
+        // reached, and mixed precision counts as used only when some FP32 step was kept
+        bool kept_fp32 = false, fp64_fallback = false;
         for (int k = 0; k <= max_refinements; ++k)
         {
             rep->final_residual_norm = norm;
@@ -2722,7 +2726,10 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
                 break;
             }
             if (k == max_refinements || total >= o->max_iterations)
+            {
+                fp64_fallback = total < o->max_iterations;
                 break;
+            }
             // r64 holds b - S x; solve S32 d = r64 to inner_rel (or to the outer target)
             PM_CUDA(cudaMemsetAsync(d32, 0, n * sizeof(float), stream));
             st = block_pcg<float, float, float>(ws, stream, ws->S32, ws->minv32, r64, d32, inner_rel, 0.5 * target, 1,
@@ -2745,15 +2752,37 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             }
             if (st.breakdown)
             {
-                std::snprintf(rep->message, sizeof(rep->message), "reduced Schur complement is not positive definite");
+                fp64_fallback = true;
                 break;
             }
             axpy_to_double_kernel<float><<<grid_for(n, 256, 4096), 256, 0, stream>>>(n, d32, x64);
             PM_LAUNCH_CHECK();
+            const double before = norm;
             true_residual<T>(ws, stream, static_cast<const T*>(ws->S), x64, q64, r64, norm, rhs_norm);
+            if (!(norm < before))
+            {
+                fp64_fallback = true;
+                break;
+            }
+            kept_fp32 = true;
+        }
+        if (!rep->converged && fp64_fallback)
+        {
+            // FP64 block-Jacobi PCG from the iterate reached (from zero when it is not finite)
+            if (!std::isfinite(norm))
+                PM_CUDA(cudaMemsetAsync(x64, 0, n * sizeof(double), stream));
+            const SolveState fs = block_pcg<T, T, double>(ws, stream, static_cast<const T*>(ws->S), ws->minv, ws->rhs,
+                                                          dp, 0.0, target, 1, std::max(0, o->max_iterations - total),
+                                                          reinterpret_cast<T*>(area));
+            total += fs.iterations;
+            if (fs.breakdown)
+                std::snprintf(rep->message, sizeof(rep->message), "reduced Schur complement is not positive definite");
+            true_residual<T>(ws, stream, static_cast<const T*>(ws->S), x64, area, area + (n + 1), norm, rhs_norm);
+            rep->final_residual_norm = norm;
+            rep->converged = fs.converged;
         }
         rep->iterations = total;
-        rep->mixed_precision_used = 1;
+        rep->mixed_precision_used = kept_fp32 ? 1 : 0;
         rep->true_relative_residual = rhs_norm > 0 ? rep->final_residual_norm / rhs_norm : 0.0;
     }
     PM_CUDA(cudaEventRecord(ws->events[4], stream));

@@ -123,6 +123,27 @@ def test_dense_backend_rejections(checkers):
         SC.solve_damped_schur_complement(big, 1e-3, _opts(linear_backend="dense"))
 
 
+def test_mixed_precision_falls_back_to_fp64_when_fp32_fails():
+    """The guarded FP32 pass (block_schur_accelerated.cpp:160-195): a system whose reduced values
+    overflow FP32 (Jacobians scaled by 1e20) breaks the FP32 inner solve, and the solve finishes
+    in FP64 PCG without reporting mixed precision as used; a well-scaled system keeps it."""
+    prob = W.small_bundle(seed=13)
+    big = dict(prob)
+    for key in ("jp", "jl"):
+        big[key] = prob[key] * 1e20
+    opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-10, precision="mixed")
+    dp, dl, rep = SC.solve_damped_schur_complement(_device_from_observations(big), 1e-3, opts)
+    assert rep["converged"], rep["message"]
+    assert not rep["mixed_precision_used"]
+    ref, _, rep_ref = SC.solve_damped_schur_complement(
+        _device_from_observations(big), 1e-3, SC.SchurComplementSolverOptions(max_iterations=500,
+                                                                              relative_tolerance=1e-10))
+    assert rep_ref["converged"]
+    assert np.linalg.norm(host(dp) - host(ref)) <= 1e-6 * np.linalg.norm(host(ref))
+    dp, dl, rep = SC.solve_damped_schur_complement(_device_from_observations(prob), 1e-3, opts)
+    assert rep["converged"] and rep["mixed_precision_used"]
+
+
 def test_point_only_float(checkers):
     """block_schur_test.cpp:531-548."""
     c = KA.POINT_ONLY
