@@ -186,6 +186,52 @@ def test_invalid_options_and_aliasing(checkers):
         SC.solve_damped_schur_complement(ne, 0.1, primary_step=buf, eliminated_step=buf)
 
 
+def test_accumulation_rejects_bad_indices_sizes_and_delta():
+    """RejectsDimensionMismatchAndNonFiniteInput (block_schur_test.cpp:506-529) on the
+    observation path: a primary index past the last block, a zero residual size and a
+    non-finite Huber delta."""
+    prob = W.small_bundle(seed=2)
+    ne = SC.DeviceNormalEquations(prob["P"], prob["L"], 6, 3)
+    args = [dev(prob[k]) for k in ("obs_primary", "obs_eliminated", "jp", "jl", "residual")]
+    bad_p = args[0].clone()
+    bad_p[5] = prob["P"]
+    with pytest.raises(N.OutOfRange):
+        ne.accumulate_observations(bad_p, *args[1:], 1.0)
+    with pytest.raises(N.InvalidArgument):
+        ne.accumulate_observations(*args, float("inf"))
+    n = len(prob["obs_primary"])
+    with pytest.raises(N.InvalidArgument):
+        N.call("pm_ne_accumulate_observations_f64", ne._h, None, n, 0, *[a.data_ptr() for a in args], 1.0)
+
+
+def test_dense_backend_generic_blocks_are_repeatable(checkers):
+    """DenseCpuEliminatedAssemblyIsBitwiseStableAcrossThreadCounts (block_schur_test.cpp:334-405):
+    36 primaries of size 9, 240 eliminated blocks of size 3; repeated dense solves agree bit for
+    bit and with the oracle's reduced PCG."""
+    P, L, bp, bl = 36, 240, 9, 3
+    o = checkers.NormalEquations(P, L, bp, bl)
+    identity = np.eye(bp).reshape(-1)
+    for p in range(P):
+        o.add_residual([p], identity, -1, None, np.zeros(bp), 0.25)
+    for l in range(L):
+        for obs in range(4):
+            p = (l * 7 + obs * 5) % P
+            jp = [0.01 * (1 + (i + l + obs) % 13) for i in range(2 * bp)]
+            jl = [0.02 * (1 + (i + l + 2 * obs) % 7) for i in range(2 * bl)]
+            o.add_residual([p], jp, l, jl, [0.001 * (l + 1), -0.002 * (obs + 1)])
+    ne = _device_ne(o)
+    opts = SC.SchurComplementSolverOptions(relative_tolerance=1e-11, absolute_tolerance=1e-13,
+                                           linear_backend="dense")
+    a1, b1, r1 = SC.solve_damped_schur_complement(ne, 0.1, opts)
+    a2, b2, r2 = SC.solve_damped_schur_complement(ne, 0.1, opts)
+    assert r1["converged"] and r2["converged"], r1["message"]
+    assert torch.equal(a1, a2) and torch.equal(b1, b2)
+    ref_p, ref_l, rep = o.solve(0.1, relative_tolerance=1e-13, max_iterations=1000)
+    assert rep["converged"]
+    assert np.linalg.norm(host(a1) - ref_p) <= 1e-8 * np.linalg.norm(ref_p)
+    assert np.linalg.norm(host(b1) - ref_l) <= 1e-8 * np.linalg.norm(ref_l)
+
+
 def test_non_spd_eliminated_block_reports_message(checkers):
     o = checkers.NormalEquations(1, 1, 1, 1)
     o.add_residual([0], [1.0], -1, None, [1.0])
