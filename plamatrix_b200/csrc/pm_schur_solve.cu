@@ -200,14 +200,31 @@ __global__ void eliminated_inverse_kernel(int64_t L, int bl_rt, const T* __restr
             for (int i = 0; i < bl * bl; ++i)
                 inv[i] = 0.0;
         }
-        for (int i = 0; i < bl * bl; ++i)
-            hinv[l * hstride + i] = inv[i];
+        double yl[MB];
         for (int r = 0; r < bl; ++r)
         {
             double s = 0.0;
             for (int c = 0; c < bl; ++c)
                 s = __dadd_rn(s, __dmul_rn(inv[r * bl + c], static_cast<double>(gl[l * bl + c])));
-            y[l * ystride + r] = s;
+            yl[r] = s;
+        }
+        if (BL == 3 && hstride == 12 && y == hinv + 9)
+        {
+            // packed [Hll^-1 | y] row of 96 bytes: six 16-byte stores
+            double2* out = reinterpret_cast<double2*>(hinv + l * 12);
+            out[0] = make_double2(inv[0], inv[1]);
+            out[1] = make_double2(inv[2], inv[3]);
+            out[2] = make_double2(inv[4], inv[5]);
+            out[3] = make_double2(inv[6], inv[7]);
+            out[4] = make_double2(inv[8], yl[0]);
+            out[5] = make_double2(yl[1], yl[2]);
+        }
+        else
+        {
+            for (int i = 0; i < bl * bl; ++i)
+                hinv[l * hstride + i] = inv[i];
+            for (int r = 0; r < bl; ++r)
+                y[l * ystride + r] = yl[r];
         }
     }
 }
@@ -839,7 +856,8 @@ __device__ __forceinline__ double stream_sum(double v, unsigned gmask)
 template <typename T>
 __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
     int64_t B, const int64_t* __restrict__ pair_offset, const int4* __restrict__ pairs,
-    const int* __restrict__ block_row, const int* __restrict__ block_col, const int* __restrict__ block_pc,
+    const int* __restrict__ block_row, const int* __restrict__ block_col, const int* __restrict__ transpose,
+    const int* __restrict__ block_pc,
     const T* __restrict__ w, const double* __restrict__ hy, const T* __restrict__ pcv, T* __restrict__ S)
 {
     const int g = threadIdx.x & (kPairLanes - 1);
@@ -894,13 +912,16 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
                 acc[r][c] = stream_sum(acc[r][c], gmask);
         const int pc = block_pc[b];
         T* out = S + b * 36 + 18 * h;
+        T* mirrored = S + int64_t(transpose[b]) * 36; // the lower block (q, p) holds the transpose
 #pragma unroll
         for (int e = 0; e < 18; ++e)
         {
             if ((e & (kPairStreams - 1)) != s)
                 continue;
             const double base = pc >= 0 ? static_cast<double>(pcv[int64_t(pc) * 36 + 18 * h + e]) : 0.0;
-            out[e] = static_cast<T>(base - acc[e / 6][e % 6]);
+            const T value = static_cast<T>(base - acc[e / 6][e % 6]);
+            out[e] = value;
+            mirrored[(e % 6) * 6 + 3 * h + e / 6] = value;
         }
     }
 }
@@ -1776,13 +1797,11 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
             a.P, ws->prim_offsets, ws->row_entries, a.w, ws->hinv, a.hpp, a.gp, a.lambda, a.min_diag, a.diag_pos,
             a.S, a.rhs);
         PM_LAUNCH_CHECK();
-        if (ws->E > 0)
-        {
-            assemble_upper6_kernel<T><<<grid_for(ws->B * kPairLanes, kUpperThreads), kUpperThreads, 0, stream>>>(
-                ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, a.block_pc, a.w, ws->hinv, a.pcv,
-                a.S);
-            PM_LAUNCH_CHECK();
-        }
+        // every upper block, also those whose only terms are primary-primary couplings
+        assemble_upper6_kernel<T><<<grid_for(ws->B * kPairLanes, kUpperThreads), kUpperThreads, 0, stream>>>(
+            ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, a.w, ws->hinv,
+            a.pcv, a.S);
+        PM_LAUNCH_CHECK();
         diag_inverse_kernel<T, 6><<<grid_for(a.P, 64, 1 << 16), 64, 0, stream>>>(a.P, a.diag_pos, a.S, a.minv,
                                                                                  a.status);
         PM_LAUNCH_CHECK();
@@ -1796,9 +1815,12 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
         assemble_kernel<T, 0, 0, 16><<<grid, kRowThreads, smem, stream>>>(a);
         PM_LAUNCH_CHECK();
     }
-    mirror_kernel<T><<<grid_for(ws->B * ne->bp * ne->bp, 256, 65535), 256, 0, stream>>>(
-        ws->B, static_cast<int>(ne->bp), ws->block_row, ws->block_col, ws->transpose, static_cast<T*>(ws->S));
-    PM_LAUNCH_CHECK();
+    if (!ws->paired) // the pair kernel writes each upper block's transpose itself
+    {
+        mirror_kernel<T><<<grid_for(ws->B * ne->bp * ne->bp, 256, 65535), 256, 0, stream>>>(
+            ws->B, static_cast<int>(ne->bp), ws->block_row, ws->block_col, ws->transpose, static_cast<T*>(ws->S));
+        PM_LAUNCH_CHECK();
+    }
 }
 
 } // namespace

@@ -144,6 +144,28 @@ def test_mixed_precision_falls_back_to_fp64_when_fp32_fails():
     assert rep["converged"] and rep["mixed_precision_used"]
 
 
+def test_primary_coupling_blocks_in_the_pair_assembly(checkers):
+    """6x3 systems with primary-primary residual blocks: one coupling adds to blocks the crosses
+    also fill, two create blocks that no eliminated block touches (their only terms); the reduced
+    system (both triangles) and the step match the reference."""
+    prob = W.large_bundle(seed=3, P=400, L=2000)
+    orc = checkers.normal_equations_from_observations(prob)
+    rng = np.random.default_rng(0)
+    for a, b in ((0, 200), (5, 6), (100, 399)):
+        orc.add_residual([a, b], rng.standard_normal(24), -1, None, rng.standard_normal(2))
+    ne = _device_ne(orc)
+    ws = SC.SchurComplementSolverWorkspace()
+    dp, dl, rep = SC.solve_damped_schur_complement(
+        ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-10), ws)
+    assert rep["converged"], rep["message"]
+    ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+    sysd = ws.export()
+    assert np.array_equal(host(sysd["row_offsets"]), ro) and np.array_equal(host(sysd["col_indices"]), ci)
+    assert np.abs(host(sysd["values"]) - vals).max() <= 1e-12 * np.abs(vals).max()
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=1e-10, max_iterations=500)
+    assert np.linalg.norm(host(dp) - dp_ref) <= 1e-6 * np.linalg.norm(dp_ref)
+
+
 def test_point_only_float(checkers):
     """block_schur_test.cpp:531-548."""
     c = KA.POINT_ONLY
