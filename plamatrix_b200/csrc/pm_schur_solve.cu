@@ -88,7 +88,8 @@ struct pm_schur_workspace
     int64_t E = 0;                 // cross pairs
     int2* row_entries = nullptr;   // C: {cross, eliminated} of every primary-list entry
     int64_t* pair_offset = nullptr; // B + 1: pairs of block b are [off[b], off[b+1]) (upper blocks only)
-    int4* pairs = nullptr;         // E: {cross (l, p), cross (l, q), l, 0}, per block in ascending l
+    int2* pairs = nullptr;         // E: {row-list entry of cross (l, p), cross (l, q)}, per block in ascending l
+    double* tfactor = nullptr;     // C x 18: T = W_lp Hll^-1 of every row-list entry (written by the diagonal pass)
     int* saved_offsets = nullptr;
     int* saved_primary = nullptr;
     int* saved_pc = nullptr;
@@ -684,7 +685,7 @@ __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets
 __global__ void pair_place_kernel(int64_t P, const int* __restrict__ prim_offsets, const int64_t* __restrict__ offset,
                                   const int* __restrict__ item_block, const int* __restrict__ item_cross,
                                   const int2* __restrict__ row_entries, unsigned* mask, int64_t* cursor,
-                                  int4* __restrict__ pairs)
+                                  int2* __restrict__ pairs)
 {
     const int lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
@@ -712,7 +713,7 @@ __global__ void pair_place_kernel(int64_t P, const int* __restrict__ prim_offset
             {
                 const int X = item_block[e];
                 const int64_t at = vcursor[X] + __popc(vmask[X] & below);
-                pairs[at] = make_int4(re.x, item_cross[e], re.y, 0);
+                pairs[at] = make_int2(j, item_cross[e]);
             }
             __syncwarp();
             for (int64_t e = e0; e < e1; ++e)
@@ -768,7 +769,8 @@ template <typename T>
 __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
     int64_t P, const int* __restrict__ prim_offsets, const int2* __restrict__ row_entries, const T* __restrict__ w,
     const double* __restrict__ hy, const T* __restrict__ hpp, const T* __restrict__ gp, double lambda,
-    double min_diag, const int* __restrict__ diag_pos, T* __restrict__ S, double* __restrict__ rhs)
+    double min_diag, const int* __restrict__ diag_pos, T* __restrict__ S, double* __restrict__ rhs,
+    double* __restrict__ tfactor)
 {
     __shared__ double part[kDiagThreads / 32][27];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -786,6 +788,7 @@ __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
             double h[12], wv[18];
             load_pairs<double, 12>(hy + int64_t(re.y) * 12, h);
             load_pairs<T, 18>(w + int64_t(re.x) * 18, wv);
+            double tall[18]; // T row of this entry, stored for the upper-block pass
 #pragma unroll
             for (int r = 0; r < 6; ++r)
             {
@@ -793,12 +796,19 @@ __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
                 double tr[3];
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
+                {
                     tr[k] = h[3 * k] * w0 + h[3 * k + 1] * w1 + h[3 * k + 2] * w2;
+                    tall[3 * r + k] = tr[k];
+                }
 #pragma unroll
                 for (int c = 0; c <= r; ++c)
                     d[r * (r + 1) / 2 + c] += tr[0] * wv[3 * c] + tr[1] * wv[3 * c + 1] + tr[2] * wv[3 * c + 2];
                 d[21 + r] += w0 * h[9] + w1 * h[10] + w2 * h[11];
             }
+            double2* tout = reinterpret_cast<double2*>(tfactor + int64_t(j) * 18);
+#pragma unroll
+            for (int e = 0; e < 9; ++e)
+                tout[e] = make_double2(tall[2 * e], tall[2 * e + 1]);
         }
 #pragma unroll
         for (int e = 0; e < 27; ++e)
@@ -855,10 +865,10 @@ __device__ __forceinline__ double stream_sum(double v, unsigned gmask)
 
 template <typename T>
 __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
-    int64_t B, const int64_t* __restrict__ pair_offset, const int4* __restrict__ pairs,
+    int64_t B, const int64_t* __restrict__ pair_offset, const int2* __restrict__ pairs,
     const int* __restrict__ block_row, const int* __restrict__ block_col, const int* __restrict__ transpose,
     const int* __restrict__ block_pc,
-    const T* __restrict__ w, const double* __restrict__ hy, const T* __restrict__ pcv, T* __restrict__ S)
+    const T* __restrict__ w, const double* __restrict__ tfactor, const T* __restrict__ pcv, T* __restrict__ S)
 {
     const int g = threadIdx.x & (kPairLanes - 1);
     const int s = g >> 1, h = g & 1;
@@ -876,29 +886,24 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
                 acc[r][c] = 0.0;
         const int64_t k1 = pair_offset[b + 1];
         int64_t k = pair_offset[b] + s;
-        int4 next = k < k1 ? pairs[k] : make_int4(0, 0, 0, 0);
+        int2 next = k < k1 ? pairs[k] : make_int2(0, 0);
         while (k < k1)
         {
-            const int4 cur = next;
+            const int2 cur = next;
             k += kPairStreams;
             if (k < k1)
                 next = pairs[k];
-            // Hll^-1 (symmetric) and this lane's three rows of W_lp (elements 9h .. 9h + 8,
-            // read as the aligned run 8h .. 8h + 9)
-            double hv[10], a[10], q[18];
-            load_pairs<double, 10>(hy + int64_t(cur.z) * 12, hv);
-            load_pairs<T, 10>(w + int64_t(cur.x) * 18 + 8 * h, a);
+            // this lane's three rows of T = W_lp Hll^-1 (elements 9h .. 9h + 8, read as the
+            // aligned run 8h .. 8h + 9; the rows of a block row lie together in row-list order)
+            double a[10], q[18];
+            load_pairs<double, 10>(tfactor + int64_t(cur.x) * 18 + 8 * h, a);
             load_pairs<T, 18>(w + int64_t(cur.y) * 18, q);
             double tr[3][3];
 #pragma unroll
             for (int r = 0; r < 3; ++r)
-            {
-                const double w0 = h ? a[3 * r + 1] : a[3 * r], w1 = h ? a[3 * r + 2] : a[3 * r + 1],
-                             w2 = h ? a[3 * r + 3] : a[3 * r + 2];
 #pragma unroll
                 for (int kk = 0; kk < 3; ++kk)
-                    tr[r][kk] = hv[3 * kk] * w0 + hv[3 * kk + 1] * w1 + hv[3 * kk + 2] * w2;
-            }
+                    tr[r][kk] = h ? a[3 * r + kk + 1] : a[3 * r + kk];
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -1593,13 +1598,15 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     Carver plan_b;
     plan_b.take<int2>(C + 1);
     plan_b.take<int64_t>(B + 2);
-    plan_b.take<int4>(E + 1);
+    plan_b.take<int2>(E + 1);
+    plan_b.take<double>(C * 18 + 2);
     ws->pair_buffer.ensure(plan_b.offset + 512, stream, "SchurComplementSolverWorkspace");
     Carver bc;
     bc.base = static_cast<char*>(ws->pair_buffer.ptr);
     ws->row_entries = bc.take<int2>(C + 1);
     ws->pair_offset = bc.take<int64_t>(B + 2);
-    ws->pairs = bc.take<int4>(E + 1);
+    ws->pairs = bc.take<int2>(E + 1);
+    ws->tfactor = bc.take<double>(C * 18 + 2);
     ws->E = E;
     PM_CUDA(cudaMemsetAsync(block_pairs, 0, size_t(B + 1) * sizeof(int), stream));
     PM_CUDA(cudaMemsetAsync(mask, 0, size_t(B + 1) * sizeof(unsigned), stream));
@@ -1795,12 +1802,12 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
     {
         assemble_diag6_kernel<T><<<grid_for(a.P, 1, 1 << 20), kDiagThreads, 0, stream>>>(
             a.P, ws->prim_offsets, ws->row_entries, a.w, ws->hinv, a.hpp, a.gp, a.lambda, a.min_diag, a.diag_pos,
-            a.S, a.rhs);
+            a.S, a.rhs, ws->tfactor);
         PM_LAUNCH_CHECK();
         // every upper block, also those whose only terms are primary-primary couplings
         assemble_upper6_kernel<T><<<grid_for(ws->B * kPairLanes, kUpperThreads), kUpperThreads, 0, stream>>>(
-            ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, a.w, ws->hinv,
-            a.pcv, a.S);
+            ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, a.w,
+            ws->tfactor, a.pcv, a.S);
         PM_LAUNCH_CHECK();
         diag_inverse_kernel<T, 6><<<grid_for(a.P, 64, 1 << 16), 64, 0, stream>>>(a.P, a.diag_pos, a.S, a.minv,
                                                                                  a.status);
