@@ -41,7 +41,7 @@ REF_SAMPLE_L = 100_000  # eliminated blocks of the reference CPU sample (5% of t
 LEARN_TRAIN, LEARN_HOLD, LEARN_STEPS = 8, 3, 20
 # DRAM bytes (read + write) of one full-size assembly (assemble_diag6 + assemble_upper6), from an
 # ncu capture of `python bench.py --steps 2 --warmup 1 --no-extras` with dram__bytes_{read,write}.sum
-ASSEMBLY_TRAFFIC_BYTES = 5_648_000_000
+ASSEMBLY_TRAFFIC_BYTES = 8_126_000_000
 BATCH_SYSTEMS = 512
 
 
