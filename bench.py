@@ -320,7 +320,7 @@ def run_ours(args):
                           "learned_true_relative_residual": r["learned"]["true_relative_residual"]}
                          for r in evaluation],
         },
-        "roofline": {"bound": "hbm", "kernel": "assemble_upper6_kernel<double> + assemble_diag6_kernel<double> (+ block-Jacobi inverse, mirror)",
+        "roofline": {"bound": "hbm", "kernel": "assemble_upper6_kernel<double> + assemble_diag6_kernel<double> (+ block-Jacobi inverse)",
                      "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": ASSEMBLY_TRAFFIC_BYTES if L == L_FULL else None,
