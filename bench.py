@@ -363,6 +363,7 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=Non
     out["spmv"] = sparse_leg(torch, S, W, stream)
     # ---- batched uneven systems
     out["batched"] = batched_leg(torch, SC, W, net)
+    out["dense_c4_max"] = dense_leg(torch, SC, W)
     # ---- CPU baseline: the reference's own CPU library on a bounded sample, scaled
     try:
         import oracle
@@ -473,6 +474,29 @@ def sparse_leg(torch, S, W, stream):
         spmv[f"coo_to_csr_laplacian128_{name}"] = {"ms": round(tc, 4), "GBps": round(cbytes / (tc * 1e-3) / 1e9, 1),
                                                    "triplets": trip, "algorithmic_bytes": cbytes}
     return spmv
+
+
+def dense_leg(torch, SC, W):
+    """The largest C4 system size (P=512, L=50,000; n = 3,072 primary unknowns): the dense backend
+    (device Cholesky, DenseCpu's counterpart) against block-Jacobi PCG, whole solve each."""
+    prob = W.bundle_problem(512, 50000, per_eliminated=4, window=40, seed=5)
+    ne = SC.DeviceNormalEquations(512, 50000, 6, 3)
+    ne.accumulate_observations(*[torch.from_numpy(prob[k]).cuda() for k in ("obs_primary", "obs_eliminated", "jp",
+                                                                            "jl", "residual")], prob["huber_delta"])
+    out = {"primary_unknowns": 512 * 6}
+    for name, backend in (("pcg", "pcg"), ("dense", "dense")):
+        ws = SC.SchurComplementSolverWorkspace()
+        opts = SC.SchurComplementSolverOptions(max_iterations=1000, relative_tolerance=1e-8, linear_backend=backend)
+        SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+        times = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            _, _, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+            times.append(rep["total_ms"])
+        out[name] = {"ms": round(statistics.median(times), 3), "solve_ms": round(rep["solve_ms"], 3),
+                     "iterations": rep["iterations"], "converged": bool(rep["converged"]),
+                     "true_relative_residual": rep["true_relative_residual"]}
+    return out
 
 
 def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
