@@ -118,7 +118,15 @@ def test_dense_backend_rejections(checkers):
     o.add_residual([0], [1.0], 0, [2.0], [1.0])
     dp, dl, rep = SC.solve_damped_schur_complement(_device_ne(o), 0.0, _opts(linear_backend="dense"))
     assert not rep["converged"] and rep["message"] == "reduced Schur complement is not positive definite"
-    big = SC.DeviceNormalEquations(SC.DENSE_MAX_UNKNOWNS // 6 + 1, 1, 6, 3)
+    # a zero pivot in a later panel (column 69 of 70): found when that panel's diagonal block is
+    # factored after the trailing update that finishes it
+    o = checkers.NormalEquations(70, 1, 1, 1)
+    for p in range(69):
+        o.add_residual([p], [1.0], -1, None, [1.0])
+    o.add_residual([], None, 0, [1.0], [1.0])
+    dp, dl, rep = SC.solve_damped_schur_complement(_device_ne(o), 0.0, _opts(linear_backend="dense"))
+    assert not rep["converged"] and rep["message"] == "reduced Schur complement is not positive definite"
+    big =SC.DeviceNormalEquations(SC.DENSE_MAX_UNKNOWNS // 6 + 1, 1, 6, 3)
     with pytest.raises(N.InvalidArgument, match="16,384"):
         SC.solve_damped_schur_complement(big, 1e-3, _opts(linear_backend="dense"))
 
