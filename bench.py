@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--eliminated", type=int, default=L_FULL, help="L (eliminated blocks)")
     ap.add_argument("--no-extras", action="store_true", help="skip SpMV / e2e / CPU-baseline legs")
     ap.add_argument("--sparse-only", action="store_true", help="only the Laplacian SpMV / COO->CSR leg")
+    ap.add_argument("--dense-only", action="store_true", help="only the dense-backend vs PCG leg (n = 3,072)")
     return ap.parse_args()
 
 
@@ -576,5 +577,10 @@ if __name__ == "__main__":
         from plamatrix_b200 import sparse as S_
         from plamatrix_b200 import workloads as W_
         print(json.dumps({"spmv": sparse_leg(torch, S_, W_, torch.cuda.current_stream())}))
+    elif a.dense_only:
+        import torch
+        from plamatrix_b200 import schur as SC_
+        from plamatrix_b200 import workloads as W_
+        print(json.dumps({"dense_c4_max": dense_leg(torch, SC_, W_)}))
     else:
         run_ours(a)
