@@ -5,8 +5,8 @@
 //     f[r(r+1)/2 + c] = sign(a) log1p(|a|),  a = S_pp[r][c] / s   (c <= r)
 //     f[21..23] = log1p(mean / max / min of ||S_pq||_F / s over q != p), f[24] = log1p(count) / 4
 //   network 25 -> 128 -> 128 -> 21 with GELU (x Phi(x)); every GEMM runs on the tensor cores
-//   (mma.sync m16n8k16, BF16 operands rounded to nearest even, FP32 accumulation); master
-//   weights, activations and gradients are FP32.
+//   (tcgen05.mma kind::f16 into tensor memory, BF16 operands rounded to nearest even, FP32
+//   accumulation); master weights, activations and gradients are FP32.
 //   preconditioner: L = chol(S_pp) (FP64), L'_ii = L_ii softplus(o_ii) / ln 2,
 //   L'_ij = L_ij + o_ij L_jj, block (L'L'^T)^-1 in FP64.
 //   loss of a solved system (x, b): sum_p ||L'L'^T x_p - b_p||^2 / sum_p ||b_p||^2.
@@ -129,101 +129,210 @@ __global__ void __launch_bounds__(128) features_kernel(int64_t P, const int* __r
     }
 }
 
-// ---------------------------------------------------------------- tensor-core GEMM
+// ---------------------------------------------------------------- tensor-core GEMM (tcgen05)
 // C (M x N) = A (M x K) B (K x N) [+ bias], A(m, k) = A[m*sam + k*sak], B(k, n) = B[k*sbk + n*sbn];
-// with H != nullptr also H = gelu(C).  CTA tile 64 x 64, four warps of 16 rows x 64 columns,
-// K in steps of 32 staged in shared memory as BF16 (round to nearest even); mma.sync
-// m16n8k16 with FP32 accumulators.  The K order is fixed: results are reproducible.
-constexpr int kTileM = 64, kTileN = 64, kTileK = 32, kTilePad = 8;
+// with H != nullptr also H = gelu(C).  One CTA of 128 threads per 128 x 64 tile of C.  K runs in
+// steps of 32: the threads stage both operands in shared memory as BF16 (round to nearest even)
+// in the K-major, unswizzled canonical layout (core matrices of 8 rows x 16 bytes; K-adjacent
+// core matrices kTcLbo bytes apart, 8-row groups kTcSbo apart); thread 0 issues two
+// tcgen05.mma kind::f16 (128 x 64 x 16, FP32 accumulator in tensor memory) and commits them to
+// an mbarrier that every thread waits on before the stage is overwritten.  The epilogue reads
+// the accumulator with tcgen05.ld (warp w owns rows 32w..32w+31).  The K order is fixed, so
+// results are reproducible.  Every wait is bounded: one that runs out sets *error, the CTA
+// issues nothing more, waits (bounded) once more for its last commit and frees its tensor
+// memory; the host turns the flag into an error.
+constexpr int kTcM = 128, kTcN = 64, kTcK = 32, kTcThreads = 128;
+constexpr uint32_t kTcCols = 64;                     // tensor-memory columns of the accumulator
+constexpr int kTcLbo = 128;                          // bytes between K-adjacent core matrices
+constexpr int kTcSbo = kTcLbo * (kTcK / 8);          // bytes between 8-row groups
+// dynamic shared memory reserved per CTA so that at most 7 CTAs share an SM: 7 x 64 columns fit
+// the 512 columns of tensor memory, and no allocation waits for another CTA
+constexpr size_t kTcSmemReserve = 16384;
+constexpr long long kTcWaitLimit = 1ll << 20;
+// kind::f16 instruction descriptor: FP32 accumulator (bits 4-5), BF16 A (7-9) and B (10-12),
+// both K-major (15, 16), N >> 3 (17-22), M >> 4 (24-28)
+constexpr uint32_t kTcIdesc =
+    (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kTcN >> 3) << 17) | (uint32_t(kTcM >> 4) << 24);
 
-__device__ __forceinline__ uint32_t pack2(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
-
-// With kchunk > 0 the K range is split over blockIdx.z (chunks of kchunk) and every split writes
-// its partial tile to C + blockIdx.z * M * ldc (no bias / activation); reduce_splits_kernel
-// adds the splits in order.
-__global__ void __launch_bounds__(128) gemm_bf16_kernel(int M, int N, int K, const float* __restrict__ A, int64_t sam,
-                                                        int64_t sak, const float* __restrict__ B, int64_t sbk,
-                                                        int64_t sbn, const float* __restrict__ bias,
-                                                        float* __restrict__ C, int64_t ldc, float* __restrict__ H,
-                                                        int kchunk)
+// element (r, k) of a staged operand tile -> its BF16 offset in the canonical layout
+__device__ __forceinline__ int tc_offset(int r, int k)
 {
-    __shared__ __align__(16) __nv_bfloat16 As[kTileM][kTileK + kTilePad]; // [m][k]
-    __shared__ __align__(16) __nv_bfloat16 Bs[kTileN][kTileK + kTilePad]; // [n][k]
+    return (r >> 3) * (kTcSbo / 2) + (k >> 3) * (kTcLbo / 2) + (r & 7) * 8 + (k & 7);
+}
+
+// shared-memory matrix descriptor: start address, leading (K) and stride (8-row) byte offsets,
+// all >> 4; version 1 (bit 46); no swizzle, base offset 0
+__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t addr)
+{
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((kTcLbo >> 4) & 0x3FFF) << 16) |
+           (uint64_t((kTcSbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (long long it = 0; it < kTcWaitLimit; ++it)
+    {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (done)
+            return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_load_32x32b_x64(uint32_t taddr, uint32_t (&r)[64])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K, const float* __restrict__ A,
+                                                             int64_t sam, int64_t sak, const float* __restrict__ B,
+                                                             int64_t sbk, int64_t sbn, const float* __restrict__ bias,
+                                                             float* __restrict__ C, int64_t ldc,
+                                                             float* __restrict__ H, int kchunk, int* __restrict__ error)
+{
+    __shared__ __align__(128) __nv_bfloat16 As[kTcM * kTcK];
+    __shared__ __align__(128) __nv_bfloat16 Bs[kTcN * kTcK];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-    const int g = lane >> 2, tq = lane & 3;
-    const int m0 = blockIdx.x * kTileM, n0 = blockIdx.y * kTileN;
+    const int m0 = blockIdx.x * kTcM, n0 = blockIdx.y * kTcN;
     const int kb = kchunk > 0 ? blockIdx.z * kchunk : 0;
     const int ke = kchunk > 0 ? min(K, kb + kchunk) : K;
     if (kchunk > 0)
         C += int64_t(blockIdx.z) * M * ldc;
-    float acc[8][4];
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
-            acc[j][e] = 0.0f;
-    for (int k0 = kb; k0 < ke; k0 += kTileK)
+    const uint32_t bar_addr = static_cast<uint32_t>(__cvta_generic_to_shared(&bar));
+    if (warp == 0)
     {
-        for (int i = t; i < kTileM * kTileK; i += 128)
+        const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&tmem_base));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(dst), "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    if (t == 32)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_addr) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const uint32_t a_addr = static_cast<uint32_t>(__cvta_generic_to_shared(As));
+    const uint32_t b_addr = static_cast<uint32_t>(__cvta_generic_to_shared(Bs));
+    uint32_t parity = 0;
+    bool issued = false, ok = true;
+    for (int k0 = kb; k0 < ke; k0 += kTcK)
+    {
+        for (int i = t; i < kTcM * kTcK; i += kTcThreads)
         {
-            const int mm = i / kTileK, kk = i - mm * kTileK;
+            const int mm = i / kTcK, kk = i - mm * kTcK;
             const int gm = m0 + mm, gk = k0 + kk;
             const float a = gm < M && gk < ke ? A[int64_t(gm) * sam + int64_t(gk) * sak] : 0.0f;
-            As[mm][kk] = __float2bfloat16_rn(a);
+            As[tc_offset(mm, kk)] = __float2bfloat16_rn(a);
         }
-        for (int i = t; i < kTileN * kTileK; i += 128)
+        for (int i = t; i < kTcN * kTcK; i += kTcThreads)
         {
-            const int nn = i / kTileK, kk = i - nn * kTileK;
+            const int nn = i / kTcK, kk = i - nn * kTcK;
             const int gn = n0 + nn, gk = k0 + kk;
             const float b = gn < N && gk < ke ? B[int64_t(gk) * sbk + int64_t(gn) * sbn] : 0.0f;
-            Bs[nn][kk] = __float2bfloat16_rn(b);
+            Bs[tc_offset(nn, kk)] = __float2bfloat16_rn(b);
         }
+        // the generic-proxy stores must be visible to the tensor core's (async-proxy) reads
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kTileK; kk += 16)
+        if (t == 0)
         {
-            const int r = warp * 16 + g;
-            const uint32_t a0 = pack2(&As[r][kk + 2 * tq]);
-            const uint32_t a1 = pack2(&As[r + 8][kk + 2 * tq]);
-            const uint32_t a2 = pack2(&As[r][kk + 2 * tq + 8]);
-            const uint32_t a3 = pack2(&As[r + 8][kk + 2 * tq + 8]);
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int h = 0; h < kTcK / 16; ++h)
             {
-                const uint32_t b0 = pack2(&Bs[j * 8 + g][kk + 2 * tq]);
-                const uint32_t b1 = pack2(&Bs[j * 8 + g][kk + 2 * tq + 8]);
-                asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, "
-                             "{%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
-                             : "+f"(acc[j][0]), "+f"(acc[j][1]), "+f"(acc[j][2]), "+f"(acc[j][3])
-                             : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+                const uint64_t ad = tc_smem_desc(a_addr + h * 2 * kTcLbo);
+                const uint64_t bd = tc_smem_desc(b_addr + h * 2 * kTcLbo);
+                const uint32_t accumulate = (issued || h > 0) ? 1u : 0u;
+                asm volatile("{\n\t.reg .pred p;\n\t"
+                             "setp.ne.b32 p, %4, 0;\n\t"
+                             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                             ::"r"(tmem), "l"(ad), "l"(bd), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u),
+                             "r"(0u), "r"(0u)
+                             : "memory");
             }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             bar_addr)
+                         : "memory");
         }
-        __syncthreads();
+        issued = true;
+        ok = __syncthreads_and(mbar_wait(bar_addr, parity)) != 0;
+        parity ^= 1u;
+        if (!ok)
+            break;
     }
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-#pragma unroll
-        for (int e = 0; e < 4; ++e)
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    if (ok)
+    {
+        uint32_t r[64];
+        if (issued)
         {
-            const int gm = m0 + warp * 16 + g + (e >= 2 ? 8 : 0);
-            const int gn = n0 + j * 8 + 2 * tq + (e & 1);
-            if (gm < M && gn < N)
+            tmem_load_32x32b_x64(tmem + (uint32_t(warp * 32) << 16), r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        }
+        else
+        {
+#pragma unroll
+            for (int j = 0; j < 64; ++j)
+                r[j] = 0u;
+        }
+        const int gm = m0 + warp * 32 + lane;
+        if (gm < M)
+        {
+#pragma unroll
+            for (int j = 0; j < kTcN; ++j)
             {
-                const float z = acc[j][e] + (bias ? bias[gn] : 0.0f);
-                C[int64_t(gm) * ldc + gn] = z;
-                if (H)
-                    H[int64_t(gm) * ldc + gn] = gelu(z);
+                const int gn = n0 + j;
+                if (gn < N)
+                {
+                    const float z = __uint_as_float(r[j]) + (bias ? bias[gn] : 0.0f);
+                    C[int64_t(gm) * ldc + gn] = z;
+                    if (H)
+                        H[int64_t(gm) * ldc + gn] = gelu(z);
+                }
             }
         }
+    }
+    else
+    {
+        if (t == 0)
+            atomicExch(error, 1);
+        mbar_wait(bar_addr, parity ^ 1u); // the commit that did not arrive in time
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTcCols) : "memory");
 }
 
 void gemm(cudaStream_t stream, int M, int N, int K, const float* A, int64_t sam, int64_t sak, const float* B,
-          int64_t sbk, int64_t sbn, const float* bias, float* C, int64_t ldc, float* H = nullptr)
+          int64_t sbk, int64_t sbn, const float* bias, float* C, int64_t ldc, int* error, float* H = nullptr)
 {
     if (M <= 0 || N <= 0)
         return;
-    const dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN);
-    gemm_bf16_kernel<<<grid, 128, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, bias, C, ldc, H, 0);
+    const dim3 grid((M + kTcM - 1) / kTcM, (N + kTcN - 1) / kTcN);
+    gemm_tc_kernel<<<grid, kTcThreads, kTcSmemReserve, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, bias, C, ldc, H,
+                                                                 0, error);
     PM_LAUNCH_CHECK();
 }
 
@@ -247,14 +356,14 @@ int split_count(int64_t K) { return static_cast<int>((K + kSplitRows - 1) / kSpl
 
 // C = A B with the K (row) dimension split over CTAs; `part` holds split_count(K) * M * N floats
 void gemm_split(cudaStream_t stream, int M, int N, int K, const float* A, int64_t sam, int64_t sak, const float* B,
-                int64_t sbk, int64_t sbn, float* C, int64_t ldc, float* part)
+                int64_t sbk, int64_t sbn, float* C, int64_t ldc, float* part, int* error)
 {
     if (M <= 0 || N <= 0)
         return;
     const int splits = split_count(K);
-    const dim3 grid((M + kTileM - 1) / kTileM, (N + kTileN - 1) / kTileN, splits);
-    gemm_bf16_kernel<<<grid, 128, 0, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, nullptr, part, N, nullptr,
-                                               kSplitRows);
+    const dim3 grid((M + kTcM - 1) / kTcM, (N + kTcN - 1) / kTcN, splits);
+    gemm_tc_kernel<<<grid, kTcThreads, kTcSmemReserve, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, nullptr, part, N,
+                                                                 nullptr, kSplitRows, error);
     PM_LAUNCH_CHECK();
     reduce_splits_kernel<<<grid_for(int64_t(M) * N, 256, 1024), 256, 0, stream>>>(M, N, splits, part, C, ldc);
     PM_LAUNCH_CHECK();
@@ -517,6 +626,17 @@ void allocate_state(pm_mlp* mlp)
 }
 
 int* bad_flag(pm_mlp* mlp) { return mlp->bad; }
+// set by a tensor-core GEMM whose bounded wait ran out (reset before every forward pass)
+int* tc_error_flag(pm_mlp* mlp) { return mlp->bad + 1; }
+
+void check_tc_error(pm_mlp* mlp, cudaStream_t stream)
+{
+    int flag = 0;
+    PM_CUDA(cudaMemcpyAsync(&flag, tc_error_flag(mlp), sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaStreamSynchronize(stream));
+    if (flag)
+        fail(PM_RUNTIME_ERROR, "learned preconditioner: a tensor-core GEMM did not complete");
+}
 
 void ensure_rows(pm_mlp* mlp, int64_t P, cudaStream_t stream)
 {
@@ -562,6 +682,7 @@ void forward(pm_mlp* mlp, const SchurView& v, cudaStream_t stream)
     mlp->rows = P;
     if (P == 0)
         return;
+    PM_CUDA(cudaMemsetAsync(tc_error_flag(mlp), 0, sizeof(int), stream));
     const unsigned grid = grid_for(P * 32, 128, 1 << 16);
     if (v.value_size == 8)
         features_kernel<double><<<grid, 128, 0, stream>>>(P, v.block_row_ptr, v.block_col, v.diag_pos,
@@ -572,10 +693,11 @@ void forward(pm_mlp* mlp, const SchurView& v, cudaStream_t stream)
     PM_LAUNCH_CHECK();
     const int M = static_cast<int>(P);
     const float* W = mlp->params;
-    gemm(stream, M, kHid, kIn, mlp->F, kInPad, 1, W + kOffW1, kHid, 1, W + kOffB1, mlp->Z1, kHid, mlp->H1);
-    gemm(stream, M, kHid, kHid, mlp->H1, kHid, 1, W + kOffW2, kHid, 1, W + kOffB2, mlp->Z2, kHid, mlp->H2);
+    int* error = tc_error_flag(mlp);
+    gemm(stream, M, kHid, kIn, mlp->F, kInPad, 1, W + kOffW1, kHid, 1, W + kOffB1, mlp->Z1, kHid, error, mlp->H1);
+    gemm(stream, M, kHid, kHid, mlp->H1, kHid, 1, W + kOffW2, kHid, 1, W + kOffB2, mlp->Z2, kHid, error, mlp->H2);
     PM_CUDA(cudaMemsetAsync(mlp->O, 0, size_t(P) * kOutPad * sizeof(float), stream));
-    gemm(stream, M, kOut, kHid, mlp->H2, kHid, 1, W + kOffW3, kOut, 1, W + kOffB3, mlp->O, kOutPad);
+    gemm(stream, M, kOut, kHid, mlp->H2, kHid, 1, W + kOffW3, kOut, 1, W + kOffB3, mlp->O, kOutPad, error);
 }
 
 void check_view(const SchurView& v)
@@ -604,10 +726,12 @@ void mlp_apply(const pm_mlp* cmlp, const SchurView& v, cudaStream_t stream)
         precond_kernel<float><<<grid, 64, 0, stream>>>(v.P, v.diag_pos, static_cast<const float*>(v.S), mlp->O,
                                                        v.minv, v.mixed ? v.minv32 : nullptr, bad_flag(mlp));
     PM_LAUNCH_CHECK();
-    int bad = 0;
-    PM_CUDA(cudaMemcpyAsync(&bad, bad_flag(mlp), sizeof(int), cudaMemcpyDeviceToHost, stream));
+    int bad[2] = {0, 0};
+    PM_CUDA(cudaMemcpyAsync(bad, bad_flag(mlp), 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
     PM_CUDA(cudaStreamSynchronize(stream));
-    if (bad)
+    if (bad[1])
+        fail(PM_RUNTIME_ERROR, "learned preconditioner: a tensor-core GEMM did not complete");
+    if (bad[0])
         fail(PM_RUNTIME_ERROR, "learned preconditioner: a corrected block is not positive definite");
 }
 
@@ -648,17 +772,18 @@ double train(pm_mlp* mlp, const SchurView& v, cudaStream_t stream, const double*
     float* G = mlp->grads;
     const float* W = mlp->params;
     float* splits = mlp->split;
-    gemm_split(stream, kHid, kOut, M, mlp->H2, 1, kHid, mlp->dO, kOutPad, 1, G + kOffW3, kOut, splits);
+    int* error = tc_error_flag(mlp);
+    gemm_split(stream, kHid, kOut, M, mlp->H2, 1, kHid, mlp->dO, kOutPad, 1, G + kOffW3, kOut, splits, error);
     colsum(stream, P, kOut, kOutPad, mlp->dO, G + kOffB3, splits);
-    gemm(stream, M, kHid, kOut, mlp->dO, kOutPad, 1, W + kOffW3, 1, kOut, nullptr, mlp->dH, kHid);
+    gemm(stream, M, kHid, kOut, mlp->dO, kOutPad, 1, W + kOffW3, 1, kOut, nullptr, mlp->dH, kHid, error);
     gelu_back_kernel<<<grid_for(P * kHid, 256, 4096), 256, 0, stream>>>(P * kHid, mlp->dH, mlp->Z2, mlp->dZ);
     PM_LAUNCH_CHECK();
-    gemm_split(stream, kHid, kHid, M, mlp->H1, 1, kHid, mlp->dZ, kHid, 1, G + kOffW2, kHid, splits);
+    gemm_split(stream, kHid, kHid, M, mlp->H1, 1, kHid, mlp->dZ, kHid, 1, G + kOffW2, kHid, splits, error);
     colsum(stream, P, kHid, kHid, mlp->dZ, G + kOffB2, splits);
-    gemm(stream, M, kHid, kHid, mlp->dZ, kHid, 1, W + kOffW2, 1, kHid, nullptr, mlp->dH, kHid);
+    gemm(stream, M, kHid, kHid, mlp->dZ, kHid, 1, W + kOffW2, 1, kHid, nullptr, mlp->dH, kHid, error);
     gelu_back_kernel<<<grid_for(P * kHid, 256, 4096), 256, 0, stream>>>(P * kHid, mlp->dH, mlp->Z1, mlp->dZ);
     PM_LAUNCH_CHECK();
-    gemm_split(stream, kIn, kHid, M, mlp->F, 1, kInPad, mlp->dZ, kHid, 1, G + kOffW1, kHid, splits);
+    gemm_split(stream, kIn, kHid, M, mlp->F, 1, kInPad, mlp->dZ, kHid, 1, G + kOffW1, kHid, splits, error);
     colsum(stream, P, kHid, kHid, mlp->dZ, G + kOffB1, splits);
     if (lr > 0.0)
     {
@@ -673,7 +798,7 @@ double train(pm_mlp* mlp, const SchurView& v, cudaStream_t stream, const double*
     int host_bad = 0;
     PM_CUDA(cudaMemcpyAsync(host, den, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     PM_CUDA(cudaMemcpyAsync(&host_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    PM_CUDA(cudaStreamSynchronize(stream));
+    check_tc_error(mlp, stream);
     if (host_bad)
         fail(PM_RUNTIME_ERROR, "learned preconditioner: a diagonal block is not positive definite");
     if (!(host[0] > 0.0))
@@ -765,6 +890,7 @@ int pm_mlp_forward(pm_mlp* mlp, pm_schur_workspace* ws, pm_stream_t stream)
         const pm::SchurView v = pm::schur_view(ws, false);
         pm::check_view(v);
         pm::forward(mlp, v, stream);
+        pm::check_tc_error(mlp, stream);
         PM_CUDA(cudaStreamSynchronize(stream));
     });
 }
