@@ -132,22 +132,24 @@ __global__ void __launch_bounds__(128) features_kernel(int64_t P, const int* __r
 // ---------------------------------------------------------------- tensor-core GEMM (tcgen05)
 // C (M x N) = A (M x K) B (K x N) [+ bias], A(m, k) = A[m*sam + k*sak], B(k, n) = B[k*sbk + n*sbn];
 // with H != nullptr also H = gelu(C).  One CTA of 128 threads per 128 x 64 tile of C.  K runs in
-// steps of 32: the threads stage both operands in shared memory as BF16 (round to nearest even)
-// in the K-major, unswizzled canonical layout (core matrices of 8 rows x 16 bytes; K-adjacent
-// core matrices kTcLbo bytes apart, 8-row groups kTcSbo apart); thread 0 issues two
-// tcgen05.mma kind::f16 (128 x 64 x 16, FP32 accumulator in tensor memory) and commits them to
-// an mbarrier that every thread waits on before the stage is overwritten.  The epilogue reads
-// the accumulator with tcgen05.ld (warp w owns rows 32w..32w+31).  The K order is fixed, so
-// results are reproducible.  Every wait is bounded: one that runs out sets *error, the CTA
-// issues nothing more, waits (bounded) once more for its last commit and frees its tensor
-// memory; the host turns the flag into an error.
+// steps of 32 over two shared-memory stages: the threads fill one stage with both operands as
+// BF16 (round to nearest even) in the K-major, unswizzled canonical layout (core matrices of 8
+// rows x 16 bytes; K-adjacent core matrices kTcLbo bytes apart, 8-row groups kTcSbo apart) while
+// the tensor core reads the other; thread 0 issues two tcgen05.mma kind::f16 per step (128 x 64
+// x 16, FP32 accumulator in tensor memory) and commits them to the stage's mbarrier, which the
+// threads wait on before they refill that stage.  The epilogue reads the accumulator with
+// tcgen05.ld (warp w owns rows 32w..32w+31).  The K order is fixed, so results are
+// reproducible.  Every wait is bounded: one that runs out sets *error, the CTA issues nothing
+// more, waits (bounded) for its last commit and frees its tensor memory; the host turns the
+// flag into an error.
 constexpr int kTcM = 128, kTcN = 64, kTcK = 32, kTcThreads = 128;
 constexpr uint32_t kTcCols = 64;                     // tensor-memory columns of the accumulator
 constexpr int kTcLbo = 128;                          // bytes between K-adjacent core matrices
 constexpr int kTcSbo = kTcLbo * (kTcK / 8);          // bytes between 8-row groups
-// dynamic shared memory reserved per CTA so that at most 7 CTAs share an SM: 7 x 64 columns fit
-// the 512 columns of tensor memory, and no allocation waits for another CTA
-constexpr size_t kTcSmemReserve = 16384;
+// dynamic shared memory reserved per CTA (beside 24.6 KB of static stages) so that at most 7
+// CTAs share an SM: 7 x 64 columns fit the 512 columns of tensor memory, and no allocation waits
+// for another CTA
+constexpr size_t kTcSmemReserve = 4096;
 constexpr long long kTcWaitLimit = 1ll << 20;
 // kind::f16 instruction descriptor: FP32 accumulator (bits 4-5), BF16 A (7-9) and B (10-12),
 // both K-major (15, 16), N >> 3 (17-22), M >> 4 (24-28)
@@ -205,9 +207,9 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
                                                              float* __restrict__ C, int64_t ldc,
                                                              float* __restrict__ H, int kchunk, int* __restrict__ error)
 {
-    __shared__ __align__(128) __nv_bfloat16 As[kTcM * kTcK];
-    __shared__ __align__(128) __nv_bfloat16 Bs[kTcN * kTcK];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(128) __nv_bfloat16 As[2][kTcM * kTcK];
+    __shared__ __align__(128) __nv_bfloat16 Bs[2][kTcN * kTcK];
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ uint32_t tmem_base;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
     const int m0 = blockIdx.x * kTcM, n0 = blockIdx.y * kTcN;
@@ -215,7 +217,8 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
     const int ke = kchunk > 0 ? min(K, kb + kchunk) : K;
     if (kchunk > 0)
         C += int64_t(blockIdx.z) * M * ldc;
-    const uint32_t bar_addr = static_cast<uint32_t>(__cvta_generic_to_shared(&bar));
+    const uint32_t bar_addr[2] = {static_cast<uint32_t>(__cvta_generic_to_shared(&bar[0])),
+                                  static_cast<uint32_t>(__cvta_generic_to_shared(&bar[1]))};
     if (warp == 0)
     {
         const uint32_t dst = static_cast<uint32_t>(__cvta_generic_to_shared(&tmem_base));
@@ -225,32 +228,69 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
     }
     if (t == 32)
     {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_addr) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_addr[0]) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_addr[1]) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = tmem_base;
-    const uint32_t a_addr = static_cast<uint32_t>(__cvta_generic_to_shared(As));
-    const uint32_t b_addr = static_cast<uint32_t>(__cvta_generic_to_shared(Bs));
-    uint32_t parity = 0;
-    bool issued = false, ok = true;
-    for (int k0 = kb; k0 < ke; k0 += kTcK)
-    {
-        for (int i = t; i < kTcM * kTcK; i += kTcThreads)
+    const bool a_kfast = sak == 1, b_kfast = sbk == 1;
+    // one step's operands in registers: every load of the step is issued before any is used, and
+    // the next step's loads are issued while the tensor core works on the current one;
+    // consecutive threads walk the operand's unit-stride index (k, or the row) so that the loads
+    // of a warp are coalesced
+    constexpr int kAPer = kTcM * kTcK / kTcThreads, kBPer = kTcN * kTcK / kTcThreads;
+    float av[kAPer], bv[kBPer];
+    auto load_step = [&](int k0) {
+#pragma unroll
+        for (int j = 0; j < kAPer; ++j)
         {
-            const int mm = i / kTcK, kk = i - mm * kTcK;
+            const int i = t + j * kTcThreads;
+            const int mm = a_kfast ? i / kTcK : i % kTcM, kk = a_kfast ? i % kTcK : i / kTcM;
             const int gm = m0 + mm, gk = k0 + kk;
-            const float a = gm < M && gk < ke ? A[int64_t(gm) * sam + int64_t(gk) * sak] : 0.0f;
-            As[tc_offset(mm, kk)] = __float2bfloat16_rn(a);
+            av[j] = gm < M && gk < ke ? A[int64_t(gm) * sam + int64_t(gk) * sak] : 0.0f;
         }
-        for (int i = t; i < kTcN * kTcK; i += kTcThreads)
+#pragma unroll
+        for (int j = 0; j < kBPer; ++j)
         {
-            const int nn = i / kTcK, kk = i - nn * kTcK;
+            const int i = t + j * kTcThreads;
+            const int nn = b_kfast ? i / kTcK : i % kTcN, kk = b_kfast ? i % kTcK : i / kTcN;
             const int gn = n0 + nn, gk = k0 + kk;
-            const float b = gn < N && gk < ke ? B[int64_t(gk) * sbk + int64_t(gn) * sbn] : 0.0f;
-            Bs[tc_offset(nn, kk)] = __float2bfloat16_rn(b);
+            bv[j] = gn < N && gk < ke ? B[int64_t(gk) * sbk + int64_t(gn) * sbn] : 0.0f;
+        }
+    };
+    // stage s is refilled at step i >= 2 once the commit of step i - 2 (completion (i >> 1) - 1 of
+    // bar[s]) has arrived; the MMAs run in issue order, so the last commit covers every step
+    int step = 0;
+    bool ok = true;
+    if (kb < ke)
+        load_step(kb);
+    for (int k0 = kb; k0 < ke; k0 += kTcK, ++step)
+    {
+        const int st = step & 1;
+        if (step >= 2)
+        {
+            ok = __syncthreads_and(mbar_wait(bar_addr[st], uint32_t((step >> 1) - 1) & 1u)) != 0;
+            if (!ok)
+                break;
+        }
+        __nv_bfloat16* as = As[st];
+        __nv_bfloat16* bs = Bs[st];
+#pragma unroll
+        for (int j = 0; j < kAPer; ++j)
+        {
+            const int i = t + j * kTcThreads;
+            const int mm = a_kfast ? i / kTcK : i % kTcM, kk = a_kfast ? i % kTcK : i / kTcM;
+            as[tc_offset(mm, kk)] = __float2bfloat16_rn(av[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < kBPer; ++j)
+        {
+            const int i = t + j * kTcThreads;
+            const int nn = b_kfast ? i / kTcK : i % kTcN, kk = b_kfast ? i % kTcK : i / kTcN;
+            bs[tc_offset(nn, kk)] = __float2bfloat16_rn(bv[j]);
         }
         // the generic-proxy stores must be visible to the tensor core's (async-proxy) reads
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -258,12 +298,14 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
         if (t == 0)
         {
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t a_addr = static_cast<uint32_t>(__cvta_generic_to_shared(as));
+            const uint32_t b_addr = static_cast<uint32_t>(__cvta_generic_to_shared(bs));
 #pragma unroll
             for (int h = 0; h < kTcK / 16; ++h)
             {
                 const uint64_t ad = tc_smem_desc(a_addr + h * 2 * kTcLbo);
                 const uint64_t bd = tc_smem_desc(b_addr + h * 2 * kTcLbo);
-                const uint32_t accumulate = (issued || h > 0) ? 1u : 0u;
+                const uint32_t accumulate = (step > 0 || h > 0) ? 1u : 0u;
                 asm volatile("{\n\t.reg .pred p;\n\t"
                              "setp.ne.b32 p, %4, 0;\n\t"
                              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
@@ -272,20 +314,23 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
                              : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                             bar_addr)
+                             bar_addr[st])
                          : "memory");
         }
-        issued = true;
-        ok = __syncthreads_and(mbar_wait(bar_addr, parity)) != 0;
-        parity ^= 1u;
-        if (!ok)
-            break;
+        if (k0 + kTcK < ke)
+            load_step(k0 + kTcK);
     }
+    // commits issued: one per completed step (a failed wait breaks before its step issues); the
+    // last one is step issued - 1, on bar[(issued - 1) & 1]
+    const int issued = step;
+    const bool waited = issued > 0 &&
+                        __syncthreads_and(mbar_wait(bar_addr[(issued - 1) & 1], uint32_t((issued - 1) >> 1) & 1u)) != 0;
+    ok = ok && (issued == 0 || waited);
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (ok)
     {
         uint32_t r[64];
-        if (issued)
+        if (issued > 0)
         {
             tmem_load_32x32b_x64(tmem + (uint32_t(warp * 32) << 16), r);
             asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
@@ -313,12 +358,8 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
             }
         }
     }
-    else
-    {
-        if (t == 0)
-            atomicExch(error, 1);
-        mbar_wait(bar_addr, parity ^ 1u); // the commit that did not arrive in time
-    }
+    else if (t == 0)
+        atomicExch(error, 1);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     if (warp == 0)
