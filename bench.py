@@ -170,8 +170,9 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from plamatrix_b200 import replicas
+
+    world, rank = replicas.world_and_rank()
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     if world > 1:
@@ -217,11 +218,7 @@ def run_ours(args):
             last = fn()
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1) / steps
-        if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = replicas.max_over_ranks(e0.elapsed_time(e1) / steps)
         return ms, last
 
     # ---- learned block-Jacobi correction: trained on this problem's own LM sequence (device
