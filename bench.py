@@ -48,7 +48,7 @@ BATCH_SYSTEMS = 512
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--eliminated", type=int, default=L_FULL, help="L (eliminated blocks)")
@@ -64,20 +64,30 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    INTERVAL_MS = 50
+
     def __init__(self, device_index: int):
         self.device_index = device_index
         self.proc = None
         self.lines = []
+        self.first = 0
 
     def start(self):
+        """Start sampling and return once the first sample has arrived (at most 3 s), so that the
+        samples kept -- those after this call -- fall inside the timed region that follows."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device_index)], stdout=subprocess.PIPE,
-                                         stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", str(self.INTERVAL_MS), "-i", str(self.device_index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except (OSError, FileNotFoundError):
             self.proc = None
+            return
+        deadline = time.time() + 3.0
+        while not self.lines and time.time() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.first = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -93,7 +103,10 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        # samples taken during the timed region; if it was shorter than one interval, the sample
+        # taken just before it
+        window = self.lines[self.first:] or self.lines[max(0, self.first - 1):self.first]
+        for line in window:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -106,7 +119,8 @@ class ClockSampler:
                 if flag.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "interval_ms": self.INTERVAL_MS,
+                "samples_in_timed_region": len(self.lines) - self.first}
 
 
 def peaks():
