@@ -53,3 +53,16 @@ def test_host_side_argument_checks(lib):
     assert lib.pm_solver_workspace_create(C.byref(sw)) == 0
     assert lib.pm_cg_f64(sw, None, None, None, None, C.byref(opts), C.byref(rep)) == N.PM_INVALID_ARGUMENT
     lib.pm_solver_workspace_destroy(sw)
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """No CPU fallback: without the built library every entry point raises instead of computing."""
+    from plamatrix_b200 import _native as N
+    from plamatrix_b200 import schur as SC
+
+    monkeypatch.setattr(N, "_lib", None)
+    monkeypatch.setattr(N, "LIB_PATH", str(tmp_path / "libplamatrix_b200.so"))
+    with pytest.raises(ImportError, match="no CPU fallback"):
+        N.load()
+    with pytest.raises(ImportError, match="no CPU fallback"):
+        SC.SchurComplementSolverWorkspace()
