@@ -37,7 +37,6 @@ WORKLOAD = ("schur_lm_P4000_L2000000: P=4,000 x 6-dof, L=2,000,000 x 3-dof, 2+Po
             "per eliminated block from a wrapped window of 40, 2-dim residuals, Huber delta 1, "
             "lambda 1e-3, FP64 true relative residual 1e-8")
 METRIC = "Schur-PCG ms to 1e-8 FP64 rel. residual: learned+mixed vs plain; SpMV HBM GB/s"
-REF_SAMPLE_L = 100_000  # eliminated blocks of the reference CPU sample (5% of the full system)
 LEARN_TRAIN, LEARN_HOLD, LEARN_STEPS = 8, 3, 20
 # DRAM bytes (read + write) of one full-size assembly (assemble_diag6 + assemble_upper6), from an
 # ncu capture of `python bench.py --steps 2 --warmup 1 --no-extras` with dram__bytes_{read,write}.sum
@@ -133,17 +132,36 @@ def peaks():
 
 
 # ------------------------------------------------------------------ reference arm / CPU baseline
-def reference_sample_ms(seed: int = 0, eliminated: int = REF_SAMPLE_L):
-    """Reference CPU library (oracle/_ref, built from the reference sources): accumulation of
-    the sample's observations + solveDampedSchurComplement(Cpu).  Returns (ms, report)."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
+
+
+def reference_step_ms(prob: dict):
+    """One LM linear step through the reference CPU library (oracle/_ref, compiled from the
+    reference sources): Huber-weighted BlockNormalEquations accumulation of every observation,
+    then solveDampedSchurComplement (Cpu backend, tol 1e-8, lambda 1e-3).  Returns (ms, report)."""
     import oracle
-    from plamatrix_b200 import workloads as W
-    prob = W.large_bundle(seed=seed, P=P_FULL, L=eliminated)
     t0 = time.perf_counter()
     ne = oracle.normal_equations_from_observations(prob, impl="ref")
-    dp, dl, rep = ne.solve(LAMBDA, relative_tolerance=TOL, max_iterations=200)
+    _, _, rep = ne.solve(LAMBDA, relative_tolerance=TOL, max_iterations=200)
     ms = (time.perf_counter() - t0) * 1e3
-    return ms, rep, len(prob["obs_primary"])
+    del ne
+    return ms, rep
+
+
+def reference_sample_text(prob: dict, steps: int) -> str:
+    return (f"reference CPU library (oracle/_ref, compiled from the reference sources with g++ -O2): "
+            f"Huber-weighted BlockNormalEquations accumulation of all {len(prob['obs_primary']):,} observations + "
+            f"solveDampedSchurComplement(Cpu backend, tol 1e-8) on the full P=4,000, L=2,000,000 system, "
+            f"{steps} step(s), each timed on its own (no scaling); 1 thread of {os.cpu_count()} "
+            f"({cpu_model()}); the reference's path has no threading")
 
 
 def run_reference(args):
@@ -154,29 +172,40 @@ def run_reference(args):
     if not oracle.available("ref"):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU library oracle/_ref not built"}))
         return
-    scale = L_FULL / REF_SAMPLE_L
+    from plamatrix_b200 import workloads as W
+    # warm-up: the same code path on the small P=20, L=2,000 workload (CPU code has no device
+    # caches or JIT to warm; a full-size warm-up step would only add a minute per step)
+    small = W.small_bundle(seed=0)
     for _ in range(args.warmup):
-        reference_sample_ms(seed=0)
-    times = []
-    reps = []
+        reference_step_ms(small)
+    prob = W.large_bundle(seed=0, P=P_FULL, L=args.eliminated)  # generated once, outside the timed steps
+    times, reps = [], []
     for k in range(args.steps):
-        ms, rep, nobs = reference_sample_ms(seed=k)
-        times.append(ms * scale)
+        ms, rep = reference_step_ms(prob)
+        times.append(ms)
         reps.append(rep)
+        print(f"reference step {k + 1}/{args.steps}: {ms / 1e3:.2f} s, {rep['iterations']} iterations",
+              file=sys.stderr, flush=True)
     value = statistics.mean(times)
-    sample = (f"reference CPU library (oracle/_ref, compiled from the reference sources): Huber-weighted "
-              f"BlockNormalEquations accumulation + solveDampedSchurComplement(Cpu backend, tol 1e-8) on "
-              f"P=4,000, L={REF_SAMPLE_L:,} ({nobs:,} observations, 5% of the full system, same distributions), "
-              f"time scaled x{scale:.0f} to L=2,000,000; single thread (the reference's path has no threading)")
+    sample = reference_sample_text(prob, args.steps)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(value, 3), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_eliminated_blocks": REF_SAMPLE_L},
-        "iterations": [r["iterations"] for r in reps],
+        "config": config_dict(args.gpus, args.eliminated),
+        "iterations": [r["iterations"] for r in reps], "converged": all(r["converged"] for r in reps),
+        "step_ms_min_median_max": [round(min(times), 1), round(statistics.median(times), 1), round(max(times), 1)],
+        "warmup_workload": "P=20, L=2,000 (same code path)",
         "cpu_baseline": {"value": round(value, 3), "unit": "ms", "cores": 1, "kind": "reference", "sample": sample},
         "e2e": {"value": round(value, 3), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def config_dict(world: int, L: int) -> dict:
+    """The workload of every arm's line (the same dict for ours and the reference)."""
+    return {"workload": WORKLOAD, "primary_blocks": P_FULL, "eliminated_blocks": L,
+            "parallelism": f"replicas x{world} (no exchange step)",
+            "l2": "inputs larger than L2 (observations 1.9 GB FP64)"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -276,7 +305,7 @@ def run_ours(args):
     schur_spmv = schur_spmv_leg(torch, ws, n, stream) if rank == 0 else None
     out = {}
     if rank == 0 and not args.no_extras:
-        out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, mixed, n, m, net)
+        out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, mixed, n, m, net, prob)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -299,9 +328,8 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": round(ms_learned, 4), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 (FP32 inner PCG, FP64 dots/refinement; BF16 tensor-core MLP)",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "observations": nobs, "eliminated_blocks": L, "primary_blocks": P_FULL,
-                   "schur_blocks": B, "cross_blocks": C_, "parallelism": f"replicas x{world} (no exchange step)",
-                   "l2": "inputs larger than L2 (observations 1.9 GB FP64)", "systems_per_step": world},
+        "config": config_dict(world, L),
+        "workload_counts": {"observations": nobs, "schur_blocks": B, "cross_blocks": C_, "systems_per_step": world},
         "plain_fp64_ms": round(ms_plain, 4),
         "mixed_ms": round(ms_mixed, 4),
         "learned_mixed_over_plain_speedup": round(ms_plain / ms_learned, 3),
@@ -345,7 +373,7 @@ def run_ours(args):
     print(json.dumps(line))
 
 
-def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=None):
+def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=None, prob=None):
     out = {}
     # ---- end to end through the public API with host buffers
     dp_h = torch.empty(n, dtype=torch.float64).pin_memory()
@@ -376,17 +404,15 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=Non
     # ---- batched uneven systems
     out["batched"] = batched_leg(torch, SC, W, net)
     out["dense_c4_max"] = dense_leg(torch, SC, W)
-    # ---- CPU baseline: the reference's own CPU library on a bounded sample, scaled
+    # ---- CPU baseline: one full-size LM linear step of the reference's own CPU library (the
+    # same host problem the device arm was built from), timed on its own, no scaling
     try:
         import oracle
-        if oracle.available("ref"):
-            ms, rep, nobs = reference_sample_ms(seed=0)
-            scale = L_FULL / REF_SAMPLE_L
+        if oracle.available("ref") and prob is not None:
+            ms, rep = reference_step_ms(prob)
             out["cpu_baseline"] = {
-                "value": round(ms * scale, 1), "unit": "ms", "cores": 1, "kind": "reference",
-                "sample": (f"reference CPU library (oracle/_ref) accumulation + solveDampedSchurComplement(Cpu) on "
-                           f"P=4,000, L={REF_SAMPLE_L:,} ({nobs:,} observations), scaled x{scale:.0f}; "
-                           f"{rep['iterations']} PCG iterations; 1 thread of {os.cpu_count()}")}
+                "value": round(ms, 1), "unit": "ms", "cores": 1, "kind": "reference",
+                "sample": reference_sample_text(prob, 1) + f"; {rep['iterations']} PCG iterations"}
     except Exception as exc:  # noqa: BLE001
         out["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 1, "kind": "reference", "sample": str(exc)}
     return out
@@ -525,9 +551,8 @@ def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
     """Independent systems P ~ U{8..512}, L ~ U{500..50,000}, 4 uniform distinct primaries per
     eliminated block: one batched launch sequence (union accumulation, pattern, assembly,
     graph-replayed per-system PCG, back-substitution) against a plain per-system loop."""
-    rng = np.random.default_rng(12345)
-    sizes = [(int(rng.integers(8, 513)), int(rng.integers(500, 50_001))) for _ in range(systems)]
-    probs = [W.bundle_problem_device(P, L, per_eliminated=4, seed=50_000 + i) for i, (P, L) in enumerate(sizes)]
+    sizes = W.uneven_family_sizes(systems)
+    probs = [W.uneven_family_system(i, P, L) for i, (P, L) in enumerate(sizes)]
     P_off = np.cumsum([0] + [P for P, _ in sizes]).astype(np.int64)
     L_off = np.cumsum([0] + [L for _, L in sizes]).astype(np.int64)
     union = {

@@ -112,9 +112,11 @@ PM_API int pm_coo_status(pm_sparse_workspace* workspace, const char* operation, 
  * No cudaMalloc / cudaFree or allocating library call is made.  Synchronous: enqueues on
  * `stream`, waits, and reports coordinate / value errors directly.  The output arrays hold
  * `capacity` entries (capacity = count always suffices); `nnz_out` (host) receives the
- * duplicate-combined nnz.  All calls share the scratch array: calls that overlap on a GPU
- * race, so serialise them.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) and caches it; make that first call before any stream capture. */
+ * duplicate-combined nnz.  All calls share the scratch array: calls that overlap on one GPU,
+ * from any stream or host thread, race, so serialise them (each device has its own copy).
+ * Every call looks up the array's device address (cudaGetSymbolAddress, which allocates
+ * nothing); the first call on a device loads the library's device code there, so make that
+ * first call before any stream capture. */
 PM_API int pm_coo_to_csr_static_f32(pm_stream_t stream, int64_t rows, int64_t cols, int64_t count,
                                     const int64_t* row_indices_d, const int64_t* col_indices_d,
                                     const float* values_d, int64_t capacity, int64_t* row_offsets_d,
@@ -441,6 +443,12 @@ PM_API int pm_mlp_forward(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stream_
  * FP64, n = 6P); with `learning_rate` > 0 one Adam step follows.  Synchronous. */
 PM_API int pm_mlp_train_step(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stream_t stream, const double* x_d,
                              const double* b_d, double learning_rate, double* loss);
+/* Polls of an mbarrier wait between the network GEMM's operand stages before it gives up (default
+ * 2^20; the final wait for the last MMA always uses 2^20).  A GEMM whose wait runs out stops
+ * issuing MMAs, frees its tensor memory once its last MMA has completed, and the call that ran it
+ * returns PM_RUNTIME_ERROR ("a tensor-core GEMM did not complete"); the network stays usable.
+ * A limit of 0 makes every multi-step GEMM give up at its first stage wait (the error path). */
+PM_API int pm_mlp_set_wait_limit(pm_mlp* mlp, int64_t polls);
 /* Host copies of the last features (P x 25), outputs (P x 21) and gradients; any may be NULL. */
 PM_API int pm_mlp_inspect(const pm_mlp* mlp, int64_t* rows, float* features, float* outputs, float* gradients);
 

@@ -18,7 +18,6 @@
 
 #include <climits>
 #include <cmath>
-#include <mutex>
 #include <sstream>
 
 namespace pm
@@ -783,8 +782,8 @@ int pm_coo_status(pm_sparse_workspace* ws, const char* operation, int64_t* nnz_o
 // the library's device code is loaded on a GPU and held by every GPU that loads the library
 // until the process exits.  Inputs are limited to kStaticMaxTriplets triplets and
 // kStaticMaxRows rows so that the scratch always fits.  All calls share the array: calls
-// that overlap on the GPU (other streams, other host threads, other devices' contexts are
-// separate) race on it, so serialise them.  Each call clears what must start at zero.
+// that overlap on one GPU, from any stream or host thread, race on it, so serialise them;
+// each device has its own copy.  Each call clears what must start at zero.
 namespace pm
 {
 namespace
@@ -802,29 +801,19 @@ namespace pm
 namespace
 {
 
-std::mutex g_static_scratch_mutex;
-void* g_static_scratch_address[64] = {};
-
-// Device address of g_static_coo_scratch for the current device.  The host-side name of the
-// array is only a stand-in, so the address is looked up once per device (with that device
-// current) and cached.  The first call on a device performs this look-up; issue that first
-// call before any stream capture.
+// Device address of g_static_coo_scratch in the current device's context.  The host-side name
+// of the array is only a stand-in, so the address is looked up with that device current.  It
+// is looked up on every call (cudaGetSymbolAddress allocates nothing): a cached address would
+// outlive a cudaDeviceReset, after which the module is loaded again and the array may move.
+// The first call on a device loads the library's device code there; issue that first call
+// before any stream capture.
 void* static_scratch_address()
 {
-    int device = 0;
-    PM_CUDA(cudaGetDevice(&device));
-    if (device < 0 || device >= 64)
-        fail(PM_RUNTIME_ERROR, "device index out of range for the static scratch table");
-    std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
-    if (!g_static_scratch_address[device])
-    {
-        void* address = nullptr;
-        const cudaError_t rc = cudaGetSymbolAddress(&address, g_static_coo_scratch);
-        if (rc != cudaSuccess || !address)
-            fail(PM_CUDA_ERROR, std::string("cudaGetSymbolAddress(static COO scratch): ") + cudaGetErrorString(rc));
-        g_static_scratch_address[device] = address;
-    }
-    return g_static_scratch_address[device];
+    void* address = nullptr;
+    const cudaError_t rc = cudaGetSymbolAddress(&address, g_static_coo_scratch);
+    if (rc != cudaSuccess || !address)
+        fail(PM_CUDA_ERROR, std::string("cudaGetSymbolAddress(static COO scratch): ") + cudaGetErrorString(rc));
+    return address;
 }
 
 // Bytes coo_prepare carves for (rows, count) triplets of type T (same layout, same order).

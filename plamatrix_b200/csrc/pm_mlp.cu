@@ -49,6 +49,7 @@ struct pm_mlp
     float *F = nullptr, *Z1 = nullptr, *H1 = nullptr, *Z2 = nullptr, *H2 = nullptr, *O = nullptr, *dO = nullptr,
           *dH = nullptr, *dZ = nullptr, *split = nullptr;
     int64_t step = 0;
+    long long wait_limit = 1ll << 20; // polls of a GEMM stage wait before it gives up
 };
 
 namespace pm
@@ -139,9 +140,12 @@ __global__ void __launch_bounds__(128) features_kernel(int64_t P, const int* __r
 // x 16, FP32 accumulator in tensor memory) and commits them to the stage's mbarrier, which the
 // threads wait on before they refill that stage.  The epilogue reads the accumulator with
 // tcgen05.ld (warp w owns rows 32w..32w+31).  The K order is fixed, so results are
-// reproducible.  Every wait is bounded: one that runs out sets *error, the CTA issues nothing
-// more, waits (bounded) for its last commit and frees its tensor memory; the host turns the
-// flag into an error.
+// reproducible.  Every wait is bounded.  A stage wait (before a step's MMAs are issued) gives up
+// after `step_wait_limit` polls: the CTA then issues nothing more, sets *error and waits for
+// its last commit with the full limit.  Tensor memory is freed only when that drain wait
+// succeeded (or nothing was issued), so no MMA can still be writing the columns; if the drain
+// itself runs out, the columns stay allocated and *error is set.  The host turns the flag into
+// an error.
 constexpr int kTcM = 128, kTcN = 64, kTcK = 32, kTcThreads = 128;
 constexpr uint32_t kTcCols = 64;                     // tensor-memory columns of the accumulator
 constexpr int kTcLbo = 128;                          // bytes between K-adjacent core matrices
@@ -170,9 +174,9 @@ __device__ __forceinline__ uint64_t tc_smem_desc(uint32_t addr)
            (uint64_t((kTcSbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit)
 {
-    for (long long it = 0; it < kTcWaitLimit; ++it)
+    for (long long it = 0; it < limit; ++it)
     {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\t"
@@ -205,7 +209,8 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
                                                              int64_t sam, int64_t sak, const float* __restrict__ B,
                                                              int64_t sbk, int64_t sbn, const float* __restrict__ bias,
                                                              float* __restrict__ C, int64_t ldc,
-                                                             float* __restrict__ H, int kchunk, int* __restrict__ error)
+                                                             float* __restrict__ H, int kchunk, int* __restrict__ error,
+                                                             long long step_wait_limit)
 {
     __shared__ __align__(128) __nv_bfloat16 As[2][kTcM * kTcK];
     __shared__ __align__(128) __nv_bfloat16 Bs[2][kTcN * kTcK];
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
         const int st = step & 1;
         if (step >= 2)
         {
-            ok = __syncthreads_and(mbar_wait(bar_addr[st], uint32_t((step >> 1) - 1) & 1u)) != 0;
+            ok = __syncthreads_and(mbar_wait(bar_addr[st], uint32_t((step >> 1) - 1) & 1u, step_wait_limit)) != 0;
             if (!ok)
                 break;
         }
@@ -323,9 +328,10 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
     // commits issued: one per completed step (a failed wait breaks before its step issues); the
     // last one is step issued - 1, on bar[(issued - 1) & 1]
     const int issued = step;
-    const bool waited = issued > 0 &&
-                        __syncthreads_and(mbar_wait(bar_addr[(issued - 1) & 1], uint32_t((issued - 1) >> 1) & 1u)) != 0;
-    ok = ok && (issued == 0 || waited);
+    const bool waited = issued > 0 && __syncthreads_and(mbar_wait(bar_addr[(issued - 1) & 1],
+                                                                  uint32_t((issued - 1) >> 1) & 1u, kTcWaitLimit)) != 0;
+    const bool drained = issued == 0 || waited;
+    ok = ok && drained;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (ok)
     {
@@ -362,18 +368,19 @@ __global__ void __launch_bounds__(kTcThreads) gemm_tc_kernel(int M, int N, int K
         atomicExch(error, 1);
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 0 && drained)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTcCols) : "memory");
 }
 
 void gemm(cudaStream_t stream, int M, int N, int K, const float* A, int64_t sam, int64_t sak, const float* B,
-          int64_t sbk, int64_t sbn, const float* bias, float* C, int64_t ldc, int* error, float* H = nullptr)
+          int64_t sbk, int64_t sbn, const float* bias, float* C, int64_t ldc, int* error, long long wait_limit,
+          float* H = nullptr)
 {
     if (M <= 0 || N <= 0)
         return;
     const dim3 grid((M + kTcM - 1) / kTcM, (N + kTcN - 1) / kTcN);
     gemm_tc_kernel<<<grid, kTcThreads, kTcSmemReserve, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, bias, C, ldc, H,
-                                                                 0, error);
+                                                                 0, error, wait_limit);
     PM_LAUNCH_CHECK();
 }
 
@@ -397,14 +404,14 @@ int split_count(int64_t K) { return static_cast<int>((K + kSplitRows - 1) / kSpl
 
 // C = A B with the K (row) dimension split over CTAs; `part` holds split_count(K) * M * N floats
 void gemm_split(cudaStream_t stream, int M, int N, int K, const float* A, int64_t sam, int64_t sak, const float* B,
-                int64_t sbk, int64_t sbn, float* C, int64_t ldc, float* part, int* error)
+                int64_t sbk, int64_t sbn, float* C, int64_t ldc, float* part, int* error, long long wait_limit)
 {
     if (M <= 0 || N <= 0)
         return;
     const int splits = split_count(K);
     const dim3 grid((M + kTcM - 1) / kTcM, (N + kTcN - 1) / kTcN, splits);
     gemm_tc_kernel<<<grid, kTcThreads, kTcSmemReserve, stream>>>(M, N, K, A, sam, sak, B, sbk, sbn, nullptr, part, N,
-                                                                 nullptr, kSplitRows, error);
+                                                                 nullptr, kSplitRows, error, wait_limit);
     PM_LAUNCH_CHECK();
     reduce_splits_kernel<<<grid_for(int64_t(M) * N, 256, 1024), 256, 0, stream>>>(M, N, splits, part, C, ldc);
     PM_LAUNCH_CHECK();
@@ -735,10 +742,12 @@ void forward(pm_mlp* mlp, const SchurView& v, cudaStream_t stream)
     const int M = static_cast<int>(P);
     const float* W = mlp->params;
     int* error = tc_error_flag(mlp);
-    gemm(stream, M, kHid, kIn, mlp->F, kInPad, 1, W + kOffW1, kHid, 1, W + kOffB1, mlp->Z1, kHid, error, mlp->H1);
-    gemm(stream, M, kHid, kHid, mlp->H1, kHid, 1, W + kOffW2, kHid, 1, W + kOffB2, mlp->Z2, kHid, error, mlp->H2);
+    gemm(stream, M, kHid, kIn, mlp->F, kInPad, 1, W + kOffW1, kHid, 1, W + kOffB1, mlp->Z1, kHid, error, mlp->wait_limit,
+         mlp->H1);
+    gemm(stream, M, kHid, kHid, mlp->H1, kHid, 1, W + kOffW2, kHid, 1, W + kOffB2, mlp->Z2, kHid, error, mlp->wait_limit,
+         mlp->H2);
     PM_CUDA(cudaMemsetAsync(mlp->O, 0, size_t(P) * kOutPad * sizeof(float), stream));
-    gemm(stream, M, kOut, kHid, mlp->H2, kHid, 1, W + kOffW3, kOut, 1, W + kOffB3, mlp->O, kOutPad, error);
+    gemm(stream, M, kOut, kHid, mlp->H2, kHid, 1, W + kOffW3, kOut, 1, W + kOffB3, mlp->O, kOutPad, error, mlp->wait_limit);
 }
 
 void check_view(const SchurView& v)
@@ -814,17 +823,17 @@ double train(pm_mlp* mlp, const SchurView& v, cudaStream_t stream, const double*
     const float* W = mlp->params;
     float* splits = mlp->split;
     int* error = tc_error_flag(mlp);
-    gemm_split(stream, kHid, kOut, M, mlp->H2, 1, kHid, mlp->dO, kOutPad, 1, G + kOffW3, kOut, splits, error);
+    gemm_split(stream, kHid, kOut, M, mlp->H2, 1, kHid, mlp->dO, kOutPad, 1, G + kOffW3, kOut, splits, error, mlp->wait_limit);
     colsum(stream, P, kOut, kOutPad, mlp->dO, G + kOffB3, splits);
-    gemm(stream, M, kHid, kOut, mlp->dO, kOutPad, 1, W + kOffW3, 1, kOut, nullptr, mlp->dH, kHid, error);
+    gemm(stream, M, kHid, kOut, mlp->dO, kOutPad, 1, W + kOffW3, 1, kOut, nullptr, mlp->dH, kHid, error, mlp->wait_limit);
     gelu_back_kernel<<<grid_for(P * kHid, 256, 4096), 256, 0, stream>>>(P * kHid, mlp->dH, mlp->Z2, mlp->dZ);
     PM_LAUNCH_CHECK();
-    gemm_split(stream, kHid, kHid, M, mlp->H1, 1, kHid, mlp->dZ, kHid, 1, G + kOffW2, kHid, splits, error);
+    gemm_split(stream, kHid, kHid, M, mlp->H1, 1, kHid, mlp->dZ, kHid, 1, G + kOffW2, kHid, splits, error, mlp->wait_limit);
     colsum(stream, P, kHid, kHid, mlp->dZ, G + kOffB2, splits);
-    gemm(stream, M, kHid, kHid, mlp->dZ, kHid, 1, W + kOffW2, 1, kHid, nullptr, mlp->dH, kHid, error);
+    gemm(stream, M, kHid, kHid, mlp->dZ, kHid, 1, W + kOffW2, 1, kHid, nullptr, mlp->dH, kHid, error, mlp->wait_limit);
     gelu_back_kernel<<<grid_for(P * kHid, 256, 4096), 256, 0, stream>>>(P * kHid, mlp->dH, mlp->Z1, mlp->dZ);
     PM_LAUNCH_CHECK();
-    gemm_split(stream, kIn, kHid, M, mlp->F, 1, kInPad, mlp->dZ, kHid, 1, G + kOffW1, kHid, splits, error);
+    gemm_split(stream, kIn, kHid, M, mlp->F, 1, kInPad, mlp->dZ, kHid, 1, G + kOffW1, kHid, splits, error, mlp->wait_limit);
     colsum(stream, P, kHid, kHid, mlp->dZ, G + kOffB1, splits);
     if (lr > 0.0)
     {
@@ -920,6 +929,17 @@ int pm_mlp_set_params(pm_mlp* mlp, const float* host)
         PM_CUDA(cudaMemcpy(mlp->params, host, pm::kParams * sizeof(float), cudaMemcpyHostToDevice));
         PM_CUDA(cudaMemset(mlp->m, 0, 2 * pm::kParams * sizeof(float)));
         mlp->step = 0;
+    });
+}
+
+int pm_mlp_set_wait_limit(pm_mlp* mlp, int64_t polls)
+{
+    return pm::guarded([&] {
+        if (!mlp)
+            pm::fail(PM_INVALID_ARGUMENT, "pm_mlp_set_wait_limit: null network");
+        if (polls < 0)
+            pm::fail(PM_INVALID_ARGUMENT, "pm_mlp_set_wait_limit: the limit must be non-negative");
+        mlp->wait_limit = polls;
     });
 }
 

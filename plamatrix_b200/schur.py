@@ -268,6 +268,7 @@ N.register("pm_mlp_set_params", [vp, vp])
 N.register("pm_mlp_forward", [vp, vp, vp])
 N.register("pm_mlp_train_step", [vp, vp, vp, vp, vp, C.c_double, vp])
 N.register("pm_mlp_inspect", [vp, vp, vp, vp, vp])
+N.register("pm_mlp_set_wait_limit", [vp, i64])
 
 
 class LearnedPreconditioner:
@@ -300,6 +301,11 @@ class LearnedPreconditioner:
         if a.size != self.param_count():
             raise N.InvalidArgument("parameter vector has the wrong length")
         N.call("pm_mlp_set_params", self._h, C.c_void_p(a.ctypes.data))
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls of a GEMM operand-stage wait before it gives up (default 2^20); see
+        pm_mlp_set_wait_limit."""
+        N.call("pm_mlp_set_wait_limit", self._h, C.c_int64(polls))
 
     def forward(self, workspace: "SchurComplementSolverWorkspace", stream=None) -> dict:
         N.call("pm_mlp_forward", self._h, workspace.handle, _stream_handle(stream))

@@ -145,6 +145,18 @@ def uneven_batch(count: int = 512, seed: int = 0, dtype=np.float64, p_range=(8, 
     return out
 
 
+def uneven_family_sizes(count: int = 512, seed: int = 12345) -> list:
+    """(P, L) of the batched uneven-systems workload: P ~ U{8..512}, L ~ U{500..50,000}."""
+    rng = np.random.default_rng(seed)
+    return [(int(rng.integers(8, 513)), int(rng.integers(500, 50_001))) for _ in range(count)]
+
+
+def uneven_family_system(index: int, P: int, L: int, device="cuda") -> dict:
+    """System `index` of the batched uneven-systems workload (4 uniform distinct primaries per
+    eliminated block, drawn on the device)."""
+    return bundle_problem_device(P, L, per_eliminated=4, seed=50_000 + index, device=device)
+
+
 def bundle_problem_device(P: int, L: int, *, per_eliminated: str | int = 4, window: int | None = None,
                           residual_size: int = 2, outlier_fraction: float = 0.05, huber_delta: float = 1.0,
                           seed: int = 0, device="cuda") -> dict:

@@ -44,6 +44,36 @@ def test_batched_matches_individual_solves():
         assert per[s]["time_ms"] >= 0.0
 
 
+def test_batched_family_matches_oracle_per_system(checkers):
+    """Eight systems of the 512-system uneven family (P ~ U{8..512}, L ~ U{500..50,000}, 4 uniform
+    distinct primaries per eliminated block) solved in one batched call; every system's steps
+    against the oracle's per-system solve (the reference's solveDampedSchurComplement, Cpu backend,
+    restated): within 1e-6 relative, iteration counts within 1."""
+    sizes = W.uneven_family_sizes(512)
+    picks = [0, 1, 2, 3, 100, 200, 300, 511]
+    probs = []
+    for i in picks:
+        P, L = sizes[i]
+        d = W.uneven_family_system(i, P, L)
+        probs.append({k: (v.cpu().numpy() if torch.is_tensor(v) else v) for k, v in d.items()})
+    union = SC.pack_observation_systems(probs)
+    ne = _ne(union)
+    opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-8)
+    dp, dl, rep, per = SC.solve_batched_schur_complement(ne, 1e-3, union["primary_offsets"], opts)
+    assert rep["converged"], rep["message"]
+    P_off, L_off = union["primary_offsets"], union["eliminated_offsets"]
+    dp_h, dl_h = dp.cpu().numpy(), dl.cpu().numpy()
+    for s, prob in enumerate(probs):
+        orc = checkers.normal_equations_from_observations(prob)
+        ref_dp, ref_dl, ref = orc.solve(1e-3, relative_tolerance=1e-8, max_iterations=500)
+        assert ref["converged"] and per[s]["converged"]
+        assert abs(per[s]["iterations"] - ref["iterations"]) <= 1, (s, per[s]["iterations"], ref["iterations"])
+        a = dp_h[6 * P_off[s]:6 * P_off[s + 1]]
+        assert np.linalg.norm(a - ref_dp) <= 1e-6 * np.linalg.norm(ref_dp)
+        a = dl_h[3 * L_off[s]:3 * L_off[s + 1]]
+        assert np.linalg.norm(a - ref_dl) <= 1e-6 * np.linalg.norm(ref_dl)
+
+
 def test_batched_rejects_coupled_systems():
     probs = _problems(3, seed=1)
     union = SC.pack_observation_systems(probs)

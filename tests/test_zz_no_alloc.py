@@ -52,15 +52,18 @@ def _triplets(seed, rows, cols, count, dtype):
 
 
 @pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
-def test_static_scratch_matches_workspace_entry_point_on_consecutive_calls(dtype):
+def test_static_scratch_matches_workspace_entry_point_on_consecutive_calls(checkers, dtype):
+    """Two calls in a row, the second at the stated maximum: bit for bit the workspace entry
+    point's CSR and the oracle's (the reference CPU conversion restated)."""
     cases = [(5000, 700, 40000, 1), (MAX_ROWS, 300, MAX_TRIPLETS, 2)]  # second call: the stated maximum
     for rows, cols, count, seed in cases:
         r, c, v = _triplets(seed, rows, cols, count, dtype)
         got = _static_csr(rows, cols, r, c, v)
-        ref = S.coo_to_csr(rows, cols, r, c, v).cpu()
-        assert np.array_equal(got[0], ref[0])
-        assert np.array_equal(got[1], ref[1])
-        assert np.array_equal(got[2].view(np.uint8), ref[2].view(np.uint8))
+        for ref in (S.coo_to_csr(rows, cols, r, c, v).cpu(),
+                    checkers.coo_to_csr(rows, cols, r.cpu().numpy(), c.cpu().numpy(), v.cpu().numpy())):
+            assert np.array_equal(got[0], ref[0])
+            assert np.array_equal(got[1], ref[1])
+            assert np.array_equal(got[2].view(np.uint8), np.asarray(ref[2]).view(np.uint8))
 
 
 def test_static_scratch_rejects_sizes_beyond_its_maximum():
