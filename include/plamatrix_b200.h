@@ -53,6 +53,16 @@ PM_API int pm_version(void);
 /* Number of kernels this library has launched in the process so far. */
 PM_API long long pm_kernel_launches(void);
 
+/* Device memory and synchronous copies (on `stream`) for callers that do not link the CUDA
+ * runtime themselves, e.g. C++ code built against the reference's CPU-only headers.  No
+ * counterpart in the reference (its DenseMatrix<GPU> / GpuAllocator own device memory there). */
+PM_API int pm_device_malloc(size_t bytes, void** out);
+PM_API int pm_device_free(void* ptr);
+PM_API int pm_copy_to_device(void* dst_d, const void* src_h, size_t bytes, pm_stream_t stream);
+PM_API int pm_copy_to_host(void* dst_h, const void* src_d, size_t bytes, pm_stream_t stream);
+/* Name of the current CUDA device (SchurComplementSolverReport::deviceName). */
+PM_API int pm_device_name(char* out, int capacity);
+
 /* =========================================================================== workspaces
  * Replaces SparseOpsWorkspace (include/plamatrix/sparse/sparse_ops.h:13-77): grow-only,
  * stream-bound temporary storage plus the deferred COO status. */
@@ -310,7 +320,16 @@ PM_API int pm_ne_check_observations(const pm_normal_equations* equations, pm_str
 enum
 {
     PM_PRECISION_NATIVE = 0, /* assembly, SpMV and PCG vectors in Scalar; dots in FP64 */
-    PM_PRECISION_MIXED = 1   /* double only: FP64 refinement around an FP32 inner PCG */
+    PM_PRECISION_MIXED = 1,  /* double only: FP64 assembly, FP64 refinement around an FP32 inner PCG
+                                (the reference's FP32 seed pass, block_schur_accelerated.cpp:131-196) */
+    /* double normal equations with 6x6 / 3x3 blocks only (other shapes run PM_PRECISION_MIXED):
+     * FP32 assembly products (V = W L^-T stored in FP32, off-diagonal Schur blocks formed and summed
+     * in FP32), FP32 SpMV and preconditioner apply; FP64 dots / alpha / beta, FP64 Cholesky of the
+     * eliminated and diagonal blocks (diagonal blocks and RHS summed in FP64), and an FP64 true
+     * residual computed matrix-free from the FP64 normal equations for every refinement step.  A
+     * refinement that fails hands the solve to FP64 PCG on an FP64 assembly.  After such a solve
+     * the workspace holds the FP32 values: pm_schur_spmv_f32 and both exports read them. */
+    PM_PRECISION_MIXED_FP32_ASSEMBLY = 2
 };
 
 typedef struct

@@ -18,6 +18,9 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference source tree the Makefile compiles from (absent on machines that only run the
+# prebuilt checkers)
+REF_SOURCE_ROOT = os.environ.get("PLAMATRIX_REFERENCE", "/root/reference")
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libplamatrix_ref.so")
 

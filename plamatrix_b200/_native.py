@@ -73,6 +73,11 @@ _SIGNATURES = {
     "pm_last_error": [],
     "pm_version": [],
     "pm_kernel_launches": [],
+    "pm_device_malloc": [C.c_size_t, vp],
+    "pm_device_free": [vp],
+    "pm_copy_to_device": [vp, vp, C.c_size_t, vp],
+    "pm_copy_to_host": [vp, vp, C.c_size_t, vp],
+    "pm_device_name": [C.c_char_p, C.c_int],
     "pm_sparse_workspace_create": [vp],
     "pm_sparse_workspace_destroy": [vp],
     "pm_sparse_workspace_close": [vp],

@@ -4,6 +4,7 @@
 #include <atomic>
 #include <mutex>
 #include <vector>
+#include <cstdio>
 
 namespace pm
 {
@@ -154,3 +155,60 @@ template void exclusive_scan<int64_t, int64_t>(const int64_t*, int64_t*, int64_t
 extern "C" const char* pm_last_error(void) { return pm::g_last_error.c_str(); }
 extern "C" int pm_version(void) { return 1; }
 extern "C" long long pm_kernel_launches(void) { return pm::g_launches.load(std::memory_order_relaxed); }
+
+// Device memory and copies for callers that do not link the CUDA runtime themselves.
+extern "C" int pm_device_malloc(size_t bytes, void** out)
+{
+    return pm::guarded([&] {
+        if (!out)
+            pm::fail(PM_INVALID_ARGUMENT, "pm_device_malloc: null output");
+        *out = nullptr;
+        if (bytes > 0)
+            PM_CUDA(cudaMalloc(out, bytes));
+    });
+}
+
+extern "C" int pm_device_free(void* ptr)
+{
+    return pm::guarded([&] {
+        if (ptr)
+            PM_CUDA(cudaFree(ptr));
+    });
+}
+
+extern "C" int pm_copy_to_device(void* dst_d, const void* src_h, size_t bytes, pm_stream_t stream)
+{
+    return pm::guarded([&] {
+        if (bytes == 0)
+            return;
+        if (!dst_d || !src_h)
+            pm::fail(PM_INVALID_ARGUMENT, "pm_copy_to_device: null pointer");
+        PM_CUDA(cudaMemcpyAsync(dst_d, src_h, bytes, cudaMemcpyHostToDevice, stream));
+        PM_CUDA(cudaStreamSynchronize(stream));
+    });
+}
+
+extern "C" int pm_copy_to_host(void* dst_h, const void* src_d, size_t bytes, pm_stream_t stream)
+{
+    return pm::guarded([&] {
+        if (bytes == 0)
+            return;
+        if (!dst_h || !src_d)
+            pm::fail(PM_INVALID_ARGUMENT, "pm_copy_to_host: null pointer");
+        PM_CUDA(cudaMemcpyAsync(dst_h, src_d, bytes, cudaMemcpyDeviceToHost, stream));
+        PM_CUDA(cudaStreamSynchronize(stream));
+    });
+}
+
+extern "C" int pm_device_name(char* out, int capacity)
+{
+    return pm::guarded([&] {
+        if (!out || capacity <= 0)
+            pm::fail(PM_INVALID_ARGUMENT, "pm_device_name: null or empty output");
+        int device = 0;
+        PM_CUDA(cudaGetDevice(&device));
+        cudaDeviceProp prop{};
+        PM_CUDA(cudaGetDeviceProperties(&prop, device));
+        std::snprintf(out, static_cast<size_t>(capacity), "%s", prop.name);
+    });
+}

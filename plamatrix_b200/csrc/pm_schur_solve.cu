@@ -88,17 +88,20 @@ struct pm_schur_workspace
     int64_t E = 0;                 // cross pairs
     int2* row_entries = nullptr;   // C: {cross, eliminated} of every primary-list entry
     int64_t* pair_offset = nullptr; // B + 1: pairs of block b are [off[b], off[b+1]) (upper blocks only)
-    int2* pairs = nullptr;         // E: {row-list entry of cross (l, p), cross (l, q)}, per block in ascending l
-    double* tfactor = nullptr;     // C x 18: T = W_lp Hll^-1 of every row-list entry (written by the diagonal pass)
+    int2* pairs = nullptr;         // E: {row-list entry of cross (l, p), row-list entry of cross (l, q)}, per block in ascending l
+    void* vfactor = nullptr;       // C x 18 (Scalar): V = W_lp L_l^-T of every row-list entry (written by the diagonal pass)
     int* saved_offsets = nullptr;
     int* saved_primary = nullptr;
     int* saved_pc = nullptr;
     // numeric
     double* hinv = nullptr;
     double* y = nullptr;
-    int hstride = 0, ystride = 0; // per eliminated block; 12 / 12 (packed [Hll^-1 | y]) for the 6x3 pairs
+    int hstride = 0, ystride = 0; // per eliminated block; 10 / 10 for the 6x3 pairs (record [L^-1 | z], see eliminated_factor3_kernel)
     void* S = nullptr;   // B * bp * bp, Scalar
     float* S32 = nullptr; // mixed-precision copy
+    bool s32_only = false; // the last assembly formed FP32 products: S32 holds the system, S only its diagonal blocks
+    double damping = 0.0, min_diag = 0.0; // of the last assembly
+    double* mf_t = nullptr; // L x 4: matrix-free FP64 product scratch (t_l = Hll^-1 W_l^T x)
     double* rhs = nullptr;
     double* minv = nullptr;
     float* minv32 = nullptr;
@@ -227,6 +230,52 @@ __global__ void eliminated_inverse_kernel(int64_t L, int bl_rt, const T* __restr
             for (int r = 0; r < bl; ++r)
                 y[l * ystride + r] = yl[r];
         }
+    }
+}
+
+// 6x3 assembly: the damped block's Cholesky factor L (Hll + damping = L L^T, the same pivot
+// test as spd_inverse) stored as L^-1 (lower, 6 values) and z = L^-1 g_l, one 80-byte record
+// [L^-1 00, 10, 11, 20, 21, 22 | z 0, 1, 2 | 0] per eliminated block (five 16-byte stores).
+// The assembly then forms V = W L^-T per cross, so W Hll^-1 W'^T = V V'^T and W Hll^-1 g = V z.
+template <typename T>
+__global__ void eliminated_factor3_kernel(int64_t L, const T* __restrict__ hll, const T* __restrict__ gl,
+                                          double lambda, double min_diag, double* __restrict__ rec,
+                                          SchurStatus* status)
+{
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < L; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        double m[9], inv[9], lo[9], work[3];
+#pragma unroll
+        for (int i = 0; i < 9; ++i)
+            m[i] = static_cast<double>(hll[l * 9 + i]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+        {
+            double& v = m[d * 3 + d];
+            v = __dadd_rn(v, __dmul_rn(lambda, fmax(fabs(v), min_diag)));
+        }
+        double i00 = 0.0, i10 = 0.0, i11 = 0.0, i20 = 0.0, i21 = 0.0, i22 = 0.0;
+        if (spd_inverse<3>(m, 3, inv, lo, work))
+        {
+            i00 = 1.0 / lo[0];
+            i11 = 1.0 / lo[4];
+            i22 = 1.0 / lo[8];
+            i10 = -(lo[3] * i00) * i11;
+            i21 = -(lo[7] * i11) * i22;
+            i20 = -(lo[6] * i00 + lo[7] * i10) * i22;
+        }
+        else
+        {
+            atomicMin(&status->eliminated_bad, static_cast<long long>(l));
+        }
+        const double g0 = static_cast<double>(gl[l * 3]), g1 = static_cast<double>(gl[l * 3 + 1]),
+                     g2 = static_cast<double>(gl[l * 3 + 2]);
+        double2* out = reinterpret_cast<double2*>(rec + l * 10);
+        out[0] = make_double2(i00, i10);
+        out[1] = make_double2(i11, i20);
+        out[2] = make_double2(i21, i22);
+        out[3] = make_double2(i00 * g0, i10 * g0 + i11 * g1);
+        out[4] = make_double2(i20 * g0 + i21 * g1 + i22 * g2, 0.0);
     }
 }
 
@@ -636,14 +685,22 @@ __global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross
     }
 }
 
-// items in row-list order: block index of (p, q) and the cross of q; pairs per block counted
-// with integer atomics (a count does not depend on the order)
+// row-list position of every cross: rowpos[prim_cross[j]] = j
+__global__ void rowpos_kernel(int64_t C, const int* __restrict__ prim_cross, int* __restrict__ rowpos)
+{
+    for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < C; j += int64_t(gridDim.x) * blockDim.x)
+        rowpos[prim_cross[j]] = static_cast<int>(j);
+}
+
+// items in row-list order: block index of (p, q) and the row-list entry of the cross (l, q);
+// pairs per block counted with integer atomics (a count does not depend on the order)
 __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
                                  const int* __restrict__ cross_eliminated, const int* __restrict__ cross_offsets,
                                  const int* __restrict__ cross_primary, int sorted, const int64_t* __restrict__ offset,
                                  const int* __restrict__ block_row_ptr, const int* __restrict__ block_col,
-                                 const int* __restrict__ diag_pos, int* __restrict__ item_block,
-                                 int* __restrict__ item_cross, int* __restrict__ block_pairs)
+                                 const int* __restrict__ diag_pos, const int* __restrict__ rowpos,
+                                 int* __restrict__ item_block, int* __restrict__ item_entry,
+                                 int* __restrict__ block_pairs)
 {
     for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
     {
@@ -670,7 +727,7 @@ __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets
                         hi = mid;
                 }
                 item_block[at] = lo; // the pattern holds (p, q) by construction
-                item_cross[at] = k;
+                item_entry[at] = rowpos[k];
                 atomicAdd(&block_pairs[lo], 1);
                 ++at;
             }
@@ -683,7 +740,7 @@ __global__ void pair_emit_kernel(int64_t P, const int* __restrict__ prim_offsets
 // item's rank in its block is the number of lower lanes with an item there (a lane bitmask per
 // block), after which the block's cursor advances by the mask's population.
 __global__ void pair_place_kernel(int64_t P, const int* __restrict__ prim_offsets, const int64_t* __restrict__ offset,
-                                  const int* __restrict__ item_block, const int* __restrict__ item_cross,
+                                  const int* __restrict__ item_block, const int* __restrict__ item_entry,
                                   const int2* __restrict__ row_entries, unsigned* mask, int64_t* cursor,
                                   int2* __restrict__ pairs)
 {
@@ -713,7 +770,7 @@ __global__ void pair_place_kernel(int64_t P, const int* __restrict__ prim_offset
             {
                 const int X = item_block[e];
                 const int64_t at = vcursor[X] + __popc(vmask[X] & below);
-                pairs[at] = make_int2(j, item_cross[e]);
+                pairs[at] = make_int2(j, item_entry[e]);
             }
             __syncwarp();
             for (int64_t e = e0; e < e1; ++e)
@@ -761,16 +818,40 @@ __device__ __forceinline__ void load_pairs(const T* __restrict__ src, double* q)
     }
 }
 
-// Diagonal block and RHS, CTA per row: thread t walks the row's crosses t, t + 256, ... (21
-// lower entries and 6 RHS terms in registers), then a fixed xor tree per warp and the warps'
-// sums in warp order.
+// N doubles to N consecutive scalars in global memory (16-byte stores for double, 8-byte for
+// float; dst aligned to two scalars)
+template <typename T, int N>
+__device__ __forceinline__ void store_pairs(T* __restrict__ dst, const double* q)
+{
+    static_assert(N % 2 == 0, "pairs of scalars");
+    if constexpr (sizeof(T) == 8)
+    {
+        double2* d2 = reinterpret_cast<double2*>(dst);
+#pragma unroll
+        for (int e = 0; e < N / 2; ++e)
+            d2[e] = make_double2(q[2 * e], q[2 * e + 1]);
+    }
+    else
+    {
+        float2* d2 = reinterpret_cast<float2*>(dst);
+#pragma unroll
+        for (int e = 0; e < N / 2; ++e)
+            d2[e] = make_float2(static_cast<float>(q[2 * e]), static_cast<float>(q[2 * e + 1]));
+    }
+}
+
+// Diagonal block and RHS, CTA per row: thread t walks the row's entries t, t + 256, ... (one
+// per cross (l, p), ascending l); per entry V = W_lp L_l^-T (6 x 3, from W and the 80-byte
+// factor record of l) is stored at the entry's row-list position for the upper-block pass, and
+// the 21 lower diagonal entries (V V^T) and 6 RHS terms (V z_l) accumulate in registers; then a
+// fixed xor tree per warp and the warps' sums in warp order.
 constexpr int kDiagThreads = 256;
-template <typename T>
+template <typename T, typename VT>
 __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
     int64_t P, const int* __restrict__ prim_offsets, const int2* __restrict__ row_entries, const T* __restrict__ w,
-    const double* __restrict__ hy, const T* __restrict__ hpp, const T* __restrict__ gp, double lambda,
+    const double* __restrict__ rec, const T* __restrict__ hpp, const T* __restrict__ gp, double lambda,
     double min_diag, const int* __restrict__ diag_pos, T* __restrict__ S, double* __restrict__ rhs,
-    double* __restrict__ tfactor)
+    VT* __restrict__ vfactor, float* __restrict__ S32)
 {
     __shared__ double part[kDiagThreads / 32][27];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -785,30 +866,27 @@ __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
         for (int j = prim_offsets[p] + t; j < J1; j += kDiagThreads)
         {
             const int2 re = row_entries[j];
-            double h[12], wv[18];
-            load_pairs<double, 12>(hy + int64_t(re.y) * 12, h);
+            double f[10], wv[18];
+            load_pairs<double, 10>(rec + int64_t(re.y) * 10, f);
             load_pairs<T, 18>(w + int64_t(re.x) * 18, wv);
-            double tall[18]; // T row of this entry, stored for the upper-block pass
+            double v[18]; // V rows: (L^-1 w_r)^T
 #pragma unroll
             for (int r = 0; r < 6; ++r)
             {
                 const double w0 = wv[3 * r], w1 = wv[3 * r + 1], w2 = wv[3 * r + 2];
-                double tr[3];
+                v[3 * r] = f[0] * w0;
+                v[3 * r + 1] = f[1] * w0 + f[2] * w1;
+                v[3 * r + 2] = f[3] * w0 + f[4] * w1 + f[5] * w2;
+            }
 #pragma unroll
-                for (int k = 0; k < 3; ++k)
-                {
-                    tr[k] = h[3 * k] * w0 + h[3 * k + 1] * w1 + h[3 * k + 2] * w2;
-                    tall[3 * r + k] = tr[k];
-                }
+            for (int r = 0; r < 6; ++r)
+            {
 #pragma unroll
                 for (int c = 0; c <= r; ++c)
-                    d[r * (r + 1) / 2 + c] += tr[0] * wv[3 * c] + tr[1] * wv[3 * c + 1] + tr[2] * wv[3 * c + 2];
-                d[21 + r] += w0 * h[9] + w1 * h[10] + w2 * h[11];
+                    d[r * (r + 1) / 2 + c] += v[3 * r] * v[3 * c] + v[3 * r + 1] * v[3 * c + 1] + v[3 * r + 2] * v[3 * c + 2];
+                d[21 + r] += v[3 * r] * f[6] + v[3 * r + 1] * f[7] + v[3 * r + 2] * f[8];
             }
-            double2* tout = reinterpret_cast<double2*>(tfactor + int64_t(j) * 18);
-#pragma unroll
-            for (int e = 0; e < 9; ++e)
-                tout[e] = make_double2(tall[2 * e], tall[2 * e + 1]);
+            store_pairs<VT, 18>(vfactor + int64_t(j) * 18, v);
         }
 #pragma unroll
         for (int e = 0; e < 27; ++e)
@@ -841,6 +919,8 @@ __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
                 if (r == c)
                     base = __dadd_rn(base, __dmul_rn(lambda, fmax(fabs(base), min_diag)));
                 S[int64_t(diag_pos[p]) * 36 + t] = static_cast<T>(base - v);
+                if (S32)
+                    S32[int64_t(diag_pos[p]) * 36 + t] = static_cast<float>(base - v);
             }
             else
             {
@@ -852,10 +932,13 @@ __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
 }
 
 // Upper blocks, 16 lanes per block: lane g = 2 s + h walks the block's pairs s, s + 8, ... for
-// rows 3h .. 3h + 2 (the two lanes of a pair load the same Hll^-1 and W_lq rows, which the
-// load unit merges), then a fixed xor tree over the 8 streams.
+// rows 3h .. 3h + 2 (S_pq -= V_lp V_lq^T; both factors come from the row-ordered V array, the
+// two lanes of a pair load the same V_lq row, which the load unit merges), then a fixed xor tree
+// over the 8 streams.
 constexpr int kUpperThreads = 256;
-__device__ __forceinline__ double stream_sum(double v, unsigned gmask)
+
+template <typename AT>
+__device__ __forceinline__ AT stream_sum_as(AT v, unsigned gmask)
 {
 #pragma unroll
     for (int o = 2; o < kPairLanes; o <<= 1)
@@ -863,12 +946,41 @@ __device__ __forceinline__ double stream_sum(double v, unsigned gmask)
     return v;
 }
 
-template <typename T>
+// N consecutive scalars (two per load) into AT registers
+template <typename VT, int N, typename AT>
+__device__ __forceinline__ void load_as(const VT* __restrict__ src, AT* q)
+{
+    if constexpr (sizeof(VT) == 8)
+    {
+        const double2* s2 = reinterpret_cast<const double2*>(src);
+#pragma unroll
+        for (int e = 0; e < N / 2; ++e)
+        {
+            const double2 v = __ldg(s2 + e);
+            q[2 * e] = static_cast<AT>(v.x);
+            q[2 * e + 1] = static_cast<AT>(v.y);
+        }
+    }
+    else
+    {
+        const float2* s2 = reinterpret_cast<const float2*>(src);
+#pragma unroll
+        for (int e = 0; e < N / 2; ++e)
+        {
+            const float2 v = __ldg(s2 + e);
+            q[2 * e] = static_cast<AT>(v.x);
+            q[2 * e + 1] = static_cast<AT>(v.y);
+        }
+    }
+}
+
+// TO: type of the assembled values, TP: type of the coupling blocks (the normal equations'),
+// VT: type of the stored V factors, AT: type of the products and their sums
+template <typename TO, typename TP, typename VT, typename AT>
 __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
     int64_t B, const int64_t* __restrict__ pair_offset, const int2* __restrict__ pairs,
     const int* __restrict__ block_row, const int* __restrict__ block_col, const int* __restrict__ transpose,
-    const int* __restrict__ block_pc,
-    const T* __restrict__ w, const double* __restrict__ tfactor, const T* __restrict__ pcv, T* __restrict__ S)
+    const int* __restrict__ block_pc, const VT* __restrict__ vfactor, const TP* __restrict__ pcv, TO* __restrict__ S)
 {
     const int g = threadIdx.x & (kPairLanes - 1);
     const int s = g >> 1, h = g & 1;
@@ -878,12 +990,12 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
     {
         if (block_col[b] <= block_row[b])
             continue;
-        double acc[3][6];
+        AT acc[3][6];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int c = 0; c < 6; ++c)
-                acc[r][c] = 0.0;
+                acc[r][c] = AT(0);
         const int64_t k1 = pair_offset[b + 1];
         int64_t k = pair_offset[b] + s;
         int2 next = k < k1 ? pairs[k] : make_int2(0, 0);
@@ -893,12 +1005,12 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
             k += kPairStreams;
             if (k < k1)
                 next = pairs[k];
-            // this lane's three rows of T = W_lp Hll^-1 (elements 9h .. 9h + 8, read as the
-            // aligned run 8h .. 8h + 9; the rows of a block row lie together in row-list order)
-            double a[10], q[18];
-            load_pairs<double, 10>(tfactor + int64_t(cur.x) * 18 + 8 * h, a);
-            load_pairs<T, 18>(w + int64_t(cur.y) * 18, q);
-            double tr[3][3];
+            // this lane's three rows of V_lp (elements 9h .. 9h + 8, read as the aligned run
+            // 8h .. 8h + 9) and all six rows of V_lq
+            AT a[10], q[18];
+            load_as<VT, 10, AT>(vfactor + int64_t(cur.x) * 18 + 8 * h, a);
+            load_as<VT, 18, AT>(vfactor + int64_t(cur.y) * 18, q);
+            AT tr[3][3];
 #pragma unroll
             for (int r = 0; r < 3; ++r)
 #pragma unroll
@@ -914,17 +1026,17 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
         for (int r = 0; r < 3; ++r)
 #pragma unroll
             for (int c = 0; c < 6; ++c)
-                acc[r][c] = stream_sum(acc[r][c], gmask);
+                acc[r][c] = stream_sum_as<AT>(acc[r][c], gmask);
         const int pc = block_pc[b];
-        T* out = S + b * 36 + 18 * h;
-        T* mirrored = S + int64_t(transpose[b]) * 36; // the lower block (q, p) holds the transpose
+        TO* out = S + b * 36 + 18 * h;
+        TO* mirrored = S + int64_t(transpose[b]) * 36; // the lower block (q, p) holds the transpose
 #pragma unroll
         for (int e = 0; e < 18; ++e)
         {
             if ((e & (kPairStreams - 1)) != s)
                 continue;
-            const double base = pc >= 0 ? static_cast<double>(pcv[int64_t(pc) * 36 + 18 * h + e]) : 0.0;
-            const T value = static_cast<T>(base - acc[e / 6][e % 6]);
+            const AT base = pc >= 0 ? static_cast<AT>(pcv[int64_t(pc) * 36 + 18 * h + e]) : AT(0);
+            const TO value = static_cast<TO>(base - acc[e / 6][e % 6]);
             out[e] = value;
             mirrored[(e % 6) * 6 + 3 * h + e / 6] = value;
         }
@@ -1352,6 +1464,115 @@ __global__ void __launch_bounds__(kVecBlock) residual_kernel(int64_t n, const do
     });
 }
 
+// FP64 matrix-free product q = S x of the damped 6x3 Schur complement, straight from the FP64
+// normal equations (used when the assembled values are FP32 only):
+//   q_p = (Hpp_p + damping) x_p + sum_q C_pq x_q - sum_{l in p} W_lp Hll^-1 sum_{q in l} W_lq^T x_q
+// where C are the primary-primary coupling blocks.  Pass 1, thread per eliminated block:
+// t_l = Hll^-1 (W_l^T x) = L^-T (L^-1 W_l^T x) from the factor record; pass 2, CTA per block row:
+// the row's crosses in row-list order, then a fixed xor tree and the warps in order.  Both passes
+// sum in fixed orders, so the product repeats bit for bit.
+template <typename T>
+__global__ void mf_eliminated6_kernel(int64_t L, const int* __restrict__ cross_offsets,
+                                      const int* __restrict__ cross_primary, const T* __restrict__ w,
+                                      const double* __restrict__ rec, const double* __restrict__ x,
+                                      double* __restrict__ t)
+{
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < L; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        double u0 = 0.0, u1 = 0.0, u2 = 0.0;
+        for (int c = cross_offsets[l]; c < cross_offsets[l + 1]; ++c)
+        {
+            double wv[18], xv[6];
+            load_pairs<T, 18>(w + int64_t(c) * 18, wv);
+            load_pairs<double, 6>(x + int64_t(cross_primary[c]) * 6, xv);
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+            {
+                u0 += wv[3 * r] * xv[r];
+                u1 += wv[3 * r + 1] * xv[r];
+                u2 += wv[3 * r + 2] * xv[r];
+            }
+        }
+        double f[10];
+        load_pairs<double, 10>(rec + l * 10, f);
+        const double v0 = f[0] * u0, v1 = f[1] * u0 + f[2] * u1, v2 = f[3] * u0 + f[4] * u1 + f[5] * u2;
+        double2* out = reinterpret_cast<double2*>(t + l * 4);
+        out[0] = make_double2(f[0] * v0 + f[1] * v1 + f[3] * v2, f[2] * v1 + f[4] * v2);
+        out[1] = make_double2(f[5] * v2, 0.0);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kDiagThreads) mf_primary6_kernel(
+    int64_t P, const int* __restrict__ prim_offsets, const int2* __restrict__ row_entries, const T* __restrict__ w,
+    const double* __restrict__ t, const T* __restrict__ hpp, double lambda, double min_diag,
+    const int* __restrict__ block_row_ptr, const int* __restrict__ block_col, const int* __restrict__ block_pc,
+    const T* __restrict__ pcv, const double* __restrict__ x, double* __restrict__ q)
+{
+    __shared__ double part[kDiagThreads / 32][6];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
+    {
+        const int p = static_cast<int>(pp);
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        const int J1 = prim_offsets[p + 1];
+        for (int j = prim_offsets[p] + tid; j < J1; j += kDiagThreads)
+        {
+            const int2 re = row_entries[j];
+            double wv[18], tv[4];
+            load_pairs<T, 18>(w + int64_t(re.x) * 18, wv);
+            load_pairs<double, 4>(t + int64_t(re.y) * 4, tv);
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+                acc[r] -= wv[3 * r] * tv[0] + wv[3 * r + 1] * tv[1] + wv[3 * r + 2] * tv[2];
+        }
+        // primary-primary coupling blocks: C_pq (upper, forward index k) or C_qp^T (lower)
+        for (int b = block_row_ptr[p] + tid; b < block_row_ptr[p + 1]; b += kDiagThreads)
+        {
+            const int code = block_pc[b];
+            if (code == -1)
+                continue;
+            const bool fwd = code >= 0;
+            const T* C = pcv + int64_t(fwd ? code : -code - 2) * 36;
+            const double* xq = x + int64_t(block_col[b]) * 6;
+#pragma unroll
+            for (int r = 0; r < 6; ++r)
+            {
+                double v = 0.0;
+#pragma unroll
+                for (int c = 0; c < 6; ++c)
+                    v += static_cast<double>(fwd ? C[r * 6 + c] : C[c * 6 + r]) * xq[c];
+                acc[r] += v;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+        {
+            const double v = warp_sum(acc[r]);
+            if (lane == 0)
+                part[warp][r] = v;
+        }
+        __syncthreads();
+        if (tid < 6)
+        {
+            double v = 0.0;
+            for (int k = 0; k < kDiagThreads / 32; ++k)
+                v = __dadd_rn(v, part[k][tid]);
+            // damped primary block times x_p (the block as stored, as the assembly uses it)
+            double d = 0.0;
+            for (int c = 0; c < 6; ++c)
+            {
+                double h = static_cast<double>(hpp[int64_t(p) * 36 + tid * 6 + c]);
+                if (c == tid)
+                    h = __dadd_rn(h, __dmul_rn(lambda, fmax(fabs(h), min_diag)));
+                d += h * x[int64_t(p) * 6 + c];
+            }
+            q[int64_t(p) * 6 + tid] = d + v;
+        }
+        __syncthreads();
+    }
+}
+
 template <typename V>
 __global__ void axpy_to_double_kernel(int64_t n, const V* __restrict__ d, double* __restrict__ x)
 {
@@ -1364,7 +1585,7 @@ template <typename T, int BP, int BL>
 __global__ void backsub_kernel(int64_t L, int bp_rt, int bl_rt, const int* __restrict__ cross_offsets,
                                const int* __restrict__ cross_primary, const T* __restrict__ w,
                                const T* __restrict__ gl, const double* __restrict__ hinv, int hstride,
-                               const T* __restrict__ dp, T* __restrict__ dl)
+                               int factor, const T* __restrict__ dp, T* __restrict__ dl)
 {
     constexpr int ML = BL > 0 ? BL : 16;
     const int bp = BP > 0 ? BP : bp_rt;
@@ -1416,12 +1637,25 @@ __global__ void backsub_kernel(int64_t L, int bp_rt, int bl_rt, const int* __res
             }
         }
         const double* H = hinv + l * hstride;
-        for (int r = 0; r < bl; ++r)
+        if (BL == 3 && factor)
         {
-            double s = 0.0;
-            for (int c = 0; c < bl; ++c)
-                s = __dadd_rn(s, __dmul_rn(H[r * bl + c], static_cast<double>(point[c])));
-            dl[l * bl + r] = static_cast<T>(s);
+            // Hll^-1 u = L^-T (L^-1 u) from the factor record [L^-1 00, 10, 11, 20, 21, 22 | z]
+            const double u0 = static_cast<double>(point[0]), u1 = static_cast<double>(point[1]),
+                         u2 = static_cast<double>(point[2]);
+            const double v0 = H[0] * u0, v1 = H[1] * u0 + H[2] * u1, v2 = H[3] * u0 + H[4] * u1 + H[5] * u2;
+            dl[l * 3] = static_cast<T>(H[0] * v0 + H[1] * v1 + H[3] * v2);
+            dl[l * 3 + 1] = static_cast<T>(H[2] * v1 + H[4] * v2);
+            dl[l * 3 + 2] = static_cast<T>(H[5] * v2);
+        }
+        else
+        {
+            for (int r = 0; r < bl; ++r)
+            {
+                double s = 0.0;
+                for (int c = 0; c < bl; ++c)
+                    s = __dadd_rn(s, __dmul_rn(H[r * bl + c], static_cast<double>(point[c])));
+                dl[l * bl + r] = static_cast<T>(s);
+            }
         }
     }
 }
@@ -1465,13 +1699,13 @@ namespace
 {
 
 template <typename T>
-void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
+void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed, bool mixed32 = false)
 {
     const int64_t n = ws->P * ws->bp;
     const int64_t bpp = ws->bp * ws->bp;
-    // 6x3 cross-pair assembly: Hll^-1 and y packed per eliminated block in 96 bytes (16-byte loads)
-    ws->hstride = ws->paired ? 12 : static_cast<int>(ws->bl * ws->bl);
-    ws->ystride = ws->paired ? 12 : static_cast<int>(ws->bl);
+    // 6x3 cross-pair assembly: one 80-byte factor record [L^-1 | z] per eliminated block
+    ws->hstride = ws->paired ? 10 : static_cast<int>(ws->bl * ws->bl);
+    ws->ystride = ws->paired ? 10 : static_cast<int>(ws->bl);
     Carver plan;
     plan.take<double>(ws->L * ws->hstride + 1);
     plan.take<double>(ws->paired ? 1 : ws->L * ws->bl + 1);
@@ -1484,13 +1718,14 @@ void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
     plan.take<SolveState>(1);
     plan.take<double>(4 * kMaxParts);
     plan.take<double>(8 * (n + 1)); // PCG / refinement vectors
+    plan.take<double>(mixed32 ? ws->L * 4 + 4 : 1);
     ws->numeric.ensure(plan.offset + 256, stream, "SchurComplementSolverWorkspace");
     Carver c;
     c.base = static_cast<char*>(ws->numeric.ptr);
     ws->hinv = c.take<double>(ws->L * ws->hstride + 1);
     ws->y = c.take<double>(ws->paired ? 1 : ws->L * ws->bl + 1);
     if (ws->paired)
-        ws->y = ws->hinv + 9;
+        ws->y = ws->hinv + 6;
     ws->S = c.take<T>(ws->B * bpp + 1);
     ws->S32 = c.take<float>(mixed ? ws->B * bpp + 1 : 1);
     ws->rhs = c.take<double>(n + 1);
@@ -1499,6 +1734,8 @@ void numeric_layout(pm_schur_workspace* ws, cudaStream_t stream, bool mixed)
     ws->status = c.take<SchurStatus>(1);
     ws->state = c.take<SolveState>(1);
     ws->partials = c.take<double>(4 * kMaxParts);
+    c.take<double>(8 * (n + 1));
+    ws->mf_t = c.take<double>(mixed32 ? ws->L * 4 + 4 : 1);
 }
 
 double* vector_area(pm_schur_workspace* ws)
@@ -1574,10 +1811,12 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     };
     ws->scratch.ensure(pass1 + 512, stream, "SchurComplementSolverWorkspace");
     run_pass1();
-    // pass 2 scratch: items (block, cross of q), pairs per block, lane masks, cursors
+    // pass 2 scratch: items (block, row-list entry of (l, q)), pairs per block, lane masks, cursors,
+    // row-list position of every cross
     Carver s2;
     s2.take<int>(E + 1);
     s2.take<int>(E + 1);
+    s2.take<int>(C + 1);
     s2.take<int>(B + 1);
     s2.take<unsigned>(B + 1);
     s2.take<int64_t>(B + 1);
@@ -1589,7 +1828,8 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     Carver c2;
     c2.base = static_cast<char*>(ws->scratch.ptr) + pass1;
     int* item_block = c2.take<int>(E + 1);
-    int* item_cross = c2.take<int>(E + 1);
+    int* item_entry = c2.take<int>(E + 1);
+    int* rowpos = c2.take<int>(C + 1);
     int* block_pairs = c2.take<int>(B + 1);
     unsigned* mask = c2.take<unsigned>(B + 1);
     int64_t* cursor = c2.take<int64_t>(B + 1);
@@ -1599,23 +1839,28 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     plan_b.take<int2>(C + 1);
     plan_b.take<int64_t>(B + 2);
     plan_b.take<int2>(E + 1);
-    plan_b.take<double>(C * 18 + 2);
+    plan_b.take<double>(C * 18 + 2); // V in the Scalar type (double at most)
     ws->pair_buffer.ensure(plan_b.offset + 512, stream, "SchurComplementSolverWorkspace");
     Carver bc;
     bc.base = static_cast<char*>(ws->pair_buffer.ptr);
     ws->row_entries = bc.take<int2>(C + 1);
     ws->pair_offset = bc.take<int64_t>(B + 2);
     ws->pairs = bc.take<int2>(E + 1);
-    ws->tfactor = bc.take<double>(C * 18 + 2);
+    ws->vfactor = bc.take<double>(C * 18 + 2);
     ws->E = E;
     PM_CUDA(cudaMemsetAsync(block_pairs, 0, size_t(B + 1) * sizeof(int), stream));
     PM_CUDA(cudaMemsetAsync(mask, 0, size_t(B + 1) * sizeof(unsigned), stream));
+    if (C > 0)
+    {
+        rowpos_kernel<<<grid_for(C, 256, 1 << 16), 256, 0, stream>>>(C, ws->prim_cross, rowpos);
+        PM_LAUNCH_CHECK();
+    }
     if (P > 0 && E > 0)
     {
         pair_emit_kernel<<<grid, 128, 0, stream>>>(P, ws->prim_offsets, ws->prim_cross, ne->cross_eliminated,
                                                    ne->cross_offsets, ne->cross_primary, sorted, offset,
-                                                   ws->block_row_ptr, ws->block_col, ws->diag_pos, item_block,
-                                                   item_cross, block_pairs);
+                                                   ws->block_row_ptr, ws->block_col, ws->diag_pos, rowpos, item_block,
+                                                   item_entry, block_pairs);
         PM_LAUNCH_CHECK();
     }
     exclusive_scan<int, int64_t>(block_pairs, ws->pair_offset, B, scan2, stream);
@@ -1631,7 +1876,7 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     if (P > 0 && E > 0)
     {
         pair_place_kernel<<<grid_for(P * 32, 256, 1 << 16), 256, 0, stream>>>(
-            P, ws->prim_offsets, offset, item_block, item_cross, ws->row_entries, mask, cursor, ws->pairs);
+            P, ws->prim_offsets, offset, item_block, item_entry, ws->row_entries, mask, cursor, ws->pairs);
         PM_LAUNCH_CHECK();
     }
     ws->paired = true;
@@ -1765,8 +2010,11 @@ void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
 
 template <typename T>
 void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, double lambda, double min_diag,
-                     cudaStream_t stream)
+                     cudaStream_t stream, bool fp32_products = false)
 {
+    ws->s32_only = false;
+    ws->damping = lambda;
+    ws->min_diag = min_diag;
     AssembleArgs<T> a;
     a.P = ne->P;
     a.bp = static_cast<int>(ne->bp);
@@ -1800,15 +2048,36 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
     };
     if (ws->paired)
     {
-        assemble_diag6_kernel<T><<<grid_for(a.P, 1, 1 << 20), kDiagThreads, 0, stream>>>(
-            a.P, ws->prim_offsets, ws->row_entries, a.w, ws->hinv, a.hpp, a.gp, a.lambda, a.min_diag, a.diag_pos,
-            a.S, a.rhs, ws->tfactor);
-        PM_LAUNCH_CHECK();
-        // every upper block, also those whose only terms are primary-primary couplings
-        assemble_upper6_kernel<T><<<grid_for(ws->B * kPairLanes, kUpperThreads), kUpperThreads, 0, stream>>>(
-            ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, a.w,
-            ws->tfactor, a.pcv, a.S);
-        PM_LAUNCH_CHECK();
+        const unsigned ugrid = grid_for(ws->B * kPairLanes, kUpperThreads);
+        if (fp32_products)
+        {
+            // FP32 products: V stored in FP32, upper blocks formed and summed in FP32 into S32;
+            // the diagonal blocks and the RHS are still summed in FP64 (S keeps the FP64 diagonal
+            // blocks for the FP64 block-Jacobi factorisation)
+            float* vf = static_cast<float*>(ws->vfactor);
+            assemble_diag6_kernel<T, float><<<grid_for(a.P, 1, 1 << 20), kDiagThreads, 0, stream>>>(
+                a.P, ws->prim_offsets, ws->row_entries, a.w, ws->hinv, a.hpp, a.gp, a.lambda, a.min_diag,
+                a.diag_pos, a.S, a.rhs, vf, ws->S32);
+            PM_LAUNCH_CHECK();
+            assemble_upper6_kernel<float, T, float, float><<<ugrid, kUpperThreads, 0, stream>>>(
+                ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, vf, a.pcv,
+                ws->S32);
+            PM_LAUNCH_CHECK();
+        }
+        else
+        {
+            T* vf = static_cast<T*>(ws->vfactor);
+            assemble_diag6_kernel<T, T><<<grid_for(a.P, 1, 1 << 20), kDiagThreads, 0, stream>>>(
+                a.P, ws->prim_offsets, ws->row_entries, a.w, ws->hinv, a.hpp, a.gp, a.lambda, a.min_diag,
+                a.diag_pos, a.S, a.rhs, vf, nullptr);
+            PM_LAUNCH_CHECK();
+            // every upper block, also those whose only terms are primary-primary couplings
+            assemble_upper6_kernel<T, T, T, double><<<ugrid, kUpperThreads, 0, stream>>>(
+                ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, vf, a.pcv,
+                a.S);
+            PM_LAUNCH_CHECK();
+        }
+        ws->s32_only = fp32_products;
         diag_inverse_kernel<T, 6><<<grid_for(a.P, 64, 1 << 16), 64, 0, stream>>>(a.P, a.diag_pos, a.S, a.minv,
                                                                                  a.status);
         PM_LAUNCH_CHECK();
@@ -1839,12 +2108,12 @@ SchurView schur_view(pm_schur_workspace* ws, bool mixed)
         return v;
     v.P = ws->P;
     v.B = ws->B;
-    v.value_size = ws->value_size;
-    v.mixed = mixed;
+    v.value_size = ws->s32_only ? 4 : ws->value_size;
+    v.mixed = mixed || ws->s32_only;
     v.block_row_ptr = ws->block_row_ptr;
     v.block_col = ws->block_col;
     v.diag_pos = ws->diag_pos;
-    v.S = ws->S;
+    v.S = ws->s32_only ? static_cast<const void*>(ws->S32) : ws->S;
     v.minv = ws->minv;
     v.minv32 = ws->minv32;
     return v;
@@ -2226,11 +2495,25 @@ void true_residual(pm_schur_workspace* ws, cudaStream_t stream, const M* S, cons
     const int64_t P = ws->P, n = P * ws->bp;
     const int bp = static_cast<int>(ws->bp);
     const unsigned sgrid = grid_for(P * 32, kVecBlock, kMaxParts);
-    if (bp == 6)
+    if (ws->s32_only)
+    {
+        // the assembled values are FP32: the FP64 product comes from the FP64 normal equations
+        const pm_normal_equations* ne = ws->last_ne;
+        mf_eliminated6_kernel<double><<<grid_for(ws->L, 128, 1 << 20), 128, 0, stream>>>(
+            ws->L, ne->cross_offsets, ne->cross_primary, static_cast<const double*>(ne->cross_values), ws->hinv, x,
+            ws->mf_t);
+        PM_LAUNCH_CHECK();
+        mf_primary6_kernel<double><<<grid_for(P, 1, 1 << 20), kDiagThreads, 0, stream>>>(
+            P, ws->prim_offsets, ws->row_entries, static_cast<const double*>(ne->cross_values), ws->mf_t,
+            static_cast<const double*>(ne->primary_diagonal), ws->damping, ws->min_diag, ws->block_row_ptr,
+            ws->block_col, ws->block_pc, static_cast<const double*>(ne->primary_cross_values), x, q);
+        PM_LAUNCH_CHECK();
+    }
+    else if (bp == 6)
         bsr_spmv_kernel<double, M, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, x, q);
     else
         bsr_spmv_kernel<double, M, 0><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, x, q);
-        PM_LAUNCH_CHECK();
+    PM_LAUNCH_CHECK();
     residual_kernel<<<grid_for(n, kVecBlock, kMaxParts), kVecBlock, 0, stream>>>(n, ws->rhs, q, r, ws->partials,
                                                                                ws->state);
     PM_LAUNCH_CHECK();
@@ -2433,19 +2716,23 @@ void schur_spmv(pm_schur_workspace* ws, cudaStream_t stream, const T* x, T* y)
 {
     if (!ws || !ws->assembled || ws->P <= 0)
         fail(PM_LOGIC_ERROR, "Schur SpMV: the workspace holds no assembled system");
-    if (ws->value_size != static_cast<int>(sizeof(T)))
-        fail(PM_INVALID_ARGUMENT, "Schur SpMV: scalar type differs from the assembled system");
+    const int vsize = ws->s32_only ? 4 : ws->value_size;
+    if (vsize != static_cast<int>(sizeof(T)))
+        fail(ws->s32_only ? PM_LOGIC_ERROR : PM_INVALID_ARGUMENT,
+             ws->s32_only ? "Schur SpMV: the last solve assembled FP32 values; use the float SpMV"
+                          : "Schur SpMV: scalar type differs from the assembled system");
     if (!x || !y || static_cast<const void*>(x) == static_cast<const void*>(y))
         fail(PM_INVALID_ARGUMENT, "Schur SpMV: vectors must be non-null and distinct");
+    const void* values = ws->s32_only ? static_cast<const void*>(ws->S32) : ws->S;
     const int64_t P = ws->P;
     const int bp = static_cast<int>(ws->bp);
     const unsigned sgrid = grid_for(P * 32, kVecBlock, 1 << 16);
     if (bp == 6)
         bsr_spmv_kernel<T, T, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col,
-                                                                  static_cast<const T*>(ws->S), x, y);
+                                                                  static_cast<const T*>(values), x, y);
     else
         bsr_spmv_kernel<T, T, 0><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col,
-                                                                  static_cast<const T*>(ws->S), x, y);
+                                                                  static_cast<const T*>(values), x, y);
     PM_LAUNCH_CHECK();
 }
 
@@ -2476,7 +2763,13 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         fail(PM_INVALID_ARGUMENT, "batched Schur solve: the dense backend solves single systems");
     if (dense && n > PM_DENSE_MAX_UNKNOWNS)
         fail(PM_INVALID_ARGUMENT, "dense Schur backend supports up to 16,384 primary unknowns");
-    const bool mixed = o->precision == PM_PRECISION_MIXED && sizeof(T) == 8 && !batch && !dense;
+    if (o->precision != PM_PRECISION_NATIVE && o->precision != PM_PRECISION_MIXED &&
+        o->precision != PM_PRECISION_MIXED_FP32_ASSEMBLY)
+        fail(PM_INVALID_ARGUMENT, "solveDampedSchurComplement: unknown precision mode");
+    // FP32 assembly products (6x6 primary / 3x3 eliminated blocks, double normal equations)
+    const bool mixed32 = o->precision == PM_PRECISION_MIXED_FP32_ASSEMBLY && sizeof(T) == 8 && !batch && !dense &&
+                         bp == 6 && bl == 3;
+    const bool mixed = (o->precision == PM_PRECISION_MIXED || mixed32) && sizeof(T) == 8 && !batch && !dense;
     if (batch)
     {
         if (sizeof(T) != 8 || bp != 6)
@@ -2512,7 +2805,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         ws->L = L;
         ws->bp = bp;
         ws->bl = bl;
-        numeric_layout<T>(ws, stream, mixed);
+        numeric_layout<T>(ws, stream, mixed, mixed32);
     }
     const bool reused = ws->pattern_builds > 0 && topology_matches(ws, ne, stream);
     if (!reused)
@@ -2521,7 +2814,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     ws->last_version = ne->topology_version;
     ws->value_size = sizeof(T);
     rep->pattern_reused = reused;
-    numeric_layout<T>(ws, stream, mixed);
+    numeric_layout<T>(ws, stream, mixed, mixed32);
     PM_CUDA(cudaMemsetAsync(ws->state, 0, sizeof(SolveState), stream));
     PM_CUDA(cudaEventRecord(ws->events[1], stream));
     // ---- eliminated inverses
@@ -2530,7 +2823,14 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     if (ne->observation_status.ptr)
         PM_CUDA(cudaMemcpyAsync(&ws->status->observation_bad, ne->observation_status.ptr, sizeof(long long),
                                 cudaMemcpyDeviceToDevice, stream));
-    if (L > 0)
+    if (L > 0 && ws->paired)
+    {
+        eliminated_factor3_kernel<T><<<grid_for(L, 128, 1 << 20), 128, 0, stream>>>(
+            L, static_cast<const T*>(ne->eliminated_diagonal), static_cast<const T*>(ne->eliminated_gradient), damping,
+            o->minimum_diagonal, ws->hinv, ws->status);
+        PM_LAUNCH_CHECK();
+    }
+    else if (L > 0)
     {
         const unsigned grid = grid_for(L, 128, 1 << 20);
         if (bl == 3)
@@ -2548,13 +2848,17 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     }
     PM_CUDA(cudaEventRecord(ws->events[2], stream));
     // ---- assembly + preconditioner + RHS
+    ws->s32_only = false;
     if (P > 0)
-        launch_assembly<T>(ws, ne, damping, o->minimum_diagonal, stream);
+        launch_assembly<T>(ws, ne, damping, o->minimum_diagonal, stream, mixed32);
     if (mixed && P > 0)
     {
-        convert_kernel<T, float><<<grid_for(ws->B * bp * bp, 256, 65535), 256, 0, stream>>>(
-            static_cast<const T*>(ws->S), ws->S32, ws->B * bp * bp);
-        PM_LAUNCH_CHECK();
+        if (!ws->s32_only)
+        {
+            convert_kernel<T, float><<<grid_for(ws->B * bp * bp, 256, 65535), 256, 0, stream>>>(
+                static_cast<const T*>(ws->S), ws->S32, ws->B * bp * bp);
+            PM_LAUNCH_CHECK();
+        }
         convert_kernel<double, float><<<grid_for(P * bp * bp, 256, 4096), 256, 0, stream>>>(ws->minv, ws->minv32,
                                                                                             P * bp * bp);
         PM_LAUNCH_CHECK();
@@ -2797,6 +3101,13 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         }
         if (!rep->converged && fp64_fallback)
         {
+            if (ws->s32_only)
+            {
+                // the FP64 PCG needs the FP64 values: assemble them now (the rare path)
+                launch_assembly<T>(ws, ne, damping, o->minimum_diagonal, stream, false);
+                if (learned)
+                    restore_block_jacobi();
+            }
             // FP64 block-Jacobi PCG from the iterate reached (from zero when it is not finite)
             if (!std::isfinite(norm))
                 PM_CUDA(cudaMemsetAsync(x64, 0, n * sizeof(double), stream));
@@ -2840,13 +3151,13 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             backsub_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(L, 6, 3, ne->cross_offsets, ne->cross_primary,
                                                               static_cast<const T*>(ne->cross_values),
                                                               static_cast<const T*>(ne->eliminated_gradient), ws->hinv,
-                                                              ws->hstride, dp, dl);
+                                                              ws->hstride, ws->paired ? 1 : 0, dp, dl);
         else
             backsub_kernel<T, 0, 0><<<grid, 128, 0, stream>>>(L, static_cast<int>(bp), static_cast<int>(bl),
                                                               ne->cross_offsets, ne->cross_primary,
                                                               static_cast<const T*>(ne->cross_values),
                                                               static_cast<const T*>(ne->eliminated_gradient), ws->hinv,
-                                                              ws->hstride, dp, dl);
+                                                              ws->hstride, 0, dp, dl);
         PM_LAUNCH_CHECK();
     }
     PM_CUDA(cudaEventRecord(ws->events[5], stream));
@@ -2861,12 +3172,22 @@ void export_system(pm_schur_workspace* ws, cudaStream_t stream, int64_t* ro, int
 {
     if (!ws || !ws->assembled)
         fail(PM_LOGIC_ERROR, "CUDA Schur values have not been assembled");
-    if (ws->value_size != static_cast<int>(sizeof(T)))
-        fail(PM_INVALID_ARGUMENT, "export scalar type differs from the assembled system");
     const int64_t bpp = ws->bp * ws->bp;
-    export_csr_kernel<T, O><<<grid_for(ws->B * bpp, 256, 65535), 256, 0, stream>>>(
-        ws->B, static_cast<int>(ws->bp), ws->P, ws->block_row_ptr, ws->block_col, ws->block_row,
-        static_cast<const T*>(ws->S), ro, ci, values);
+    if (ws->s32_only)
+    {
+        // FP32-assembled values (mixed precision with FP32 products), widened for a double export
+        export_csr_kernel<float, O><<<grid_for(ws->B * bpp, 256, 65535), 256, 0, stream>>>(
+            ws->B, static_cast<int>(ws->bp), ws->P, ws->block_row_ptr, ws->block_col, ws->block_row, ws->S32, ro, ci,
+            values);
+    }
+    else
+    {
+        if (ws->value_size != static_cast<int>(sizeof(T)))
+            fail(PM_INVALID_ARGUMENT, "export scalar type differs from the assembled system");
+        export_csr_kernel<T, O><<<grid_for(ws->B * bpp, 256, 65535), 256, 0, stream>>>(
+            ws->B, static_cast<int>(ws->bp), ws->P, ws->block_row_ptr, ws->block_col, ws->block_row,
+            static_cast<const T*>(ws->S), ro, ci, values);
+    }
     PM_LAUNCH_CHECK();
     if (rhs)
         PM_CUDA(cudaMemcpyAsync(rhs, ws->rhs, ws->P * ws->bp * sizeof(double), cudaMemcpyDeviceToDevice, stream));

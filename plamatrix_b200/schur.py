@@ -54,7 +54,7 @@ N.register("pm_schur_dims", [vp, vp, vp, vp])
 N.register("pm_schur_spmv_f32", [vp, vp, vp, vp])
 N.register("pm_schur_spmv_f64", [vp, vp, vp, vp])
 
-PRECISION = {"native": 0, "mixed": 1}
+PRECISION = {"native": 0, "mixed": 1, "mixed_fp32_assembly": 2}
 
 
 LINEAR_BACKEND = {"pcg": 0, "dense": 1}

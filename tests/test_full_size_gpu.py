@@ -7,7 +7,8 @@ for bit to the reference library at smaller sizes.
 
 Checked here at full size: the reduced system's scalar-CSR pattern bit for bit, its values and
 RHS within 1e-12 of the largest entry, and the primary / eliminated steps of the plain FP64,
-mixed-precision and learned + mixed solves within 1e-6 relative of the oracle's steps."""
+mixed-precision (FP64 assembly, and FP32 assembly products) and learned + mixed (FP32 assembly
+products) solves within 1e-6 relative of the oracle's steps."""
 import numpy as np
 import pytest
 import torch
@@ -42,11 +43,11 @@ def _learned_net():
     return net
 
 
-@pytest.mark.parametrize("variant", ["plain", "mixed", "learned_mixed"])
+@pytest.mark.parametrize("variant", ["plain", "mixed", "mixed_fp32_assembly", "learned_mixed"])
 def test_full_size_step_matches_oracle(full_size, variant):
     kw = {"max_iterations": 200, "relative_tolerance": 1e-8}
     if variant != "plain":
-        kw["precision"] = "mixed"
+        kw["precision"] = "mixed" if variant == "mixed" else "mixed_fp32_assembly"
     if variant == "learned_mixed":
         kw["learned"] = _learned_net()
     ws = SC.SchurComplementSolverWorkspace()

@@ -476,6 +476,44 @@ def test_small_bundle_solve_matches_reference(checkers, precision):
     assert np.linalg.norm(res) / np.linalg.norm(rhs) <= 1e-9
 
 
+def test_fp32_assembly_products_match_reference(checkers):
+    """Mixed precision with FP32 assembly products (6x6 / 3x3): the FP32-assembled reduced system
+    within FP32 rounding of the reference's (pattern bit-exact, values within 1e-6 of the largest
+    entry, RHS summed in FP64 within 1e-12), and the step refined to the FP64 tolerance by the
+    matrix-free FP64 residual: within 1e-6 of the reference's steps, FP64 true residual <= 1e-10."""
+    prob = W.small_bundle(seed=2)
+    orc = checkers.normal_equations_from_observations(prob)
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=1e-10, max_iterations=500)
+    ne = _device_from_observations(prob)
+    ws = SC.SchurComplementSolverWorkspace()
+    opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-10,
+                                           precision="mixed_fp32_assembly")
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+    assert rep["converged"] and rep["mixed_precision_used"], rep["message"]
+    assert rep["true_relative_residual"] <= 1e-10 * 1.01
+    assert np.linalg.norm(host(dp) - dp_ref) <= 1e-6 * np.linalg.norm(dp_ref)
+    assert np.linalg.norm(host(dl) - dl_ref) <= 1e-6 * np.linalg.norm(dl_ref)
+    ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+    res = rhs - csr_matvec(ro, ci, vals, host(dp))
+    assert np.linalg.norm(res) / np.linalg.norm(rhs) <= 1e-10 * 1.5
+    sysd = ws.export()
+    assert np.array_equal(host(sysd["row_offsets"]), ro) and np.array_equal(host(sysd["col_indices"]), ci)
+    assert np.abs(host(sysd["values"]) - vals).max() <= 1e-6 * np.abs(vals).max()
+    assert np.abs(host(sysd["rhs"]) - rhs).max() <= 1e-12 * np.abs(rhs).max()
+    # the workspace now holds FP32 values: the float SpMV reads them, the double one refuses
+    x = np.random.default_rng(1).standard_normal(len(ro) - 1)
+    y = host(ws.spmv(dev(x.astype(np.float32))))
+    ref = csr_matvec(ro, ci, vals, x)
+    assert np.abs(y - ref).max() <= 1e-5 * np.abs(ref).max()
+    with pytest.raises(N.LogicError):
+        ws.spmv(dev(x))
+    # a plain solve on the same workspace assembles FP64 values again
+    dp2, _, rep2 = SC.solve_damped_schur_complement(
+        ne, 1e-3, SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-10), ws)
+    assert rep2["converged"]
+    assert np.abs(host(ws.export()["values"]) - vals).max() <= 1e-12 * np.abs(vals).max()
+
+
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
 def test_reduced_system_spmv_matches_reference(checkers, dtype):
     """y = S x through the block-CSR SpMV of the assembled system against the reference's

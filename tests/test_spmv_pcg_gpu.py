@@ -228,9 +228,16 @@ def test_full_size_laplacian_jacobi_pcg_matches_oracle(checkers, dtype):
     assert rep["converged"] and rep_ref["converged"]
     assert abs(rep["iterations"] - rep_ref["iterations"]) <= (1 if dtype == np.float64 else 2)
     xr = host(x).astype(np.float64)
-    res = b.astype(np.float64) - checkers.csr_spmv(ro, ci, v.astype(np.float64), xr)
-    rel = np.linalg.norm(res) / np.linalg.norm(b.astype(np.float64))
-    assert rel <= (1.5e-8 if dtype == np.float64 else 1e-6), rel
+    b64 = b.astype(np.float64)
+    rel = np.linalg.norm(b64 - checkers.csr_spmv(ro, ci, v.astype(np.float64), xr)) / np.linalg.norm(b64)
+    if dtype == np.float64:
+        assert rel <= 1.5e-8, rel
+    else:
+        # an FP32-stored solution cannot reach 1e-8 in the FP64 residual: its rounding alone gives
+        # ~eps32 ||A|| ||x|| / ||b||; the device must be within 2x of the oracle's own FP32 solution
+        rel_ref = np.linalg.norm(b64 - checkers.csr_spmv(ro, ci, v.astype(np.float64), x_ref.astype(np.float64)))
+        rel_ref /= np.linalg.norm(b64)
+        assert rel <= max(1.5e-8, 2.0 * rel_ref), (rel, rel_ref)
     tol = 1e-6 if dtype == np.float64 else 1e-4
     assert np.linalg.norm(xr - x_ref) <= tol * np.linalg.norm(x_ref)
 
