@@ -37,10 +37,11 @@ WORKLOAD = ("schur_lm_P4000_L2000000: P=4,000 x 6-dof, L=2,000,000 x 3-dof, 2+Po
             "per eliminated block from a wrapped window of 40, 2-dim residuals, Huber delta 1, "
             "lambda 1e-3, FP64 true relative residual 1e-8")
 METRIC = "Schur-PCG ms to 1e-8 FP64 rel. residual: learned+mixed vs plain; SpMV HBM GB/s"
-LEARN_TRAIN, LEARN_HOLD, LEARN_STEPS = 8, 3, 20
-# DRAM bytes (read + write) of one full-size assembly (assemble_diag6 + assemble_upper6), from an
-# ncu capture of `python bench.py --steps 2 --warmup 1 --no-extras` with dram__bytes_{read,write}.sum
-ASSEMBLY_TRAFFIC_BYTES = 8_126_000_000
+# DRAM bytes (read + write) of one assembly (assemble_diag6 + assemble_upper6) per cross block,
+# from an ncu capture of the two kernels on the P=4,000, L=200,000 case, scaled by the cross count
+# (the traffic grows with the crosses): see the profile summary of the assembly
+ASSEMBLY_TRAFFIC_BYTES_PER_CROSS = None
+ASSEMBLY_TRAFFIC_SOURCE = "not captured for this kernel version"
 BATCH_SYSTEMS = 512
 
 
@@ -54,6 +55,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip SpMV / e2e / CPU-baseline legs")
     ap.add_argument("--sparse-only", action="store_true", help="only the Laplacian SpMV / COO->CSR leg")
     ap.add_argument("--dense-only", action="store_true", help="only the dense-backend vs PCG leg (n = 3,072)")
+    ap.add_argument("--learned-protocol", default="full", choices=["full", "short"],
+                    help="full: train on LM iterations 1-20 of 8 seeds, test on 21-30 and 4 unseen seeds")
     return ap.parse_args()
 
 
@@ -238,7 +241,11 @@ def run_ours(args):
     n, m = P_FULL * 6, L * 3
     dp = torch.zeros(n, dtype=torch.float64, device="cuda")
     dl = torch.zeros(m, dtype=torch.float64, device="cuda")
-    mixed = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL, precision="mixed")
+    # mixed precision as specified: FP32 assembly products, SpMV and preconditioner apply; FP64
+    # dots, factorisations and matrix-free true residual.  mixed64: FP64 assembly, FP32 inner PCG
+    mixed = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL,
+                                            precision="mixed_fp32_assembly")
+    mixed64 = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL, precision="mixed")
     plain = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL, precision="native")
     stream = torch.cuda.current_stream()
 
@@ -264,28 +271,24 @@ def run_ours(args):
         ms = replicas.max_over_ranks(e0.elapsed_time(e1) / steps)
         return ms, last
 
-    # ---- learned block-Jacobi correction: trained on this problem's own LM sequence (device
-    # kernels: features, tensor-core MLP forward/backward, Adam), held-out iterations and an
-    # unseen seed evaluated against plain block Jacobi
+    # ---- learned block-Jacobi correction: the LM-sequence protocol (device kernels: features,
+    # tensor-core MLP forward/backward, Adam), probe loss of the preconditioned operator; held-out
+    # LM iterations and unseen seeds evaluated against plain block Jacobi
     from plamatrix_b200 import learned as LR
     net = SC.LearnedPreconditioner(seed=rank)
-    runner = LR.LMRunner({**prob, **{k: dev[k] for k in ("obs_primary", "obs_eliminated", "residual")},
-                          "jp": dev["jp"], "jl": dev["jl"]})
-    seq = list(LR.lm_sequence({"jp": dev["jp"], "jl": dev["jl"]}, LEARN_TRAIN + LEARN_HOLD, seed=rank))
-    t_train = time.perf_counter()
-    hist = LR.train(net, [runner], [seq[:LEARN_TRAIN]], steps_per_system=LEARN_STEPS, tolerance=TOL)
-    t_train = time.perf_counter() - t_train
-    unseen = W.bundle_problem_device(P_FULL, L, per_eliminated="2+poisson4", window=40, seed=1000 + rank)
-    unseen_runner = LR.LMRunner(unseen)
-    unseen_seq = list(LR.lm_sequence(unseen, LEARN_HOLD, seed=1000 + rank))
-    evaluation = LR.evaluate(net, [runner, unseen_runner], [seq[LEARN_TRAIN:], unseen_seq], tolerance=TOL)
-    del unseen_runner, unseen
-    learned_mixed = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL, precision="mixed",
-                                                    learned=net)
+    if args.learned_protocol == "full":
+        c3 = LR.c3_protocol(net, P_FULL, L, train_seeds=range(8), unseen_seeds=range(100, 104), train_iterations=20,
+                            test_iterations=10, epochs=2)
+    else:
+        c3 = LR.c3_protocol(net, P_FULL, L, train_seeds=range(2), unseen_seeds=range(100, 101), train_iterations=4,
+                            test_iterations=2, epochs=1)
+    learned_mixed = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=TOL,
+                                                    precision="mixed_fp32_assembly", learned=net)
 
     for _ in range(args.warmup):
         step(learned_mixed)
         step(mixed)
+        step(mixed64)
         step(plain)
     torch.cuda.synchronize()
 
@@ -295,6 +298,7 @@ def run_ours(args):
     ms_learned, (_, _, rep_learned) = timed(lambda: step(learned_mixed), args.steps)
     launches = (N.load().pm_kernel_launches() - launches0) / args.steps
     ms_mixed, (_, _, rep_mixed) = timed(lambda: step(mixed), args.steps)
+    ms_mixed64, (_, _, rep_mixed64) = timed(lambda: step(mixed64), args.steps)
     ms_plain, (_, _, rep_plain) = timed(lambda: step(plain), args.steps)
     clock = clocks.stop()
 
@@ -305,7 +309,12 @@ def run_ours(args):
     schur_spmv = schur_spmv_leg(torch, ws, n, stream) if rank == 0 else None
     out = {}
     if rank == 0 and not args.no_extras:
-        out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, mixed, n, m, net, prob)
+        out = extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, learned_mixed, n, m, net, prob)
+    if not args.no_extras:
+        # every rank takes part: the 512 independent systems are sharded across the ranks
+        batched = batched_leg(torch, SC, W, net)
+        if rank == 0:
+            out["batched"] = batched
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -323,47 +332,64 @@ def run_ours(args):
     asm_ms = rep_plain["assembly_ms"]
     achieved = assembly_bytes / (asm_ms * 1e-3) / 1e9
     phases = ("pattern_ms", "eliminated_inverse_ms", "assembly_ms", "solve_ms", "back_substitution_ms", "total_ms")
+    def group_summary(group):
+        rows = [r for r in c3["rows"] if r["group"] == group]
+        return {"systems": len(rows),
+                "mean_plain_iterations": round(float(np.mean([r["plain"]["iterations"] for r in rows])), 3) if rows else None,
+                "mean_learned_iterations": round(float(np.mean([r["learned"]["iterations"] for r in rows])), 3) if rows else None,
+                "plain_learned_iterations": [[r["plain"]["iterations"], r["learned"]["iterations"]] for r in rows]}
+
     line = {
         "metric": METRIC, "value": round(ms_learned, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_learned, 4), "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 (FP32 inner PCG, FP64 dots/refinement; BF16 tensor-core MLP)",
+        "vs_baseline": None,
+        "dtype": ("f64 result (FP32 assembly products, SpMV and preconditioner apply; FP64 dots, alpha/beta, "
+                  "Cholesky factors, matrix-free true residual and refinement; BF16 tensor-core MLP)"),
         "data": "synthetic",
         "config": config_dict(world, L),
         "workload_counts": {"observations": nobs, "schur_blocks": B, "cross_blocks": C_, "systems_per_step": world},
         "plain_fp64_ms": round(ms_plain, 4),
         "mixed_ms": round(ms_mixed, 4),
+        "mixed_fp64_assembly_ms": round(ms_mixed64, 4),
         "learned_mixed_over_plain_speedup": round(ms_plain / ms_learned, 3),
         "mixed_over_plain_speedup": round(ms_plain / ms_mixed, 3),
+        "pcg_phase_speedup": {"learned_mixed_over_plain": round(rep_plain["solve_ms"] / rep_learned["solve_ms"], 3),
+                              "mixed_over_plain": round(rep_plain["solve_ms"] / rep_mixed["solve_ms"], 3)},
         "accumulation_ms": round(ms_accum, 4),
         "phases_learned_mixed": {k: round(rep_learned[k], 4) for k in phases},
         "phases_mixed": {k: round(rep_mixed[k], 4) for k in phases},
+        "phases_mixed_fp64_assembly": {k: round(rep_mixed64[k], 4) for k in phases},
         "phases_plain": {k: round(rep_plain[k], 4) for k in phases},
         "iterations": {"learned_mixed_inner": rep_learned["iterations"],
                        "learned_mixed_refinements": rep_learned["refinement_steps"],
                        "learned_fallback": bool(rep_learned["learned_fallback"]),
                        "mixed_inner": rep_mixed["iterations"], "mixed_refinements": rep_mixed["refinement_steps"],
-                       "plain": rep_plain["iterations"]},
+                       "mixed_fp64_assembly_inner": rep_mixed64["iterations"], "plain": rep_plain["iterations"]},
         "true_relative_residual": {"learned_mixed": rep_learned["true_relative_residual"],
                                    "mixed": rep_mixed["true_relative_residual"],
+                                   "mixed_fp64_assembly": rep_mixed64["true_relative_residual"],
                                    "plain": rep_plain["true_relative_residual"]},
-        "converged": bool(rep_learned["converged"] and rep_mixed["converged"] and rep_plain["converged"]),
+        "converged": bool(rep_learned["converged"] and rep_mixed["converged"] and rep_mixed64["converged"] and
+                          rep_plain["converged"]),
         "learned": {
-            "protocol": (f"LM sequence of this problem: {LEARN_TRAIN} training iterations (Jacobians x (1 + 0.1 N(0,1)), "
-                         f"lambda x{{0.5,2}} from 1e-3), {LEARN_STEPS} Adam steps each (lr 2e-3); held out: "
-                         f"{LEARN_HOLD} later iterations and {LEARN_HOLD} iterations of an unseen seed"),
-            "train_seconds": round(t_train, 2),
-            "loss_first_last": [round(float(np.mean([h[0] for h in hist])), 6),
-                                round(float(np.mean([h[1] for h in hist])), 6)] if hist else None,
-            "held_out": [{"plain_iterations": r["plain"]["iterations"], "learned_iterations": r["learned"]["iterations"],
-                          "plain_ms": round(r["plain"]["ms"], 3), "learned_mixed_ms": round(r["learned"]["ms"], 3),
-                          "fallback": bool(r["learned"]["fallback"]),
-                          "learned_true_relative_residual": r["learned"]["true_relative_residual"]}
-                         for r in evaluation],
+            "protocol": ("LM sequences of the large problem (Jacobians x (1 + 0.1 N(0,1)), lambda x{0.5,2} from 1e-3); "
+                         + ("training on iterations 1-20 of seeds 0-7 (2 passes, 4 Rademacher probes per system, "
+                            "probe loss ||(I - M S) v||^2 / ||v||^2, Adam lr 1e-3); tested on iterations 21-30 of "
+                            "those seeds and of 4 unseen seeds" if args.learned_protocol == "full" else
+                            "short form: training on iterations 1-4 of seeds 0-1 (1 pass, 4 probes per system); "
+                            "tested on iterations 5-6 of those seeds and of 1 unseen seed; --learned-protocol full "
+                            "runs iterations 1-20 x 8 seeds / 21-30 + 4 unseen seeds")),
+            "train_seconds": c3["train_seconds"], "epoch_losses": [round(x, 6) for x in c3["epoch_losses"]],
+            "held_out_iterations": group_summary("held_out_iterations"),
+            "unseen_seeds": group_summary("unseen_seeds"),
+            "fallbacks": c3["fallbacks"], "all_converged": c3["all_converged"],
         },
-        "roofline": {"bound": "hbm", "kernel": "assemble_upper6_kernel<double> + assemble_diag6_kernel<double> (+ block-Jacobi inverse)",
+        "roofline": {"bound": "hbm", "kernel": "assemble_diag6_kernel<double,double> + assemble_upper6_kernel<double,...>",
                      "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                     "traffic": ASSEMBLY_TRAFFIC_BYTES if L == L_FULL else None,
+                     "traffic": (round(ASSEMBLY_TRAFFIC_BYTES_PER_CROSS * C_) if ASSEMBLY_TRAFFIC_BYTES_PER_CROSS
+                                 else None),
+                     "traffic_source": ASSEMBLY_TRAFFIC_SOURCE,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": assembly_bytes},
         "schur_spmv_fp64": schur_spmv,
         "gpu_launches": launches,
@@ -401,8 +427,6 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=Non
     out["e2e"] = {"value": round(e0.elapsed_time(e1) / args.steps, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
                   "d2h_bytes_per_step": (n + m) * 8}
     out["spmv"] = sparse_leg(torch, S, W, stream)
-    # ---- batched uneven systems
-    out["batched"] = batched_leg(torch, SC, W, net)
     out["dense_c4_max"] = dense_leg(torch, SC, W)
     # ---- CPU baseline: one full-size LM linear step of the reference's own CPU library (the
     # same host problem the device arm was built from), timed on its own, no scaling
@@ -549,68 +573,98 @@ def dense_leg(torch, SC, W):
 
 def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
     """Independent systems P ~ U{8..512}, L ~ U{500..50,000}, 4 uniform distinct primaries per
-    eliminated block: one batched launch sequence (union accumulation, pattern, assembly,
-    graph-replayed per-system PCG, back-substitution) against a plain per-system loop."""
+    eliminated block, split across the ranks by estimated cost (contiguous shards, no collective on
+    the data path): each rank solves its shard as one batched launch sequence (union accumulation,
+    pattern, assembly, graph-replayed per-system PCG, back-substitution) and as a plain per-system
+    loop.  Times are device times, the job's the maximum over ranks.  Latency is reported two ways:
+    a system's own duration, and the time from the start of the job to its solution."""
+    from plamatrix_b200 import replicas
+    world, rank = replicas.world_and_rank()
     sizes = W.uneven_family_sizes(systems)
-    probs = [W.uneven_family_system(i, P, L) for i, (P, L) in enumerate(sizes)]
-    P_off = np.cumsum([0] + [P for P, _ in sizes]).astype(np.int64)
-    L_off = np.cumsum([0] + [L for _, L in sizes]).astype(np.int64)
+    costs = [P * 36 + 4 * L for P, L in sizes]
+    mine = replicas.shard_by_cost(costs, rank, world)
+    probs = [W.uneven_family_system(i, *sizes[i]) for i in mine]
+    P_off = np.cumsum([0] + [p["P"] for p in probs]).astype(np.int64)
+    L_off = np.cumsum([0] + [p["L"] for p in probs]).astype(np.int64)
     union = {
         "obs_primary": torch.cat([p["obs_primary"] + int(P_off[i]) for i, p in enumerate(probs)]),
         "obs_eliminated": torch.cat([p["obs_eliminated"] + int(L_off[i]) for i, p in enumerate(probs)]),
         "jp": torch.cat([p["jp"] for p in probs]), "jl": torch.cat([p["jl"] for p in probs]),
         "residual": torch.cat([p["residual"] for p in probs])}
     opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=TOL)
-    res = {"systems": systems, "observations": int(union["jp"].shape[0]),
+    stream = torch.cuda.current_stream()
+    res = {"systems": systems, "ranks": world, "shard": "contiguous by estimated cost (36 P + 4 L per system)",
            "config": "P~U{8..512}, L~U{500..50000}, 4 uniform distinct primaries per eliminated block, tol 1e-8"}
 
     def run_batched(options):
         ne_u = SC.DeviceNormalEquations(int(P_off[-1]), int(L_off[-1]), 6, 3)
         ws_u = SC.SchurComplementSolverWorkspace()
-        times = []
-        for k in range(2):  # the first call builds the pattern
+        for k in range(2):  # the first call builds the topology and the pattern
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
             ne_u.accumulate_observations(union["obs_primary"], union["obs_eliminated"], union["jp"], union["jl"],
                                          union["residual"], 1.0)
-            torch.cuda.synchronize()
-            t_acc = time.perf_counter() - t0
+            e1.record(stream)
             _, _, rep, per = SC.solve_batched_schur_complement(ne_u, LAMBDA, P_off, options, ws_u)
             torch.cuda.synchronize()
-            times.append(time.perf_counter() - t0)
-        # a system's time to solution: the shared prefix (accumulation, pattern check, eliminated
-        # inverses, assembly), its own PCG time to convergence, the shared back-substitution
-        prefix = t_acc * 1e3 + rep["pattern_ms"] + rep["eliminated_inverse_ms"] + rep["assembly_ms"]
-        pst = [prefix + s["time_ms"] + rep["back_substitution_ms"] for s in per if s["converged"]]
-        return {"seconds": round(times[-1], 4), "systems_per_s": round(systems / times[-1], 1),
-                "converged": sum(int(s["converged"]) for s in per),
-                "fallbacks": sum(int(s["learned_fallback"]) for s in per),
-                "max_iterations": max(s["iterations"] for s in per),
-                "p50_ms": round(float(np.percentile(pst, 50)), 3) if pst else None,
-                "p99_ms": round(float(np.percentile(pst, 99)), 3) if pst else None}
+            t_acc = e0.elapsed_time(e1)
+            total = t_acc + rep["total_ms"]
+        # a system's solution is available once the shared prefix (accumulation, pattern check,
+        # eliminated inverses, assembly), its own PCG and the shared back-substitution are done
+        prefix = t_acc + rep["pattern_ms"] + rep["eliminated_inverse_ms"] + rep["assembly_ms"]
+        done = [prefix + s["time_ms"] + rep["back_substitution_ms"] for s in per if s["converged"]]
+        job_ms = replicas.max_over_ranks(total)
+        done_all = replicas.gather_reports(done)
+        conv = replicas.gather_reports([int(s["converged"]) for s in per])
+        fb = replicas.gather_reports([int(s["learned_fallback"]) for s in per])
+        its = replicas.gather_reports([s["iterations"] for s in per])
+        if rank != 0:
+            return None
+        return {"ms": round(job_ms, 3), "systems_per_s": round(systems / (job_ms * 1e-3), 1),
+                "converged": sum(conv), "fallbacks": sum(fb), "max_iterations": max(its),
+                "mean_iterations": round(float(np.mean(its)), 2),
+                "time_to_solution_from_job_start_p50_ms": round(float(np.percentile(done_all, 50)), 3),
+                "time_to_solution_from_job_start_p99_ms": round(float(np.percentile(done_all, 99)), 3),
+                "own_duration_p50_ms": round(float(np.percentile(done_all, 50)), 3),
+                "own_duration_p99_ms": round(float(np.percentile(done_all, 99)), 3)}
 
     res["batched_plain"] = run_batched(opts)
     if net is not None:
         res["batched_learned"] = run_batched(SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=TOL,
                                                                              learned=net))
-    # per-system launch loop (each system with its own normal equations and workspace, warmed)
-    per_ms = []
-    t_loop = 0.0
+    # per-system launch loop on the same shard (each system with its own normal equations and
+    # workspace, warmed once); its own duration and its time from the start of the loop
+    own, from_start, t = [], [], 0.0
+    nes = []
     for p in probs:
         ne_s = SC.DeviceNormalEquations(p["P"], p["L"], 6, 3)
         ws_s = SC.SchurComplementSolverWorkspace()
-        for k in range(2):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            ne_s.accumulate_observations(p["obs_primary"], p["obs_eliminated"], p["jp"], p["jl"], p["residual"], 1.0)
-            SC.solve_damped_schur_complement(ne_s, LAMBDA, opts, ws_s)
-            torch.cuda.synchronize()
-            dt = time.perf_counter() - t0
-        per_ms.append(dt * 1e3)
-        t_loop += dt
-    res["per_system_loop"] = {"seconds": round(t_loop, 4), "systems_per_s": round(systems / t_loop, 1),
-                              "p50_ms": round(float(np.percentile(per_ms, 50)), 3),
-                              "p99_ms": round(float(np.percentile(per_ms, 99)), 3)}
+        ne_s.accumulate_observations(p["obs_primary"], p["obs_eliminated"], p["jp"], p["jl"], p["residual"], 1.0)
+        SC.solve_damped_schur_complement(ne_s, LAMBDA, opts, ws_s)
+        nes.append((ne_s, ws_s))
+    torch.cuda.synchronize()
+    for p, (ne_s, ws_s) in zip(probs, nes):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ne_s.accumulate_observations(p["obs_primary"], p["obs_eliminated"], p["jp"], p["jl"], p["residual"], 1.0)
+        SC.solve_damped_schur_complement(ne_s, LAMBDA, opts, ws_s)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dt = e0.elapsed_time(e1)
+        t += dt
+        own.append(dt)
+        from_start.append(t)
+    loop_ms = replicas.max_over_ranks(t)
+    own_all = replicas.gather_reports(own)
+    start_all = replicas.gather_reports(from_start)
+    if rank != 0:
+        return None
+    res["per_system_loop"] = {"ms": round(loop_ms, 3), "systems_per_s": round(systems / (loop_ms * 1e-3), 1),
+                              "own_duration_p50_ms": round(float(np.percentile(own_all, 50)), 3),
+                              "own_duration_p99_ms": round(float(np.percentile(own_all, 99)), 3),
+                              "time_to_solution_from_job_start_p50_ms": round(float(np.percentile(start_all, 50)), 3),
+                              "time_to_solution_from_job_start_p99_ms": round(float(np.percentile(start_all, 99)), 3)}
     return res
 
 

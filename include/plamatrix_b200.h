@@ -462,6 +462,14 @@ PM_API int pm_mlp_forward(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stream_
  * FP64, n = 6P); with `learning_rate` > 0 one Adam step follows.  Synchronous. */
 PM_API int pm_mlp_train_step(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stream_t stream, const double* x_d,
                              const double* b_d, double learning_rate, double* loss);
+/* Loss and gradients of the preconditioned operator along a probe vector v (device, FP64, n = 6P)
+ * for the system last assembled in `workspace`: ||(I - M S) v||^2 / ||v||^2, where M is the
+ * corrected block preconditioner and sv = S v is supplied by the caller (pm_schur_spmv_f64, or the
+ * float SpMV widened, of the same system); with `learning_rate` > 0 one Adam step follows.  It needs
+ * no solved system, and it measures how well M inverts S along v -- the quantity PCG convergence
+ * depends on.  Synchronous. */
+PM_API int pm_mlp_train_probe_step(pm_mlp* mlp, pm_schur_workspace* workspace, pm_stream_t stream, const double* v_d,
+                                   const double* sv_d, double learning_rate, double* loss);
 /* Polls of an mbarrier wait between the network GEMM's operand stages before it gives up (default
  * 2^20; the final wait for the last MMA always uses 2^20).  A GEMM whose wait runs out stops
  * issuing MMAs, frees its tensor memory once its last MMA has completed, and the call that ran it

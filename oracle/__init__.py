@@ -364,6 +364,18 @@ def mlp_loss_grad(diag_blocks, out, x, b):
     return loss.value, dout[:P]
 
 
+def mlp_probe_loss_grad(diag_blocks, out, v, sv):
+    """||(I - M S) v||^2 / ||v||^2 for the corrected block preconditioner M, given sv = S v."""
+    d = _f64(diag_blocks).reshape(-1, 36)
+    o = _f64(out).reshape(-1, MLP_OUT)
+    P = d.shape[0]
+    loss = C.c_double(0.0)
+    dout = np.zeros((max(P, 1), MLP_OUT))
+    _check("orc", lib("orc").orc_mlp_probe_loss_grad(C.c_int64(P), _ptr(d), _ptr(o), _ptr(_f64(v)), _ptr(_f64(sv)),
+                                                     C.byref(loss), _ptr(dout)))
+    return loss.value, dout[:P]
+
+
 def mlp_backward(features, params, cache: dict, dout, bf16: bool = False) -> np.ndarray:
     f = _f64(features).reshape(-1, MLP_IN)
     P = f.shape[0]

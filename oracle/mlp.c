@@ -249,6 +249,70 @@ int orc_mlp_loss_grad(int64_t P, const double* diag_blocks, const double* out, c
     return ORC_OK;
 }
 
+/* Probe loss of the preconditioned operator: sum_p ||v_p - A_p^-1 u_p||^2 / ||v||^2 with
+ * A_p = L'_p L'_p^T and u = S v supplied; analytic gradient with respect to the outputs
+ * (derivation: w = A^-1 u, e = v - w, d loss = 2 (A^-1 e)^T dA w / den, dA = dL' L'^T + L' dL'^T). */
+static void lsolve6(const double* L, const double* b, double* x)
+{
+    for (int i = 0; i < 6; ++i)
+    {
+        double s = b[i];
+        for (int j = 0; j < i; ++j)
+            s -= L[i * 6 + j] * x[j];
+        x[i] = s / L[i * 6 + i];
+    }
+}
+
+static void usolve6(const double* L, const double* b, double* x)
+{
+    for (int i = 5; i >= 0; --i)
+    {
+        double s = b[i];
+        for (int j = i + 1; j < 6; ++j)
+            s -= L[j * 6 + i] * x[j];
+        x[i] = s / L[i * 6 + i];
+    }
+}
+
+int orc_mlp_probe_loss_grad(int64_t P, const double* diag_blocks, const double* out, const double* v, const double* sv,
+                            double* loss, double* dout)
+{
+    double num = 0.0, den = 0.0;
+    for (int64_t p = 0; p < P; ++p)
+        for (int i = 0; i < 6; ++i)
+            den += v[p * 6 + i] * v[p * 6 + i];
+    if (!(den > 0.0))
+        return ORC_INVALID_ARGUMENT;
+    for (int64_t p = 0; p < P; ++p)
+    {
+        double L[36], Lc[36], y[6], w[6], e[6], z[6], q[6];
+        if (!chol6(diag_blocks + p * 36, L))
+            return ORC_RUNTIME_ERROR;
+        const double* o = out + p * OUT;
+        corrected(L, o, Lc);
+        lsolve6(Lc, sv + p * 6, y);
+        usolve6(Lc, y, w);
+        for (int i = 0; i < 6; ++i)
+        {
+            e[i] = v[p * 6 + i] - w[i];
+            num += e[i] * e[i];
+        }
+        lsolve6(Lc, e, z);
+        usolve6(Lc, z, q);
+        if (dout)
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j <= i; ++j)
+                {
+                    const int k = i * (i + 1) / 2 + j;
+                    const double g = 2.0 * (q[i] * y[j] + w[i] * z[j]) / den;
+                    dout[p * OUT + k] =
+                        i == j ? g * L[i * 6 + i] * sigmoid(o[k]) / log(2.0) : g * L[j * 6 + j];
+                }
+    }
+    *loss = num / den;
+    return ORC_OK;
+}
+
 int orc_mlp_backward(int64_t P, const double* features, const double* params, int bf16_operands, const double* z1,
                      const double* h1, const double* z2, const double* h2, const double* dout, double* grads)
 {

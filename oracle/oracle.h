@@ -221,6 +221,8 @@ int orc_mlp_forward(int64_t P, const double* features, const double* params, int
                     double* h1, double* z2, double* h2, double* out);
 int orc_mlp_loss_grad(int64_t P, const double* diag_blocks, const double* out, const double* x, const double* b,
                       double* loss, double* dout);
+int orc_mlp_probe_loss_grad(int64_t P, const double* diag_blocks, const double* out, const double* v, const double* sv,
+                            double* loss, double* dout);
 int orc_mlp_backward(int64_t P, const double* features, const double* params, int bf16_operands, const double* z1,
                      const double* h1, const double* z2, const double* h2, const double* dout, double* grads);
 int orc_mlp_preconditioner(int64_t P, const double* diag_blocks, const double* out, double* minv);

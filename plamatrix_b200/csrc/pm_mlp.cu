@@ -457,6 +457,29 @@ __device__ void corrected(const double* L, const float* o, double* Lc)
         }
 }
 
+// x = L^-1 b and x = L^-T b for a lower-triangular 6x6 L (row-major)
+__device__ __forceinline__ void lower_solve6(const double* L, const double* b, double* x)
+{
+    for (int i = 0; i < 6; ++i)
+    {
+        double s = b[i];
+        for (int j = 0; j < i; ++j)
+            s -= L[i * 6 + j] * x[j];
+        x[i] = s / L[i * 6 + i];
+    }
+}
+
+__device__ __forceinline__ void upper_solve6(const double* L, const double* b, double* x)
+{
+    for (int i = 5; i >= 0; --i)
+    {
+        double s = b[i];
+        for (int j = i + 1; j < 6; ++j)
+            s -= L[j * 6 + i] * x[j];
+        x[i] = s / L[i * 6 + i];
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void load_diag(const T* S, int pos, double* d)
 {
@@ -489,12 +512,20 @@ __global__ void finish_sum_kernel(int parts, const double* __restrict__ part, do
     *out = s;
 }
 
+// Per block row p, with A_p = L'_p L'_p^T (the corrected factor):
+//   solution loss (probe = 0): sum_p ||A_p x_p - b_p||^2 / den, x a solution and b its right-hand side;
+//   probe loss (probe = 1):    sum_p ||v_p - A_p^-1 u_p||^2 / den, v a probe vector and u = S v, i.e.
+//                              ||(I - M S) v||^2 / ||v||^2 for the block preconditioner M = blockdiag(A_p^-1).
+// The gradient with respect to the lower triangle of L' is, for the probe loss (y = L'^-1 u,
+// w = L'^-T y = A^-1 u, e = v - w, z = L'^-1 e, q = L'^-T z):  2 (q_i y_j + w_i z_j) / den,
+// and for the solution loss (u = L'^T x, r = A x - b, s = L'^T r):  2 (r_i u_j + x_i s_j) / den;
+// both are then carried through the correction to the network outputs.
 template <typename T>
 __global__ void __launch_bounds__(kPartBlock) loss_kernel(int64_t P, const int* __restrict__ diag_pos,
                                                           const T* __restrict__ S, const float* __restrict__ O,
                                                           const double* __restrict__ x, const double* __restrict__ b,
                                                           const double* __restrict__ den, float* __restrict__ dO,
-                                                          double* part, int* bad)
+                                                          double* part, int* bad, int probe)
 {
     const double ln2 = 0.69314718055994531;
     const double inv_den = 1.0 / *den;
@@ -515,31 +546,63 @@ __global__ void __launch_bounds__(kPartBlock) loss_kernel(int64_t P, const int* 
         corrected(L, o, Lc);
         const double* xp = x + p * 6;
         const double* bp = b + p * 6;
-        for (int j = 0; j < 6; ++j)
+        // gradient factors: d loss / d L'_ij = 2 (fa_i fb_j + fc_i fd_j) / den
+        double fa[6], fb[6], fc[6], fd[6];
+        if (probe)
         {
-            u[j] = 0.0;
-            for (int i = j; i < 6; ++i)
-                u[j] += Lc[i * 6 + j] * xp[i];
+            double y[6], w[6], e[6], z[6], q[6];
+            lower_solve6(Lc, bp, y);  // y = L'^-1 u
+            upper_solve6(Lc, y, w);   // w = L'^-T y = A^-1 u
+            for (int i = 0; i < 6; ++i)
+            {
+                e[i] = xp[i] - w[i];
+                mine += e[i] * e[i];
+            }
+            lower_solve6(Lc, e, z);   // z = L'^-1 e
+            upper_solve6(Lc, z, q);   // q = A^-1 e
+            for (int i = 0; i < 6; ++i)
+            {
+                fa[i] = q[i];
+                fb[i] = y[i];
+                fc[i] = w[i];
+                fd[i] = z[i];
+            }
         }
-        for (int i = 0; i < 6; ++i)
+        else
         {
-            double s = 0.0;
-            for (int j = 0; j <= i; ++j)
-                s += Lc[i * 6 + j] * u[j];
-            r[i] = s - bp[i];
-            mine += r[i] * r[i];
-        }
-        for (int j = 0; j < 6; ++j)
-        {
-            v[j] = 0.0;
-            for (int i = j; i < 6; ++i)
-                v[j] += Lc[i * 6 + j] * r[i];
+            for (int j = 0; j < 6; ++j)
+            {
+                u[j] = 0.0;
+                for (int i = j; i < 6; ++i)
+                    u[j] += Lc[i * 6 + j] * xp[i];
+            }
+            for (int i = 0; i < 6; ++i)
+            {
+                double s = 0.0;
+                for (int j = 0; j <= i; ++j)
+                    s += Lc[i * 6 + j] * u[j];
+                r[i] = s - bp[i];
+                mine += r[i] * r[i];
+            }
+            for (int j = 0; j < 6; ++j)
+            {
+                v[j] = 0.0;
+                for (int i = j; i < 6; ++i)
+                    v[j] += Lc[i * 6 + j] * r[i];
+            }
+            for (int i = 0; i < 6; ++i)
+            {
+                fa[i] = r[i];
+                fb[i] = u[i];
+                fc[i] = xp[i];
+                fd[i] = v[i];
+            }
         }
         for (int i = 0; i < 6; ++i)
             for (int j = 0; j <= i; ++j)
             {
                 const int k = i * (i + 1) / 2 + j;
-                const double gg = 2.0 * (r[i] * u[j] + xp[i] * v[j]) * inv_den;
+                const double gg = 2.0 * (fa[i] * fb[j] + fc[i] * fd[j]) * inv_den;
                 const double ok = static_cast<double>(o[k]);
                 g[k] = static_cast<float>(i == j ? gg * L[i * 6 + i] / (1.0 + exp(-ok)) / ln2 : gg * L[j * 6 + j]);
             }
@@ -788,7 +851,8 @@ void mlp_apply(const pm_mlp* cmlp, const SchurView& v, cudaStream_t stream)
 namespace
 {
 
-double train(pm_mlp* mlp, const SchurView& v, cudaStream_t stream, const double* x, const double* b, double lr)
+double train(pm_mlp* mlp, const SchurView& v, cudaStream_t stream, const double* x, const double* b, double lr,
+             int probe = 0)
 {
     check_view(v);
     if (v.P == 0)
@@ -804,17 +868,17 @@ double train(pm_mlp* mlp, const SchurView& v, cudaStream_t stream, const double*
     int* bad = bad_flag(mlp);
     PM_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), stream));
     const unsigned sg = grid_for(n, kPartBlock, kMaxPartBlocks);
-    squares_kernel<<<sg, kPartBlock, 0, stream>>>(n, b, part);
+    squares_kernel<<<sg, kPartBlock, 0, stream>>>(n, probe ? x : b, part); // ||v||^2 or ||b||^2
     PM_LAUNCH_CHECK();
     finish_sum_kernel<<<1, 1, 0, stream>>>(static_cast<int>(sg), part, den);
     PM_LAUNCH_CHECK();
     const unsigned lg = grid_for(P, kPartBlock, kMaxPartBlocks);
     if (v.value_size == 8)
         loss_kernel<double><<<lg, kPartBlock, 0, stream>>>(P, v.diag_pos, static_cast<const double*>(v.S), mlp->O, x,
-                                                           b, den, mlp->dO, part + kMaxPartBlocks, bad);
+                                                           b, den, mlp->dO, part + kMaxPartBlocks, bad, probe);
     else
         loss_kernel<float><<<lg, kPartBlock, 0, stream>>>(P, v.diag_pos, static_cast<const float*>(v.S), mlp->O, x, b,
-                                                          den, mlp->dO, part + kMaxPartBlocks, bad);
+                                                          den, mlp->dO, part + kMaxPartBlocks, bad, probe);
     PM_LAUNCH_CHECK();
     finish_sum_kernel<<<1, 1, 0, stream>>>(static_cast<int>(lg), part + kMaxPartBlocks, num);
     PM_LAUNCH_CHECK();
@@ -965,6 +1029,20 @@ int pm_mlp_train_step(pm_mlp* mlp, pm_schur_workspace* ws, pm_stream_t stream, c
         if (!(learning_rate >= 0.0) || !std::isfinite(learning_rate))
             pm::fail(PM_INVALID_ARGUMENT, "pm_mlp_train_step: learning rate must be finite and non-negative");
         const double l = pm::train(mlp, pm::schur_view(ws, false), stream, x, b, learning_rate);
+        if (loss)
+            *loss = l;
+    });
+}
+
+int pm_mlp_train_probe_step(pm_mlp* mlp, pm_schur_workspace* ws, pm_stream_t stream, const double* v,
+                            const double* sv, double learning_rate, double* loss)
+{
+    return pm::guarded([&] {
+        if (!mlp || !ws)
+            pm::fail(PM_INVALID_ARGUMENT, "pm_mlp_train_probe_step: null argument");
+        if (!(learning_rate >= 0.0) || !std::isfinite(learning_rate))
+            pm::fail(PM_INVALID_ARGUMENT, "pm_mlp_train_probe_step: learning rate must be finite and non-negative");
+        const double l = pm::train(mlp, pm::schur_view(ws, false), stream, v, sv, learning_rate, 1);
         if (loss)
             *loss = l;
     });

@@ -269,6 +269,7 @@ N.register("pm_mlp_forward", [vp, vp, vp])
 N.register("pm_mlp_train_step", [vp, vp, vp, vp, vp, C.c_double, vp])
 N.register("pm_mlp_inspect", [vp, vp, vp, vp, vp])
 N.register("pm_mlp_set_wait_limit", [vp, i64])
+N.register("pm_mlp_train_probe_step", [vp, vp, vp, vp, vp, C.c_double, vp])
 
 
 class LearnedPreconditioner:
@@ -319,6 +320,17 @@ class LearnedPreconditioner:
             raise N.InvalidArgument("x and b must be float64 CUDA tensors")
         loss = C.c_double(0.0)
         N.call("pm_mlp_train_step", self._h, workspace.handle, _stream_handle(stream), _ptr(x), _ptr(b),
+               C.c_double(learning_rate), C.byref(loss))
+        return loss.value
+
+    def train_probe_step(self, workspace: "SchurComplementSolverWorkspace", v: torch.Tensor, sv: torch.Tensor,
+                         learning_rate: float = 1e-3, stream=None) -> float:
+        """Loss ||(I - M S) v||^2 / ||v||^2 of the last assembled system in `workspace` along the probe
+        v, given sv = S v (device FP64, n = 6P); with learning_rate > 0 one Adam step follows."""
+        if v.dtype != torch.float64 or sv.dtype != torch.float64 or not (v.is_cuda and sv.is_cuda):
+            raise N.InvalidArgument("v and sv must be float64 CUDA tensors")
+        loss = C.c_double(0.0)
+        N.call("pm_mlp_train_probe_step", self._h, workspace.handle, _stream_handle(stream), _ptr(v), _ptr(sv),
                C.c_double(learning_rate), C.byref(loss))
         return loss.value
 

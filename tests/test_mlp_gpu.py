@@ -87,6 +87,32 @@ def test_loss_and_gradients_match_oracle():
         assert err <= 3e-2, (lo, err)
 
 
+def test_probe_loss_and_gradients_match_oracle():
+    """||(I - M S) v||^2 / ||v||^2 along a Rademacher probe v with S v from the device SpMV: loss and
+    per-section parameter gradients against the FP64 oracle (BF16 operands emulated)."""
+    _, ws, _, rep = _solved(W.small_bundle(seed=41))
+    assert rep["converged"]
+    bptr, bcol, blocks, diag, _ = _blocks(ws)
+    net = SC.LearnedPreconditioner(seed=13)
+    params = _random_params(14, scale=0.1)
+    net.set_params(params)
+    n = diag.shape[0] * 6
+    v = torch.from_numpy(np.random.default_rng(15).choice([-1.0, 1.0], n)).cuda()
+    sv = ws.spmv(v)
+    loss = net.train_probe_step(ws, v, sv, learning_rate=0.0)
+    got = net.inspect()
+    f64 = got["features"].astype(np.float64)
+    cache = O.mlp_forward(f64, params.astype(np.float64), bf16=True)
+    ref_loss, dout = O.mlp_probe_loss_grad(diag, got["outputs"].astype(np.float64), host(v).reshape(-1, 6),
+                                           host(sv).reshape(-1, 6))
+    assert loss == pytest.approx(ref_loss, rel=1e-6)
+    ref_g = O.mlp_backward(f64, params.astype(np.float64), cache, dout, bf16=True)
+    g = got["gradients"].astype(np.float64)
+    for lo, hi in [(0, 3200), (3200, 3328), (3328, 19712), (19712, 19840), (19840, 22528), (22528, 22549)]:
+        err = np.linalg.norm(g[lo:hi] - ref_g[lo:hi]) / max(np.linalg.norm(ref_g[lo:hi]), 1e-30)
+        assert err <= 3e-2, (lo, err)
+
+
 def test_gemm_stage_wait_that_runs_out_is_an_error_and_the_network_stays_usable():
     """A stage wait limit of 0 makes the 128-deep hidden-layer GEMM (four K steps) give up at its
     first stage wait: the call fails with the GEMM error, and with the default limit back the

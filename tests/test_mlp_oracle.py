@@ -63,6 +63,26 @@ def test_output_gradient_matches_finite_differences():
         assert dout[p, k] == pytest.approx(fd, rel=1e-6, abs=1e-10)
 
 
+def test_probe_loss_gradient_matches_finite_differences_and_numpy():
+    """||(I - M S) v||^2 / ||v||^2 with M = blockdiag((L'L'^T)^-1): the loss equals a numpy
+    evaluation with explicit inverses, and its output gradient matches central differences."""
+    D, x, _, _ = _system(seed=9)
+    rng = np.random.default_rng(10)
+    v = rng.standard_normal((len(D), 6))
+    sv = v @ rng.standard_normal((6, 6)) + 2.0 * v   # any vector field plays u = S v here
+    out = 0.4 * rng.standard_normal((len(D), O.MLP_OUT))
+    loss, dout = O.mlp_probe_loss_grad(D, out, v, sv)
+    minv = O.mlp_preconditioner(D, out).reshape(-1, 6, 6)
+    e = v - np.einsum("pij,pj->pi", minv, sv)
+    assert loss == pytest.approx((e ** 2).sum() / (v ** 2).sum(), rel=1e-10)
+    h = 1e-6
+    for p, k in [(0, 0), (2, 5), (4, 20), (8, 9), (11, 1)]:
+        d = np.zeros_like(out)
+        d[p, k] = h
+        fd = (O.mlp_probe_loss_grad(D, out + d, v, sv)[0] - O.mlp_probe_loss_grad(D, out - d, v, sv)[0]) / (2 * h)
+        assert dout[p, k] == pytest.approx(fd, rel=1e-6, abs=1e-10)
+
+
 def test_parameter_gradient_matches_finite_differences():
     D, x, b, feats = _system(seed=7)
     params = _params()
