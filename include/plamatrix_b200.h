@@ -60,6 +60,8 @@ PM_API int pm_device_malloc(size_t bytes, void** out);
 PM_API int pm_device_free(void* ptr);
 PM_API int pm_copy_to_device(void* dst_d, const void* src_h, size_t bytes, pm_stream_t stream);
 PM_API int pm_copy_to_host(void* dst_h, const void* src_d, size_t bytes, pm_stream_t stream);
+/* Wait for the work queued on `stream` (what a caller does before pm_coo_status). */
+PM_API int pm_stream_synchronize(pm_stream_t stream);
 /* Name of the current CUDA device (SchurComplementSolverReport::deviceName). */
 PM_API int pm_device_name(char* out, int capacity);
 

@@ -405,7 +405,8 @@ public:
     SparseOpsWorkspace(const SparseOpsWorkspace&) = delete;
     SparseOpsWorkspace& operator=(const SparseOpsWorkspace&) = delete;
     SparseOpsWorkspace(SparseOpsWorkspace&& o) noexcept : _ws(std::exchange(o._ws, nullptr)) {}
-    /// SparseOpsWorkspace::checkStatus (src/sparse/coo_to_csr.cu:531-534): throws the deferred error
+    /// SparseOpsWorkspace::checkStatus (src/sparse/coo_to_csr.cu:531-534): throws the deferred error;
+    /// the caller synchronises the stream first, as with the reference
     void checkStatus(const char* operation) { check(pm_coo_status(_ws, operation, nullptr)); }
     std::int64_t combinedNnz(const char* operation)
     {
@@ -460,6 +461,7 @@ plamatrix::CSRMatrix<S, plamatrix::Device::CPU> cooToCsr(Index rows, Index cols,
     else
         check(pm_coo_to_csr_count_f32(ws.handle(), nullptr, rows, cols, count, r.as<Index>(), c.as<Index>(),
                                       v.as<S>()));
+    check(pm_stream_synchronize(nullptr));
     const Index nnz = ws.combinedNnz("cooToCsr");
     DeviceBuffer ro(static_cast<std::size_t>(rows + 1) * sizeof(Index)),
         co(static_cast<std::size_t>(nnz + 1) * sizeof(Index)), vo(static_cast<std::size_t>(nnz + 1) * sizeof(S));
@@ -467,6 +469,7 @@ plamatrix::CSRMatrix<S, plamatrix::Device::CPU> cooToCsr(Index rows, Index cols,
         check(pm_coo_to_csr_fill_f64(ws.handle(), nullptr, nnz, ro.as<Index>(), co.as<Index>(), vo.as<S>()));
     else
         check(pm_coo_to_csr_fill_f32(ws.handle(), nullptr, nnz, ro.as<Index>(), co.as<Index>(), vo.as<S>()));
+    check(pm_stream_synchronize(nullptr));
     ws.checkStatus("cooToCsr");
     plamatrix::CSRMatrix<S, plamatrix::Device::CPU> out(rows, cols, nnz);
     ro.download(out.rowOffsets(), static_cast<std::size_t>(rows + 1));

@@ -78,6 +78,7 @@ _SIGNATURES = {
     "pm_copy_to_device": [vp, vp, C.c_size_t, vp],
     "pm_copy_to_host": [vp, vp, C.c_size_t, vp],
     "pm_device_name": [C.c_char_p, C.c_int],
+    "pm_stream_synchronize": [vp],
     "pm_sparse_workspace_create": [vp],
     "pm_sparse_workspace_destroy": [vp],
     "pm_sparse_workspace_close": [vp],

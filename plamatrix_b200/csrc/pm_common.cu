@@ -200,6 +200,11 @@ extern "C" int pm_copy_to_host(void* dst_h, const void* src_d, size_t bytes, pm_
     });
 }
 
+extern "C" int pm_stream_synchronize(pm_stream_t stream)
+{
+    return pm::guarded([&] { PM_CUDA(cudaStreamSynchronize(stream)); });
+}
+
 extern "C" int pm_device_name(char* out, int capacity)
 {
     return pm::guarded([&] {

@@ -571,6 +571,40 @@ def test_windowed_bundle_matches_oracle(checkers):
     assert rep["true_relative_residual"] <= 1e-8 * 1.01
 
 
+@pytest.mark.parametrize("precision", ["native", "mixed_fp32_assembly"])
+def test_fused_and_two_pass_assemblies_agree(precision):
+    """The one-pass 6x3 assembly (crosses of every eliminated block sorted by primary, as the
+    observation path stores them) against the two-pass one (the same state uploaded with every
+    eliminated block's crosses reversed, which routes it to the kernels with stored factors and
+    per-block pair lists): same pattern, values within rounding, same steps."""
+    prob = W.large_bundle(seed=13, P=300, L=12000)
+    ne_sorted = _device_from_observations(prob)
+    state = ne_sorted.download()
+    offs = state["adjacency_offsets"]
+    order = np.concatenate([np.arange(offs[l], offs[l + 1])[::-1] for l in range(len(offs) - 1)])
+    shuffled = dict(state)
+    shuffled["cross_primary"] = state["cross_primary"][order]
+    shuffled["cross_values"] = state["cross_values"][order]
+    ne_rev = SC.DeviceNormalEquations(prob["P"], prob["L"], 6, 3)
+    ne_rev.upload(shuffled)
+    opts = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=1e-10, precision=precision)
+    got = []
+    for ne in (ne_sorted, ne_rev):
+        ws = SC.SchurComplementSolverWorkspace()
+        dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+        assert rep["converged"], rep["message"]
+        got.append((host(dp), host(dl), ws.export()))
+    (dp_a, dl_a, sa), (dp_b, dl_b, sb) = got
+    assert np.array_equal(host(sa["row_offsets"]), host(sb["row_offsets"]))
+    assert np.array_equal(host(sa["col_indices"]), host(sb["col_indices"]))
+    va, vb = host(sa["values"]), host(sb["values"])
+    tol = 1e-12 if precision == "native" else 1e-6
+    assert np.abs(va - vb).max() <= tol * np.abs(vb).max()
+    assert np.abs(host(sa["rhs"]) - host(sb["rhs"])).max() <= 1e-12 * np.abs(host(sb["rhs"])).max()
+    assert np.linalg.norm(dp_a - dp_b) <= 1e-8 * np.linalg.norm(dp_b)
+    assert np.linalg.norm(dl_a - dl_b) <= 1e-8 * np.linalg.norm(dl_b)
+
+
 def test_repeated_solves_are_bitwise_identical(checkers):
     prob = W.large_bundle(seed=9, P=300, L=10000)
     ne = _device_from_observations(prob)
