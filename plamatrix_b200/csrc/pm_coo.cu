@@ -104,135 +104,6 @@ __global__ void __launch_bounds__(256) scatter_kernel(const int64_t* __restrict_
     sorted_values[pos] = values ? values[i] : T(0);
 }
 
-// 1'-2') the same bucketed layout for large inputs without scattered 8-byte stores.  Triplets
-// arrive in random row order, so writing each straight into its row bucket costs two
-// partial-sector writes per triplet.  Instead rows are grouped into kBins coarse bins of
-// 2^shift consecutive rows:
-//   bin_count_kernel   -- validation (as count_kernel) and a per-tile histogram of the bins;
-//   (exclusive scan of the bin-major histogram -> each tile's start inside each bin)
-//   bin_scatter_kernel -- each tile writes its triplets into its runs of the bins (kBinTile
-//                          triplets per tile, ~kBinTile / kBins per run: coalesced runs);
-//   bin_bucket_kernel  -- CTA per bin: per-row counts of the bin in shared memory, row bucket
-//                          starts, and the entries placed into their row buckets inside the bin's
-//                          own window of the bucket arrays (L2-resident writes).
-// Positions inside a row bucket depend on scheduling, as with count_kernel's atomics; the
-// per-row sort by the unique key (col, source offset) that follows fixes the order.
-constexpr int kBins = 256;
-constexpr int kBinTile = 16384;
-constexpr int kBinThreads = 512;
-constexpr int kBinRowsMax = 8192; // rows of one bin (shared-memory counters)
-
-template <typename T>
-__global__ void __launch_bounds__(kBinThreads) bin_count_kernel(const int64_t* __restrict__ rows,
-                                                               const int64_t* __restrict__ cols,
-                                                               const T* __restrict__ values, int64_t count,
-                                                               int64_t row_count, int64_t col_count, int shift,
-                                                               int tiles, int* __restrict__ hist, CooStatus* status)
-{
-    __shared__ int h[kBins];
-    for (int b = threadIdx.x; b < kBins; b += blockDim.x)
-        h[b] = 0;
-    __syncthreads();
-    const int64_t t0 = int64_t(blockIdx.x) * kBinTile;
-    const int64_t t1 = min(count, t0 + kBinTile);
-    for (int64_t i = t0 + threadIdx.x; i < t1; i += blockDim.x)
-    {
-        const int64_t row = rows[i];
-        const int64_t col = cols[i];
-        if (values && !finite_value(values[i]))
-            atomicMin(&status->invalid_value, static_cast<unsigned long long>(i));
-        if (row < 0 || row >= row_count || col < 0 || col >= col_count)
-        {
-            atomicMin(&status->invalid_source, static_cast<unsigned long long>(i));
-            continue;
-        }
-        atomicAdd(&h[row >> shift], 1);
-    }
-    __syncthreads();
-    for (int b = threadIdx.x; b < kBins; b += blockDim.x)
-        hist[int64_t(b) * tiles + blockIdx.x] = h[b];
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kBinThreads) bin_scatter_kernel(const int64_t* __restrict__ rows,
-                                                                 const int64_t* __restrict__ cols,
-                                                                 const T* __restrict__ values, int64_t count,
-                                                                 int64_t row_count, int64_t col_count, int shift,
-                                                                 int tiles, const int* __restrict__ start,
-                                                                 uint64_t* __restrict__ bin_keys,
-                                                                 T* __restrict__ bin_values, int* __restrict__ bin_rows)
-{
-    __shared__ int cursor[kBins];
-    for (int b = threadIdx.x; b < kBins; b += blockDim.x)
-        cursor[b] = start[int64_t(b) * tiles + blockIdx.x];
-    __syncthreads();
-    const int64_t t0 = int64_t(blockIdx.x) * kBinTile;
-    const int64_t t1 = min(count, t0 + kBinTile);
-    for (int64_t i = t0 + threadIdx.x; i < t1; i += blockDim.x)
-    {
-        const int64_t row = rows[i];
-        const int64_t col = cols[i];
-        if (row < 0 || row >= row_count || col < 0 || col >= col_count)
-            continue;
-        const int pos = atomicAdd(&cursor[row >> shift], 1);
-        bin_keys[pos] = (static_cast<uint64_t>(col) << 32) | static_cast<uint64_t>(i);
-        bin_values[pos] = values ? values[i] : T(0);
-        bin_rows[pos] = static_cast<int>(row);
-    }
-}
-
-// CTA per bin: rows [b << shift, (b + 1) << shift) and entries [start[b * tiles], start[(b + 1) * tiles])
-template <typename T>
-__global__ void __launch_bounds__(kBinThreads) bin_bucket_kernel(int64_t row_count, int shift, int tiles,
-                                                                const int* __restrict__ start,
-                                                                const uint64_t* __restrict__ bin_keys,
-                                                                const T* __restrict__ bin_values,
-                                                                const int* __restrict__ bin_rows,
-                                                                int* __restrict__ bucket_start,
-                                                                uint64_t* __restrict__ keys, T* __restrict__ values)
-{
-    __shared__ int cnt[kBinRowsMax];
-    __shared__ int warp_tot[kBinThreads / 32 + 1];
-    const int b = blockIdx.x;
-    const int64_t r0 = int64_t(b) << shift;
-    if (r0 >= row_count)
-        return;
-    const int nr = static_cast<int>(min(int64_t(1) << shift, row_count - r0));
-    const int e0 = start[int64_t(b) * tiles];
-    const int e1 = start[int64_t(b + 1) * tiles]; // start holds kBins * tiles + 1 entries (the total last)
-    for (int r = threadIdx.x; r < nr; r += blockDim.x)
-        cnt[r] = 0;
-    __syncthreads();
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x)
-        atomicAdd(&cnt[bin_rows[e] - r0], 1);
-    __syncthreads();
-    // exclusive scan of cnt[0..nr) in place: each thread scans a contiguous run of rows
-    const int per = (nr + blockDim.x - 1) / blockDim.x;
-    const int a0 = min(nr, static_cast<int>(threadIdx.x) * per), a1 = min(nr, a0 + per);
-    int run = 0;
-    for (int r = a0; r < a1; ++r)
-        run += cnt[r];
-    int total = 0;
-    const int before = block_exclusive_scan<int, kBinThreads>(run, warp_tot, total);
-    int at = e0 + before;
-    for (int r = a0; r < a1; ++r)
-    {
-        const int c = cnt[r];
-        cnt[r] = at;
-        bucket_start[r0 + r] = at;
-        at += c;
-    }
-    if (b == gridDim.x - 1 && threadIdx.x == 0)
-        bucket_start[row_count] = start[int64_t(kBins) * tiles];
-    __syncthreads();
-    for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x)
-    {
-        const int pos = atomicAdd(&cnt[bin_rows[e] - r0], 1);
-        keys[pos] = bin_keys[e];
-        values[pos] = bin_values[e];
-    }
-}
-
 // bitonic network over N register-resident (key, value) pairs; indices are compile-time
 template <int N, typename T>
 __device__ __forceinline__ void register_sort(uint64_t (&k)[N], T (&v)[N])
@@ -623,14 +494,6 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     const size_t scan_bytes = scan_scratch_bytes(rows + 1, sizeof(int64_t)) + scan_scratch_bytes(rows + 1, sizeof(int));
     const size_t n = static_cast<size_t>(count > 0 ? count : 1);
     const size_t R = static_cast<size_t>(rows + 1);
-    // large inputs group the rows into coarse bins first (bin_*_kernel); small ones, and row
-    // counts beyond what the bins' shared-memory counters hold, bucket each triplet directly
-    int shift = 0;
-    while ((int64_t(kBins) << shift) < rows)
-        ++shift;
-    const bool binned = count >= int64_t(16) * kBinTile && (int64_t(1) << shift) <= kBinRowsMax;
-    const int tiles = binned ? static_cast<int>((count + kBinTile - 1) / kBinTile) : 0;
-    const size_t hist_n = binned ? size_t(kBins) * tiles + 1 : 1;
     Carver plan;
     plan.take<CooStatus>(1);
     plan.take<int>(R);
@@ -644,9 +507,6 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     plan.take<int>(R);
     plan.take<int64_t>(R + 1);
     plan.take<char>(scan_bytes);
-    plan.take<int>(hist_n);
-    plan.take<int>(hist_n);
-    plan.take<char>(binned ? scan_scratch_bytes(hist_n, sizeof(int)) : 1);
     ws->buffer.ensure(plan.offset + 256, stream, "SparseOpsWorkspace");
     Carver carve;
     carve.base = static_cast<char*>(ws->buffer.ptr);
@@ -662,9 +522,6 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     ws->long_rows = carve.take<int>(R);
     ws->row_offsets = carve.take<int64_t>(R + 1);
     ws->scan_scratch = carve.take<char>(scan_bytes);
-    int* hist = carve.take<int>(hist_n);
-    int* hist_start = carve.take<int>(hist_n);
-    void* hist_scan = carve.take<char>(binned ? scan_scratch_bytes(hist_n, sizeof(int)) : 1);
     ws->rows = rows;
     ws->cols = cols;
     ws->count = count;
@@ -685,39 +542,14 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
         return;
     }
     T* sorted_values = static_cast<T*>(ws->values);
-    if (binned)
-    {
-        // the spare key / value arrays and the slot array hold the binned triplets
-        bin_count_kernel<T><<<tiles, kBinThreads, 0, stream>>>(row_indices, col_indices, values, count, rows, cols,
-                                                               shift, tiles, hist, ws->status);
-        PM_LAUNCH_CHECK();
-        exclusive_scan<int, int>(hist, hist_start, static_cast<int64_t>(kBins) * tiles, hist_scan, stream);
-        bin_scatter_kernel<T><<<tiles, kBinThreads, 0, stream>>>(row_indices, col_indices, values, count, rows, cols,
-                                                                 shift, tiles, hist_start, ws->spare_keys,
-                                                                 static_cast<T*>(ws->spare_values), ws->slots);
-        PM_LAUNCH_CHECK();
-        const unsigned bins_used = static_cast<unsigned>((rows + (int64_t(1) << shift) - 1) >> shift);
-        if (rows == 0)
-            PM_CUDA(cudaMemsetAsync(ws->bucket_start, 0, sizeof(int), stream));
-        else
-        {
-            bin_bucket_kernel<T><<<bins_used, kBinThreads, 0, stream>>>(
-                rows, shift, tiles, hist_start, ws->spare_keys, static_cast<const T*>(ws->spare_values), ws->slots,
-                ws->bucket_start, ws->keys, sorted_values);
-            PM_LAUNCH_CHECK();
-        }
-    }
-    else
-    {
-        PM_CUDA(cudaMemsetAsync(ws->bucket_sizes, 0, rows * sizeof(int), stream));
-        count_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, values, count, rows, cols,
-                                                                  ws->bucket_sizes, ws->slots, ws->status);
-        PM_LAUNCH_CHECK();
-        exclusive_scan<int, int>(ws->bucket_sizes, ws->bucket_start, rows, ws->scan_scratch, stream);
-        scatter_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, values, count, ws->slots,
-                                                                    ws->bucket_start, ws->keys, sorted_values);
-        PM_LAUNCH_CHECK();
-    }
+    PM_CUDA(cudaMemsetAsync(ws->bucket_sizes, 0, rows * sizeof(int), stream));
+    count_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, values, count, rows, cols,
+                                                              ws->bucket_sizes, ws->slots, ws->status);
+    PM_LAUNCH_CHECK();
+    exclusive_scan<int, int>(ws->bucket_sizes, ws->bucket_start, rows, ws->scan_scratch, stream);
+    scatter_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, values, count, ws->slots,
+                                                                ws->bucket_start, ws->keys, sorted_values);
+    PM_LAUNCH_CHECK();
     if (rows > 0)
     {
         sort_short_kernel<T><<<grid_for(rows, 128), 128, 0, stream>>>(ws->bucket_start, rows, ws->keys, sorted_values,
@@ -1004,10 +836,6 @@ size_t static_plan_bytes(int64_t rows, int64_t count)
     plan.take<int>(R);
     plan.take<int64_t>(R + 1);
     plan.take<char>(scan_bytes);
-    // the coarse-bin arrays coo_prepare carves (one entry each: these sizes never bin)
-    plan.take<int>(1);
-    plan.take<int>(1);
-    plan.take<char>(1);
     return plan.offset + 256;
 }
 
