@@ -85,7 +85,6 @@ struct pm_schur_workspace
     // 6x3 assembly cross pairs (pattern lifetime, own buffer)
     pm::DeviceBuffer pair_buffer;
     bool paired = false;           // the 6x3 factor-record path applies to this pattern
-    bool fused = false;            // ... and the fused one-pass assembly (no pair lists, no stored V)
     int64_t E = 0;                 // cross pairs
     int2* row_entries = nullptr;   // C: {cross, eliminated} of every primary-list entry
     int64_t* pair_offset = nullptr; // B + 1: pairs of block b are [off[b], off[b+1]) (upper blocks only)
@@ -686,20 +685,6 @@ __global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross
     }
 }
 
-// largest upper-block count of a row and largest number of later crosses of an eliminated block
-// (the limits of the fused assembly kernel)
-__global__ void fused_limits_kernel(int64_t P, const int* __restrict__ block_row_ptr, const int* __restrict__ diag_pos,
-                                    int64_t L, const int* __restrict__ cross_offsets, int* __restrict__ out)
-{
-    int u = 0, k = 0;
-    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
-        u = max(u, block_row_ptr[p + 1] - diag_pos[p] - 1);
-    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < L; l += int64_t(gridDim.x) * blockDim.x)
-        k = max(k, cross_offsets[l + 1] - cross_offsets[l] - 1);
-    atomicMax(out, u);
-    atomicMax(out + 1, k);
-}
-
 // row-list position of every cross: rowpos[prim_cross[j]] = j
 __global__ void rowpos_kernel(int64_t C, const int* __restrict__ prim_cross, int* __restrict__ rowpos)
 {
@@ -1055,302 +1040,6 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
             out[e] = value;
             mirrored[(e % 6) * 6 + 3 * h + e / 6] = value;
         }
-    }
-}
-
-// ===================================================================== fused 6x3 assembly
-// One pass, CTA per block row p, no factor stored in HBM.  The row's entries (crosses (l, p),
-// ascending l) are taken in chunks.  For each entry the CTA forms V_lp = W_lp L_l^-T in shared
-// memory from W and the 80-byte factor record; for each later cross (l, q), q > p, of the same
-// eliminated block -- its crosses are sorted by primary, so they follow (l, p) contiguously in W
-// -- it forms V_lq as an "item".  A stable warp-level counting sort buckets the chunk's items by
-// upper block (match-any ranks, no atomics).  Owner threads then sum in fixed order:
-//   diagonal entry (r, c):  sum_e V_ep[r] . V_ep[c]          (36 slots)
-//   RHS row r:              sum_e V_ep[r] . z_e              (6 slots)
-//   upper block b, row r:   sum_items V_ep[r] . V_iq[c], c = 0..5  (6 slots per block)
-// a slot being one thread's running sums across the row's chunks.  Nothing is atomic and every
-// sum has a fixed order, so repeated assemblies are bitwise identical.  Rows with more than
-// kFusedMaxUpper upper blocks, or eliminated blocks with more than kFusedItems later crosses, are
-// left to the two-pass kernels (the host checks this at pattern time).
-constexpr int kFusedThreads = 256;
-constexpr int kFusedEntries = 128;  // row entries per chunk
-constexpr int kFusedItems = 384;    // later-cross items per chunk
-constexpr int kFusedMaxUpper = 96;  // upper blocks per row
-constexpr int kFusedSlots = 42 + 6 * kFusedMaxUpper;
-constexpr int kFusedSlotsPerThread = (kFusedSlots + kFusedThreads - 1) / kFusedThreads;
-
-template <typename AT>
-struct FusedSmem
-{
-    double vp[kFusedEntries][18]; // V_lp of the chunk's entries (FP64: the diagonal and RHS sums use it)
-    AT vq[kFusedItems][18];       // V_lq of the chunk's items, in the product type
-    double z[kFusedEntries][3];   // z_l = L^-1 g_l of the chunk's entries
-    double li[kFusedEntries][6]; // L^-1 of the chunk's entries (for the items)
-    int cross[kFusedEntries];   // cross index of each entry
-    int first[kFusedEntries + 1]; // first item of each entry (prefix of later-cross counts)
-    short item_entry[kFusedItems];
-    short item_block[kFusedItems];
-    short order[kFusedItems];   // items bucketed by block, ascending item index inside a bucket
-    int ucol[kFusedMaxUpper];   // block columns of the row's upper blocks (ascending)
-    int ustart[kFusedMaxUpper + 1];
-    int ucursor[kFusedMaxUpper];
-    int take;                   // entries in the current chunk
-};
-
-template <typename T, typename AT, typename TO>
-__global__ void __launch_bounds__(kFusedThreads, 2) assemble_fused6_kernel(
-    int64_t P, const int* __restrict__ prim_offsets, const int2* __restrict__ row_entries,
-    const int* __restrict__ cross_offsets, const int* __restrict__ cross_primary, const T* __restrict__ w,
-    const double* __restrict__ rec, const T* __restrict__ hpp, const T* __restrict__ gp, double lambda,
-    double min_diag, const int* __restrict__ block_row_ptr, const int* __restrict__ diag_pos,
-    const int* __restrict__ block_col, const int* __restrict__ transpose, const int* __restrict__ block_pc,
-    const T* __restrict__ pcv, T* __restrict__ S, TO* __restrict__ SO, double* __restrict__ rhs,
-    int* __restrict__ overflow)
-{
-    extern __shared__ __align__(16) unsigned char fused_raw[];
-    FusedSmem<AT>& sm = *reinterpret_cast<FusedSmem<AT>*>(fused_raw);
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    for (int64_t pp = blockIdx.x; pp < P; pp += gridDim.x)
-    {
-        const int p = static_cast<int>(pp);
-        const int dpos = diag_pos[p];
-        const int U = block_row_ptr[p + 1] - dpos - 1; // upper blocks (columns > p follow the diagonal)
-        const int slots = 42 + 6 * U;
-        for (int b = t; b < U; b += kFusedThreads)
-            sm.ucol[b] = block_col[dpos + 1 + b];
-        AT acc[kFusedSlotsPerThread][6];
-#pragma unroll
-        for (int k = 0; k < kFusedSlotsPerThread; ++k)
-#pragma unroll
-            for (int c = 0; c < 6; ++c)
-                acc[k][c] = AT(0);
-        double dacc = 0.0; // diagonal / RHS slot (threads 0..41): always summed in FP64
-        const int J0 = prim_offsets[p], J1 = prim_offsets[p + 1];
-        for (int j0 = J0; j0 < J1;)
-        {
-            // ---- chunk: the longest run of entries whose later crosses fit kFusedItems
-            int later = 0, cross = 0, l = 0;
-            const bool mine = t < kFusedEntries && j0 + t < J1;
-            if (mine)
-            {
-                const int2 re = row_entries[j0 + t];
-                cross = re.x;
-                l = re.y;
-                later = cross_offsets[l + 1] - cross - 1;
-            }
-            // inclusive scan of `later` over the first kFusedEntries threads (warps 0-3)
-            int incl = later;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1)
-            {
-                const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o)
-                    incl += v;
-            }
-            if (lane == 31 && warp < kFusedEntries / 32)
-                sm.ucursor[warp] = incl; // warp totals (ucursor reused as scratch)
-            __syncthreads();
-            int before = 0;
-            for (int k = 0; k < warp && k < kFusedEntries / 32; ++k)
-                before += sm.ucursor[k];
-            incl += before;
-            const bool fits = mine && incl <= kFusedItems;
-            const int take = __syncthreads_count(fits); // fits holds for a prefix of the entries
-            if (t == 0)
-            {
-                sm.take = take;
-                sm.first[0] = 0;
-            }
-            if (fits)
-            {
-                sm.cross[t] = cross;
-                sm.first[t + 1] = incl;
-                // ---- A1: V_lp, z and L^-1 of the entry
-                double f[10], wv[18];
-                load_pairs<double, 10>(rec + int64_t(l) * 10, f);
-                load_pairs<T, 18>(w + int64_t(cross) * 18, wv);
-#pragma unroll
-                for (int r = 0; r < 6; ++r)
-                {
-                    const double w0 = wv[3 * r], w1 = wv[3 * r + 1], w2 = wv[3 * r + 2];
-                    sm.vp[t][3 * r] = f[0] * w0;
-                    sm.vp[t][3 * r + 1] = f[1] * w0 + f[2] * w1;
-                    sm.vp[t][3 * r + 2] = f[3] * w0 + f[4] * w1 + f[5] * w2;
-                }
-#pragma unroll
-                for (int k = 0; k < 6; ++k)
-                    sm.li[t][k] = f[k];
-                sm.z[t][0] = f[6];
-                sm.z[t][1] = f[7];
-                sm.z[t][2] = f[8];
-            }
-            __syncthreads();
-            const int ne = sm.take;
-            if (ne == 0)
-            {
-                // an eliminated block with more later crosses than a chunk holds (the host routes
-                // such systems to the two-pass kernels): give up on the row, never spin
-                if (t == 0)
-                    atomicExch(overflow, 1);
-                break;
-            }
-            const int items = sm.first[ne];
-            // ---- A2: items (l, q) of the chunk: V_lq and their upper block
-            for (int i = t; i < items; i += kFusedThreads)
-            {
-                int lo = 0, hi = ne - 1; // entry e with first[e] <= i < first[e + 1]
-                while (lo < hi)
-                {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (sm.first[mid] <= i)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                const int e = lo;
-                const int c = sm.cross[e] + 1 + (i - sm.first[e]);
-                const int q = cross_primary[c];
-                int blo = 0, bhi = U - 1; // q is a column of the row's pattern by construction
-                while (blo < bhi)
-                {
-                    const int mid = (blo + bhi) >> 1;
-                    if (sm.ucol[mid] < q)
-                        blo = mid + 1;
-                    else
-                        bhi = mid;
-                }
-                double wv[18];
-                load_pairs<T, 18>(w + int64_t(c) * 18, wv);
-                const double* f = sm.li[e];
-#pragma unroll
-                for (int r = 0; r < 6; ++r)
-                {
-                    const double w0 = wv[3 * r], w1 = wv[3 * r + 1], w2 = wv[3 * r + 2];
-                    sm.vq[i][3 * r] = static_cast<AT>(f[0] * w0);
-                    sm.vq[i][3 * r + 1] = static_cast<AT>(f[1] * w0 + f[2] * w1);
-                    sm.vq[i][3 * r + 2] = static_cast<AT>(f[3] * w0 + f[4] * w1 + f[5] * w2);
-                }
-                sm.item_entry[i] = static_cast<short>(e);
-                sm.item_block[i] = static_cast<short>(blo);
-            }
-            __syncthreads();
-            // ---- A3 (warp 0): stable counting sort of the items by block
-            if (warp == 0)
-            {
-                for (int b = lane; b <= U; b += 32)
-                    sm.ustart[b] = 0;
-                __syncwarp();
-                for (int base = 0; base < items; base += 32)
-                {
-                    const int i = base + lane;
-                    const int b = i < items ? sm.item_block[i] : -1;
-                    const unsigned m = __match_any_sync(0xffffffffu, b);
-                    if (b >= 0 && lane == __ffs(m) - 1)
-                        sm.ustart[b + 1] += __popc(m);
-                    __syncwarp();
-                }
-                if (lane == 0)
-                    for (int b = 0; b < U; ++b)
-                        sm.ustart[b + 1] += sm.ustart[b];
-                __syncwarp();
-                for (int b = lane; b < U; b += 32)
-                    sm.ucursor[b] = sm.ustart[b];
-                __syncwarp();
-                const unsigned below = (1u << lane) - 1u;
-                for (int base = 0; base < items; base += 32)
-                {
-                    const int i = base + lane;
-                    const int b = i < items ? sm.item_block[i] : -1;
-                    const unsigned m = __match_any_sync(0xffffffffu, b);
-                    if (b >= 0)
-                        sm.order[sm.ucursor[b] + __popc(m & below)] = static_cast<short>(i);
-                    __syncwarp();
-                    if (b >= 0 && lane == __ffs(m) - 1)
-                        sm.ucursor[b] += __popc(m);
-                    __syncwarp();
-                }
-            }
-            __syncthreads();
-            // ---- B: owner slots
-#pragma unroll
-            for (int k = 0; k < kFusedSlotsPerThread; ++k)
-            {
-                const int slot = t + k * kFusedThreads;
-                if (slot >= slots)
-                    continue;
-                if (slot < 36)
-                {
-                    const int r = slot / 6, c = slot % 6;
-                    for (int e = 0; e < ne; ++e)
-                        dacc += sm.vp[e][3 * r] * sm.vp[e][3 * c] + sm.vp[e][3 * r + 1] * sm.vp[e][3 * c + 1] +
-                                sm.vp[e][3 * r + 2] * sm.vp[e][3 * c + 2];
-                }
-                else if (slot < 42)
-                {
-                    const int r = slot - 36;
-                    for (int e = 0; e < ne; ++e)
-                        dacc += sm.vp[e][3 * r] * sm.z[e][0] + sm.vp[e][3 * r + 1] * sm.z[e][1] +
-                                sm.vp[e][3 * r + 2] * sm.z[e][2];
-                }
-                else
-                {
-                    const int b = (slot - 42) / 6, r = (slot - 42) % 6;
-                    for (int o = sm.ustart[b]; o < sm.ustart[b + 1]; ++o)
-                    {
-                        const int i = sm.order[o];
-                        const int e = sm.item_entry[i];
-                        const AT a0 = static_cast<AT>(sm.vp[e][3 * r]), a1 = static_cast<AT>(sm.vp[e][3 * r + 1]),
-                                 a2 = static_cast<AT>(sm.vp[e][3 * r + 2]);
-#pragma unroll
-                        for (int c = 0; c < 6; ++c)
-                            acc[k][c] += a0 * sm.vq[i][3 * c] + a1 * sm.vq[i][3 * c + 1] + a2 * sm.vq[i][3 * c + 2];
-                    }
-                }
-            }
-            j0 += ne;
-            __syncthreads(); // the chunk's shared memory is read before the next chunk writes it
-        }
-        // ---- row results
-#pragma unroll
-        for (int k = 0; k < kFusedSlotsPerThread; ++k)
-        {
-            const int slot = t + k * kFusedThreads;
-            if (slot >= slots)
-                continue;
-            if (slot < 36)
-            {
-                const int r = slot / 6, c = slot % 6;
-                double base = static_cast<double>(hpp[int64_t(p) * 36 + slot]);
-                if (r == c)
-                    base = __dadd_rn(base, __dmul_rn(lambda, fmax(fabs(base), min_diag)));
-                const double v = base - dacc;
-                S[int64_t(dpos) * 36 + slot] = static_cast<T>(v);
-                if (SO)
-                    SO[int64_t(dpos) * 36 + slot] = static_cast<TO>(v);
-            }
-            else if (slot < 42)
-            {
-                const int r = slot - 36;
-                rhs[int64_t(p) * 6 + r] = -static_cast<double>(gp[int64_t(p) * 6 + r]) + dacc;
-            }
-            else
-            {
-                const int b = (slot - 42) / 6, r = (slot - 42) % 6;
-                const int64_t blk = int64_t(dpos) + 1 + b;
-                const int pc = block_pc[blk];
-                TO* out = (SO ? SO : reinterpret_cast<TO*>(S)) + blk * 36 + r * 6;
-                TO* mirrored = (SO ? SO : reinterpret_cast<TO*>(S)) + int64_t(transpose[blk]) * 36 + r;
-#pragma unroll
-                for (int c = 0; c < 6; ++c)
-                {
-                    const AT base = pc >= 0 ? static_cast<AT>(pcv[int64_t(pc) * 36 + r * 6 + c]) : AT(0);
-                    const TO value = static_cast<TO>(base - acc[k][c]);
-                    out[c] = value;
-                    mirrored[c * 6] = value;
-                }
-            }
-        }
-        __syncthreads(); // ucol of this row read before the next row writes it
     }
 }
 
@@ -2094,45 +1783,8 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
 {
     const int64_t P = ne->P, C = ne->cross_count, B = ws->B;
     ws->paired = false;
-    ws->fused = false;
     const int sorted = ne->crosses_sorted ? 1 : 0;
     const unsigned grid = static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(P, 8 * sm_count())));
-    if (sorted && P > 0)
-    {
-        // the fused kernel needs each eliminated block's crosses sorted by primary (its later
-        // crosses follow it contiguously) and bounded row / block widths
-        ws->scratch.ensure(512, stream, "SchurComplementSolverWorkspace");
-        int* lim = static_cast<int*>(ws->scratch.ptr);
-        PM_CUDA(cudaMemsetAsync(lim, 0, 2 * sizeof(int), stream));
-        fused_limits_kernel<<<grid_for(std::max(P, ne->L), 256, 1024), 256, 0, stream>>>(
-            P, ws->block_row_ptr, ws->diag_pos, ne->L, ne->cross_offsets, lim);
-        PM_LAUNCH_CHECK();
-        int host_lim[2] = {0, 0};
-        PM_CUDA(cudaMemcpyAsync(host_lim, lim, sizeof(host_lim), cudaMemcpyDeviceToHost, stream));
-        PM_CUDA(cudaStreamSynchronize(stream));
-        if (host_lim[0] <= kFusedMaxUpper && host_lim[1] <= kFusedItems)
-        {
-            Carver plan_b;
-            plan_b.take<int2>(C + 1);
-            ws->pair_buffer.ensure(plan_b.offset + 512, stream, "SchurComplementSolverWorkspace");
-            Carver bc;
-            bc.base = static_cast<char*>(ws->pair_buffer.ptr);
-            ws->row_entries = bc.take<int2>(C + 1);
-            ws->pair_offset = nullptr;
-            ws->pairs = nullptr;
-            ws->vfactor = nullptr;
-            ws->E = 0;
-            if (C > 0)
-            {
-                row_entries_kernel<<<grid_for(C, 256, 1 << 16), 256, 0, stream>>>(C, ws->prim_cross,
-                                                                                 ne->cross_eliminated, ws->row_entries);
-                PM_LAUNCH_CHECK();
-            }
-            ws->paired = true;
-            ws->fused = true;
-            return;
-        }
-    }
     Carver s1;
     s1.take<int>(C + 1);
     s1.take<int64_t>(C + 2);
@@ -2397,32 +2049,7 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
     if (ws->paired)
     {
         const unsigned ugrid = grid_for(ws->B * kPairLanes, kUpperThreads);
-        int* overflow = reinterpret_cast<int*>(ws->status) + 6; // pad[0] of the status block
-        if (ws->fused)
-        {
-            PM_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int), stream));
-            const unsigned fgrid = grid_for(a.P, 1, 1 << 20);
-            if (fp32_products)
-            {
-                const size_t smem = sizeof(FusedSmem<float>);
-                set_smem(reinterpret_cast<const void*>(assemble_fused6_kernel<T, float, float>), smem);
-                assemble_fused6_kernel<T, float, float><<<fgrid, kFusedThreads, smem, stream>>>(
-                    a.P, ws->prim_offsets, ws->row_entries, ne->cross_offsets, ne->cross_primary, a.w, ws->hinv, a.hpp,
-                    a.gp, a.lambda, a.min_diag, ws->block_row_ptr, a.diag_pos, ws->block_col, ws->transpose,
-                    a.block_pc, a.pcv, a.S, ws->S32, a.rhs, overflow);
-            }
-            else
-            {
-                const size_t smem = sizeof(FusedSmem<double>);
-                set_smem(reinterpret_cast<const void*>(assemble_fused6_kernel<T, double, T>), smem);
-                assemble_fused6_kernel<T, double, T><<<fgrid, kFusedThreads, smem, stream>>>(
-                    a.P, ws->prim_offsets, ws->row_entries, ne->cross_offsets, ne->cross_primary, a.w, ws->hinv, a.hpp,
-                    a.gp, a.lambda, a.min_diag, ws->block_row_ptr, a.diag_pos, ws->block_col, ws->transpose,
-                    a.block_pc, a.pcv, a.S, static_cast<T*>(nullptr), a.rhs, overflow);
-            }
-            PM_LAUNCH_CHECK();
-        }
-        else if (fp32_products)
+        if (fp32_products)
         {
             // FP32 products: V stored in FP32, upper blocks formed and summed in FP32 into S32;
             // the diagonal blocks and the RHS are still summed in FP64 (S keeps the FP64 diagonal
@@ -3276,8 +2903,6 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             fail(PM_INVALID_ARGUMENT, "evaluateHuberLoss: squared residual norm must be finite and non-negative "
                                       "(observation " + std::to_string(bad) + ")");
     }
-    if (ws->host_status->pad[0])
-        fail(PM_RUNTIME_ERROR, "Schur assembly: an eliminated block has more crosses than the fused assembly holds");
     if (ws->host_status->eliminated_bad != kNone)
     {
         timings(3);

@@ -56,9 +56,12 @@ def test_known_answers_async_on_side_stream(case):
 
 
 @pytest.mark.parametrize("dtype", [np.float32, np.float64])
-@pytest.mark.parametrize("shape", ["short", "long", "huge", "dup_heavy"])
+@pytest.mark.parametrize("shape", ["short", "long", "huge", "dup_heavy", "large", "large_skew"])
 def test_random_matches_oracle_bitwise(checkers, dtype, shape):
-    rng = np.random.default_rng(hash(shape) % 1000)
+    """Shapes of every bucketing tier: short rows, shared-memory and merged long rows, heavy
+    duplicates, and large inputs (1.2M triplets over 500k rows; 600k triplets with a third of them
+    in three rows)."""
+    rng = np.random.default_rng(sum(map(ord, shape)))
     if shape == "short":
         rows, cols, n = 5000, 300, 30000
         r = rng.integers(0, rows, n)
@@ -68,9 +71,16 @@ def test_random_matches_oracle_bitwise(checkers, dtype, shape):
     elif shape == "huge":          # rows longer than one 2048-entry chunk (merge tier)
         rows, cols, n = 3, 100000, 50000
         r = rng.choice(rows, n, p=[0.8, 0.15, 0.05])
-    else:                          # many duplicates with cancellation
+    elif shape == "dup_heavy":     # many duplicates with cancellation
         rows, cols, n = 200, 4, 40000
         r = rng.integers(0, rows, n)
+    elif shape == "large":
+        rows, cols, n = 500_000, 3000, 1_200_000
+        r = rng.integers(0, rows, n)
+    else:                          # a few rows holding a third of the triplets (merge tier)
+        rows, cols, n = 300_000, 200_000, 600_000
+        r = rng.integers(0, rows, n)
+        r[: n // 3] = rng.choice([7, 123_456, 299_999], n // 3)
     c = rng.integers(0, cols, n)
     v = (rng.standard_normal(n) * 10.0 ** rng.integers(-4, 9, n)).astype(dtype)
     ref = checkers.coo_to_csr(rows, cols, r, c, v)

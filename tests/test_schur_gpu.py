@@ -572,11 +572,10 @@ def test_windowed_bundle_matches_oracle(checkers):
 
 
 @pytest.mark.parametrize("precision", ["native", "mixed_fp32_assembly"])
-def test_fused_and_two_pass_assemblies_agree(precision):
-    """The one-pass 6x3 assembly (crosses of every eliminated block sorted by primary, as the
-    observation path stores them) against the two-pass one (the same state uploaded with every
-    eliminated block's crosses reversed, which routes it to the kernels with stored factors and
-    per-block pair lists): same pattern, values within rounding, same steps."""
+def test_assembly_does_not_depend_on_the_order_of_crosses(precision):
+    """The same normal equations with every eliminated block's crosses in ascending primary order
+    (as the observation path stores them) and reversed (an uploaded state in another adjacency
+    order): same pattern, values within rounding, same steps."""
     prob = W.large_bundle(seed=13, P=300, L=12000)
     ne_sorted = _device_from_observations(prob)
     state = ne_sorted.download()
