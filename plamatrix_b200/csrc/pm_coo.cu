@@ -43,6 +43,14 @@ struct CooStatus
     int pad;
 };
 
+// (key, value) of one scattered triplet: a single 16-byte store into its row bucket
+template <typename T>
+struct alignas(16) CooRec
+{
+    uint64_t key;
+    T value;
+};
+
 __device__ __forceinline__ uint32_t key_col(uint64_t key) { return static_cast<uint32_t>(key >> 32); }
 __device__ __forceinline__ unsigned source_of(uint64_t key) { return static_cast<unsigned>(key & 0xffffffffu); }
 
@@ -86,12 +94,13 @@ __global__ void __launch_bounds__(256) count_kernel(const int64_t* __restrict__ 
     slots[i] = atomicAdd(&bucket_sizes[row], 1);
 }
 
-// 2) scatter (key, value) into the row buckets
+// 2) scatter (key, value) into the row buckets as one 16-byte record per triplet (the sorts
+// below read the records and write the sorted keys and values)
 template <typename T>
 __global__ void __launch_bounds__(256) scatter_kernel(const int64_t* __restrict__ rows, const int64_t* __restrict__ cols,
                                                       const T* __restrict__ values, int64_t count,
                                                       const int* __restrict__ slots, const int* __restrict__ bucket_start,
-                                                      uint64_t* __restrict__ keys, T* __restrict__ sorted_values)
+                                                      CooRec<T>* __restrict__ recs)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= count)
@@ -100,8 +109,10 @@ __global__ void __launch_bounds__(256) scatter_kernel(const int64_t* __restrict_
     if (slot < 0)
         return;
     const int pos = bucket_start[rows[i]] + slot;
-    keys[pos] = (static_cast<uint64_t>(cols[i]) << 32) | static_cast<uint64_t>(i);
-    sorted_values[pos] = values ? values[i] : T(0);
+    CooRec<T> r;
+    r.key = (static_cast<uint64_t>(cols[i]) << 32) | static_cast<uint64_t>(i);
+    r.value = values ? values[i] : T(0);
+    recs[pos] = r;
 }
 
 // bitonic network over N register-resident (key, value) pairs; indices are compile-time
@@ -137,6 +148,7 @@ __device__ __forceinline__ void register_sort(uint64_t (&k)[N], T (&v)[N])
 // 3) short rows: one thread per row, sorted in registers; long rows are queued
 template <typename T>
 __global__ void __launch_bounds__(128) sort_short_kernel(const int* __restrict__ bucket_start, int64_t row_count,
+                                                         const CooRec<T>* __restrict__ recs,
                                                          uint64_t* __restrict__ keys, T* __restrict__ values,
                                                          int* __restrict__ unique_count, int* __restrict__ long_rows,
                                                          CooStatus* status)
@@ -153,6 +165,12 @@ __global__ void __launch_bounds__(128) sort_short_kernel(const int* __restrict__
     }
     if (len <= 1)
     {
+        if (len == 1)
+        {
+            const CooRec<T> one = recs[start];
+            keys[start] = one.key;
+            values[start] = one.value;
+        }
         unique_count[r] = len;
         return;
     }
@@ -161,8 +179,17 @@ __global__ void __launch_bounds__(128) sort_short_kernel(const int* __restrict__
 #pragma unroll
     for (int q = 0; q < kShortMax; ++q)
     {
-        k[q] = q < len ? keys[start + q] : kPadKey;
-        v[q] = q < len ? values[start + q] : T(0);
+        if (q < len)
+        {
+            const CooRec<T> one = recs[start + q];
+            k[q] = one.key;
+            v[q] = one.value;
+        }
+        else
+        {
+            k[q] = kPadKey;
+            v[q] = T(0);
+        }
     }
     register_sort<kShortMax, T>(k, v);
     int unique = 0;
@@ -233,6 +260,7 @@ __device__ __forceinline__ int merge_split(const uint64_t* a, int na, const uint
 // `spare`), all inside the CTA.  Also counts the distinct columns of the row.
 template <typename T>
 __global__ void __launch_bounds__(kLongThreads) sort_long_kernel(const int* __restrict__ bucket_start,
+                                                                 const CooRec<T>* __restrict__ recs,
                                                                  uint64_t* __restrict__ keys, T* __restrict__ values,
                                                                  uint64_t* __restrict__ spare_keys,
                                                                  T* __restrict__ spare_values,
@@ -260,8 +288,17 @@ __global__ void __launch_bounds__(kLongThreads) sort_long_kernel(const int* __re
                 m <<= 1;
             for (int i = threadIdx.x; i < m; i += blockDim.x)
             {
-                sk[i] = i < n ? rk[c0 + i] : kPadKey;
-                sv[i] = i < n ? rv[c0 + i] : T(0);
+                if (i < n)
+                {
+                    const CooRec<T> one = recs[start + c0 + i];
+                    sk[i] = one.key;
+                    sv[i] = one.value;
+                }
+                else
+                {
+                    sk[i] = kPadKey;
+                    sv[i] = T(0);
+                }
             }
             __syncthreads();
             smem_bitonic<T>(sk, sv, m);
@@ -507,6 +544,7 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     plan.take<int>(R);
     plan.take<int64_t>(R + 1);
     plan.take<char>(scan_bytes);
+    plan.take<CooRec<T>>(n);
     ws->buffer.ensure(plan.offset + 256, stream, "SparseOpsWorkspace");
     Carver carve;
     carve.base = static_cast<char*>(ws->buffer.ptr);
@@ -522,6 +560,7 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     ws->long_rows = carve.take<int>(R);
     ws->row_offsets = carve.take<int64_t>(R + 1);
     ws->scan_scratch = carve.take<char>(scan_bytes);
+    CooRec<T>* recs = carve.take<CooRec<T>>(n);
     ws->rows = rows;
     ws->cols = cols;
     ws->count = count;
@@ -548,15 +587,16 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     PM_LAUNCH_CHECK();
     exclusive_scan<int, int>(ws->bucket_sizes, ws->bucket_start, rows, ws->scan_scratch, stream);
     scatter_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, values, count, ws->slots,
-                                                                ws->bucket_start, ws->keys, sorted_values);
+                                                                ws->bucket_start, recs);
     PM_LAUNCH_CHECK();
     if (rows > 0)
     {
-        sort_short_kernel<T><<<grid_for(rows, 128), 128, 0, stream>>>(ws->bucket_start, rows, ws->keys, sorted_values,
+        sort_short_kernel<T><<<grid_for(rows, 128), 128, 0, stream>>>(ws->bucket_start, rows, recs, ws->keys,
+                                                                      sorted_values,
                                                                       ws->unique_count, ws->long_rows, ws->status);
         PM_LAUNCH_CHECK();
         sort_long_kernel<T><<<2 * sm_count(), kLongThreads, 0, stream>>>(
-            ws->bucket_start, ws->keys, sorted_values, ws->spare_keys, static_cast<T*>(ws->spare_values),
+            ws->bucket_start, recs, ws->keys, sorted_values, ws->spare_keys, static_cast<T*>(ws->spare_values),
             ws->unique_count, ws->long_rows, ws->status);
         PM_LAUNCH_CHECK();
     }
@@ -836,6 +876,7 @@ size_t static_plan_bytes(int64_t rows, int64_t count)
     plan.take<int>(R);
     plan.take<int64_t>(R + 1);
     plan.take<char>(scan_bytes);
+    plan.take<CooRec<T>>(n);
     return plan.offset + 256;
 }
 
