@@ -40,8 +40,9 @@ METRIC = "Schur-PCG ms to 1e-8 FP64 rel. residual: learned+mixed vs plain; SpMV 
 # DRAM bytes (read + write) of one assembly (assemble_diag6 + assemble_upper6) per cross block,
 # from an ncu capture of the two kernels on the P=4,000, L=200,000 case, scaled by the cross count
 # (the traffic grows with the crosses): see the profile summary of the assembly
-ASSEMBLY_TRAFFIC_BYTES_PER_CROSS = None
-ASSEMBLY_TRAFFIC_SOURCE = "not captured for this kernel version"
+ASSEMBLY_TRAFFIC_BYTES_PER_CROSS = 633.3e6 / 1_200_542
+ASSEMBLY_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of assemble_diag6 + assemble_upper6 on "
+                           "P=4,000, L=200,000 (633.3 MB for 1,200,542 crosses), scaled by the cross count")
 BATCH_SYSTEMS = 512
 
 
@@ -384,7 +385,7 @@ def run_ours(args):
             "unseen_seeds": group_summary("unseen_seeds"),
             "fallbacks": c3["fallbacks"], "all_converged": c3["all_converged"],
         },
-        "roofline": {"bound": "hbm", "kernel": "assemble_diag6_kernel<double,double> + assemble_upper6_kernel<double,...>",
+        "roofline": {"bound": "hbm", "kernel": "assemble_diag6_kernel + assemble_upper6_kernel (FP64, plain step)",
                      "achieved": round(achieved, 1),
                      "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": (round(ASSEMBLY_TRAFFIC_BYTES_PER_CROSS * C_) if ASSEMBLY_TRAFFIC_BYTES_PER_CROSS

@@ -88,6 +88,8 @@ struct pm_schur_workspace
     int64_t E = 0;                 // cross pairs
     int2* row_entries = nullptr;   // C: {cross, eliminated} of every primary-list entry
     int64_t* pair_offset = nullptr; // B + 1: pairs of block b are [off[b], off[b+1]) (upper blocks only)
+    int* upper_list = nullptr;     // U: the upper blocks (column > row), ascending
+    int64_t U = 0;
     int2* pairs = nullptr;         // E: {row-list entry of cross (l, p), row-list entry of cross (l, q)}, per block in ascending l
     void* vfactor = nullptr;       // C x 18 (Scalar): V = W_lp L_l^-T of every row-list entry (written by the diagonal pass)
     int* saved_offsets = nullptr;
@@ -685,6 +687,22 @@ __global__ void row_entries_kernel(int64_t C, const int* __restrict__ prim_cross
     }
 }
 
+// upper blocks of every row (they follow its diagonal block): counts, then the list
+__global__ void upper_count_kernel(int64_t P, const int* __restrict__ block_row_ptr, const int* __restrict__ diag_pos,
+                                   int* __restrict__ count)
+{
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+        count[p] = block_row_ptr[p + 1] - diag_pos[p] - 1;
+}
+
+__global__ void upper_list_kernel(int64_t P, const int* __restrict__ diag_pos, const int* __restrict__ offset,
+                                  int* __restrict__ list)
+{
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+        for (int j = offset[p]; j < offset[p + 1]; ++j)
+            list[j] = diag_pos[p] + 1 + (j - offset[p]);
+}
+
 // row-list position of every cross: rowpos[prim_cross[j]] = j
 __global__ void rowpos_kernel(int64_t C, const int* __restrict__ prim_cross, int* __restrict__ rowpos)
 {
@@ -977,19 +995,18 @@ __device__ __forceinline__ void load_as(const VT* __restrict__ src, AT* q)
 // TO: type of the assembled values, TP: type of the coupling blocks (the normal equations'),
 // VT: type of the stored V factors, AT: type of the products and their sums
 template <typename TO, typename TP, typename VT, typename AT>
-__global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
-    int64_t B, const int64_t* __restrict__ pair_offset, const int2* __restrict__ pairs,
-    const int* __restrict__ block_row, const int* __restrict__ block_col, const int* __restrict__ transpose,
-    const int* __restrict__ block_pc, const VT* __restrict__ vfactor, const TP* __restrict__ pcv, TO* __restrict__ S)
+__global__ void __launch_bounds__(kUpperThreads, 3) assemble_upper6_kernel(
+    int64_t U, const int* __restrict__ upper_list, const int64_t* __restrict__ pair_offset,
+    const int2* __restrict__ pairs, const int* __restrict__ transpose, const int* __restrict__ block_pc,
+    const VT* __restrict__ vfactor, const TP* __restrict__ pcv, TO* __restrict__ S)
 {
     const int g = threadIdx.x & (kPairLanes - 1);
     const int s = g >> 1, h = g & 1;
     const unsigned gmask = 0xffffu << (threadIdx.x & 16);
     const int64_t groups = int64_t(gridDim.x) * (kUpperThreads / kPairLanes);
-    for (int64_t b = (int64_t(blockIdx.x) * kUpperThreads + threadIdx.x) / kPairLanes; b < B; b += groups)
+    for (int64_t u = (int64_t(blockIdx.x) * kUpperThreads + threadIdx.x) / kPairLanes; u < U; u += groups)
     {
-        if (block_col[b] <= block_row[b])
-            continue;
+        const int64_t b = upper_list[u];
         AT acc[3][6];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -1006,10 +1023,10 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
             if (k < k1)
                 next = pairs[k];
             // this lane's three rows of V_lp (elements 9h .. 9h + 8, read as the aligned run
-            // 8h .. 8h + 9) and all six rows of V_lq
-            AT a[10], q[18];
+            // 8h .. 8h + 9), then the six rows of V_lq in two halves of three (elements 0 .. 8 and
+            // 9 .. 17, read as the aligned runs 0 .. 9 and 8 .. 17) to keep fewer values live
+            AT a[10];
             load_as<VT, 10, AT>(vfactor + int64_t(cur.x) * 18 + 8 * h, a);
-            load_as<VT, 18, AT>(vfactor + int64_t(cur.y) * 18, q);
             AT tr[3][3];
 #pragma unroll
             for (int r = 0; r < 3; ++r)
@@ -1017,10 +1034,18 @@ __global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
                 for (int kk = 0; kk < 3; ++kk)
                     tr[r][kk] = h ? a[3 * r + kk + 1] : a[3 * r + kk];
 #pragma unroll
-            for (int r = 0; r < 3; ++r)
+            for (int half = 0; half < 2; ++half)
+            {
+                AT q[10];
+                load_as<VT, 10, AT>(vfactor + int64_t(cur.y) * 18 + 8 * half, q);
+                const int o = half; // run offset: element 9 * half sits at q[half]
 #pragma unroll
-                for (int c = 0; c < 6; ++c)
-                    acc[r][c] += tr[r][0] * q[3 * c] + tr[r][1] * q[3 * c + 1] + tr[r][2] * q[3 * c + 2];
+                for (int r = 0; r < 3; ++r)
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        acc[r][3 * half + c] += tr[r][0] * q[o + 3 * c] + tr[r][1] * q[o + 3 * c + 1] +
+                                                tr[r][2] * q[o + 3 * c + 2];
+            }
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -1817,6 +1842,9 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     s2.take<int>(E + 1);
     s2.take<int>(E + 1);
     s2.take<int>(C + 1);
+    s2.take<int>(P + 1);
+    s2.take<int>(P + 2);
+    s2.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
     s2.take<int>(B + 1);
     s2.take<unsigned>(B + 1);
     s2.take<int64_t>(B + 1);
@@ -1830,6 +1858,9 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     int* item_block = c2.take<int>(E + 1);
     int* item_entry = c2.take<int>(E + 1);
     int* rowpos = c2.take<int>(C + 1);
+    int* upper_count = c2.take<int>(P + 1);
+    int* upper_offset = c2.take<int>(P + 2);
+    void* upper_scan = c2.take<char>(scan_scratch_bytes(P + 1, sizeof(int)));
     int* block_pairs = c2.take<int>(B + 1);
     unsigned* mask = c2.take<unsigned>(B + 1);
     int64_t* cursor = c2.take<int64_t>(B + 1);
@@ -1840,6 +1871,8 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     plan_b.take<int64_t>(B + 2);
     plan_b.take<int2>(E + 1);
     plan_b.take<double>(C * 18 + 2); // V in the Scalar type (double at most)
+    const int64_t U = (B - P) / 2;   // every row holds its diagonal block; the rest pair up by transpose
+    plan_b.take<int>(U + 1);
     ws->pair_buffer.ensure(plan_b.offset + 512, stream, "SchurComplementSolverWorkspace");
     Carver bc;
     bc.base = static_cast<char*>(ws->pair_buffer.ptr);
@@ -1847,7 +1880,17 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     ws->pair_offset = bc.take<int64_t>(B + 2);
     ws->pairs = bc.take<int2>(E + 1);
     ws->vfactor = bc.take<double>(C * 18 + 2);
+    ws->upper_list = bc.take<int>(U + 1);
+    ws->U = U;
     ws->E = E;
+    if (P > 0)
+    {
+        upper_count_kernel<<<grid_for(P, 256, 4096), 256, 0, stream>>>(P, ws->block_row_ptr, ws->diag_pos, upper_count);
+        PM_LAUNCH_CHECK();
+        exclusive_scan<int, int>(upper_count, upper_offset, P, upper_scan, stream);
+        upper_list_kernel<<<grid_for(P, 128, 4096), 128, 0, stream>>>(P, ws->diag_pos, upper_offset, ws->upper_list);
+        PM_LAUNCH_CHECK();
+    }
     PM_CUDA(cudaMemsetAsync(block_pairs, 0, size_t(B + 1) * sizeof(int), stream));
     PM_CUDA(cudaMemsetAsync(mask, 0, size_t(B + 1) * sizeof(unsigned), stream));
     if (C > 0)
@@ -2048,7 +2091,7 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
     };
     if (ws->paired)
     {
-        const unsigned ugrid = grid_for(ws->B * kPairLanes, kUpperThreads);
+        const unsigned ugrid = grid_for(std::max<int64_t>(ws->U, 1) * kPairLanes, kUpperThreads);
         if (fp32_products)
         {
             // FP32 products: V stored in FP32, upper blocks formed and summed in FP32 into S32;
@@ -2060,8 +2103,7 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
                 a.diag_pos, a.S, a.rhs, vf, ws->S32);
             PM_LAUNCH_CHECK();
             assemble_upper6_kernel<float, T, float, float><<<ugrid, kUpperThreads, 0, stream>>>(
-                ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, vf, a.pcv,
-                ws->S32);
+                ws->U, ws->upper_list, ws->pair_offset, ws->pairs, ws->transpose, a.block_pc, vf, a.pcv, ws->S32);
             PM_LAUNCH_CHECK();
         }
         else
@@ -2073,8 +2115,7 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
             PM_LAUNCH_CHECK();
             // every upper block, also those whose only terms are primary-primary couplings
             assemble_upper6_kernel<T, T, T, double><<<ugrid, kUpperThreads, 0, stream>>>(
-                ws->B, ws->pair_offset, ws->pairs, ws->block_row, ws->block_col, ws->transpose, a.block_pc, vf, a.pcv,
-                a.S);
+                ws->U, ws->upper_list, ws->pair_offset, ws->pairs, ws->transpose, a.block_pc, vf, a.pcv, a.S);
             PM_LAUNCH_CHECK();
         }
         ws->s32_only = fp32_products;
