@@ -995,7 +995,7 @@ __device__ __forceinline__ void load_as(const VT* __restrict__ src, AT* q)
 // TO: type of the assembled values, TP: type of the coupling blocks (the normal equations'),
 // VT: type of the stored V factors, AT: type of the products and their sums
 template <typename TO, typename TP, typename VT, typename AT>
-__global__ void __launch_bounds__(kUpperThreads, 3) assemble_upper6_kernel(
+__global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
     int64_t U, const int* __restrict__ upper_list, const int64_t* __restrict__ pair_offset,
     const int2* __restrict__ pairs, const int* __restrict__ transpose, const int* __restrict__ block_pc,
     const VT* __restrict__ vfactor, const TP* __restrict__ pcv, TO* __restrict__ S)
