@@ -428,6 +428,8 @@ def extras(args, torch, SC, S, W, ne, ws, host, dev, dp, dl, opts, n, m, net=Non
     out["e2e"] = {"value": round(e0.elapsed_time(e1) / args.steps, 3), "unit": "ms", "h2d_bytes_per_step": h2d,
                   "d2h_bytes_per_step": (n + m) * 8}
     out["spmv"] = sparse_leg(torch, S, W, stream)
+    out["c1_jacobi_pcg"] = c1_pcg_leg(torch, S, W, stream)
+    out["c0"] = c0_leg(torch, SC, W, stream)
     out["dense_c4_max"] = dense_leg(torch, SC, W)
     # ---- CPU baseline: one full-size LM linear step of the reference's own CPU library (the
     # same host problem the device arm was built from), timed on its own, no scaling
@@ -547,6 +549,100 @@ def sparse_leg(torch, S, W, stream):
         spmv[f"coo_to_csr_laplacian128_{name}"] = {"ms": round(tc, 4), "GBps": round(cbytes / (tc * 1e-3) / 1e9, 1),
                                                    "triplets": trip, "algorithmic_bytes": cbytes}
     return spmv
+
+
+def c1_pcg_leg(torch, S, W, stream):
+    """Jacobi PCG to a relative residual of 1e-8 on the 128^3 Laplacian (+ 1e-2 shift), FP64 and
+    FP32, b ~ U(-1, 1): device time (CUDA events, median of 3 after a warm solve), iterations and
+    the FP64 true relative residual of the solution; the reference CPU library's pcg (its
+    iterative_solver_cpu.cpp, one thread) on the same matrix and right-hand side beside it."""
+    out = {}
+    lap = W.laplacian_coo(128, seed=0, dtype=np.float64)
+    n = lap["rows"]
+    r_d, c_d = torch.from_numpy(lap["row_indices"]).cuda(), torch.from_numpy(lap["col_indices"]).cuda()
+    csr64 = S.coo_to_csr(n, n, r_d, c_d, torch.from_numpy(lap["values"]).cuda())
+    op64 = S.CsrOperand(csr64)
+    for dt, name in ((torch.float64, "f64"), (torch.float32, "f32")):
+        csr = csr64 if dt == torch.float64 else S.coo_to_csr(n, n, r_d, c_d, torch.from_numpy(lap["values"]).to(dt).cuda())
+        b = torch.from_numpy(lap["rhs"]).to(dt).cuda()
+        opts = S.IterativeSolverOptions(relative_tolerance=1e-8, max_iterations=2000)
+        op = op64 if dt == torch.float64 else S.CsrOperand(csr)
+        sws = S.IterativeSolverWorkspace()
+        times, rep = [], None
+        for k in range(4):
+            x = torch.zeros(n, dtype=dt, device="cuda")
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rep = S.pcg(op, b, x, workspace=sws, options=opts)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if k > 0:
+                times.append(e0.elapsed_time(e1))
+        x64 = x.to(torch.float64)
+        b64 = b.to(torch.float64)
+        res = b64 - op64.spmv(x64, torch.empty_like(x64))
+        entry = {"ms": round(statistics.median(times), 3), "iterations": rep["iterations"],
+                 "converged": bool(rep["converged"]),
+                 "true_relative_residual": float(torch.linalg.norm(res) / torch.linalg.norm(b64))}
+        try:
+            import oracle
+            if oracle.available("ref"):
+                ro, ci, v = csr.cpu()
+                t0 = time.perf_counter()
+                _, rref = oracle.pcg(ro, ci, v, lap["rhs"].astype(v.dtype), relative_tolerance=1e-8,
+                                     max_iterations=2000, impl="ref")
+                entry["reference_cpu"] = {"ms": round((time.perf_counter() - t0) * 1e3, 1),
+                                          "iterations": rref["iterations"], "converged": bool(rref["converged"]),
+                                          "cores": 1}
+        except Exception as exc:  # noqa: BLE001
+            entry["reference_cpu"] = {"error": str(exc)}
+        out[name] = entry
+    return out
+
+
+def c0_leg(torch, SC, W, stream):
+    """The small Schur workload (P=20, L=2,000, 8,000 observations, tol 1e-10): one device LM linear
+    step from device observations (accumulation, assembly, block-Jacobi PCG, back-substitution;
+    median of 10 after 3 warm steps, CUDA events) against the reference CPU library's accumulation
+    + solveDampedSchurComplement with the Cpu backend and with DenseCpu (its OpenMP dense Cholesky,
+    all host threads), median of 5."""
+    prob = W.small_bundle(seed=1)
+    dev = {k: torch.from_numpy(prob[k]).cuda() for k in ("obs_primary", "obs_eliminated", "jp", "jl", "residual")}
+    ne = SC.DeviceNormalEquations(prob["P"], prob["L"], 6, 3)
+    ws = SC.SchurComplementSolverWorkspace()
+    opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-10)
+    times = []
+    for k in range(13):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ne.accumulate_observations(dev["obs_primary"], dev["obs_eliminated"], dev["jp"], dev["jl"], dev["residual"],
+                                   prob["huber_delta"])
+        _, _, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if k >= 3:
+            times.append(e0.elapsed_time(e1))
+    out = {"workload": "P=20, L=2,000, 4 distinct uniform primaries per eliminated block, tol 1e-10",
+           "device_ms": round(statistics.median(times), 3), "device_iterations": rep["iterations"]}
+    try:
+        import oracle
+        if oracle.available("ref"):
+            for backend, key in (("cpu", "reference_cpu"), ("dense_cpu", "reference_dense_cpu")):
+                t = []
+                for _ in range(6):
+                    t0 = time.perf_counter()
+                    ref_ne = oracle.normal_equations_from_observations(prob, impl="ref")
+                    _, _, rrep = ref_ne.solve(1e-3, backend=backend, relative_tolerance=1e-10, max_iterations=500)
+                    t.append((time.perf_counter() - t0) * 1e3)
+                    del ref_ne
+                out[key] = {"ms": round(statistics.median(t[1:]), 3), "iterations": rrep["iterations"],
+                            "converged": bool(rrep["converged"]),
+                            "threads": os.cpu_count() if backend == "dense_cpu" else 1}
+    except Exception as exc:  # noqa: BLE001
+        out["reference_error"] = str(exc)
+    return out
 
 
 def dense_leg(torch, SC, W):
