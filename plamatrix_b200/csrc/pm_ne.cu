@@ -30,6 +30,7 @@ pm_normal_equations::~pm_normal_equations()
     if (by_eliminated_order)
         pm_sparse_workspace_destroy(by_eliminated_order);
     cross_runs.release();
+    observation_slots.release();
     observation_status.release();
 }
 
@@ -91,9 +92,8 @@ __global__ void cross_owner_kernel(const int* __restrict__ offsets, int64_t L, i
             owner[c] = static_cast<int>(l);
 }
 
-// crosses of the observation path: one per distinct primary of each eliminated bucket,
-// in ascending primary order
-// in ascending primary order; cross_run[c] is the bucket position of the cross's first observation
+// crosses of the observation path: one per distinct primary of each eliminated bucket, in
+// ascending primary order; cross_run[c] is the bucket position of the cross's first observation
 __global__ void observation_crosses_kernel(CooView v, const int* __restrict__ cross_offsets,
                                            int* __restrict__ cross_primary, int* __restrict__ cross_run)
 {
@@ -113,6 +113,23 @@ __global__ void observation_crosses_kernel(CooView v, const int* __restrict__ cr
         if (l == v.rows - 1)
             cross_run[at] = e;
     }
+}
+
+// position of every observation in the input-order buckets (indexed by observation)
+__global__ void order_position_kernel(CooView vo, int* __restrict__ position)
+{
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < vo.count; q += int64_t(gridDim.x) * blockDim.x)
+        position[static_cast<uint32_t>(vo.keys[q])] = static_cast<int>(q);
+}
+
+// slot[q] for every input-order bucket position q: the cross c of that observation, stored as
+// c when it is the cross's first observation in input order and as ~c otherwise
+__global__ void observation_slots_kernel(int64_t C, const uint64_t* __restrict__ keys, const int* __restrict__ cross_run,
+                                         const int* __restrict__ position, int* __restrict__ slot)
+{
+    for (int64_t c = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; c < C; c += int64_t(gridDim.x) * blockDim.x)
+        for (int q = cross_run[c]; q < cross_run[c + 1]; ++q)
+            slot[position[static_cast<uint32_t>(keys[q])]] = q == cross_run[c] ? static_cast<int>(c) : ~static_cast<int>(c);
 }
 
 __global__ void compare_kernel(const int64_t* __restrict__ a, const int64_t* __restrict__ b, int64_t n, int* differs)
@@ -396,13 +413,20 @@ __global__ void __launch_bounds__(128) cross_accumulate63_kernel(int64_t C, cons
     }
 }
 
-// Two-row residuals, thread per eliminated block: Hll and g_l over the block's observations in
-// input order (the sums of eliminated_diagonal3_kernel), the Huber weight evaluated inline and
-// rows read in pairs of scalars; the next observation index is loaded one step ahead.
+// Two-row residuals, thread per eliminated block, one pass over the block's observations in
+// input order: Hll and g_l (the sums of eliminated_diagonal3_kernel) and every cross block W
+// (the sums of cross_accumulate63_kernel), the Huber weight evaluated once per observation and
+// rows read in pairs of scalars.  slot[q] names the cross of input-order position q: its first
+// observation starts the cross's W from zero, a later one (~c) adds to the row this thread
+// stored before, so every W is its observations' sum in input order.  A thread's crosses are
+// contiguous in W (crosses are grouped by eliminated block), so its row stores fill whole
+// sectors.  The next observation's index and slot are loaded one step ahead.
 template <typename T>
-__global__ void __launch_bounds__(128) eliminated3_m2_kernel(CooView vo, const T* __restrict__ jl,
-                                                             const T* __restrict__ res, T delta, T* __restrict__ hll,
-                                                             T* __restrict__ gl, long long* first_bad)
+__global__ void __launch_bounds__(128) eliminated_cross3_m2_kernel(CooView vo, const int* __restrict__ slot,
+                                                                   const T* __restrict__ jp, const T* __restrict__ jl,
+                                                                   const T* __restrict__ res, T delta,
+                                                                   T* __restrict__ hll, T* __restrict__ gl,
+                                                                   T* __restrict__ w, long long* first_bad)
 {
     for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < vo.rows; l += int64_t(gridDim.x) * blockDim.x)
     {
@@ -416,19 +440,43 @@ __global__ void __launch_bounds__(128) eliminated3_m2_kernel(CooView vo, const T
         const int e = vo.bucket_start[l + 1];
         int q = vo.bucket_start[l];
         uint64_t next = q < e ? vo.keys[q] : 0;
+        int next_slot = q < e ? slot[q] : 0;
         for (; q < e; ++q)
         {
             const int64_t i = static_cast<uint32_t>(next);
+            const int s = next_slot;
             if (q + 1 < e)
+            {
                 next = vo.keys[q + 1];
-            T r[2], J[6];
+                next_slot = slot[q + 1];
+            }
+            T r[2], Jl[6], Jp[12];
             load_vec<T, 2>(res + i * 2, r);
-            load_vec<T, 6>(jl + i * 6, J);
+            load_vec<T, 6>(jl + i * 6, Jl);
+            load_vec<T, 12>(jp + i * 12, Jp);
             const T squared = squared_norm(r, 2);
             note_nonfinite(squared, i, first_bad);
             const T weight = huber_weight_of(squared, delta);
-            eliminated3_row(H, g, weight, J, r[0]);
-            eliminated3_row(H, g, weight, J + 3, r[1]);
+            eliminated3_row(H, g, weight, Jl, r[0]);
+            eliminated3_row(H, g, weight, Jl + 3, r[1]);
+            const int64_t c = s >= 0 ? s : ~s;
+            T W[18];
+            if (s >= 0)
+            {
+#pragma unroll
+                for (int k = 0; k < 18; ++k)
+                    W[k] = T(0);
+            }
+            else
+            {
+                // a repeated (primary, eliminated) pair: this thread's own earlier store
+#pragma unroll
+                for (int k = 0; k < 18; ++k)
+                    W[k] = w[c * 18 + k];
+            }
+            cross63_row(W, weight, Jp, Jl);
+            cross63_row(W, weight, Jp + 6, Jl + 3);
+            store_vec<T, 18>(w + c * 18, W);
         }
 #pragma unroll
         for (int k = 0; k < 9; ++k)
@@ -436,68 +484,6 @@ __global__ void __launch_bounds__(128) eliminated3_m2_kernel(CooView vo, const T
 #pragma unroll
         for (int k = 0; k < 3; ++k)
             gl[l * 3 + k] = g[k];
-    }
-}
-
-// Two-row residuals, thread per cross: W over the cross's observations in input order (the
-// sums of cross_accumulate63_kernel), weight inline, rows read in pairs of scalars.  A warp's
-// 32 consecutive W rows (contiguous in memory) leave through shared memory in coalesced
-// 16-byte stores.  (Reading the observations in input order and scattering single-observation
-// W rows instead measured 1.7x slower: scattered 144-byte writes cost more than the gathers.)
-constexpr int kCrossThreads = 128;
-template <typename T>
-__global__ void __launch_bounds__(kCrossThreads) cross63_m2_kernel(int64_t C, const uint64_t* __restrict__ keys,
-                                                                   const int* __restrict__ cross_run,
-                                                                   const T* __restrict__ jp, const T* __restrict__ jl,
-                                                                   const T* __restrict__ res, T delta,
-                                                                   T* __restrict__ w)
-{
-    __shared__ __align__(16) T stage[kCrossThreads / 32][32 * 18];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t step = int64_t(gridDim.x) * kCrossThreads;
-    for (int64_t base = int64_t(blockIdx.x) * kCrossThreads; base < C; base += step)
-    {
-        const int64_t c = base + threadIdx.x;
-        T W[18];
-#pragma unroll
-        for (int k = 0; k < 18; ++k)
-            W[k] = T(0);
-        if (c < C)
-        {
-            for (int q = cross_run[c]; q < cross_run[c + 1]; ++q)
-            {
-                const int64_t i = static_cast<uint32_t>(keys[q]);
-                T r[2], Jp[12], Jl[6];
-                load_vec<T, 2>(res + i * 2, r);
-                load_vec<T, 12>(jp + i * 12, Jp);
-                load_vec<T, 6>(jl + i * 6, Jl);
-                const T weight = huber_weight(r, 2, delta);
-                cross63_row(W, weight, Jp, Jl);
-                cross63_row(W, weight, Jp + 6, Jl + 3);
-            }
-        }
-        T* st = stage[warp];
-        store_vec<T, 18>(st + lane * 18, W);
-        __syncwarp();
-        // the warp's rows [c0, c0 + n) are contiguous in W
-        const int64_t c0 = base + warp * 32;
-        const int n = c0 < C ? static_cast<int>(C - c0 < 32 ? C - c0 : 32) : 0;
-        constexpr int kPer = 16 / sizeof(T); // scalars per 16-byte piece
-        for (int piece = lane; piece < n * 18 / kPer; piece += 32)
-        {
-            if constexpr (sizeof(T) == 8)
-                reinterpret_cast<double2*>(w + c0 * 18)[piece] = reinterpret_cast<const double2*>(st)[piece];
-            else
-                reinterpret_cast<float4*>(w + c0 * 18)[piece] = reinterpret_cast<const float4*>(st)[piece];
-        }
-        if constexpr (sizeof(T) == 4)
-        {
-            // a float row is 72 bytes: an odd row count leaves one 8-byte tail
-            if (lane == 0 && (n * 18) % kPer != 0)
-                reinterpret_cast<float2*>(w + c0 * 18)[(n * 18) / 2 - 1] =
-                    reinterpret_cast<const float2*>(st)[(n * 18) / 2 - 1];
-        }
-        __syncwarp();
     }
 }
 
@@ -829,6 +815,20 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
             cross_owner_kernel<<<grid_for(ne->L, 256, 4096), 256, 0, stream>>>(ne->cross_offsets, ne->L,
                                                                                ne->cross_eliminated);
             PM_LAUNCH_CHECK();
+            if (count > 0)
+            {
+                // slot map of the fused eliminated / cross pass (second half: scratch positions)
+                ne->observation_slots.ensure(size_t(2 * (count + 1)) * sizeof(int) + 256, stream,
+                                             "normal equations");
+                int* slots = static_cast<int*>(ne->observation_slots.ptr);
+                int* position = slots + (count + 1);
+                const CooView vo = coo_view(ne->by_eliminated_order);
+                order_position_kernel<<<grid_for(count, 256, 1 << 20), 256, 0, stream>>>(vo, position);
+                PM_LAUNCH_CHECK();
+                observation_slots_kernel<<<grid_for(crosses, 256, 1 << 20), 256, 0, stream>>>(
+                    crosses, ve.keys, static_cast<const int*>(ne->cross_runs.ptr), position, slots);
+                PM_LAUNCH_CHECK();
+            }
 
         }
         else
@@ -881,15 +881,10 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
         const unsigned grid = grid_for(ne->L, 128, 1 << 20);
         if (rows2)
         {
-            eliminated3_m2_kernel<T><<<grid, 128, 0, stream>>>(coo_view(ne->by_eliminated_order), jl, res, delta, hll,
-                                                               gl, first_bad);
+            eliminated_cross3_m2_kernel<T><<<grid, 128, 0, stream>>>(
+                coo_view(ne->by_eliminated_order), static_cast<const int*>(ne->observation_slots.ptr), jp, jl, res,
+                delta, hll, gl, w, first_bad);
             PM_LAUNCH_CHECK();
-            if (ne->cross_count > 0)
-            {
-                cross63_m2_kernel<T><<<grid_for(ne->cross_count, kCrossThreads, 1 << 20), kCrossThreads, 0, stream>>>(
-                    ne->cross_count, ve.keys, static_cast<const int*>(ne->cross_runs.ptr), jp, jl, res, delta, w);
-                PM_LAUNCH_CHECK();
-            }
         }
         else if (bp == 6 && bl == 3)
         {

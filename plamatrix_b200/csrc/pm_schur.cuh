@@ -33,6 +33,7 @@ struct pm_normal_equations
     pm_sparse_workspace* by_primary = nullptr;    // observations bucketed by primary block
     pm_sparse_workspace* by_eliminated_order = nullptr; // observations bucketed by eliminated block, input order
     pm::DeviceBuffer cross_runs;                  // C + 1: first by_eliminated position of every cross
+    pm::DeviceBuffer observation_slots;           // N: cross of every by_eliminated_order position (~c: not its first)
     pm::DeviceBuffer observation_copy;            // saved index arrays + zero column
     pm::DeviceBuffer weights;                     // Huber weight of every observation
     pm::DeviceBuffer observation_status;          // long long: first observation with a non-finite squared norm
