@@ -292,6 +292,14 @@ def run_ours(args):
         step(mixed64)
         step(plain)
     torch.cuda.synchronize()
+    # the upper-block assembly launch shape, timed on this system (FP64 products: the last warm-up
+    # step was plain) before the timed region; the fastest is kept for every arm
+    tune = ws.autotune_assembly(ne, repeats=3)
+    tune["shapes"] = ["%d streams x %d lanes" % ws.assembly_shape_info(k) for k in range(len(tune["shape_ms"]))]
+    tune["shape_ms"] = [round(t, 4) for t in tune["shape_ms"]]
+    tune["ms"] = round(tune["ms"], 4)
+    step(plain)
+    torch.cuda.synchronize()
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -393,6 +401,7 @@ def run_ours(args):
                      "traffic_source": ASSEMBLY_TRAFFIC_SOURCE,
                      "peak_kind": peak_kind, "algorithmic_bytes_per_launch": assembly_bytes},
         "schur_spmv_fp64": schur_spmv,
+        "assembly_autotune": tune,
         "gpu_launches": launches,
         "clocks": clock,
     }
@@ -721,6 +730,10 @@ def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
         return {"ms": round(job_ms, 3), "systems_per_s": round(systems / (job_ms * 1e-3), 1),
                 "converged": sum(conv), "fallbacks": sum(fb), "max_iterations": max(its),
                 "mean_iterations": round(float(np.mean(its)), 2),
+                "phases_ms_rank0": {"accumulation": round(t_acc, 3), "pattern": round(rep["pattern_ms"], 3),
+                                    "eliminated_inverse": round(rep["eliminated_inverse_ms"], 3),
+                                    "assembly": round(rep["assembly_ms"], 3), "pcg": round(rep["solve_ms"], 3),
+                                    "back_substitution": round(rep["back_substitution_ms"], 3)},
                 "time_to_solution_from_job_start_p50_ms": round(float(np.percentile(done_all, 50)), 3),
                 "time_to_solution_from_job_start_p99_ms": round(float(np.percentile(done_all, 99)), 3),
                 "own_duration_p50_ms": round(float(np.percentile(done_all, 50)), 3),

@@ -400,6 +400,23 @@ PM_API int pm_schur_solve_f32(pm_schur_workspace* workspace, pm_stream_t stream,
 PM_API int pm_schur_solve_f64(pm_schur_workspace* workspace, pm_stream_t stream, const pm_normal_equations* equations,
                               double damping, const pm_schur_options* options, double* primary_step_d,
                               double* eliminated_step_d, pm_schur_report* report);
+/* Assembly launch shapes (no counterpart in the reference, whose assembly launch is fixed,
+ * block_schur_device_assembly.cu:211-220).  The upper-block pass of the 6x3 assembly has
+ * pm_schur_assembly_shape_count() lane layouts ({pair streams, lanes per pair}); each sums every
+ * block in a fixed order of its own, so a shape gives repeatable values, and shapes differ from
+ * one another only by rounding.  pm_schur_autotune_assembly times every shape `repeats` times on
+ * the system `workspace` last solved (`equations` must be that system), keeps the fastest in the
+ * workspace and reports its index, its mean ms and (shape_ms_h, may be NULL, one per shape)
+ * every shape's mean ms.  It reassembles the system, so the workspace needs a new solve before
+ * its values are exported or multiplied.  Synchronous.  Systems outside the 6x3 path have one
+ * shape: *shape_h = 0, *best_ms_h = -1. */
+PM_API int pm_schur_assembly_shape_count(void);
+PM_API int pm_schur_assembly_shape_info(int shape, int* pair_streams_h, int* lanes_per_pair_h);
+PM_API int pm_schur_set_assembly_shape(pm_schur_workspace* workspace, int shape);
+PM_API int pm_schur_assembly_shape(const pm_schur_workspace* workspace, int* shape_h);
+PM_API int pm_schur_autotune_assembly(pm_schur_workspace* workspace, pm_stream_t stream,
+                                      const pm_normal_equations* equations, int repeats, int* shape_h,
+                                      double* best_ms_h, double* shape_ms_h);
 /* The last assembled reduced system in the reference's scalar-CSR layout
  * (block_schur_sparse_assembly.h:129-153, 262-272): row_offsets (n+1), col_indices and values
  * (nnz), reduced RHS (n, FP64) and block-Jacobi inverses (P*bp*bp, FP64).  Any may be NULL. */

@@ -92,6 +92,7 @@ struct pm_schur_workspace
     int64_t U = 0;
     int2* pairs = nullptr;         // E: {row-list entry of cross (l, p), row-list entry of cross (l, q)}, per block in ascending l
     void* vfactor = nullptr;       // C x 18 (Scalar): V = W_lp L_l^-T of every row-list entry (written by the diagonal pass)
+    int upper_shape = 0;           // launch shape of the upper-block pass (index into kUpperShapes)
     int* saved_offsets = nullptr;
     int* saved_primary = nullptr;
     int* saved_pc = nullptr;
@@ -646,12 +647,12 @@ __global__ void __launch_bounds__(kRowThreads) assemble_kernel(AssembleArgs<T> a
 // The pattern build lists, for every upper block (p, q), its cross pairs {cross (l, p),
 // cross (l, q), l} in ascending l; the crosses {cross, l} of every row are its row list, also
 // in ascending l.  Two numeric kernels: a CTA per row sums the diagonal block and RHS over the
-// row's crosses, and 16 lanes of a warp per upper block sum its pairs.  Lanes stride over their
+// row's crosses, and a group of lanes per upper block sums its pairs.  Lanes stride over their
 // crosses or pairs, keep their sums in registers (no float atomics) and combine them with fixed
-// shuffle trees.  An upper-block lane holds three of the six rows (8 pair streams x 2 row
-// halves).  Every sum runs in a fixed order: scheduling never changes a result.
-constexpr int kPairLanes = 16;  // lanes per block
-constexpr int kPairStreams = 8; // pair streams of an upper block (two lanes each)
+// shuffle trees.  The upper-block lane layout is a launch shape (UpperShape): pair streams x
+// lanes per pair, a lane holding three of the six rows (2 lanes per pair) or one 3x3 quadrant
+// (4 lanes per pair).  Every sum runs in a fixed order for a given shape: scheduling never
+// changes a result.
 
 // items of row-list entry j: one per later primary of its eliminated block
 __global__ void pair_count_kernel(int64_t P, const int* __restrict__ prim_offsets, const int* __restrict__ prim_cross,
@@ -949,17 +950,19 @@ __global__ void __launch_bounds__(kDiagThreads, 2) assemble_diag6_kernel(
     }
 }
 
-// Upper blocks, 16 lanes per block: lane g = 2 s + h walks the block's pairs s, s + 8, ... for
-// rows 3h .. 3h + 2 (S_pq -= V_lp V_lq^T; both factors come from the row-ordered V array, the
-// two lanes of a pair load the same V_lq row, which the load unit merges), then a fixed xor tree
-// over the 8 streams.
+// Upper blocks, STREAMS x SPLIT lanes per block: lane g = SPLIT s + k walks the block's pairs
+// s, s + STREAMS, ... (S_pq -= V_lp V_lq^T; both factors come from the row-ordered V array, and
+// the lanes of a pair load the same rows, which the load unit merges).  SPLIT 2: lane k holds
+// output rows 3k .. 3k + 2 against all six columns; SPLIT 4: lane k = 2 kr + kc holds the 3x3
+// quadrant (rows 3 kr.., columns 3 kc..), fewer registers per lane for more resident warps.  A
+// fixed xor tree over the streams ends it.
 constexpr int kUpperThreads = 256;
 
-template <typename AT>
+template <typename AT, int LANES, int FIRST>
 __device__ __forceinline__ AT stream_sum_as(AT v, unsigned gmask)
 {
 #pragma unroll
-    for (int o = 2; o < kPairLanes; o <<= 1)
+    for (int o = FIRST; o < LANES; o <<= 1)
         v += __shfl_xor_sync(gmask, v, o);
     return v;
 }
@@ -992,78 +995,87 @@ __device__ __forceinline__ void load_as(const VT* __restrict__ src, AT* q)
     }
 }
 
+// three V rows (elements 9 h .. 9 h + 8 of an 18-element row) as t[3][3], read as the aligned
+// run 8 h .. 8 h + 9
+template <typename VT, typename AT>
+__device__ __forceinline__ void load_v_half(const VT* __restrict__ row, int h, AT (&t)[3][3])
+{
+    AT a[10];
+    load_as<VT, 10, AT>(row + 8 * h, a);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            t[r][k] = h ? a[3 * r + k + 1] : a[3 * r + k];
+}
+
 // TO: type of the assembled values, TP: type of the coupling blocks (the normal equations'),
 // VT: type of the stored V factors, AT: type of the products and their sums
-template <typename TO, typename TP, typename VT, typename AT>
-__global__ void __launch_bounds__(kUpperThreads, 2) assemble_upper6_kernel(
+template <typename TO, typename TP, typename VT, typename AT, int STREAMS, int SPLIT>
+__global__ void __launch_bounds__(kUpperThreads, SPLIT == 4 ? 3 : 2) assemble_upper6_kernel(
     int64_t U, const int* __restrict__ upper_list, const int64_t* __restrict__ pair_offset,
     const int2* __restrict__ pairs, const int* __restrict__ transpose, const int* __restrict__ block_pc,
     const VT* __restrict__ vfactor, const TP* __restrict__ pcv, TO* __restrict__ S)
 {
-    const int g = threadIdx.x & (kPairLanes - 1);
-    const int s = g >> 1, h = g & 1;
-    const unsigned gmask = 0xffffu << (threadIdx.x & 16);
-    const int64_t groups = int64_t(gridDim.x) * (kUpperThreads / kPairLanes);
-    for (int64_t u = (int64_t(blockIdx.x) * kUpperThreads + threadIdx.x) / kPairLanes; u < U; u += groups)
+    constexpr int LANES = STREAMS * SPLIT;
+    constexpr int COLS = SPLIT == 2 ? 6 : 3; // output columns a lane holds
+    static_assert(LANES <= 32 && (LANES & (LANES - 1)) == 0, "lanes per block: a power of two up to a warp");
+    const int g = threadIdx.x & (LANES - 1);
+    const int s = g / SPLIT, k = g % SPLIT;
+    const int kr = SPLIT == 2 ? k : k >> 1, kc = SPLIT == 2 ? 0 : k & 1;
+    const unsigned gmask = LANES == 32 ? 0xffffffffu : ((1u << LANES) - 1u) << (threadIdx.x & 31 & ~(LANES - 1));
+    const int64_t groups = int64_t(gridDim.x) * (kUpperThreads / LANES);
+    for (int64_t u = (int64_t(blockIdx.x) * kUpperThreads + threadIdx.x) / LANES; u < U; u += groups)
     {
         const int64_t b = upper_list[u];
-        AT acc[3][6];
+        AT acc[3][COLS];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int c = 0; c < 6; ++c)
+            for (int c = 0; c < COLS; ++c)
                 acc[r][c] = AT(0);
         const int64_t k1 = pair_offset[b + 1];
-        int64_t k = pair_offset[b] + s;
-        int2 next = k < k1 ? pairs[k] : make_int2(0, 0);
-        while (k < k1)
+        int64_t kk = pair_offset[b] + s;
+        int2 next = kk < k1 ? pairs[kk] : make_int2(0, 0);
+        while (kk < k1)
         {
             const int2 cur = next;
-            k += kPairStreams;
-            if (k < k1)
-                next = pairs[k];
-            // this lane's three rows of V_lp (elements 9h .. 9h + 8, read as the aligned run
-            // 8h .. 8h + 9), then the six rows of V_lq in two halves of three (elements 0 .. 8 and
-            // 9 .. 17, read as the aligned runs 0 .. 9 and 8 .. 17) to keep fewer values live
-            AT a[10];
-            load_as<VT, 10, AT>(vfactor + int64_t(cur.x) * 18 + 8 * h, a);
+            kk += STREAMS;
+            if (kk < k1)
+                next = pairs[kk];
             AT tr[3][3];
+            load_v_half<VT, AT>(vfactor + int64_t(cur.x) * 18, kr, tr);
+            // V_lq three rows at a time (both halves for SPLIT 2) to keep fewer values live
 #pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int kk = 0; kk < 3; ++kk)
-                    tr[r][kk] = h ? a[3 * r + kk + 1] : a[3 * r + kk];
-#pragma unroll
-            for (int half = 0; half < 2; ++half)
+            for (int half = 0; half < COLS / 3; ++half)
             {
-                AT q[10];
-                load_as<VT, 10, AT>(vfactor + int64_t(cur.y) * 18 + 8 * half, q);
-                const int o = half; // run offset: element 9 * half sits at q[half]
+                AT tq[3][3];
+                load_v_half<VT, AT>(vfactor + int64_t(cur.y) * 18, SPLIT == 2 ? half : kc, tq);
 #pragma unroll
                 for (int r = 0; r < 3; ++r)
 #pragma unroll
                     for (int c = 0; c < 3; ++c)
-                        acc[r][3 * half + c] += tr[r][0] * q[o + 3 * c] + tr[r][1] * q[o + 3 * c + 1] +
-                                                tr[r][2] * q[o + 3 * c + 2];
+                        acc[r][3 * half + c] += tr[r][0] * tq[c][0] + tr[r][1] * tq[c][1] + tr[r][2] * tq[c][2];
             }
         }
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int c = 0; c < 6; ++c)
-                acc[r][c] = stream_sum_as<AT>(acc[r][c], gmask);
+            for (int c = 0; c < COLS; ++c)
+                acc[r][c] = stream_sum_as<AT, LANES, SPLIT>(acc[r][c], gmask);
         const int pc = block_pc[b];
-        TO* out = S + b * 36 + 18 * h;
+        TO* out = S + b * 36;
         TO* mirrored = S + int64_t(transpose[b]) * 36; // the lower block (q, p) holds the transpose
 #pragma unroll
-        for (int e = 0; e < 18; ++e)
+        for (int e = 0; e < 3 * COLS; ++e)
         {
-            if ((e & (kPairStreams - 1)) != s)
+            if ((e & (STREAMS - 1)) != s)
                 continue;
-            const AT base = pc >= 0 ? static_cast<AT>(pcv[int64_t(pc) * 36 + 18 * h + e]) : AT(0);
-            const TO value = static_cast<TO>(base - acc[e / 6][e % 6]);
-            out[e] = value;
-            mirrored[(e % 6) * 6 + 3 * h + e / 6] = value;
+            const int row = 3 * kr + e / COLS, col = 3 * kc + e % COLS;
+            const AT base = pc >= 0 ? static_cast<AT>(pcv[int64_t(pc) * 36 + row * 6 + col]) : AT(0);
+            const TO value = static_cast<TO>(base - acc[e / COLS][e % COLS]);
+            out[row * 6 + col] = value;
+            mirrored[col * 6 + row] = value;
         }
     }
 }
@@ -1836,8 +1848,8 @@ void build_pairs(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaStre
     };
     ws->scratch.ensure(pass1 + 512, stream, "SchurComplementSolverWorkspace");
     run_pass1();
-    // pass 2 scratch: items (block, row-list entry of (l, q)), pairs per block, lane masks, cursors,
-    // row-list position of every cross
+    // pass 2 scratch: items (block, row-list entry of (l, q)), row-list position of every cross,
+    // upper-block counts, pairs per block, lane masks, cursors
     Carver s2;
     s2.take<int>(E + 1);
     s2.take<int>(E + 1);
@@ -2051,6 +2063,39 @@ void build_pattern(pm_schur_workspace* ws, const pm_normal_equations* ne, cudaSt
     ws->pattern_builds += 1;
 }
 
+// Launch shapes of the upper-block pass: {pair streams, lanes per pair}.  Shape 0 is the default;
+// pm_schur_autotune_assembly times them all on the caller's system and keeps the fastest.
+struct UpperShape
+{
+    int streams, split;
+};
+constexpr UpperShape kUpperShapes[] = {{8, 2}, {4, 2}, {16, 2}, {4, 4}, {8, 4}};
+constexpr int kUpperShapeCount = sizeof(kUpperShapes) / sizeof(kUpperShapes[0]);
+
+template <typename TO, typename TP, typename VT, typename AT, int STREAMS, int SPLIT>
+void launch_upper_shape(pm_schur_workspace* ws, const int* block_pc, const VT* vf, const TP* pcv, TO* S,
+                        cudaStream_t stream)
+{
+    const unsigned grid = grid_for(std::max<int64_t>(ws->U, 1) * STREAMS * SPLIT, kUpperThreads);
+    assemble_upper6_kernel<TO, TP, VT, AT, STREAMS, SPLIT><<<grid, kUpperThreads, 0, stream>>>(
+        ws->U, ws->upper_list, ws->pair_offset, ws->pairs, ws->transpose, block_pc, vf, pcv, S);
+    PM_LAUNCH_CHECK();
+}
+
+template <typename TO, typename TP, typename VT, typename AT>
+void launch_upper(pm_schur_workspace* ws, const int* block_pc, const VT* vf, const TP* pcv, TO* S,
+                  cudaStream_t stream)
+{
+    switch (ws->upper_shape)
+    {
+    case 1: launch_upper_shape<TO, TP, VT, AT, 4, 2>(ws, block_pc, vf, pcv, S, stream); break;
+    case 2: launch_upper_shape<TO, TP, VT, AT, 16, 2>(ws, block_pc, vf, pcv, S, stream); break;
+    case 3: launch_upper_shape<TO, TP, VT, AT, 4, 4>(ws, block_pc, vf, pcv, S, stream); break;
+    case 4: launch_upper_shape<TO, TP, VT, AT, 8, 4>(ws, block_pc, vf, pcv, S, stream); break;
+    default: launch_upper_shape<TO, TP, VT, AT, 8, 2>(ws, block_pc, vf, pcv, S, stream); break;
+    }
+}
+
 template <typename T>
 void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, double lambda, double min_diag,
                      cudaStream_t stream, bool fp32_products = false)
@@ -2091,7 +2136,6 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
     };
     if (ws->paired)
     {
-        const unsigned ugrid = grid_for(std::max<int64_t>(ws->U, 1) * kPairLanes, kUpperThreads);
         if (fp32_products)
         {
             // FP32 products: V stored in FP32, upper blocks formed and summed in FP32 into S32;
@@ -2102,9 +2146,7 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
                 a.P, ws->prim_offsets, ws->row_entries, a.w, ws->hinv, a.hpp, a.gp, a.lambda, a.min_diag,
                 a.diag_pos, a.S, a.rhs, vf, ws->S32);
             PM_LAUNCH_CHECK();
-            assemble_upper6_kernel<float, T, float, float><<<ugrid, kUpperThreads, 0, stream>>>(
-                ws->U, ws->upper_list, ws->pair_offset, ws->pairs, ws->transpose, a.block_pc, vf, a.pcv, ws->S32);
-            PM_LAUNCH_CHECK();
+            launch_upper<float, T, float, float>(ws, a.block_pc, vf, a.pcv, ws->S32, stream);
         }
         else
         {
@@ -2114,9 +2156,7 @@ void launch_assembly(pm_schur_workspace* ws, const pm_normal_equations* ne, doub
                 a.diag_pos, a.S, a.rhs, vf, nullptr);
             PM_LAUNCH_CHECK();
             // every upper block, also those whose only terms are primary-primary couplings
-            assemble_upper6_kernel<T, T, T, double><<<ugrid, kUpperThreads, 0, stream>>>(
-                ws->U, ws->upper_list, ws->pair_offset, ws->pairs, ws->transpose, a.block_pc, vf, a.pcv, a.S);
-            PM_LAUNCH_CHECK();
+            launch_upper<T, T, T, double>(ws, a.block_pc, vf, a.pcv, a.S, stream);
         }
         ws->s32_only = fp32_products;
         diag_inverse_kernel<T, 6><<<grid_for(a.P, 64, 1 << 16), 64, 0, stream>>>(a.P, a.diag_pos, a.S, a.minv,
@@ -3242,6 +3282,58 @@ void export_system(pm_schur_workspace* ws, cudaStream_t stream, int64_t* ro, int
         PM_CUDA(cudaMemcpyAsync(minv, ws->minv, ws->P * bpp * sizeof(double), cudaMemcpyDeviceToDevice, stream));
 }
 
+template <typename T>
+void autotune_assembly(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_equations* ne, int repeats,
+                       int* shape, double* best_ms, double* shape_ms)
+{
+    if (!ws || !ne || !shape || !best_ms)
+        fail(PM_INVALID_ARGUMENT, "assembly autotune arguments must be non-null");
+    if (repeats <= 0)
+        fail(PM_INVALID_ARGUMENT, "assembly autotune needs at least one repeat");
+    if (!ws->assembled || ws->last_ne != ne || ws->last_version != ne->topology_version)
+        fail(PM_LOGIC_ERROR, "assembly autotune needs the workspace to have solved these normal equations");
+    if (!ws->paired)
+    {
+        *shape = 0;
+        *best_ms = -1.0;
+        if (shape_ms)
+            shape_ms[0] = -1.0;
+        return;
+    }
+    const bool fp32 = ws->s32_only;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    PM_CUDA(cudaEventCreate(&e0));
+    PM_CUDA(cudaEventCreate(&e1));
+    double best = 0.0;
+    int chosen = -1;
+    for (int k = 0; k < kUpperShapeCount; ++k)
+    {
+        ws->upper_shape = k;
+        launch_assembly<T>(ws, ne, ws->damping, ws->min_diag, stream, fp32); // warm-up
+        PM_CUDA(cudaEventRecord(e0, stream));
+        for (int r = 0; r < repeats; ++r)
+            launch_assembly<T>(ws, ne, ws->damping, ws->min_diag, stream, fp32);
+        PM_CUDA(cudaEventRecord(e1, stream));
+        PM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        const double mean = double(ms) / repeats;
+        if (shape_ms)
+            shape_ms[k] = mean;
+        if (chosen < 0 || mean < best)
+        {
+            best = mean;
+            chosen = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ws->upper_shape = chosen;
+    ws->assembled = false; // values and their FP32 copies now belong to the last shape timed
+    *shape = chosen;
+    *best_ms = best;
+}
+
 } // namespace
 } // namespace pm
 
@@ -3276,6 +3368,53 @@ int pm_schur_workspace_close(pm_schur_workspace* ws)
 }
 
 int64_t pm_schur_pattern_build_count(const pm_schur_workspace* ws) { return ws ? ws->pattern_builds : 0; }
+
+int pm_schur_assembly_shape_count(void) { return pm::kUpperShapeCount; }
+
+int pm_schur_assembly_shape_info(int shape, int* streams, int* split)
+{
+    return pm::guarded([&] {
+        if (!streams || !split)
+            pm::fail(PM_INVALID_ARGUMENT, "shape outputs must be non-null");
+        if (shape < 0 || shape >= pm::kUpperShapeCount)
+            pm::fail(PM_INVALID_ARGUMENT, "assembly shape out of range");
+        *streams = pm::kUpperShapes[shape].streams;
+        *split = pm::kUpperShapes[shape].split;
+    });
+}
+
+int pm_schur_set_assembly_shape(pm_schur_workspace* ws, int shape)
+{
+    return pm::guarded([&] {
+        if (!ws)
+            pm::fail(PM_INVALID_ARGUMENT, "workspace is null");
+        if (shape < 0 || shape >= pm::kUpperShapeCount)
+            pm::fail(PM_INVALID_ARGUMENT, "assembly shape out of range");
+        ws->upper_shape = shape;
+    });
+}
+
+int pm_schur_assembly_shape(const pm_schur_workspace* ws, int* shape)
+{
+    return pm::guarded([&] {
+        if (!ws || !shape)
+            pm::fail(PM_INVALID_ARGUMENT, "workspace and shape output must be non-null");
+        *shape = ws->upper_shape;
+    });
+}
+
+int pm_schur_autotune_assembly(pm_schur_workspace* ws, pm_stream_t stream, const pm_normal_equations* ne, int repeats,
+                               int* shape, double* best_ms, double* shape_ms)
+{
+    return pm::guarded([&] {
+        if (!ws)
+            pm::fail(PM_INVALID_ARGUMENT, "workspace is null");
+        if (ws->value_size == 4)
+            pm::autotune_assembly<float>(ws, static_cast<cudaStream_t>(stream), ne, repeats, shape, best_ms, shape_ms);
+        else
+            pm::autotune_assembly<double>(ws, static_cast<cudaStream_t>(stream), ne, repeats, shape, best_ms, shape_ms);
+    });
+}
 
 int pm_schur_dims(const pm_schur_workspace* ws, int64_t* dimension, int64_t* nnz, int64_t* blocks)
 {

@@ -52,6 +52,11 @@ N.register("pm_schur_workspace_close", [vp])
 N.register("pm_schur_pattern_build_count", [vp], C.c_int64)
 N.register("pm_schur_dims", [vp, vp, vp, vp])
 N.register("pm_schur_spmv_f32", [vp, vp, vp, vp])
+N.register("pm_schur_assembly_shape_count", [], C.c_int)
+N.register("pm_schur_set_assembly_shape", [vp, C.c_int])
+N.register("pm_schur_assembly_shape_info", [C.c_int, vp, vp])
+N.register("pm_schur_assembly_shape", [vp, vp])
+N.register("pm_schur_autotune_assembly", [vp, vp, vp, C.c_int, vp, vp, vp])
 N.register("pm_schur_spmv_f64", [vp, vp, vp, vp])
 
 PRECISION = {"native": 0, "mixed": 1, "mixed_fp32_assembly": 2}
@@ -198,6 +203,38 @@ class SchurComplementSolverWorkspace:
         n, nnz, b = C.c_int64(), C.c_int64(), C.c_int64()
         N.call("pm_schur_dims", self._h, C.byref(n), C.byref(nnz), C.byref(b))
         return n.value, nnz.value, b.value
+
+    @staticmethod
+    def assembly_shape_count() -> int:
+        """Number of launch shapes of the upper-block assembly pass."""
+        return int(N.load().pm_schur_assembly_shape_count())
+
+    @staticmethod
+    def assembly_shape_info(shape: int) -> tuple:
+        """(pair streams, lanes per pair) of an assembly launch shape."""
+        streams, split = C.c_int(), C.c_int()
+        N.call("pm_schur_assembly_shape_info", int(shape), C.byref(streams), C.byref(split))
+        return streams.value, split.value
+
+    @property
+    def assembly_shape(self) -> int:
+        shape = C.c_int()
+        N.call("pm_schur_assembly_shape", self._h, C.byref(shape))
+        return shape.value
+
+    @assembly_shape.setter
+    def assembly_shape(self, shape: int) -> None:
+        N.call("pm_schur_set_assembly_shape", self._h, int(shape))
+
+    def autotune_assembly(self, equations, repeats: int = 3, stream=None) -> dict:
+        """Time every assembly launch shape on the system this workspace last solved (`equations`),
+        keep the fastest; the workspace then needs a new solve before export / spmv."""
+        count = self.assembly_shape_count()
+        shape, best = C.c_int(), C.c_double()
+        per = (C.c_double * count)()
+        N.call("pm_schur_autotune_assembly", self._h, _stream_handle(stream), equations.handle, int(repeats),
+               C.byref(shape), C.byref(best), per)
+        return {"shape": shape.value, "ms": best.value, "shape_ms": [per[k] for k in range(count)]}
 
     def spmv(self, x: torch.Tensor, out: torch.Tensor | None = None, stream=None) -> torch.Tensor:
         """y = S x on the last assembled reduced system."""

@@ -69,3 +69,19 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
         N.load()
     with pytest.raises(ImportError, match="no CPU fallback"):
         SC.SchurComplementSolverWorkspace()
+
+
+def test_assembly_shape_table(lib):
+    """The assembly launch shapes are host-side data: readable without a GPU."""
+    count = lib.pm_schur_assembly_shape_count()
+    assert count >= 2
+    seen = set()
+    for k in range(count):
+        streams, split = C.c_int(), C.c_int()
+        assert lib.pm_schur_assembly_shape_info(k, C.byref(streams), C.byref(split)) == 0
+        assert split.value in (2, 4) and streams.value * split.value <= 32
+        seen.add((streams.value, split.value))
+    assert len(seen) == count
+    streams, split = C.c_int(), C.c_int()
+    assert lib.pm_schur_assembly_shape_info(count, C.byref(streams), C.byref(split)) != 0
+    assert lib.pm_schur_set_assembly_shape(None, 0) != 0

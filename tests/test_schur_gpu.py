@@ -625,3 +625,69 @@ def test_empty_observations_give_zero_normal_equations():
     assert ne.counts()[0] == 0
     assert not got["primary_diagonal"].any() and not got["eliminated_diagonal"].any()
     assert got["adjacency_offsets"].tolist() == [0, 0, 0, 0, 0]
+
+
+@pytest.mark.parametrize("precision", ["native", "mixed_fp32_assembly"])
+def test_every_assembly_shape_matches_reference(checkers, precision):
+    """Each launch shape of the upper-block assembly pass (pair streams x lanes per pair) on a
+    windowed system against the reference's reduced system: pattern bit-exact, values within
+    rounding (FP64: 1e-12 of the largest entry; FP32 products: 1e-6), repeatable bit for bit per
+    shape, and the steps within 1e-8 of each other across shapes."""
+    prob = W.large_bundle(seed=17, P=200, L=8000)
+    orc = checkers.normal_equations_from_observations(prob)
+    ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+    ne = _device_from_observations(prob)
+    opts = SC.SchurComplementSolverOptions(max_iterations=200, relative_tolerance=1e-10, precision=precision)
+    shapes = SC.SchurComplementSolverWorkspace.assembly_shape_count()
+    assert shapes >= 2
+    tol = 1e-12 if precision == "native" else 1e-6
+    steps = []
+    for shape in range(shapes):
+        ws = SC.SchurComplementSolverWorkspace()
+        ws.assembly_shape = shape
+        assert ws.assembly_shape == shape
+        dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+        assert rep["converged"], (shape, rep["message"])
+        sysd = ws.export()
+        assert np.array_equal(host(sysd["row_offsets"]), ro) and np.array_equal(host(sysd["col_indices"]), ci)
+        v = host(sysd["values"])
+        assert np.abs(v - vals).max() <= tol * np.abs(vals).max(), shape
+        dp2, dl2, _ = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+        assert torch.equal(dp, dp2) and torch.equal(dl, dl2), shape
+        assert np.array_equal(host(ws.export()["values"]), v), shape
+        steps.append(host(dp))
+    for s in steps[1:]:
+        assert np.linalg.norm(s - steps[0]) <= 1e-8 * np.linalg.norm(steps[0])
+    with pytest.raises(N.InvalidArgument):
+        SC.SchurComplementSolverWorkspace().assembly_shape = shapes
+
+
+def test_assembly_autotune_keeps_the_fastest_shape(checkers):
+    """The autotuner times every shape on the solved system, keeps the fastest, leaves the
+    workspace needing a new solve, and that solve matches the reference."""
+    prob = W.large_bundle(seed=19, P=200, L=8000)
+    orc = checkers.normal_equations_from_observations(prob)
+    dp_ref, dl_ref, rep_ref = orc.solve(1e-3, relative_tolerance=1e-8, max_iterations=200)
+    ne = _device_from_observations(prob)
+    ws = SC.SchurComplementSolverWorkspace()
+    other = SC.DeviceNormalEquations(3, 4, 6, 3)
+    with pytest.raises(N.LogicError):
+        ws.autotune_assembly(ne)  # nothing solved yet
+    opts = SC.SchurComplementSolverOptions(max_iterations=200)
+    SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+    with pytest.raises(N.LogicError):
+        ws.autotune_assembly(other)  # not the system last solved
+    with pytest.raises(N.InvalidArgument):
+        ws.autotune_assembly(ne, repeats=0)
+    tuned = ws.autotune_assembly(ne, repeats=2)
+    count = SC.SchurComplementSolverWorkspace.assembly_shape_count()
+    assert 0 <= tuned["shape"] < count and len(tuned["shape_ms"]) == count
+    assert all(t > 0 for t in tuned["shape_ms"])
+    assert tuned["ms"] == min(tuned["shape_ms"])
+    assert ws.assembly_shape == tuned["shape"]
+    with pytest.raises(N.LogicError):
+        ws.export()  # reassembled by the autotuner: a new solve comes first
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+    assert rep["converged"] and rep["pattern_reused"]
+    assert np.linalg.norm(host(dp) - dp_ref) <= 1e-6 * np.linalg.norm(dp_ref)
+    assert np.linalg.norm(host(dl) - dl_ref) <= 1e-6 * np.linalg.norm(dl_ref)
