@@ -740,9 +740,14 @@ def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
                 "own_duration_p99_ms": round(float(np.percentile(done_all, 99)), 3)}
 
     res["batched_plain"] = run_batched(opts)
+    # mixed precision: FP64 assembly, iterations on the FP32 values and blocks, FP64 checks
+    res["batched_mixed"] = run_batched(SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=TOL,
+                                                                       precision="mixed"))
     if net is not None:
         res["batched_learned"] = run_batched(SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=TOL,
                                                                              learned=net))
+        res["batched_learned_mixed"] = run_batched(SC.SchurComplementSolverOptions(
+            max_iterations=500, relative_tolerance=TOL, learned=net, precision="mixed"))
     # per-system launch loop on the same shard (each system with its own normal equations and
     # workspace, warmed once); its own duration and its time from the start of the loop
     own, from_start, t = [], [], 0.0

@@ -440,7 +440,12 @@ PM_API int pm_schur_spmv_f64(pm_schur_workspace* workspace, pm_stream_t stream, 
  * beta and convergence on the device, with its iteration captured in a CUDA graph that is
  * replayed until no system is active.  Every system converges to its own tolerance
  * (options->relative_tolerance of its own initial residual).  A system whose learned PCG
- * stagnates restarts from its iterate with plain block Jacobi.  FP64 vectors and dots. */
+ * stagnates restarts from its iterate with plain block Jacobi.  FP64 vectors and dots.  With
+ * options->precision PM_PRECISION_MIXED (or MIXED_FP32_ASSEMBLY, treated the same here) the
+ * values are assembled in FP64 and the iterations read FP32 copies of the values and of the
+ * preconditioner blocks; every system that converges is checked against its FP64 true residual
+ * and iterates on from it when the check misses (up to options->max_refinements checks, 8 when
+ * 0); report->mixed_precision_used and report->refinement_steps (checks run) describe it. */
 typedef struct
 {
     int converged;

@@ -514,9 +514,13 @@ __global__ void __launch_bounds__(128) primary_accumulate6_kernel(CooView v, int
 #pragma unroll
         for (int k = 0; k < W; ++k)
             sum[k] = T(0);
+        // the next observation's index is loaded one step ahead
+        uint64_t next = lo + lane < hi ? v.keys[lo + lane] : 0;
         for (int q = lo + lane; q < hi; q += 32)
         {
-            const int64_t i = static_cast<uint32_t>(v.keys[q]);
+            const int64_t i = static_cast<uint32_t>(next);
+            if (q + 32 < hi)
+                next = v.keys[q + 32];
             if constexpr (M == 2)
             {
                 T r[2], J[12];

@@ -2297,11 +2297,11 @@ __global__ void batch_alpha_kernel(int64_t systems, const int* __restrict__ sys_
 
 // x += alpha p, r -= alpha q (Mode 0), or r = b - q, x kept (Mode 1, restarting systems);
 // then z = Minv r and the row sums of r.z and r.r (p = z on restart)
-template <int Mode>
+template <int Mode, typename PM = double>
 __global__ void batch_update_kernel(int64_t P, const int* __restrict__ row_sys, const BatchState* __restrict__ bs,
                                     double* __restrict__ x, double* __restrict__ p_vec, const double* __restrict__ q,
                                     const double* __restrict__ b, double* __restrict__ r, double* __restrict__ z,
-                                    const double* __restrict__ minv, double* __restrict__ row_rz,
+                                    const PM* __restrict__ minv, double* __restrict__ row_rz,
                                     double* __restrict__ row_rr)
 {
     for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
@@ -2328,13 +2328,13 @@ __global__ void batch_update_kernel(int64_t P, const int* __restrict__ row_sys, 
                 r[p * 6 + k] = rr[k];
             }
         }
-        const double* m = minv + p * 36;
+        const PM* m = minv + p * 36;
         double rz = 0.0, r2 = 0.0;
         for (int k = 0; k < 6; ++k)
         {
             double zk = 0.0;
             for (int c = 0; c < 6; ++c)
-                zk += m[k * 6 + c] * rr[c];
+                zk += static_cast<double>(m[k * 6 + c]) * rr[c];
             z[p * 6 + k] = zk;
             if (Mode == 1)
                 p_vec[p * 6 + k] = zk;
@@ -2461,7 +2461,7 @@ __global__ void batch_check_kernel(int64_t P, const int* __restrict__ row_ptr, c
 template <typename T>
 __global__ void batch_fallback_kernel(int64_t P, const int* __restrict__ row_sys, BatchState* __restrict__ bs,
                                       const int* __restrict__ diag_pos, const T* __restrict__ S,
-                                      double* __restrict__ minv, double* __restrict__ x)
+                                      double* __restrict__ minv, float* __restrict__ minv32, double* __restrict__ x)
 {
     for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
     {
@@ -2481,7 +2481,23 @@ __global__ void batch_fallback_kernel(int64_t P, const int* __restrict__ row_sys
                 inv[k] = 0.0;
         for (int k = 0; k < 36; ++k)
             minv[p * 36 + k] = inv[k];
+        if (minv32)
+            for (int k = 0; k < 36; ++k)
+                minv32[p * 36 + k] = static_cast<float>(inv[k]);
     }
+}
+
+// mixed precision: every system that converged on the FP32 operator restarts from its iterate
+// for an FP64 check (true residual b - S x with the FP64 values, tolerance and iteration count
+// kept); it stays converged only if that residual meets its tolerance
+__global__ void batch_verify_kernel(int64_t systems, BatchState* __restrict__ bs)
+{
+    for (int64_t s = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < systems; s += int64_t(gridDim.x) * blockDim.x)
+        if (bs[s].converged)
+        {
+            bs[s].converged = 0;
+            bs[s].restart = 2;
+        }
 }
 
 __global__ void batch_flag_restart_kernel(int64_t systems, BatchState* __restrict__ bs, int* __restrict__ fallen)
@@ -2621,7 +2637,7 @@ struct BatchSpec
 // initial guesses.  Fills the per-system reports and the summary in `rep`.
 template <typename M>
 void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& spec, const pm_schur_options* o,
-                 bool learned, int window, double* x, pm_schur_report* rep)
+                 bool learned, bool mixed, int window, double* x, pm_schur_report* rep)
 {
     const int64_t P = ws->P, NS = spec.systems;
     const M* S = static_cast<const M*>(ws->S);
@@ -2709,11 +2725,21 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
     PM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < kChunk; ++k)
     {
-        batch_spmv_kernel<M, 0><<<rgrid, kVecBlock, 0, stream>>>(P, ws->block_row_ptr, ws->block_col, S, pv, q, row_dot,
-                                                                 row_sys, bs);
+        // mixed precision: the iterations read the FP32 values and preconditioner blocks (FP64
+        // vectors, dots, alpha and beta); every (re)start reads the FP64 ones
+        if (mixed)
+            batch_spmv_kernel<float, 0><<<rgrid, kVecBlock, 0, stream>>>(P, ws->block_row_ptr, ws->block_col, ws->S32,
+                                                                         pv, q, row_dot, row_sys, bs);
+        else
+            batch_spmv_kernel<M, 0><<<rgrid, kVecBlock, 0, stream>>>(P, ws->block_row_ptr, ws->block_col, S, pv, q,
+                                                                     row_dot, row_sys, bs);
         batch_alpha_kernel<<<sgrid, 128, 0, stream>>>(NS, sys_row, row_dot, bs);
-        batch_update_kernel<0><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, x, pv, q, ws->rhs, r, z, ws->minv, row_rz,
-                                                          row_rr);
+        if (mixed)
+            batch_update_kernel<0, float><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, x, pv, q, ws->rhs, r, z,
+                                                                     ws->minv32, row_rz, row_rr);
+        else
+            batch_update_kernel<0><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, x, pv, q, ws->rhs, r, z, ws->minv, row_rz,
+                                                              row_rr);
         cudaMemsetAsync(flags, 0, sizeof(int), stream);
         batch_beta_kernel<0><<<sgrid, 128, 0, stream>>>(NS, sys_row, row_rz, row_rr, bs, maxit,
                                                         learned ? window : 0, rel, abs_tol, rule, flags);
@@ -2738,7 +2764,7 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
                 break;
         }
     };
-    int issued = 0;
+    int issued = 0, checks = 0;
     try
     {
         start();
@@ -2746,13 +2772,31 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
         if (learned)
         {
             // systems whose learned PCG stagnated restart from their iterate with block Jacobi
-            batch_fallback_kernel<M><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, ws->diag_pos, S, ws->minv, x);
+            batch_fallback_kernel<M><<<pgrid, 128, 0, stream>>>(P, row_sys, bs, ws->diag_pos, S, ws->minv,
+                                                                mixed ? ws->minv32 : nullptr, x);
             PM_LAUNCH_CHECK();
             batch_flag_restart_kernel<<<grid_for(NS, 128, 4096), 128, 0, stream>>>(NS, bs, fallen);
             PM_LAUNCH_CHECK();
             start();
             int again = 0;
             run(again);
+        }
+        // mixed precision: FP64 checks of the systems that converged on the FP32 operator; those
+        // that miss their tolerance iterate on from the FP64 residual (iterative refinement)
+        const int max_checks = o->max_refinements > 0 ? o->max_refinements : 8;
+        while (mixed && checks < max_checks)
+        {
+            batch_verify_kernel<<<grid_for(NS, 128, 4096), 128, 0, stream>>>(NS, bs);
+            PM_LAUNCH_CHECK();
+            start();
+            ++checks;
+            PM_CUDA(cudaMemcpyAsync(host_count, flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            PM_CUDA(cudaEventRecord(ws->sync_event, stream));
+            PM_CUDA(cudaEventSynchronize(ws->sync_event));
+            if (*host_count == 0)
+                break;
+            int more = 0;
+            run(more);
         }
     }
     catch (...)
@@ -2790,6 +2834,8 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
     }
     rep->converged = all;
     rep->iterations = most;
+    rep->mixed_precision_used = mixed ? 1 : 0;
+    rep->refinement_steps = checks;
     rep->initial_residual_norm = std::sqrt(std::max(0.0, r0));
     rep->final_residual_norm = std::sqrt(std::max(0.0, r1));
     if (!all)
@@ -2855,7 +2901,11 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     // FP32 assembly products (6x6 primary / 3x3 eliminated blocks, double normal equations)
     const bool mixed32 = o->precision == PM_PRECISION_MIXED_FP32_ASSEMBLY && sizeof(T) == 8 && !batch && !dense &&
                          bp == 6 && bl == 3;
-    const bool mixed = (o->precision == PM_PRECISION_MIXED || mixed32) && sizeof(T) == 8 && !batch && !dense;
+    // batched solves: FP64 assembly with FP32 iterations for either mixed mode (their FP64 checks
+    // read the assembled FP64 values)
+    const bool mixed = (o->precision == PM_PRECISION_MIXED || mixed32 ||
+                        (batch && o->precision == PM_PRECISION_MIXED_FP32_ASSEMBLY)) &&
+                       sizeof(T) == 8 && !dense;
     if (batch)
     {
         if (sizeof(T) != 8 || bp != 6)
@@ -3082,7 +3132,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     }
     else if (batch)
     {
-        batched_pcg<T>(ws, stream, *batch, o, learned, window, reinterpret_cast<double*>(dp), rep);
+        batched_pcg<T>(ws, stream, *batch, o, learned, mixed, window, reinterpret_cast<double*>(dp), rep);
         for (int64_t s = 0; s < batch->systems; ++s)
             rep->learned_fallback = rep->learned_fallback || batch->out[s].learned_fallback;
     }

@@ -100,3 +100,40 @@ def test_batched_learned_with_per_system_fallback():
     assert plain["converged"], plain["message"]
     assert rep["converged"], [(s["converged"], s["iterations"], s["learned_fallback"], s["breakdown"]) for s in per]
     assert torch.linalg.norm(dp - plain_dp) <= 1e-6 * torch.linalg.norm(plain_dp)
+
+
+@pytest.mark.parametrize("learned", [False, True])
+def test_batched_mixed_precision_meets_the_fp64_tolerance_per_system(checkers, learned):
+    """Mixed precision in the batched solve: FP64 assembly, iterations on the FP32 values and
+    preconditioner blocks (FP64 vectors and dots), then an FP64 true-residual check of every system
+    that converged, which iterates on from the FP64 residual when the check misses.  Every system
+    meets its tolerance on the reference's FP64 reduced system, and its steps agree with the
+    oracle's per-system solve within 1e-6."""
+    sizes = W.uneven_family_sizes(512)
+    picks = [0, 5, 150, 400]
+    probs = []
+    for i in picks:
+        P, L = sizes[i]
+        d = W.uneven_family_system(i, P, L)
+        probs.append({k: (v.cpu().numpy() if torch.is_tensor(v) else v) for k, v in d.items()})
+    union = SC.pack_observation_systems(probs)
+    ne = _ne(union)
+    net = SC.LearnedPreconditioner(seed=5) if learned else None
+    opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-8, precision="mixed",
+                                           learned=net)
+    dp, dl, rep, per = SC.solve_batched_schur_complement(ne, 1e-3, union["primary_offsets"], opts)
+    assert rep["converged"], rep["message"]
+    assert rep["mixed_precision_used"] and rep["refinement_steps"] >= 1
+    P_off, L_off = union["primary_offsets"], union["eliminated_offsets"]
+    dp_h, dl_h = dp.cpu().numpy(), dl.cpu().numpy()
+    for s, prob in enumerate(probs):
+        orc = checkers.normal_equations_from_observations(prob)
+        ref_dp, ref_dl, ref = orc.solve(1e-3, relative_tolerance=1e-8, max_iterations=500)
+        assert ref["converged"] and per[s]["converged"]
+        a = dp_h[6 * P_off[s]:6 * P_off[s + 1]]
+        ro, ci, vals, rhs = orc.schur_system(1e-3, with_preconditioner=False)
+        res = rhs - np.array([vals[ro[i]:ro[i + 1]] @ a[ci[ro[i]:ro[i + 1]]] for i in range(len(ro) - 1)])
+        assert np.linalg.norm(res) <= 1e-8 * 1.01 * np.linalg.norm(rhs), s
+        assert np.linalg.norm(a - ref_dp) <= 1e-6 * np.linalg.norm(ref_dp)
+        b = dl_h[3 * L_off[s]:3 * L_off[s + 1]]
+        assert np.linalg.norm(b - ref_dl) <= 1e-6 * np.linalg.norm(ref_dl)
