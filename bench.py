@@ -705,7 +705,11 @@ def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
     def run_batched(options):
         ne_u = SC.DeviceNormalEquations(int(P_off[-1]), int(L_off[-1]), 6, 3)
         ws_u = SC.SchurComplementSolverWorkspace()
+        tune = None
         for k in range(2):  # the first call builds the topology and the pattern
+            if k == 1:
+                # the union's assembly launch shape, timed on the system the first call solved
+                tune = ws_u.autotune_assembly(ne_u, repeats=2)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
@@ -728,6 +732,8 @@ def batched_leg(torch, SC, W, net, systems=BATCH_SYSTEMS):
         if rank != 0:
             return None
         return {"ms": round(job_ms, 3), "systems_per_s": round(systems / (job_ms * 1e-3), 1),
+                "assembly_shape_rank0": "%d streams x %d lanes" % ws_u.assembly_shape_info(tune["shape"]),
+                "assembly_shape_ms_rank0": [round(t, 3) for t in tune["shape_ms"]],
                 "converged": sum(conv), "fallbacks": sum(fb), "max_iterations": max(its),
                 "mean_iterations": round(float(np.mean(its)), 2),
                 "phases_ms_rank0": {"accumulation": round(t_acc, 3), "pattern": round(rep["pattern_ms"], 3),

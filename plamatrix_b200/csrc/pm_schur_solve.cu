@@ -2069,7 +2069,7 @@ struct UpperShape
 {
     int streams, split;
 };
-constexpr UpperShape kUpperShapes[] = {{8, 2}, {4, 2}, {16, 2}, {4, 4}, {8, 4}};
+constexpr UpperShape kUpperShapes[] = {{8, 2}, {4, 2}, {16, 2}, {4, 4}, {8, 4}, {2, 2}, {1, 2}};
 constexpr int kUpperShapeCount = sizeof(kUpperShapes) / sizeof(kUpperShapes[0]);
 
 template <typename TO, typename TP, typename VT, typename AT, int STREAMS, int SPLIT>
@@ -2092,6 +2092,8 @@ void launch_upper(pm_schur_workspace* ws, const int* block_pc, const VT* vf, con
     case 2: launch_upper_shape<TO, TP, VT, AT, 16, 2>(ws, block_pc, vf, pcv, S, stream); break;
     case 3: launch_upper_shape<TO, TP, VT, AT, 4, 4>(ws, block_pc, vf, pcv, S, stream); break;
     case 4: launch_upper_shape<TO, TP, VT, AT, 8, 4>(ws, block_pc, vf, pcv, S, stream); break;
+    case 5: launch_upper_shape<TO, TP, VT, AT, 2, 2>(ws, block_pc, vf, pcv, S, stream); break;
+    case 6: launch_upper_shape<TO, TP, VT, AT, 1, 2>(ws, block_pc, vf, pcv, S, stream); break;
     default: launch_upper_shape<TO, TP, VT, AT, 8, 2>(ws, block_pc, vf, pcv, S, stream); break;
     }
 }
