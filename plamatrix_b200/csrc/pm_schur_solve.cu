@@ -1267,7 +1267,8 @@ __global__ void __launch_bounds__(kVecBlock) bsr_spmv_kernel(int64_t P, int bp, 
         if (p < P && lane < bp)
         {
             double v = 0.0;
-            for (int r = 0; r < bp; ++r)
+#pragma unroll
+            for (int r = 0; r < (BP > 0 ? BP : 16); ++r)
                 v = lane == r ? out[r] : v;
             y[p * bp + lane] = static_cast<V>(v);
         }
@@ -1297,7 +1298,8 @@ __global__ void __launch_bounds__(kVecBlock) pcg_bsr_kernel(int64_t P, int bp, c
         if (p < P && lane < bp)
         {
             double v = 0.0;
-            for (int r = 0; r < bp; ++r)
+#pragma unroll
+            for (int r = 0; r < (BP > 0 ? BP : 16); ++r)
                 v = lane == r ? out[r] : v;
             const V qv = static_cast<V>(v);
             q[p * bp + lane] = qv;
