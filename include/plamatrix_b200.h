@@ -437,8 +437,9 @@ PM_API int pm_schur_spmv_f64(pm_schur_workspace* workspace, pm_stream_t stream, 
  * [offsets[s], offsets[s+1]) and its own eliminated blocks; no observation couples two
  * systems).  Pattern, assembly, eliminated inverses and back-substitution run once over the
  * union; the block-Jacobi (or learned, options->learned) PCG keeps per-system dots, alpha,
- * beta and convergence on the device, with its iteration captured in a CUDA graph that is
- * replayed until no system is active.  Every system converges to its own tolerance
+ * beta and convergence on the device; its iterations run as one CUDA graph whose 'while'
+ * conditional node repeats a captured chunk of iterations until no system is active, decided
+ * on the device (no host check between chunks).  Every system converges to its own tolerance
  * (options->relative_tolerance of its own initial residual).  A system whose learned PCG
  * stagnates restarts from its iterate with plain block Jacobi.  FP64 vectors and dots.  With
  * options->precision PM_PRECISION_MIXED (or MIXED_FP32_ASSEMBLY, treated the same here) the

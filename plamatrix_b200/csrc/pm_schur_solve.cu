@@ -2211,8 +2211,8 @@ namespace
 // Many independent systems assembled as one block-diagonal union (system s owns the block rows
 // [row0[s], row0[s+1])).  One set of kernels serves every system: per-system dots are summed
 // by one warp per system over its rows in a fixed order, alpha / beta / convergence are
-// per-system device state, converged systems stop updating, and the iteration is captured
-// once in a CUDA graph that the host replays until no system is active.
+// per-system device state, converged systems stop updating, and the iterations are captured
+// once into the body of a CUDA graph 'while' node that repeats until no system is active.
 struct BatchState
 {
     double rho, alpha, beta, tol, rr, rr0, window_sq;
@@ -2443,6 +2443,19 @@ __global__ void batch_direction_kernel(int64_t P, const int* __restrict__ row_sy
     }
 }
 
+// Condition of the device-driven iteration loop (a CUDA graph 'while' node): another chunk of
+// iterations while any system is active, at most max_chunks chunks per launch of the loop.
+__global__ void batch_continue_kernel(cudaGraphConditionalHandle handle, const int* __restrict__ active,
+                                      int* __restrict__ chunks, int max_chunks)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0)
+    {
+        const int done = *chunks + 1;
+        *chunks = done;
+        cudaGraphSetConditional(handle, *active > 0 && done < max_chunks ? 1u : 0u);
+    }
+}
+
 __global__ void batch_rows_kernel(int64_t systems, const int* __restrict__ sys_row, int* __restrict__ row_sys)
 {
     for (int64_t s = blockIdx.x; s < systems; s += gridDim.x)
@@ -2668,7 +2681,7 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
     double* z = c.take<double>(6 * P + 1);
     double* pv = c.take<double>(6 * P + 1);
     double* q = c.take<double>(6 * P + 1);
-    int* flags = c.take<int>(4); // [0] active count, [1] coupling check
+    int* flags = c.take<int>(4); // [0] active count, [1] coupling check, [2] chunks run by the loop
     int* fallen = c.take<int>(NS + 1);
     std::vector<int> rows32(NS + 1);
     for (int64_t s = 0; s <= NS; ++s)
@@ -2722,11 +2735,34 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
                                                         rel, abs_tol, rule, flags);
         PM_LAUNCH_CHECK();
     };
-    // one CUDA graph holds kChunk iterations of every active system
+    // The iterations run as one CUDA graph: a 'while' conditional node whose body holds kChunk
+    // iterations of every active system and ends with batch_continue_kernel, which keeps the
+    // loop going on the device while any system is active (no host check between chunks).
     constexpr int kChunk = 8;
+    const int max_chunks = (maxit + kChunk - 1) / kChunk + 1;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    PM_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    PM_CUDA(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle = 0;
+    cudaGraph_t body = nullptr;
+    {
+        const cudaError_t made = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        const cudaError_t added = made == cudaSuccess ? cudaGraphAddNode(&node, graph, nullptr, 0, &cp) : made;
+        if (added != cudaSuccess)
+        {
+            cudaGraphDestroy(graph);
+            fail(PM_CUDA_ERROR, std::string("batched Schur solve: conditional graph node: ") +
+                                    cudaGetErrorString(added));
+        }
+        body = cp.conditional.phGraph_out[0];
+    }
+    PM_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < kChunk; ++k)
     {
         // mixed precision: the iterations read the FP32 values and preconditioner blocks (FP64
@@ -2751,28 +2787,34 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
         for (int l = 0; l < 5; ++l)
             count_launch();
     }
-    const cudaError_t cap = cudaStreamEndCapture(stream, &graph);
+    batch_continue_kernel<<<1, 32, 0, stream>>>(handle, flags, flags + 2, max_chunks);
+    count_launch();
+    cudaGraph_t captured = nullptr;
+    const cudaError_t cap = cudaStreamEndCapture(stream, &captured);
     if (cap != cudaSuccess)
+    {
+        cudaGraphDestroy(graph);
         fail(PM_CUDA_ERROR, std::string("batched Schur solve: graph capture failed: ") + cudaGetErrorString(cap));
-    PM_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-    int* host_count = reinterpret_cast<int*>(ws->host_state); // pinned; the state is not used here
-    auto run = [&](int& issued) {
-        while (issued < maxit)
+    }
+    {
+        const cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+        if (inst != cudaSuccess)
         {
-            PM_CUDA(cudaGraphLaunch(exec, stream));
-            issued += kChunk;
-            PM_CUDA(cudaMemcpyAsync(host_count, flags, sizeof(int), cudaMemcpyDeviceToHost, stream));
-            PM_CUDA(cudaEventRecord(ws->sync_event, stream));
-            PM_CUDA(cudaEventSynchronize(ws->sync_event));
-            if (*host_count == 0)
-                break;
+            cudaGraphDestroy(graph);
+            fail(PM_CUDA_ERROR, std::string("batched Schur solve: graph instantiation: ") + cudaGetErrorString(inst));
         }
+    }
+    int* host_count = reinterpret_cast<int*>(ws->host_state); // pinned; the state is not used here
+    // one launch of the loop: it ends on the device once no system is active
+    auto run = [&]() {
+        PM_CUDA(cudaMemsetAsync(flags + 2, 0, sizeof(int), stream));
+        PM_CUDA(cudaGraphLaunch(exec, stream));
     };
-    int issued = 0, checks = 0;
+    int checks = 0;
     try
     {
         start();
-        run(issued);
+        run();
         if (learned)
         {
             // systems whose learned PCG stagnated restart from their iterate with block Jacobi
@@ -2782,8 +2824,7 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
             batch_flag_restart_kernel<<<grid_for(NS, 128, 4096), 128, 0, stream>>>(NS, bs, fallen);
             PM_LAUNCH_CHECK();
             start();
-            int again = 0;
-            run(again);
+            run();
         }
         // mixed precision: FP64 checks of the systems that converged on the FP32 operator; those
         // that miss their tolerance iterate on from the FP64 residual (iterative refinement)
@@ -2799,8 +2840,7 @@ void batched_pcg(pm_schur_workspace* ws, cudaStream_t stream, const BatchSpec& s
             PM_CUDA(cudaEventSynchronize(ws->sync_event));
             if (*host_count == 0)
                 break;
-            int more = 0;
-            run(more);
+            run();
         }
     }
     catch (...)
