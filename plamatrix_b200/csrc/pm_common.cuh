@@ -239,9 +239,11 @@ struct CooView
     const int64_t* row_offsets; // rows + 1 (scan of unique_count)
 };
 
+// keep_sorted: store every row's sorted keys and values (coo_view readers need them); a
+// conversion that only fills a CSR passes false, and its fill re-sorts the short rows
 template <typename T>
 void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int64_t cols, int64_t count,
-                 const int64_t* row_indices, const int64_t* col_indices, const T* values);
+                 const int64_t* row_indices, const int64_t* col_indices, const T* values, bool keep_sorted = true);
 CooView coo_view(const pm_sparse_workspace* ws);
 int64_t coo_internal_status(pm_sparse_workspace* ws, cudaStream_t stream, const char* operation);
 

@@ -146,12 +146,14 @@ __device__ __forceinline__ void register_sort(uint64_t (&k)[N], T (&v)[N])
 }
 
 // 3) short rows: one thread per row, sorted in registers; long rows are queued
+// store == 0: only the unique count of every short row (the fill re-sorts them; keys and values
+// of short rows are not written)
 template <typename T>
 __global__ void __launch_bounds__(128) sort_short_kernel(const int* __restrict__ bucket_start, int64_t row_count,
                                                          const CooRec<T>* __restrict__ recs,
                                                          uint64_t* __restrict__ keys, T* __restrict__ values,
                                                          int* __restrict__ unique_count, int* __restrict__ long_rows,
-                                                         CooStatus* status)
+                                                         CooStatus* status, int store)
 {
     const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (r >= row_count)
@@ -165,7 +167,7 @@ __global__ void __launch_bounds__(128) sort_short_kernel(const int* __restrict__
     }
     if (len <= 1)
     {
-        if (len == 1)
+        if (len == 1 && store)
         {
             const CooRec<T> one = recs[start];
             keys[start] = one.key;
@@ -199,8 +201,11 @@ __global__ void __launch_bounds__(128) sort_short_kernel(const int* __restrict__
     {
         if (q < len)
         {
-            keys[start + q] = k[q];
-            values[start + q] = v[q];
+            if (store)
+            {
+                keys[start + q] = k[q];
+                values[start + q] = v[q];
+            }
             const uint32_t col = key_col(k[q]);
             unique += (q == 0 || col != previous) ? 1 : 0;
             previous = col;
@@ -429,6 +434,72 @@ __global__ void __launch_bounds__(128) write_short_kernel(const int* __restrict_
     emit(at, capacity, col, sum, col_out, val_out);
 }
 
+// 5') the same from the scattered records: every short row is sorted in registers again (the
+// count phase kept only its unique count) and its runs combined serially in key order
+template <typename T>
+__global__ void __launch_bounds__(128) write_short_resort_kernel(const int* __restrict__ bucket_start,
+                                                                 int64_t row_count, const CooRec<T>* __restrict__ recs,
+                                                                 const int64_t* __restrict__ row_offsets,
+                                                                 int64_t capacity, int64_t* __restrict__ col_out,
+                                                                 T* __restrict__ val_out, CooStatus* status)
+{
+    const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (r >= row_count)
+        return;
+    const int start = bucket_start[r];
+    const int len = bucket_start[r + 1] - start;
+    if (len > kShortMax || len == 0)
+        return;
+    int64_t at = row_offsets[r];
+    if (len == 1)
+    {
+        const CooRec<T> one = recs[start];
+        emit(at, capacity, key_col(one.key), one.value, col_out, val_out);
+        return;
+    }
+    uint64_t k[kShortMax];
+    T v[kShortMax];
+#pragma unroll
+    for (int q = 0; q < kShortMax; ++q)
+    {
+        if (q < len)
+        {
+            const CooRec<T> one = recs[start + q];
+            k[q] = one.key;
+            v[q] = one.value;
+        }
+        else
+        {
+            k[q] = kPadKey;
+            v[q] = T(0);
+        }
+    }
+    register_sort<kShortMax, T>(k, v);
+    uint32_t col = key_col(k[0]);
+    T sum = v[0];
+#pragma unroll
+    for (int q = 1; q < kShortMax; ++q)
+    {
+        if (q < len)
+        {
+            const uint32_t c = key_col(k[q]);
+            if (c != col)
+            {
+                emit(at++, capacity, col, sum, col_out, val_out);
+                col = c;
+                sum = v[q];
+            }
+            else
+            {
+                sum += v[q];
+                if (!finite_value(sum))
+                    atomicMin(&status->invalid_value, static_cast<unsigned long long>(source_of(k[q])));
+            }
+        }
+    }
+    emit(at, capacity, col, sum, col_out, val_out);
+}
+
 // 6) combine runs of long rows: one CTA per row; run heads found by a block scan, each
 // head thread sums its run serially in key order
 template <typename T>
@@ -498,6 +569,8 @@ struct pm_sparse_workspace
     int* long_rows = nullptr;
     int64_t* row_offsets = nullptr;
     void* scan_scratch = nullptr;
+    void* recs = nullptr;             // the scattered (key, value) records of the last conversion
+    bool short_rows_kept = true;      // short rows' sorted keys / values are stored (else re-sorted at fill)
 };
 
 namespace pm
@@ -519,7 +592,7 @@ void check_metadata(int64_t rows, int64_t cols, int64_t count)
 
 template <typename T>
 void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int64_t cols, int64_t count,
-                 const int64_t* row_indices, const int64_t* col_indices, const T* values)
+                 const int64_t* row_indices, const int64_t* col_indices, const T* values, bool keep_sorted)
 {
     if (!ws)
         fail(PM_INVALID_ARGUMENT, "cooToCsr GPU workspace is null");
@@ -561,6 +634,8 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     ws->row_offsets = carve.take<int64_t>(R + 1);
     ws->scan_scratch = carve.take<char>(scan_bytes);
     CooRec<T>* recs = carve.take<CooRec<T>>(n);
+    ws->recs = recs;
+    ws->short_rows_kept = keep_sorted;
     ws->rows = rows;
     ws->cols = cols;
     ws->count = count;
@@ -592,8 +667,8 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     if (rows > 0)
     {
         sort_short_kernel<T><<<grid_for(rows, 128), 128, 0, stream>>>(ws->bucket_start, rows, recs, ws->keys,
-                                                                      sorted_values,
-                                                                      ws->unique_count, ws->long_rows, ws->status);
+                                                                      sorted_values, ws->unique_count, ws->long_rows,
+                                                                      ws->status, keep_sorted ? 1 : 0);
         PM_LAUNCH_CHECK();
         sort_long_kernel<T><<<2 * sm_count(), kLongThreads, 0, stream>>>(
             ws->bucket_start, recs, ws->keys, sorted_values, ws->spare_keys, static_cast<T*>(ws->spare_values),
@@ -606,9 +681,9 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
 }
 
 template void coo_prepare<float>(pm_sparse_workspace*, cudaStream_t, int64_t, int64_t, int64_t, const int64_t*,
-                                  const int64_t*, const float*);
+                                  const int64_t*, const float*, bool);
 template void coo_prepare<double>(pm_sparse_workspace*, cudaStream_t, int64_t, int64_t, int64_t, const int64_t*,
-                                   const int64_t*, const double*);
+                                   const int64_t*, const double*, bool);
 
 CooView coo_view(const pm_sparse_workspace* ws)
 {
@@ -656,9 +731,14 @@ void coo_fill(pm_sparse_workspace* ws, cudaStream_t stream, int64_t nnz, int64_t
     if (ws->count == 0 || ws->rows == 0)
         return;
     const T* sorted_values = static_cast<const T*>(ws->values);
-    write_short_kernel<T><<<grid_for(ws->rows, 128), 128, 0, stream>>>(ws->bucket_start, ws->rows, ws->keys,
-                                                                       sorted_values, ws->row_offsets, nnz, col_out,
-                                                                       val_out, ws->status);
+    if (ws->short_rows_kept)
+        write_short_kernel<T><<<grid_for(ws->rows, 128), 128, 0, stream>>>(ws->bucket_start, ws->rows, ws->keys,
+                                                                           sorted_values, ws->row_offsets, nnz,
+                                                                           col_out, val_out, ws->status);
+    else
+        write_short_resort_kernel<T><<<grid_for(ws->rows, 128), 128, 0, stream>>>(
+            ws->bucket_start, ws->rows, static_cast<const CooRec<T>*>(ws->recs), ws->row_offsets, nnz, col_out,
+            val_out, ws->status);
     PM_LAUNCH_CHECK();
     write_long_kernel<T><<<2 * sm_count(), kLongThreads, 0, stream>>>(ws->bucket_start, ws->keys, sorted_values,
                                                                       ws->row_offsets, nnz, col_out, val_out,
@@ -680,7 +760,7 @@ int coo_async(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int64_
             fail(PM_RUNTIME_ERROR, "cooToCsrAsync empty input requires output nnz=0");
         }
         require_values(count, v);
-        coo_prepare<T>(ws, stream, rows, cols, count, ri, ci, v);
+        coo_prepare<T>(ws, stream, rows, cols, count, ri, ci, v, false);
         coo_fill<T>(ws, stream, nnz, ro, co, vo, true);
     });
 }
@@ -726,7 +806,7 @@ int pm_coo_to_csr_count_f32(pm_sparse_workspace* ws, pm_stream_t stream, int64_t
 {
     return pm::guarded([&] {
         pm::require_values(count, v);
-        pm::coo_prepare<float>(ws, stream, rows, cols, count, ri, ci, v);
+        pm::coo_prepare<float>(ws, stream, rows, cols, count, ri, ci, v, false);
     });
 }
 int pm_coo_to_csr_count_f64(pm_sparse_workspace* ws, pm_stream_t stream, int64_t rows, int64_t cols, int64_t count,
@@ -734,7 +814,7 @@ int pm_coo_to_csr_count_f64(pm_sparse_workspace* ws, pm_stream_t stream, int64_t
 {
     return pm::guarded([&] {
         pm::require_values(count, v);
-        pm::coo_prepare<double>(ws, stream, rows, cols, count, ri, ci, v);
+        pm::coo_prepare<double>(ws, stream, rows, cols, count, ri, ci, v, false);
     });
 }
 int pm_coo_to_csr_fill_f32(pm_sparse_workspace* ws, pm_stream_t stream, int64_t nnz, int64_t* ro, int64_t* co,
@@ -905,7 +985,7 @@ void coo_static(cudaStream_t stream, int64_t rows, int64_t cols, int64_t count, 
     pm_sparse_workspace ws;
     ws.buffer.ptr = base;
     ws.buffer.bytes = kStaticScratchBytes;
-    coo_prepare<T>(&ws, stream, rows, cols, count, ri, ci, v);
+    coo_prepare<T>(&ws, stream, rows, cols, count, ri, ci, v, false);
     PM_CUDA(cudaStreamSynchronize(stream));
     int64_t nnz = 0;
     int status = pm_coo_status(&ws, "cooToCsr", &nnz);
