@@ -71,10 +71,11 @@ __global__ void init_status_kernel(CooStatus* status)
     status->pad = 0;
 }
 
-// 1) validate and reserve a slot inside the row bucket
+// 1) validate the indices and reserve a slot inside the row bucket (values are checked by the
+// scatter, which reads them anyway)
 template <typename T>
 __global__ void __launch_bounds__(256) count_kernel(const int64_t* __restrict__ rows, const int64_t* __restrict__ cols,
-                                                    const T* __restrict__ values, int64_t count, int64_t row_count,
+                                                    int64_t count, int64_t row_count,
                                                     int64_t col_count, int* __restrict__ bucket_sizes,
                                                     int* __restrict__ slots, CooStatus* status)
 {
@@ -83,8 +84,6 @@ __global__ void __launch_bounds__(256) count_kernel(const int64_t* __restrict__ 
         return;
     const int64_t row = rows[i];
     const int64_t col = cols[i];
-    if (values && !finite_value(values[i]))
-        atomicMin(&status->invalid_value, static_cast<unsigned long long>(i));
     if (row < 0 || row >= row_count || col < 0 || col >= col_count)
     {
         atomicMin(&status->invalid_source, static_cast<unsigned long long>(i));
@@ -100,18 +99,22 @@ template <typename T>
 __global__ void __launch_bounds__(256) scatter_kernel(const int64_t* __restrict__ rows, const int64_t* __restrict__ cols,
                                                       const T* __restrict__ values, int64_t count,
                                                       const int* __restrict__ slots, const int* __restrict__ bucket_start,
-                                                      CooRec<T>* __restrict__ recs)
+                                                      CooRec<T>* __restrict__ recs, CooStatus* status)
 {
     const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= count)
         return;
+    // every value is checked here, also those of triplets whose indices the count rejected
+    const T value = values ? values[i] : T(0);
+    if (!finite_value(value))
+        atomicMin(&status->invalid_value, static_cast<unsigned long long>(i));
     const int slot = slots[i];
     if (slot < 0)
         return;
     const int pos = bucket_start[rows[i]] + slot;
     CooRec<T> r;
     r.key = (static_cast<uint64_t>(cols[i]) << 32) | static_cast<uint64_t>(i);
-    r.value = values ? values[i] : T(0);
+    r.value = value;
     recs[pos] = r;
 }
 
@@ -657,12 +660,12 @@ void coo_prepare(pm_sparse_workspace* ws, cudaStream_t stream, int64_t rows, int
     }
     T* sorted_values = static_cast<T*>(ws->values);
     PM_CUDA(cudaMemsetAsync(ws->bucket_sizes, 0, rows * sizeof(int), stream));
-    count_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, values, count, rows, cols,
+    count_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, count, rows, cols,
                                                               ws->bucket_sizes, ws->slots, ws->status);
     PM_LAUNCH_CHECK();
     exclusive_scan<int, int>(ws->bucket_sizes, ws->bucket_start, rows, ws->scan_scratch, stream);
     scatter_kernel<T><<<grid_for(count, 256), 256, 0, stream>>>(row_indices, col_indices, values, count, ws->slots,
-                                                                ws->bucket_start, recs);
+                                                                ws->bucket_start, recs, ws->status);
     PM_LAUNCH_CHECK();
     if (rows > 0)
     {
