@@ -40,9 +40,9 @@ METRIC = "Schur-PCG ms to 1e-8 FP64 rel. residual: learned+mixed vs plain; SpMV 
 # DRAM bytes (read + write) of one assembly (assemble_diag6 + assemble_upper6) per cross block,
 # from an ncu capture of the two kernels on the P=4,000, L=200,000 case, scaled by the cross count
 # (the traffic grows with the crosses): see the profile summary of the assembly
-ASSEMBLY_TRAFFIC_BYTES_PER_CROSS = 633.3e6 / 1_200_542
+ASSEMBLY_TRAFFIC_BYTES_PER_CROSS = 632.66e6 / 1_200_542
 ASSEMBLY_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of assemble_diag6 + assemble_upper6 on "
-                           "P=4,000, L=200,000 (633.3 MB for 1,200,542 crosses), scaled by the cross count")
+                           "P=4,000, L=200,000 (632.7 MB for 1,200,542 crosses), scaled by the cross count")
 BATCH_SYSTEMS = 512
 
 
