@@ -50,7 +50,7 @@ struct SolveState // device-side PCG / refinement scalars
 {
     double rho, alpha, beta, tolerance, initial_squared, residual_squared, rhs_squared;
     double true_squared;
-    int iterations, max_iterations, done, converged, breakdown, pad;
+    int iterations, max_iterations, done, converged, breakdown, chunks; // chunks: bodies run by the PCG graph
     unsigned int ticket[4];
     // stagnation watch: every `window` iterations the residual norm must have halved
     double window_squared;
@@ -117,8 +117,31 @@ struct pm_schur_workspace
     cudaEvent_t sync_event = nullptr;
     cudaStream_t graph_stream = nullptr; // batched PCG: graphs are captured and replayed here
     cudaEvent_t graph_events[2] = {};
+    // block PCG iteration graphs ('while' node around a chunk of iterations), one per operand set
+    struct PcgGraph
+    {
+        const void* key[6] = {};
+        int64_t P = -1;
+        int types = -1;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+    };
+    PcgGraph pcg_graphs[4];
+    int pcg_graph_next = 0;
+    void drop_pcg_graphs()
+    {
+        for (auto& g : pcg_graphs)
+        {
+            if (g.exec)
+                cudaGraphExecDestroy(g.exec);
+            if (g.graph)
+                cudaGraphDestroy(g.graph);
+            g = PcgGraph{};
+        }
+    }
     ~pm_schur_workspace()
     {
+        drop_pcg_graphs();
         pattern.release();
         numeric.release();
         scratch.release();
@@ -1408,7 +1431,7 @@ template <typename V>
 __global__ void pcg_block_direction_kernel(int64_t n, const V* __restrict__ z, V* __restrict__ p,
                                            const SolveState* st)
 {
-    if (st->done)
+    if (st->done || st->iterations == 0) // the first iteration's direction is z itself (set by the init)
         return;
     const double beta = st->beta;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
@@ -2527,12 +2550,46 @@ __global__ void batch_flag_restart_kernel(int64_t systems, BatchState* __restric
         }
 }
 
-// One preconditioned CG solve on the block-CSR operand (matrix M, vectors V, inverses PM),
-// device-driven; the host polls `done` on a doubling schedule.  Returns the final state.
-template <typename V, typename M, typename PM>
-SolveState block_pcg(pm_schur_workspace* ws, cudaStream_t stream, const M* S, const PM* minv, const double* rhs,
-                     V* x, double rel, double abs_tol, int rule, int max_iterations, V* scratch, int window = 0)
+// Condition of the block PCG's iteration graph: another chunk while the solve is not done, at
+// most max_iterations / kPcgChunk + 1 chunks (the update kernel also ends the solve at
+// max_iterations).
+constexpr int kPcgChunk = 4; // iterations per graph body (even: the residual ping-pong returns to r0)
+__global__ void pcg_continue_kernel(cudaGraphConditionalHandle handle, SolveState* st)
 {
+    if (threadIdx.x == 0 && blockIdx.x == 0)
+    {
+        const int chunks = st->chunks + 1;
+        st->chunks = chunks;
+        cudaGraphSetConditional(handle, !st->done && chunks <= st->max_iterations / kPcgChunk + 1 ? 1u : 0u);
+    }
+}
+
+// The iteration graph of one operand set (S, inverses, x, scratch vectors and the workspace's
+// state), built on first use and kept in the workspace: a CUDA graph 'while' node whose body is
+// kPcgChunk iterations (direction, block SpMV with p.q, update with r.z / r.r) and
+// pcg_continue_kernel, so the device decides when the solve is done.
+template <typename V, typename M, typename PM>
+cudaGraphExec_t pcg_iteration_graph(pm_schur_workspace* ws, const M* S, const PM* minv, V* x, V* scratch)
+{
+    const void* key[6] = {S, minv, x, scratch, ws->block_row_ptr, ws->block_col};
+    const int types = int(sizeof(V) == 8) | int(sizeof(M) == 8) << 1 | int(sizeof(PM) == 8) << 2 |
+                      int(ws->bp == 6) << 3;
+    for (auto& g : ws->pcg_graphs)
+        if (g.exec && g.P == ws->P && g.types == types && std::equal(key, key + 6, g.key))
+            return g.exec;
+    if (!ws->graph_stream)
+    {
+        PM_CUDA(cudaStreamCreateWithFlags(&ws->graph_stream, cudaStreamNonBlocking));
+        for (auto& e : ws->graph_events)
+            PM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    auto& slot = ws->pcg_graphs[ws->pcg_graph_next];
+    ws->pcg_graph_next = (ws->pcg_graph_next + 1) % 4;
+    if (slot.exec)
+        cudaGraphExecDestroy(slot.exec);
+    if (slot.graph)
+        cudaGraphDestroy(slot.graph);
+    slot = pm_schur_workspace::PcgGraph{};
     const int64_t P = ws->P, n = ws->P * ws->bp;
     const int bp = static_cast<int>(ws->bp);
     V* r0 = scratch;
@@ -2543,6 +2600,81 @@ SolveState block_pcg(pm_schur_workspace* ws, cudaStream_t stream, const M* S, co
     const unsigned sgrid = grid_for(P * 32, kVecBlock, kMaxParts);
     const unsigned ugrid = grid_for(P, kVecBlock, kMaxParts);
     const unsigned dgrid = grid_for(n, kVecBlock, 4096);
+    cudaGraph_t graph = nullptr;
+    PM_CUDA(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle = 0;
+    cudaGraph_t body = nullptr;
+    {
+        const cudaError_t made = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        const cudaError_t added = made == cudaSuccess ? cudaGraphAddNode(&node, graph, nullptr, 0, &cp) : made;
+        if (added != cudaSuccess)
+        {
+            cudaGraphDestroy(graph);
+            fail(PM_CUDA_ERROR, std::string("Schur PCG: conditional graph node: ") + cudaGetErrorString(added));
+        }
+        body = cp.conditional.phGraph_out[0];
+    }
+    const cudaStream_t gs = ws->graph_stream;
+    PM_CUDA(cudaStreamBeginCaptureToGraph(gs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kPcgChunk; ++k)
+    {
+        V* r_in = (k & 1) ? r1 : r0;
+        V* r_out = (k & 1) ? r0 : r1;
+        pcg_block_direction_kernel<V><<<dgrid, kVecBlock, 0, gs>>>(n, z, p, ws->state);
+        if (bp == 6)
+        {
+            pcg_bsr_kernel<V, M, 6><<<sgrid, kVecBlock, 0, gs>>>(P, bp, ws->block_row_ptr, ws->block_col, S, p, q,
+                                                                 ws->partials, ws->state);
+            pcg_block_update_kernel<V, PM, 6><<<ugrid, kVecBlock, 0, gs>>>(P, bp, x, p, q, r_in, r_out, z, minv,
+                                                                           ws->partials, ws->state);
+        }
+        else
+        {
+            pcg_bsr_kernel<V, M, 0><<<sgrid, kVecBlock, 0, gs>>>(P, bp, ws->block_row_ptr, ws->block_col, S, p, q,
+                                                                 ws->partials, ws->state);
+            pcg_block_update_kernel<V, PM, 0><<<ugrid, kVecBlock, 0, gs>>>(P, bp, x, p, q, r_in, r_out, z, minv,
+                                                                           ws->partials, ws->state);
+        }
+    }
+    pcg_continue_kernel<<<1, 32, 0, gs>>>(handle, ws->state);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t cap = cudaStreamEndCapture(gs, &captured);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t inst = cap == cudaSuccess ? cudaGraphInstantiate(&exec, graph, 0) : cap;
+    if (inst != cudaSuccess)
+    {
+        cudaGraphDestroy(graph);
+        fail(PM_CUDA_ERROR, std::string("Schur PCG: iteration graph: ") + cudaGetErrorString(inst));
+    }
+    std::copy(key, key + 6, slot.key);
+    slot.P = P;
+    slot.types = types;
+    slot.graph = graph;
+    slot.exec = exec;
+    return exec;
+}
+
+// One preconditioned CG solve on the block-CSR operand (matrix M, vectors V, inverses PM): the
+// initial residual, then the iteration graph (the device ends it), then one read of the final
+// state, which is returned.
+template <typename V, typename M, typename PM>
+SolveState block_pcg(pm_schur_workspace* ws, cudaStream_t stream, const M* S, const PM* minv, const double* rhs,
+                     V* x, double rel, double abs_tol, int rule, int max_iterations, V* scratch, int window = 0)
+{
+    const int64_t P = ws->P, n = ws->P * ws->bp;
+    const int bp = static_cast<int>(ws->bp);
+    V* r0 = scratch;
+    V* z = r0 + 2 * (n + 1);
+    V* p = z + (n + 1);
+    V* q = p + (n + 1);
+    const unsigned sgrid = grid_for(P * 32, kVecBlock, kMaxParts);
+    const unsigned ugrid = grid_for(P, kVecBlock, kMaxParts);
     const bool six = bp == 6;
     if (six)
         bsr_spmv_kernel<V, M, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, x, q);
@@ -2558,46 +2690,19 @@ SolveState block_pcg(pm_schur_workspace* ws, cudaStream_t stream, const M* S, co
                                                                                 abs_tol, rule, max_iterations, window,
                                                                                 ws->partials, ws->state);
     PM_LAUNCH_CHECK();
-    int issued = 0, check_every = 1;
-    V* r_in = r0;
-    V* r_out = r1;
-    while (true)
+    // the iterations: one launch of the operand set's iteration graph, which stops on the device
+    if (max_iterations > 0)
     {
-        const int chunk = std::min(check_every, max_iterations - issued);
-        for (int k = 0; k < chunk; ++k)
-        {
-            if (issued > 0)
-                pcg_block_direction_kernel<V><<<dgrid, kVecBlock, 0, stream>>>(n, z, p, ws->state);
-                PM_LAUNCH_CHECK();
-            if (six)
-            {
-                pcg_bsr_kernel<V, M, 6><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, p,
-                                                                         q, ws->partials, ws->state);
-                PM_LAUNCH_CHECK();
-                pcg_block_update_kernel<V, PM, 6><<<ugrid, kVecBlock, 0, stream>>>(P, bp, x, p, q, r_in, r_out, z, minv,
-                                                                                   ws->partials, ws->state);
-                PM_LAUNCH_CHECK();
-            }
-            else
-            {
-                pcg_bsr_kernel<V, M, 0><<<sgrid, kVecBlock, 0, stream>>>(P, bp, ws->block_row_ptr, ws->block_col, S, p,
-                                                                         q, ws->partials, ws->state);
-                PM_LAUNCH_CHECK();
-                pcg_block_update_kernel<V, PM, 0><<<ugrid, kVecBlock, 0, stream>>>(P, bp, x, p, q, r_in, r_out, z, minv,
-                                                                                   ws->partials, ws->state);
-                PM_LAUNCH_CHECK();
-            }
-            PM_LAUNCH_CHECK();
-            std::swap(r_in, r_out);
-            ++issued;
-        }
-        PM_CUDA(cudaMemcpyAsync(ws->host_state, ws->state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
-        PM_CUDA(cudaEventRecord(ws->sync_event, stream));
-        PM_CUDA(cudaEventSynchronize(ws->sync_event));
-        if (ws->host_state->done || issued >= max_iterations)
-            break;
-        check_every = std::min(check_every * 2, 16);
+        const cudaGraphExec_t exec = pcg_iteration_graph<V, M, PM>(ws, S, minv, x, scratch);
+        PM_CUDA(cudaMemsetAsync(&ws->state->chunks, 0, sizeof(int), stream));
+        PM_CUDA(cudaGraphLaunch(exec, stream));
     }
+    PM_CUDA(cudaMemcpyAsync(ws->host_state, ws->state, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaEventRecord(ws->sync_event, stream));
+    PM_CUDA(cudaEventSynchronize(ws->sync_event));
+    if (max_iterations > 0) // the kernels the graph ran: kPcgChunk x 3 + 1 per body
+        for (int k = 0; k < ws->host_state->chunks * (3 * kPcgChunk + 1); ++k)
+            count_launch();
     return *ws->host_state;
 }
 
@@ -3449,6 +3554,7 @@ int pm_schur_workspace_close(pm_schur_workspace* ws)
     return pm::guarded([&] {
         if (!ws)
             pm::fail(PM_INVALID_ARGUMENT, "workspace is null");
+        ws->drop_pcg_graphs(); // they hold pointers into the buffers released here
         ws->pattern.release();
         ws->numeric.release();
         ws->scratch.release();
