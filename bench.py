@@ -206,10 +206,14 @@ def run_reference(args):
 
 
 def config_dict(world: int, L: int) -> dict:
-    """The workload of every arm's line (the same dict for ours and the reference)."""
-    return {"workload": WORKLOAD, "primary_blocks": P_FULL, "eliminated_blocks": L,
+    """The workload of every arm's line (the same dict for ours and the reference); a run with
+    another eliminated-block count names its own L."""
+    workload = WORKLOAD if L == L_FULL else WORKLOAD.replace("L2000000", f"L{L}").replace(
+        "L=2,000,000", f"L={L:,}")
+    return {"workload": workload, "primary_blocks": P_FULL, "eliminated_blocks": L,
             "parallelism": f"replicas x{world} (no exchange step)",
-            "l2": "inputs larger than L2 (observations 1.9 GB FP64)"}
+            "l2": "inputs larger than L2 (observations 1.9 GB FP64)" if L == L_FULL else
+            "observations %.2f GB FP64" % (L * 6 * 160 / 1e9)}
 
 
 # ------------------------------------------------------------------ our arm

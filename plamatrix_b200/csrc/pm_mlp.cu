@@ -823,7 +823,34 @@ void check_view(const SchurView& v)
 
 } // namespace
 
-void mlp_apply(const pm_mlp* cmlp, const SchurView& v, cudaStream_t stream)
+// Plain block Jacobi again, on the device, when the network's blocks are unusable (a block not
+// positive definite, or a tensor-core GEMM that gave up): every row's FP64 inverse of its own
+// diagonal block.  Nothing is done when both flags are clear.
+template <typename T>
+__global__ void learned_guard_kernel(int64_t P, const int* __restrict__ diag_pos, const T* __restrict__ S,
+                                     double* __restrict__ minv, float* __restrict__ minv32, const int* __restrict__ bad)
+{
+    if (!bad[0] && !bad[1])
+        return;
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < P; p += int64_t(gridDim.x) * blockDim.x)
+    {
+        double m[36], inv[36], lower[36], work[6];
+        const T* d = S + int64_t(diag_pos[p]) * 36;
+        for (int r = 0; r < 6; ++r)
+            for (int c = 0; c < 6; ++c)
+                m[r * 6 + c] = static_cast<double>(r >= c ? d[r * 6 + c] : d[c * 6 + r]);
+        if (!spd_inverse<6>(m, 6, inv, lower, work))
+            for (int k = 0; k < 36; ++k)
+                inv[k] = 0.0;
+        for (int k = 0; k < 36; ++k)
+            minv[p * 36 + k] = inv[k];
+        if (minv32)
+            for (int k = 0; k < 36; ++k)
+                minv32[p * 36 + k] = static_cast<float>(inv[k]);
+    }
+}
+
+void mlp_apply(const pm_mlp* cmlp, const SchurView& v, cudaStream_t stream, int* flags_host)
 {
     pm_mlp* mlp = const_cast<pm_mlp*>(cmlp); // parameters are read only; scratch is reused
     check_view(v);
@@ -832,20 +859,28 @@ void mlp_apply(const pm_mlp* cmlp, const SchurView& v, cudaStream_t stream)
         return;
     PM_CUDA(cudaMemsetAsync(bad_flag(mlp), 0, sizeof(int), stream));
     const unsigned grid = grid_for(v.P, 64, 4096);
+    float* const m32 = v.mixed ? v.minv32 : nullptr;
     if (v.value_size == 8)
+    {
         precond_kernel<double><<<grid, 64, 0, stream>>>(v.P, v.diag_pos, static_cast<const double*>(v.S), mlp->O,
-                                                        v.minv, v.mixed ? v.minv32 : nullptr, bad_flag(mlp));
+                                                        v.minv, m32, bad_flag(mlp));
+        PM_LAUNCH_CHECK();
+        learned_guard_kernel<double><<<grid, 64, 0, stream>>>(v.P, v.diag_pos, static_cast<const double*>(v.S),
+                                                              v.minv, m32, bad_flag(mlp));
+    }
     else
+    {
         precond_kernel<float><<<grid, 64, 0, stream>>>(v.P, v.diag_pos, static_cast<const float*>(v.S), mlp->O,
-                                                       v.minv, v.mixed ? v.minv32 : nullptr, bad_flag(mlp));
+                                                       v.minv, m32, bad_flag(mlp));
+        PM_LAUNCH_CHECK();
+        learned_guard_kernel<float><<<grid, 64, 0, stream>>>(v.P, v.diag_pos, static_cast<const float*>(v.S),
+                                                             v.minv, m32, bad_flag(mlp));
+    }
     PM_LAUNCH_CHECK();
-    int bad[2] = {0, 0};
-    PM_CUDA(cudaMemcpyAsync(bad, bad_flag(mlp), 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-    PM_CUDA(cudaStreamSynchronize(stream));
-    if (bad[1])
-        fail(PM_RUNTIME_ERROR, "learned preconditioner: a tensor-core GEMM did not complete");
-    if (bad[0])
-        fail(PM_RUNTIME_ERROR, "learned preconditioner: a corrected block is not positive definite");
+    // [0]: a corrected block was not positive definite, [1]: a GEMM gave up; read by the caller
+    // after its next synchronisation
+    if (flags_host)
+        PM_CUDA(cudaMemcpyAsync(flags_host, bad_flag(mlp), 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
 }
 
 namespace

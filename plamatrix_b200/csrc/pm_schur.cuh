@@ -128,7 +128,9 @@ SchurView schur_view(pm_schur_workspace* ws, bool mixed);
 template <typename T>
 void dense_schur_factor_solve(cudaStream_t stream, int64_t P, int bp, const int* row_ptr, const int* block_col,
                               const T* S, double* A, double* x, int* status);
-// features -> network -> (L'L'^T)^-1 of every diagonal block into v.minv (and v.minv32)
-void mlp_apply(const pm_mlp* mlp, const SchurView& v, cudaStream_t stream);
+// features -> network -> (L'L'^T)^-1 of every diagonal block into v.minv (and v.minv32); when the
+// network's blocks are unusable the device puts plain block Jacobi back.  flags_host (pinned,
+// two ints, may be null) receives {block not positive definite, GEMM gave up} asynchronously.
+void mlp_apply(const pm_mlp* mlp, const SchurView& v, cudaStream_t stream, int* flags_host);
 
 } // namespace pm

@@ -44,6 +44,7 @@ struct SchurStatus
     long long row_too_wide;
     int pad[2]; // pad[1]: scratch flag of the topology comparison
     long long observation_bad; // the normal equations' first observation with a non-finite residual norm
+    int learned_bad[2];        // host copy only: the learned blocks were unusable / a GEMM gave up
 };
 
 struct SolveState // device-side PCG / refinement scalars
@@ -3211,12 +3212,17 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             PM_LAUNCH_CHECK();
         }
     };
+    // the network's outcome flags arrive in the pinned status with the next synchronisation; the
+    // report takes them when the solve ends
+    ws->host_status->learned_bad[0] = ws->host_status->learned_bad[1] = 0;
+    bool learned_flags = false;
     if (learned)
     {
         try
         {
-            mlp_apply(o->learned, schur_view(ws, mixed), stream);
+            mlp_apply(o->learned, schur_view(ws, mixed), stream, ws->host_status->learned_bad);
             rep->learned_used = 1;
+            learned_flags = true;
         }
         catch (const Error&)
         {
@@ -3225,6 +3231,14 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             rep->learned_fallback = 1;
         }
     }
+    // after a synchronisation: a network whose blocks the device replaced by block Jacobi
+    auto note_learned = [&]() {
+        if (learned_flags && (ws->host_status->learned_bad[0] || ws->host_status->learned_bad[1]))
+        {
+            rep->learned_used = 0;
+            rep->learned_fallback = 1;
+        }
+    };
     // ---- PCG
     double* area = vector_area(ws);
     SolveState st{};
@@ -3425,6 +3439,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         PM_CUDA(cudaEventRecord(ws->events[5], stream));
         PM_CUDA(cudaEventSynchronize(ws->events[5]));
         timings(5);
+        note_learned();
         if (rep->message[0] == '\0')
             std::snprintf(rep->message, sizeof(rep->message), "PCG iteration limit reached");
         return;
@@ -3449,6 +3464,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     PM_CUDA(cudaEventRecord(ws->events[5], stream));
     PM_CUDA(cudaEventSynchronize(ws->events[5]));
     timings(5);
+    note_learned();
     std::snprintf(rep->message, sizeof(rep->message), "converged");
 }
 

@@ -133,6 +133,28 @@ def test_gemm_stage_wait_that_runs_out_is_an_error_and_the_network_stays_usable(
         net.set_wait_limit(-1)
 
 
+@pytest.mark.parametrize("precision", ["native", "mixed"])
+def test_network_that_gives_up_inside_a_solve_falls_back_on_the_device(precision):
+    """A GEMM stage wait that runs out inside a solve: the device puts plain block Jacobi back
+    before the PCG (no host round trip), the report says so, and the solve is block Jacobi's."""
+    prob = W.small_bundle(seed=41)
+    net = SC.LearnedPreconditioner(seed=9)
+    net.set_params(_random_params(10))
+    net.set_wait_limit(0)
+    try:
+        opts = SC.SchurComplementSolverOptions(max_iterations=500, relative_tolerance=1e-10, learned=net,
+                                               precision=precision)
+        _, _, dp, rep = _solved(prob, options=opts)
+    finally:
+        net.set_wait_limit(1 << 20)
+    _, _, dp_plain, rep_plain = _solved(prob, options=SC.SchurComplementSolverOptions(
+        max_iterations=500, relative_tolerance=1e-10, precision=precision))
+    assert rep["converged"], rep["message"]
+    assert rep["learned_fallback"] and not rep["learned_used"]
+    assert rep["iterations"] == rep_plain["iterations"]
+    assert torch.allclose(dp, dp_plain, rtol=1e-9, atol=1e-12)
+
+
 def test_zero_network_matches_block_jacobi():
     prob = W.small_bundle(seed=35)
     _, _, dp_plain, rep_plain = _solved(prob)

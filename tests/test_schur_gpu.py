@@ -691,3 +691,20 @@ def test_assembly_autotune_keeps_the_fastest_shape(checkers):
     assert rep["converged"] and rep["pattern_reused"]
     assert np.linalg.norm(host(dp) - dp_ref) <= 1e-6 * np.linalg.norm(dp_ref)
     assert np.linalg.norm(host(dl) - dl_ref) <= 1e-6 * np.linalg.norm(dl_ref)
+
+
+def test_one_workspace_alternating_systems_matches_fresh_workspaces():
+    """The PCG iteration graphs a workspace keeps (one per operand set) follow the system: solves
+    that alternate between two systems of different sizes, and between plain and mixed
+    precision, on one workspace equal solves on fresh workspaces bit for bit."""
+    probs = [W.large_bundle(seed=21, P=150, L=6000), W.small_bundle(seed=22)]
+    nes = [_device_from_observations(p) for p in probs]
+    plain = SC.SchurComplementSolverOptions(max_iterations=300, relative_tolerance=1e-10)
+    mixed = SC.SchurComplementSolverOptions(max_iterations=300, relative_tolerance=1e-10, precision="mixed")
+    shared = SC.SchurComplementSolverWorkspace()
+    for ne, opts in [(nes[0], plain), (nes[1], plain), (nes[0], mixed), (nes[1], mixed), (nes[0], plain)]:
+        dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, shared)
+        dp_f, dl_f, rep_f = SC.solve_damped_schur_complement(ne, 1e-3, opts, SC.SchurComplementSolverWorkspace())
+        assert rep["converged"] and rep_f["converged"]
+        assert rep["iterations"] == rep_f["iterations"]
+        assert torch.equal(dp, dp_f) and torch.equal(dl, dl_f)
