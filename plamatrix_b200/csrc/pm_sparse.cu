@@ -11,7 +11,8 @@
 //     vector update fused with preconditioner apply and the r.z / r.r dots); every dot is
 //     accumulated in FP64 per block and finished by the last block to arrive, in a fixed
 //     order, which also evaluates alpha / beta, breakdown and convergence on the device;
-//   * the host only polls a device "done" flag on a doubling schedule.
+//   * the iterations run as a CUDA graph whose 'while' node repeats a chunk of them until the
+//     device state says done; the host reads the state once, after the solve.
 #include "pm_common.cuh"
 
 #include <cmath>
@@ -288,7 +289,7 @@ struct PcgState
     int nonfinite_init;
     long long jacobi_bad_row;
     unsigned int ticket[3];
-    int pad;
+    int chunks; // bodies run by the iteration graph
 };
 
 // Last block to arrive sums the per-block partials (fixed order) and runs `finish`.
@@ -584,11 +585,24 @@ __global__ void __launch_bounds__(kReduceBlock) pcg_update_kernel(int64_t n, T* 
 template <typename T>
 __global__ void pcg_direction_kernel(int64_t n, const T* __restrict__ z, T* __restrict__ p, const PcgState* st)
 {
-    if (st->done)
+    if (st->done || st->iterations == 0) // the first iteration's direction is z itself (set by the init)
         return;
     const double beta = st->beta;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
         p[i] = static_cast<T>(static_cast<double>(z[i]) + beta * static_cast<double>(p[i]));
+}
+
+// Condition of the CG / PCG iteration graph: another chunk while the solve is not done, at most
+// max_iterations / kCgChunk + 1 chunks (the update kernel also ends the solve at max_iterations).
+constexpr int kCgChunk = 4; // iterations per graph body (even: the residual ping-pong returns to r0)
+__global__ void cg_continue_kernel(cudaGraphConditionalHandle handle, PcgState* st)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0)
+    {
+        const int chunks = st->chunks + 1;
+        st->chunks = chunks;
+        cudaGraphSetConditional(handle, !st->done && chunks <= st->max_iterations / kCgChunk + 1 ? 1u : 0u);
+    }
 }
 
 __global__ void pcg_reset_kernel(PcgState* st, int max_iterations)
@@ -631,8 +645,35 @@ struct pm_solver_workspace
     pm::DeviceBuffer buffer;
     int* host_done = nullptr; // pinned
     cudaEvent_t event = nullptr;
+    // CG / PCG iteration graphs ('while' node around a chunk of iterations), one per operand set
+    struct IterationGraph
+    {
+        const void* key[5] = {};
+        int64_t n = -1;
+        int shape = 0, mode = -1, value_size = 0;
+        int64_t block_size = 0;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+    };
+    IterationGraph graphs[4];
+    int graph_next = 0;
+    cudaStream_t capture_stream = nullptr;
+    void drop_graphs()
+    {
+        for (auto& g : graphs)
+        {
+            if (g.exec)
+                cudaGraphExecDestroy(g.exec);
+            if (g.graph)
+                cudaGraphDestroy(g.graph);
+            g = IterationGraph{};
+        }
+    }
     ~pm_solver_workspace()
     {
+        drop_graphs();
+        if (capture_stream)
+            cudaStreamDestroy(capture_stream);
         buffer.release();
         if (host_done)
             cudaFreeHost(host_done);
@@ -931,6 +972,96 @@ void launch_pcg_spmv(const pm_csr* A, const T* p, T* q, double* partials, PcgSta
     PM_LAUNCH_CHECK();
 }
 
+// The iteration graph of one operand set (matrix and its SpMV shape, solution, preconditioner and
+// the workspace's buffer), built on first use and kept in the workspace: a CUDA graph 'while' node
+// whose body is kCgChunk iterations (direction, SpMV with p.q, update with the dots) and
+// cg_continue_kernel, so the device decides when the solve is done.
+template <typename T>
+cudaGraphExec_t cg_iteration_graph(pm_solver_workspace* ws, const pm_csr* A, T* x, const T* blocks, int64_t bs,
+                                   int mode)
+{
+    const int64_t n = A->rows;
+    const int shape = use_stream(A) ? 0 : lanes_per_row(A);
+    const void* key[5] = {A, A->values, x, blocks, ws->buffer.ptr};
+    for (auto& g : ws->graphs)
+        if (g.exec && g.n == n && g.shape == shape && g.mode == mode && g.block_size == bs &&
+            g.value_size == int(sizeof(T)) && std::equal(key, key + 5, g.key))
+            return g.exec;
+    if (!ws->capture_stream)
+        PM_CUDA(cudaStreamCreateWithFlags(&ws->capture_stream, cudaStreamNonBlocking));
+    auto& slot = ws->graphs[ws->graph_next];
+    ws->graph_next = (ws->graph_next + 1) % 4;
+    if (slot.exec)
+        cudaGraphExecDestroy(slot.exec);
+    if (slot.graph)
+        cudaGraphDestroy(slot.graph);
+    slot = pm_solver_workspace::IterationGraph{};
+    Carver c;
+    c.base = static_cast<char*>(ws->buffer.ptr);
+    PcgState* st = c.take<PcgState>(1);
+    double* partials = c.take<double>(3 * kMaxReduceBlocks);
+    T* r0 = c.take<T>(n);
+    T* r1 = c.take<T>(n);
+    T* z = c.take<T>(n);
+    T* p = c.take<T>(n);
+    T* q = c.take<T>(n);
+    T* inv = c.take<T>(n);
+    const unsigned vgrid = grid_for(n, kReduceBlock, kMaxReduceBlocks);
+    const unsigned sgrid = use_stream(A) ? grid_for(n, kReduceBlock, kMaxReduceBlocks)
+                                         : grid_for(n * lanes_per_row(A), kReduceBlock, kMaxReduceBlocks);
+    cudaGraph_t graph = nullptr;
+    PM_CUDA(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle handle = 0;
+    cudaGraph_t body = nullptr;
+    {
+        const cudaError_t made = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        const cudaError_t added = made == cudaSuccess ? cudaGraphAddNode(&node, graph, nullptr, 0, &cp) : made;
+        if (added != cudaSuccess)
+        {
+            cudaGraphDestroy(graph);
+            fail(PM_CUDA_ERROR, std::string("CUDA iterative solver: conditional graph node: ") +
+                                    cudaGetErrorString(added));
+        }
+        body = cp.conditional.phGraph_out[0];
+    }
+    const cudaStream_t cs = ws->capture_stream;
+    PM_CUDA(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kCgChunk; ++k)
+    {
+        T* r_in = (k & 1) ? r1 : r0;
+        T* r_out = (k & 1) ? r0 : r1;
+        pcg_direction_kernel<T><<<vgrid, kReduceBlock, 0, cs>>>(n, z, p, st);
+        launch_pcg_spmv<T>(A, p, q, partials, st, sgrid, cs);
+        pcg_update_kernel<T><<<vgrid, kReduceBlock, 0, cs>>>(n, x, p, q, r_in, r_out, z, mode, inv, blocks, bs,
+                                                              partials, st);
+    }
+    cg_continue_kernel<<<1, 32, 0, cs>>>(handle, st);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t cap = cudaStreamEndCapture(cs, &captured);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t inst = cap == cudaSuccess ? cudaGraphInstantiate(&exec, graph, 0) : cap;
+    if (inst != cudaSuccess)
+    {
+        cudaGraphDestroy(graph);
+        fail(PM_CUDA_ERROR, std::string("CUDA iterative solver: iteration graph: ") + cudaGetErrorString(inst));
+    }
+    std::copy(key, key + 5, slot.key);
+    slot.n = n;
+    slot.shape = shape;
+    slot.mode = mode;
+    slot.block_size = bs;
+    slot.value_size = int(sizeof(T));
+    slot.graph = graph;
+    slot.exec = exec;
+    return exec;
+}
+
 // mode: 0 = CG, 1 = Jacobi PCG, 2 = caller block inverses
 template <typename T>
 void solve(pm_solver_workspace* ws, cudaStream_t stream, const pm_csr* A, const T* b, T* x, const T* blocks,
@@ -1000,35 +1131,20 @@ void solve(pm_solver_workspace* ws, cudaStream_t stream, const pm_csr* A, const 
     pcg_init_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, b, q, r0, z, p, mode, inv, blocks, bs,
                                                             o->relative_tolerance, o->absolute_tolerance, partials, st);
     PM_LAUNCH_CHECK();
-    int issued = 0;
-    int check_every = 1;
-    T* r_in = r0;
-    T* r_out = r1;
+    // the iterations: one launch of the operand set's iteration graph, which stops on the device
     PcgState* host = reinterpret_cast<PcgState*>(ws->host_done);
-    bool finished = false;
-    while (!finished)
+    if (o->max_iterations > 0)
     {
-        const int chunk = std::min(check_every, o->max_iterations - issued);
-        for (int k = 0; k < chunk; ++k)
-        {
-            if (issued > 0)
-            {
-                pcg_direction_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, z, p, st);
-                PM_LAUNCH_CHECK();
-            }
-            launch_pcg_spmv<T>(A, p, q, partials + kMaxReduceBlocks * 0, st, sgrid, stream);
-            pcg_update_kernel<T><<<vgrid, kReduceBlock, 0, stream>>>(n, x, p, q, r_in, r_out, z, mode, inv, blocks, bs,
-                                                                      partials + kMaxReduceBlocks * 0, st);
-            PM_LAUNCH_CHECK();
-            std::swap(r_in, r_out);
-            ++issued;
-        }
-        PM_CUDA(cudaMemcpyAsync(host, st, sizeof(PcgState), cudaMemcpyDeviceToHost, stream));
-        PM_CUDA(cudaEventRecord(ws->event, stream));
-        PM_CUDA(cudaEventSynchronize(ws->event));
-        finished = host->done || issued >= o->max_iterations;
-        check_every = std::min(check_every * 2, 32);
+        const cudaGraphExec_t exec = cg_iteration_graph<T>(ws, A, x, blocks, bs, mode);
+        PM_CUDA(cudaMemsetAsync(&st->chunks, 0, sizeof(int), stream));
+        PM_CUDA(cudaGraphLaunch(exec, stream));
     }
+    PM_CUDA(cudaMemcpyAsync(host, st, sizeof(PcgState), cudaMemcpyDeviceToHost, stream));
+    PM_CUDA(cudaEventRecord(ws->event, stream));
+    PM_CUDA(cudaEventSynchronize(ws->event));
+    if (o->max_iterations > 0) // the kernels the graph ran: three per iteration and the condition
+        for (int k = 0; k < host->chunks * (3 * kCgChunk + 1); ++k)
+            count_launch();
     const PcgState s = *host;
     if (s.jacobi_bad_row != kNone)
     {
@@ -1315,6 +1431,7 @@ int pm_solver_workspace_close(pm_solver_workspace* ws)
     return pm::guarded([&] {
         if (!ws)
             pm::fail(PM_INVALID_ARGUMENT, "workspace is null");
+        ws->drop_graphs(); // they hold pointers into the buffer released here
         ws->buffer.release();
     });
 }
