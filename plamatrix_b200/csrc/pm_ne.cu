@@ -200,6 +200,11 @@ __device__ __forceinline__ void cross63_row(T* W, T weight, const T* prow, const
     }
 }
 
+// position of entry (c, o), c <= o, of a symmetric 6x6 block in its packed upper triangle
+__host__ __device__ constexpr int upper6(int c, int o) { return c * 6 - c * (c - 1) / 2 + (o - c); }
+
+// One residual row's terms of the primary block: the upper triangle (w J_c) J_o, o >= c (21
+// entries, packed), then the gradient (w J_c) r (6 entries).  The lower triangle is the mirror.
 template <typename T>
 __device__ __forceinline__ void primary6_row(T* sum, T weight, const T* jrow, T rr)
 {
@@ -207,10 +212,10 @@ __device__ __forceinline__ void primary6_row(T* sum, T weight, const T* jrow, T 
     for (int c = 0; c < 6; ++c)
     {
         const T wv = mul_rn(weight, jrow[c]);
-        sum[36 + c] = add_rn(sum[36 + c], mul_rn(wv, rr));
+        sum[21 + c] = add_rn(sum[21 + c], mul_rn(wv, rr));
 #pragma unroll
-        for (int o = 0; o < 6; ++o)
-            sum[c * 6 + o] = add_rn(sum[c * 6 + o], mul_rn(wv, jrow[o]));
+        for (int o = c; o < 6; ++o)
+            sum[upper6(c, o)] = add_rn(sum[upper6(c, o)], mul_rn(wv, jrow[o]));
     }
 }
 
@@ -489,18 +494,20 @@ __global__ void __launch_bounds__(128) eliminated_cross3_m2_kernel(CooView vo, c
 
 // Per primary block (6x6): Hpp and g_p over its observations.  Warp w of the block owns a
 // contiguous slice of the primary's observation list (a multiple of 32 long) and lane j of it the
-// observations lo_w + j, lo_w + j + 32, ...; every lane sums its 42 terms serially, the lanes of a
-// warp are combined by a fixed xor-shuffle tree and the warps in warp order.  The reduction tree
-// depends only on the list length, never on scheduling.
+// observations lo_w + j, lo_w + j + 32, ...; every lane sums its 27 terms serially (Hpp's upper
+// triangle and g_p), the lanes of a warp are combined by a fixed xor-shuffle tree and the warps in
+// warp order; Hpp's lower triangle is written as the mirror of the upper.  The reduction tree
+// depends only on the list length, never on scheduling.  At most 128 registers: four CTAs per SM
+// (a 4,000-primary system then runs 6.8 waves of 592 CTAs instead of 9.0 of 444).
 // M == 2: two-row residuals read in pairs of scalars, Huber weight evaluated inline (weights
 // unused); M == 0: any residual size m, weights precomputed.
 template <typename T, int M>
-__global__ void __launch_bounds__(128) primary_accumulate6_kernel(CooView v, int m, const T* __restrict__ jp,
+__global__ void __launch_bounds__(128, 4) primary_accumulate6_kernel(CooView v, int m, const T* __restrict__ jp,
                                                                   const T* __restrict__ res, T delta,
                                                                   const T* __restrict__ weights, T* __restrict__ hpp,
                                                                   T* __restrict__ gp)
 {
-    constexpr int W = 42; // 36 Hpp entries + 6 gradient entries
+    constexpr int W = 27; // 21 upper Hpp entries + 6 gradient entries
     constexpr int kWarps = 4;
     __shared__ T part[kWarps][W];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -555,15 +562,17 @@ __global__ void __launch_bounds__(128) primary_accumulate6_kernel(CooView v, int
                 part[warp][k] = sum[k];
         }
         __syncthreads();
-        if (threadIdx.x < W)
+        if (threadIdx.x < 42)
         {
+            const int t = threadIdx.x;
+            const int k = t < 36 ? upper6(min(t / 6, t % 6), max(t / 6, t % 6)) : t - 15;
             T total = T(0);
             for (int wi = 0; wi < kWarps; ++wi)
-                total = add_rn(total, part[wi][threadIdx.x]);
-            if (threadIdx.x < 36)
-                hpp[p * 36 + threadIdx.x] = total;
+                total = add_rn(total, part[wi][k]);
+            if (t < 36)
+                hpp[p * 36 + t] = total;
             else
-                gp[p * 6 + (threadIdx.x - 36)] = total;
+                gp[p * 6 + (t - 36)] = total;
         }
         __syncthreads();
     }

@@ -36,6 +36,11 @@ constexpr long long kNone = 0x7fffffffffffffffLL;
 constexpr int kRowThreads = 128;
 constexpr int kVecBlock = 256;
 constexpr int kMaxParts = 1024;
+// the plain block-CSR SpMV keeps four CTAs of kVecBlock threads resident per SM (<= 64
+// registers): a warp per block row then covers 4,736 rows in one wave (at the 66 registers it
+// took unbounded only three fit, and a 4,000-row system ran 1.13 waves).  The PCG's and the
+// batched SpMV take <= 64 registers unbounded; bounding them made ptxas spill.
+constexpr int kSpmvCtasPerSm = 4;
 
 struct SchurStatus
 {
@@ -1274,7 +1279,7 @@ __device__ __forceinline__ void bsr_row(const int* __restrict__ row_ptr, const i
 
 // plain y = S x (vector type V)
 template <typename V, typename M, int BP>
-__global__ void __launch_bounds__(kVecBlock) bsr_spmv_kernel(int64_t P, int bp, const int* __restrict__ row_ptr,
+__global__ void __launch_bounds__(kVecBlock, kSpmvCtasPerSm) bsr_spmv_kernel(int64_t P, int bp, const int* __restrict__ row_ptr,
                                                              const int* __restrict__ block_col,
                                                              const M* __restrict__ S, const V* __restrict__ x,
                                                              V* __restrict__ y)
