@@ -444,21 +444,38 @@ __global__ void __launch_bounds__(128) eliminated_cross3_m2_kernel(CooView vo, c
             g[k] = T(0);
         const int e = vo.bucket_start[l + 1];
         int q = vo.bucket_start[l];
-        uint64_t next = q < e ? vo.keys[q] : 0;
-        int next_slot = q < e ? slot[q] : 0;
-        for (; q < e; ++q)
+        // software pipeline: the next observation's rows are loaded before the current one is
+        // summed (two observations in flight per thread), its index one step further ahead
+        T r[2], Jl[6], Jp[12];
+        int64_t i = 0;
+        int s = 0;
+        if (q < e)
         {
-            const int64_t i = static_cast<uint32_t>(next);
-            const int s = next_slot;
-            if (q + 1 < e)
-            {
-                next = vo.keys[q + 1];
-                next_slot = slot[q + 1];
-            }
-            T r[2], Jl[6], Jp[12];
+            i = static_cast<uint32_t>(vo.keys[q]);
+            s = slot[q];
             load_vec<T, 2>(res + i * 2, r);
             load_vec<T, 6>(jl + i * 6, Jl);
             load_vec<T, 12>(jp + i * 12, Jp);
+        }
+        uint64_t next = q + 1 < e ? vo.keys[q + 1] : 0;
+        int next_slot = q + 1 < e ? slot[q + 1] : 0;
+        for (; q < e; ++q)
+        {
+            T rn[2], Jln[6], Jpn[12];
+            const int64_t in = static_cast<uint32_t>(next);
+            const int sn = next_slot;
+            const bool more = q + 1 < e;
+            if (more)
+            {
+                load_vec<T, 2>(res + in * 2, rn);
+                load_vec<T, 6>(jl + in * 6, Jln);
+                load_vec<T, 12>(jp + in * 12, Jpn);
+                if (q + 2 < e)
+                {
+                    next = vo.keys[q + 2];
+                    next_slot = slot[q + 2];
+                }
+            }
             const T squared = squared_norm(r, 2);
             note_nonfinite(squared, i, first_bad);
             const T weight = huber_weight_of(squared, delta);
@@ -482,6 +499,20 @@ __global__ void __launch_bounds__(128) eliminated_cross3_m2_kernel(CooView vo, c
             cross63_row(W, weight, Jp, Jl);
             cross63_row(W, weight, Jp + 6, Jl + 3);
             store_vec<T, 18>(w + c * 18, W);
+            if (more)
+            {
+#pragma unroll
+                for (int k = 0; k < 2; ++k)
+                    r[k] = rn[k];
+#pragma unroll
+                for (int k = 0; k < 6; ++k)
+                    Jl[k] = Jln[k];
+#pragma unroll
+                for (int k = 0; k < 12; ++k)
+                    Jp[k] = Jpn[k];
+                i = in;
+                s = sn;
+            }
         }
 #pragma unroll
         for (int k = 0; k < 9; ++k)
