@@ -1348,6 +1348,45 @@ __global__ void __launch_bounds__(kVecBlock) pcg_bsr_kernel(int64_t P, int bp, c
     });
 }
 
+// the last block of an update: iteration count, residual norm, convergence / limit / stagnation,
+// beta and rho (tot = {r.z, r.r})
+__device__ __forceinline__ void update_finish(SolveState* st, const double (&tot)[2])
+{
+    st->iterations += 1;
+    st->residual_squared = tot[1];
+    const double norm = sqrt(fmax(0.0, tot[1]));
+    if (!isfinite(tot[1]))
+    {
+        st->breakdown = 1;
+        st->done = 1;
+        return;
+    }
+    if (norm <= st->tolerance)
+    {
+        st->converged = 1;
+        st->done = 1;
+        return;
+    }
+    if (st->iterations >= st->max_iterations)
+    {
+        st->done = 1;
+        return;
+    }
+    if (st->window > 0 && st->iterations - st->window_start >= st->window)
+    {
+        if (tot[1] > 0.25 * st->window_squared) // the norm did not halve over the window
+        {
+            st->stagnated = 1;
+            st->done = 1;
+            return;
+        }
+        st->window_start = st->iterations;
+        st->window_squared = tot[1];
+    }
+    st->beta = tot[0] / st->rho;
+    st->rho = tot[0];
+}
+
 // x += alpha p; r_out = r_in - alpha q; z = Minv r_out; r.z, r.r; convergence; beta
 template <typename V, typename PM, int BP>
 __global__ void __launch_bounds__(kVecBlock) pcg_block_update_kernel(int64_t P, int bp_rt, V* __restrict__ x,
@@ -1396,41 +1435,59 @@ __global__ void __launch_bounds__(kVecBlock) pcg_block_update_kernel(int64_t P, 
             mine[0] += r[k] * static_cast<double>(zk);
         }
     }
-    finish_reduce<2>(mine, partials, &st->ticket[2], [&](double (&tot)[2]) {
-        st->iterations += 1;
-        st->residual_squared = tot[1];
-        const double norm = sqrt(fmax(0.0, tot[1]));
-        if (!isfinite(tot[1]))
+    finish_reduce<2>(mine, partials, &st->ticket[2], [&](double (&tot)[2]) { update_finish(st, tot); });
+}
+
+// x += alpha p; r_out = r_in - alpha q; z = Minv r_out; r.z, r.r for 6x6 blocks, eight lanes per
+// block row (lane k < 6 owns entry k; the row's residual reaches every lane by shuffles), so a
+// 4,000-row system spreads over 125 CTAs instead of 16.  Every entry takes the same arithmetic as
+// pcg_block_update_kernel's; the dot partials are summed per lane.
+template <typename V, typename PM>
+__global__ void __launch_bounds__(kVecBlock) pcg_block_update6_kernel(int64_t P, V* __restrict__ x,
+                                                                      const V* __restrict__ p_vec,
+                                                                      const V* __restrict__ q, const V* __restrict__ r_in,
+                                                                      V* __restrict__ r_out, V* __restrict__ z,
+                                                                      const PM* __restrict__ minv, double* partials,
+                                                                      SolveState* st)
+{
+    if (st->done)
+        return;
+    const double alpha = st->alpha;
+    const int lane = threadIdx.x & 31, k = lane & 7, base = lane & ~7;
+    const int64_t groups = int64_t(gridDim.x) * (blockDim.x / 8);
+    const int64_t first = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) / 8;
+    const int64_t span = (P + groups - 1) / groups; // warp-uniform trip count (the shuffles)
+    double mine[2] = {0.0, 0.0};
+    for (int64_t t = 0; t < span; ++t)
+    {
+        const int64_t row = first + t * groups;
+        const bool own = row < P && k < 6;
+        double rk = 0.0;
+        if (own)
         {
-            st->breakdown = 1;
-            st->done = 1;
-            return;
+            const int64_t i = row * 6 + k;
+            x[i] = static_cast<V>(static_cast<double>(x[i]) + alpha * static_cast<double>(p_vec[i]));
+            rk = static_cast<double>(static_cast<V>(static_cast<double>(r_in[i]) - alpha * static_cast<double>(q[i])));
+            r_out[i] = static_cast<V>(rk);
+            mine[1] += rk * rk;
         }
-        if (norm <= st->tolerance)
+        double r[6];
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            r[c] = __shfl_sync(0xffffffffu, rk, base + c);
+        if (own)
         {
-            st->converged = 1;
-            st->done = 1;
-            return;
+            const PM* m = minv + row * 36 + k * 6;
+            double sum = 0.0;
+#pragma unroll
+            for (int c = 0; c < 6; ++c)
+                sum += static_cast<double>(m[c]) * r[c];
+            const V zk = static_cast<V>(sum);
+            z[row * 6 + k] = zk;
+            mine[0] += rk * static_cast<double>(zk);
         }
-        if (st->iterations >= st->max_iterations)
-        {
-            st->done = 1;
-            return;
-        }
-        if (st->window > 0 && st->iterations - st->window_start >= st->window)
-        {
-            if (tot[1] > 0.25 * st->window_squared) // the norm did not halve over the window
-            {
-                st->stagnated = 1;
-                st->done = 1;
-                return;
-            }
-            st->window_start = st->iterations;
-            st->window_squared = tot[1];
-        }
-        st->beta = tot[0] / st->rho;
-        st->rho = tot[0];
-    });
+    }
+    finish_reduce<2>(mine, partials, &st->ticket[2], [&](double (&tot)[2]) { update_finish(st, tot); });
 }
 
 template <typename V>
@@ -2605,6 +2662,7 @@ cudaGraphExec_t pcg_iteration_graph(pm_schur_workspace* ws, const M* S, const PM
     V* q = p + (n + 1);
     const unsigned sgrid = grid_for(P * 32, kVecBlock, kMaxParts);
     const unsigned ugrid = grid_for(P, kVecBlock, kMaxParts);
+    const unsigned u6grid = grid_for(P * 8, kVecBlock, kMaxParts);
     const unsigned dgrid = grid_for(n, kVecBlock, 4096);
     cudaGraph_t graph = nullptr;
     PM_CUDA(cudaGraphCreate(&graph, 0));
@@ -2637,8 +2695,8 @@ cudaGraphExec_t pcg_iteration_graph(pm_schur_workspace* ws, const M* S, const PM
         {
             pcg_bsr_kernel<V, M, 6><<<sgrid, kVecBlock, 0, gs>>>(P, bp, ws->block_row_ptr, ws->block_col, S, p, q,
                                                                  ws->partials, ws->state);
-            pcg_block_update_kernel<V, PM, 6><<<ugrid, kVecBlock, 0, gs>>>(P, bp, x, p, q, r_in, r_out, z, minv,
-                                                                           ws->partials, ws->state);
+            pcg_block_update6_kernel<V, PM><<<u6grid, kVecBlock, 0, gs>>>(P, x, p, q, r_in, r_out, z, minv,
+                                                                          ws->partials, ws->state);
         }
         else
         {
