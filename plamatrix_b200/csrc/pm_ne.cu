@@ -132,11 +132,17 @@ __global__ void observation_slots_kernel(int64_t C, const uint64_t* __restrict__
             slot[position[static_cast<uint32_t>(keys[q])]] = q == cross_run[c] ? static_cast<int>(c) : ~static_cast<int>(c);
 }
 
-__global__ void compare_kernel(const int64_t* __restrict__ a, const int64_t* __restrict__ b, int64_t n, int* differs)
+// *differs = 1 when either caller index array differs from the saved copy (int32: the saved
+// arrays passed the topology build's range checks, so widening them back is exact)
+__global__ void compare_kernel(const int64_t* __restrict__ a, const int* __restrict__ a_saved,
+                               const int64_t* __restrict__ b, const int* __restrict__ b_saved, int64_t n,
+                               int* differs)
 {
+    bool diff = false;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-        if (a[i] != b[i])
-            *differs = 1;
+        diff |= (a[i] != static_cast<int64_t>(a_saved[i])) | (b[i] != static_cast<int64_t>(b_saved[i]));
+    if (__any_sync(0xffffffffu, diff) && (threadIdx.x & 31) == 0)
+        *differs = 1;
 }
 
 template <typename T>
@@ -795,26 +801,24 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
         fail(PM_INVALID_ARGUMENT, "observation arrays must be non-null");
     // ---- topology (cached while the index arrays are unchanged)
     bool rebuild = !ne->observation_topology || ne->observation_count != count || ne->residual_size != m;
-    int64_t* saved_primary = nullptr;
-    int64_t* saved_eliminated = nullptr;
+    int* saved_primary = nullptr;
+    int* saved_eliminated = nullptr;
     int64_t* zeros = nullptr;
     int* differs = nullptr;
     auto carve = [&]() {
         Carver c;
         c.base = static_cast<char*>(ne->observation_copy.ptr);
-        saved_primary = c.take<int64_t>(count + 1);
-        saved_eliminated = c.take<int64_t>(count + 1);
         zeros = c.take<int64_t>(count + 1);
+        saved_primary = c.take<int>(count + 1);
+        saved_eliminated = c.take<int>(count + 1);
         differs = c.take<int>(1);
     };
     if (!rebuild)
     {
         carve();
         PM_CUDA(cudaMemsetAsync(differs, 0, sizeof(int), stream));
-        compare_kernel<<<grid_for(count, 256, 4096), 256, 0, stream>>>(obs_primary, saved_primary, count, differs);
-        PM_LAUNCH_CHECK();
-        compare_kernel<<<grid_for(count, 256, 4096), 256, 0, stream>>>(obs_eliminated, saved_eliminated, count,
-                                                                         differs);
+        compare_kernel<<<grid_for(count, 256, 4096), 256, 0, stream>>>(obs_primary, saved_primary, obs_eliminated,
+                                                                         saved_eliminated, count, differs);
         PM_LAUNCH_CHECK();
         int host_differs = 0;
         PM_CUDA(cudaMemcpyAsync(&host_differs, differs, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -825,8 +829,8 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
     {
         Carver plan;
         plan.take<int64_t>(count + 1);
-        plan.take<int64_t>(count + 1);
-        plan.take<int64_t>(count + 1);
+        plan.take<int>(count + 1);
+        plan.take<int>(count + 1);
         plan.take<int>(1);
         ne->observation_copy.ensure(plan.offset + 256, stream, "normal equations");
         carve();
@@ -881,9 +885,10 @@ void ne_accumulate(pm_normal_equations* ne, cudaStream_t stream, int64_t count, 
         }
         if (count > 0)
         {
-            PM_CUDA(cudaMemcpyAsync(saved_primary, obs_primary, count * sizeof(int64_t), cudaMemcpyDeviceToDevice, stream));
-            PM_CUDA(cudaMemcpyAsync(saved_eliminated, obs_eliminated, count * sizeof(int64_t), cudaMemcpyDeviceToDevice,
-                                    stream));
+            narrow_kernel<<<grid_for(count, 256, 4096), 256, 0, stream>>>(obs_primary, saved_primary, count);
+            PM_LAUNCH_CHECK();
+            narrow_kernel<<<grid_for(count, 256, 4096), 256, 0, stream>>>(obs_eliminated, saved_eliminated, count);
+            PM_LAUNCH_CHECK();
         }
         ne->observation_count = count;
         ne->residual_size = m;
