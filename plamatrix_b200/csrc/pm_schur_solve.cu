@@ -1607,9 +1607,10 @@ __global__ void mf_eliminated6_kernel(int64_t L, const int* __restrict__ cross_o
         double u0 = 0.0, u1 = 0.0, u2 = 0.0;
         for (int c = cross_offsets[l]; c < cross_offsets[l + 1]; ++c)
         {
-            double wv[18], xv[6];
+            double wv[18];
             load_pairs<T, 18>(w + int64_t(c) * 18, wv);
-            load_pairs<double, 6>(x + int64_t(cross_primary[c]) * 6, xv);
+            // x is the caller's step vector (no 16-byte alignment promised): element by element
+            const double* xv = x + int64_t(cross_primary[c]) * 6;
 #pragma unroll
             for (int r = 0; r < 6; ++r)
             {

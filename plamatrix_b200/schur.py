@@ -283,6 +283,11 @@ def solve_damped_schur_complement(equations: DeviceNormalEquations, damping: flo
     dt = equations.tdtype
     dp = primary_step if primary_step is not None else torch.zeros(max(n, 1), dtype=dt, device="cuda")
     dl = eliminated_step if eliminated_step is not None else torch.zeros(max(m, 1), dtype=dt, device="cuda")
+    for name, t, size in (("primary_step", dp, n), ("eliminated_step", dl, m)):
+        # the native solve writes `size` scalars through the pointer
+        if not t.is_cuda or not t.is_contiguous() or t.dtype != dt or t.numel() < size:
+            raise N.InvalidArgument(f"{name} must be a contiguous CUDA tensor of dtype {dt} with at least "
+                                    f"{size} elements")
     rep = SchurReport()
     N.call(f"pm_schur_solve_{equations.sfx}", ws.handle, _stream_handle(stream), equations.handle,
            equations.ct(damping), C.byref(opts.c()), _ptr(dp), _ptr(dl), C.byref(rep))

@@ -41,6 +41,14 @@ def _check_device(name: str, t: torch.Tensor, dtype=None):
         raise N.InvalidArgument(f"{name} must have dtype {dtype}, got {t.dtype}")
 
 
+def _check_vector(name: str, t: torch.Tensor, dtype, size: int):
+    """A contiguous CUDA vector of `dtype` with exactly `size` elements: the native calls take
+    raw pointers and read or write `size` scalars through them."""
+    _check_device(name, t, dtype)
+    if t.numel() != size:
+        raise N.InvalidArgument(f"{name} must have {size} elements, got {t.numel()}")
+
+
 class SparseOpsWorkspace:
     """Grow-only, stream-bound scratch + deferred COO status (sparse_ops.h:13-77)."""
 
@@ -148,12 +156,14 @@ class CsrOperand:
         self._h = h
         self.matrix = matrix
         self.sfx = sfx
+        self.dtype = matrix.values.dtype
 
     @property
     def handle(self):
         return self._h
 
     def set_values(self, values: torch.Tensor) -> None:
+        _check_vector("values", values, self.dtype, self.matrix.nnz)
         N.call("pm_csr_set_values", self._h, _ptr(values))
         self.matrix = CSRMatrix(self.matrix.rows, self.matrix.cols, self.matrix.row_offsets,
                                 self.matrix.col_indices, values)
@@ -165,6 +175,8 @@ class CsrOperand:
         y = torch.empty(self.matrix.rows, dtype=x.dtype, device=x.device) if out is None else out
         if y.numel() != self.matrix.rows:
             raise N.PlamatrixError("spmv output dimension mismatch")
+        _check_device("x", x, self.dtype)
+        _check_device("out", y, self.dtype)
         N.call(f"pm_csr_spmv_{self.sfx}", self._h, _stream_handle(stream), _ptr(x), _ptr(y))
         return y
 
@@ -199,6 +211,8 @@ class CsrOperand:
         for name, t in (("input", B), ("output", y)):
             if t.numel() > 0 and t.shape[1] > 1 and t.stride() != (1, t.shape[0]):
                 raise N.InvalidArgument(f"spmm {name} must be column-major (strides (1, rows))")
+            if not t.is_cuda or t.dtype != self.dtype:
+                raise N.InvalidArgument(f"spmm {name} must be a CUDA matrix of dtype {self.dtype}")
         N.call(f"pm_csr_spmm_{self.sfx}", self._h, _stream_handle(stream), B.shape[0], B.shape[1], _ptr(B),
                y.shape[0], y.shape[1], _ptr(y))
         return y
@@ -266,6 +280,12 @@ class IterativeSolverWorkspace:
 
 def _solve(kind: str, matrix, rhs, solution, workspace, options, stream, blocks=None, block_size=0) -> dict:
     op = matrix if isinstance(matrix, CsrOperand) else CsrOperand(matrix, stream)
+    _check_vector("rhs", rhs, op.dtype, op.matrix.rows)
+    _check_vector("solution", solution, op.dtype, op.matrix.cols)
+    if kind == "block_pcg":
+        if block_size <= 0:
+            raise N.InvalidArgument("block size must be positive")
+        _check_vector("inverse_blocks", blocks, op.dtype, op.matrix.rows * int(block_size))
     ws = workspace or IterativeSolverWorkspace()
     opts = (options or IterativeSolverOptions()).c()
     rep = N.SolverReport()
@@ -339,6 +359,8 @@ class AsyncIterativeSolverState:
 
 def _fixed(kind, matrix, rhs, solution, iterations, workspace, stream):
     op = matrix if isinstance(matrix, CsrOperand) else CsrOperand(matrix, stream)
+    _check_vector("rhs", rhs, op.dtype, op.matrix.rows)
+    _check_vector("solution", solution, op.dtype, op.matrix.cols)
     ws = workspace or IterativeSolverWorkspace()
     h = C.c_void_p()
     N.call(f"pm_{kind}_fixed_iterations_async_{op.sfx}", ws.handle, _stream_handle(stream), op.handle, _ptr(rhs),

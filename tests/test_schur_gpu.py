@@ -708,3 +708,41 @@ def test_one_workspace_alternating_systems_matches_fresh_workspaces():
         assert rep["converged"] and rep_f["converged"]
         assert rep["iterations"] == rep_f["iterations"]
         assert torch.equal(dp, dp_f) and torch.equal(dl, dl_f)
+
+
+@pytest.mark.parametrize("precision", ["native", "mixed", "mixed_fp32_assembly"])
+def test_step_vectors_need_no_16_byte_alignment(precision):
+    """The caller's step vectors may start 8 bytes past a 16-byte boundary (a view one element
+    into a buffer): every kernel reads and writes them element by element, and the steps equal
+    those of aligned vectors bit for bit."""
+    prob = W.large_bundle(seed=29, P=120, L=6000)
+    ne = _device_from_observations(prob)
+    n, m = 120 * 6, 6000 * 3
+    opts = SC.SchurComplementSolverOptions(max_iterations=300, relative_tolerance=1e-9, precision=precision)
+    ws = SC.SchurComplementSolverWorkspace()
+    dp, dl, rep = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws)
+    assert rep["converged"], rep["message"]
+    pbuf = torch.zeros(n + 1, dtype=torch.float64, device="cuda")
+    lbuf = torch.zeros(m + 1, dtype=torch.float64, device="cuda")
+    dp1, dl1 = pbuf[1:], lbuf[1:]
+    assert dp1.data_ptr() % 16 == 8 and dl1.data_ptr() % 16 == 8
+    ws2 = SC.SchurComplementSolverWorkspace()
+    _, _, rep2 = SC.solve_damped_schur_complement(ne, 1e-3, opts, ws2, dp1, dl1)
+    assert rep2["converged"] and rep2["iterations"] == rep["iterations"]
+    assert torch.equal(dp1, dp) and torch.equal(dl1, dl)
+
+
+def test_step_vectors_are_checked():
+    """Step vectors of the wrong type, device or length are refused before any device work."""
+    prob = W.large_bundle(seed=29, P=40, L=600)
+    ne = _device_from_observations(prob)
+    ws = SC.SchurComplementSolverWorkspace()
+    n, m = 40 * 6, 600 * 3
+    good_p = torch.zeros(n, dtype=torch.float64, device="cuda")
+    good_l = torch.zeros(m, dtype=torch.float64, device="cuda")
+    for dp, dl in ((good_p[:-1], good_l), (good_p, good_l[:-1]), (good_p.float(), good_l),
+                   (good_p.cpu(), good_l), (torch.zeros(2 * n, dtype=torch.float64, device="cuda")[::2], good_l)):
+        with pytest.raises(N.InvalidArgument):
+            SC.solve_damped_schur_complement(ne, 1e-3, SC.SchurComplementSolverOptions(), ws, dp, dl)
+    _, _, rep = SC.solve_damped_schur_complement(ne, 1e-3, SC.SchurComplementSolverOptions(), ws, good_p, good_l)
+    assert rep["converged"]

@@ -276,3 +276,29 @@ def test_fixed_iterations_match_the_adaptive_solver(checkers, kind, dtype):
     assert z["iterations"] == 0 and z["initial_residual"] == z["final_residual"]
     with pytest.raises(N.InvalidArgument):
         getattr(S, f"{kind}_fixed_iterations_async")(op, b, torch.zeros_like(x_fixed), -1)
+
+
+def test_vectors_are_checked(checkers):
+    """Vectors of the wrong type, device or length are refused before the native call (which
+    takes raw pointers and would read or write past them)."""
+    A, _ = _csr(checkers, 3, 3, [0, 1, 2], [0, 1, 2], [2.0, 3.0, 4.0], np.float64)
+    op = S.CsrOperand(A)
+    good = torch.ones(3, dtype=torch.float64, device="cuda")
+    bad = (torch.ones(3, dtype=torch.float32, device="cuda"), torch.ones(2, dtype=torch.float64, device="cuda"),
+           torch.ones(3, dtype=torch.float64), torch.ones(6, dtype=torch.float64, device="cuda")[::2])
+    for t in bad:
+        for call in (lambda: S.pcg(op, t, torch.zeros_like(good)), lambda: S.cg(op, good, t),
+                     lambda: S.block_pcg(op, good, torch.zeros_like(good), t, 1),
+                     lambda: S.pcg_fixed_iterations_async(op, t, torch.zeros_like(good), 2),
+                     lambda: op.set_values(t)):
+            with pytest.raises(N.InvalidArgument):
+                call()
+        with pytest.raises(N.PlamatrixError):
+            op.spmv(t)
+    with pytest.raises(N.InvalidArgument):
+        op.spmm(S.dense_matrix(3, 2, dtype=torch.float32))
+    with pytest.raises(N.InvalidArgument):
+        S.block_pcg(op, good, torch.zeros_like(good), good, 0)
+    x = torch.zeros_like(good)
+    assert S.pcg(op, good, x)["converged"]
+    assert torch.allclose(x, torch.tensor([0.5, 1 / 3, 0.25], dtype=torch.float64, device="cuda"))
