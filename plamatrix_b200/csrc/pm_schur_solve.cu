@@ -1596,7 +1596,7 @@ __global__ void __launch_bounds__(kVecBlock) residual_kernel(int64_t n, const do
 // t_l = Hll^-1 (W_l^T x) = L^-T (L^-1 W_l^T x) from the factor record; pass 2, CTA per block row:
 // the row's crosses in row-list order, then a fixed xor tree and the warps in order.  Both passes
 // sum in fixed orders, so the product repeats bit for bit.
-template <typename T>
+template <typename T, bool X16>
 __global__ void mf_eliminated6_kernel(int64_t L, const int* __restrict__ cross_offsets,
                                       const int* __restrict__ cross_primary, const T* __restrict__ w,
                                       const double* __restrict__ rec, const double* __restrict__ x,
@@ -1607,10 +1607,17 @@ __global__ void mf_eliminated6_kernel(int64_t L, const int* __restrict__ cross_o
         double u0 = 0.0, u1 = 0.0, u2 = 0.0;
         for (int c = cross_offsets[l]; c < cross_offsets[l + 1]; ++c)
         {
-            double wv[18];
+            double wv[18], xv[6];
             load_pairs<T, 18>(w + int64_t(c) * 18, wv);
-            // x is the caller's step vector (no 16-byte alignment promised): element by element
-            const double* xv = x + int64_t(cross_primary[c]) * 6;
+            // x is the caller's step vector: pairs when it starts on a 16-byte boundary (X16,
+            // checked by the host), element by element otherwise
+            const double* xp = x + int64_t(cross_primary[c]) * 6;
+            if constexpr (X16)
+                load_pairs<double, 6>(xp, xv);
+            else
+#pragma unroll
+                for (int r = 0; r < 6; ++r)
+                    xv[r] = xp[r];
 #pragma unroll
             for (int r = 0; r < 6; ++r)
             {
@@ -2788,9 +2795,15 @@ void true_residual(pm_schur_workspace* ws, cudaStream_t stream, const M* S, cons
     {
         // the assembled values are FP32: the FP64 product comes from the FP64 normal equations
         const pm_normal_equations* ne = ws->last_ne;
-        mf_eliminated6_kernel<double><<<grid_for(ws->L, 128, 1 << 20), 128, 0, stream>>>(
-            ws->L, ne->cross_offsets, ne->cross_primary, static_cast<const double*>(ne->cross_values), ws->hinv, x,
-            ws->mf_t);
+        const unsigned egrid = grid_for(ws->L, 128, 1 << 20);
+        if (reinterpret_cast<uintptr_t>(x) % 16 == 0)
+            mf_eliminated6_kernel<double, true><<<egrid, 128, 0, stream>>>(
+                ws->L, ne->cross_offsets, ne->cross_primary, static_cast<const double*>(ne->cross_values), ws->hinv,
+                x, ws->mf_t);
+        else
+            mf_eliminated6_kernel<double, false><<<egrid, 128, 0, stream>>>(
+                ws->L, ne->cross_offsets, ne->cross_primary, static_cast<const double*>(ne->cross_values), ws->hinv,
+                x, ws->mf_t);
         PM_LAUNCH_CHECK();
         mf_primary6_kernel<double><<<grid_for(P, 1, 1 << 20), kDiagThreads, 0, stream>>>(
             P, ws->prim_offsets, ws->row_entries, static_cast<const double*>(ne->cross_values), ws->mf_t,
