@@ -1714,6 +1714,24 @@ __global__ void axpy_to_double_kernel(int64_t n, const V* __restrict__ d, double
 }
 
 // ===================================================================== 5. back-substitution
+// dl_l = Hll^-1 (-g_l - W_l^T dp) = -L^-T z_l - t_l when the FP64 matrix-free pass that certified
+// dp ran at dp itself: t_l = Hll^-1 W_l^T dp is what it stored, z_l = L^-1 g_l sits in the factor
+// record [L^-1 00, 10, 11, 20, 21, 22 | z].  Reads 112 bytes per eliminated block instead of the
+// block's cross blocks.
+__global__ void backsub_from_t_kernel(int64_t L, const double* __restrict__ rec, const double* __restrict__ t,
+                                      double* __restrict__ dl)
+{
+    for (int64_t l = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; l < L; l += int64_t(gridDim.x) * blockDim.x)
+    {
+        double f[10], u[4];
+        load_pairs<double, 10>(rec + l * 10, f);
+        load_pairs<double, 4>(t + l * 4, u);
+        dl[l * 3] = -(f[0] * f[6] + f[1] * f[7] + f[3] * f[8]) - u[0];
+        dl[l * 3 + 1] = -(f[2] * f[7] + f[4] * f[8]) - u[1];
+        dl[l * 3 + 2] = -(f[5] * f[8]) - u[2];
+    }
+}
+
 template <typename T, int BP, int BL>
 __global__ void backsub_kernel(int64_t L, int bp_rt, int bl_rt, const int* __restrict__ cross_offsets,
                                const int* __restrict__ cross_primary, const T* __restrict__ w,
@@ -3318,6 +3336,9 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     };
     // ---- PCG
     double* area = vector_area(ws);
+    // the FP64 matrix-free pass last run at the final step (mixed precision with FP32 values):
+    // its t_l = Hll^-1 W_l^T dp is the back-substitution's product too
+    bool t_at_step = false;
     SolveState st{};
     if (n == 0)
     {
@@ -3469,6 +3490,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
             PM_LAUNCH_CHECK();
             const double before = norm;
             true_residual<T>(ws, stream, static_cast<const T*>(ws->S), x64, q64, r64, norm, rhs_norm);
+            t_at_step = ws->s32_only && ws->paired && ws->hstride == 10;
             if (!(norm < before))
             {
                 fp64_fallback = true;
@@ -3478,6 +3500,7 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
         }
         if (!rep->converged && fp64_fallback)
         {
+            t_at_step = false; // the FP64 PCG below moves the step
             if (ws->s32_only)
             {
                 // the FP64 PCG needs the FP64 values: assemble them now (the rare path)
@@ -3525,7 +3548,9 @@ void schur_solve(pm_schur_workspace* ws, cudaStream_t stream, const pm_normal_eq
     if (L > 0)
     {
         const unsigned grid = grid_for(L, 128, 1 << 20);
-        if (bp == 6 && bl == 3)
+        if (t_at_step && bp == 6 && bl == 3 && sizeof(T) == 8)
+            backsub_from_t_kernel<<<grid, 128, 0, stream>>>(L, ws->hinv, ws->mf_t, reinterpret_cast<double*>(dl));
+        else if (bp == 6 && bl == 3)
             backsub_kernel<T, 6, 3><<<grid, 128, 0, stream>>>(L, 6, 3, ne->cross_offsets, ne->cross_primary,
                                                               static_cast<const T*>(ne->cross_values),
                                                               static_cast<const T*>(ne->eliminated_gradient), ws->hinv,
