@@ -211,6 +211,40 @@ def test_small_bundle_matches_reference_bitwise(checkers, dtype):
     assert ra[2]["iterations"] == rb[2]["iterations"]
 
 
+BUNDLE_SHAPES = {
+    # the large workload's distribution (2 + Poisson(4) distinct primaries from a wrapped window
+    # of 40, 5% outliers under the Huber loss) at 1/667 of its size
+    "windowed_2_poisson4": dict(P=60, L=3000, per_eliminated="2+poisson4", window=40),
+    # block sizes other than 6 x 3 and three rows per residual: the generic paths
+    "blocks_4x2_m3": dict(P=30, L=1500, per_eliminated=3, bp=4, bl=2, residual_size=3),
+    # most primaries observed by nothing: rows held up by the damping alone
+    "unobserved_primaries": dict(P=60, L=12, per_eliminated=1),
+}
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("shape", sorted(BUNDLE_SHAPES))
+def test_bundle_shapes_match_reference_bitwise(checkers, shape, dtype):
+    """Ragged and non-default problems: oracle and reference agree bit for bit on the normal
+    equations, the Schur system and the PCG solution with its iteration count."""
+    if not checkers.available("ref"):
+        pytest.skip("reference library not built")
+    kw = dict(BUNDLE_SHAPES[shape])
+    prob = W.bundle_problem(kw.pop("P"), kw.pop("L"), seed=5, dtype=dtype, **kw)
+    a = checkers.normal_equations_from_observations(prob, dtype=dtype, impl="orc")
+    b = checkers.normal_equations_from_observations(prob, dtype=dtype, impl="ref")
+    ea, eb = a.export(), b.export()
+    for key in ea:
+        assert np.array_equal(ea[key], eb[key]), key
+    for x, y in zip(a.schur_system(1e-3, with_preconditioner=False), b.schur_system(1e-3)):
+        assert np.array_equal(x, y)
+    ra = a.solve(1e-3, relative_tolerance=1e-10, max_iterations=500)
+    rb = b.solve(1e-3, relative_tolerance=1e-10, max_iterations=500)
+    assert ra[2]["converged"] and rb[2]["converged"]
+    assert np.array_equal(ra[0], rb[0]) and np.array_equal(ra[1], rb[1])
+    assert ra[2]["iterations"] == rb[2]["iterations"]
+
+
 def test_merge_matches_serial(checkers):
     for impl in _impls(checkers):
         serial = _build(checkers, KA.synthetic_residuals, impl)
