@@ -46,6 +46,34 @@ def test_coo_random_matches_reference_bitwise(checkers):
             assert np.array_equal(x.view(np.uint8), y.view(np.uint8))
 
 
+def _coo_edge_shapes(dtype):
+    rng = np.random.default_rng(7)
+    n = 5000
+    yield "one_coordinate", 3, 3, np.full(n, 1), np.full(n, 2), \
+        (rng.standard_normal(n) * 10.0 ** rng.integers(-4, 9, n)).astype(dtype)
+    yield "signed_zeros", 2, 2, np.array([0, 0, 1, 1, 1, 0]), np.array([0, 0, 1, 1, 1, 1]), \
+        np.array([0.0, -0.0, -0.0, 0.0, -0.0, -0.0], dtype)
+    yield "zero_rows", 0, 5, np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, dtype)
+    yield "mostly_empty_rows", 1000, 1000, rng.integers(0, 3, 200), rng.integers(0, 1000, 200), \
+        rng.standard_normal(200).astype(dtype)
+    yield "wide_rows", 4, 100000, rng.integers(0, 4, 50000), rng.integers(0, 100000, 50000), \
+        rng.standard_normal(50000).astype(dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_coo_edge_shapes_match_reference_bitwise(checkers, dtype):
+    """One coordinate repeated 5,000 times (the summation order of a long duplicate run), signed
+    zeros, zero rows, mostly empty rows and 12,500-entry rows: byte for byte the reference's CSR."""
+    if not checkers.available("ref"):
+        pytest.skip("reference library not built")
+    for name, rows, cols, r, c, v in _coo_edge_shapes(dtype):
+        a = checkers.coo_to_csr(rows, cols, r, c, v, impl="orc")
+        b = checkers.coo_to_csr(rows, cols, r, c, v, impl="ref")
+        assert len(a[0]) == rows + 1, name
+        for x, y in zip(a, b):
+            assert np.array_equal(x.view(np.uint8), y.view(np.uint8)), name
+
+
 @pytest.mark.parametrize("case", KA.SPMV_CASES)
 def test_spmv_known_answers(checkers, case):
     for impl in _impls(checkers):
@@ -107,10 +135,11 @@ def test_pcg_matches_reference_bitwise(checkers):
         ro, ci, v = checkers.coo_to_csr(lap["rows"], lap["cols"], lap["row_indices"], lap["col_indices"],
                                         lap["values"].astype(dtype))
         b = lap["rhs"].astype(dtype)
-        xa, ra = checkers.pcg(ro, ci, v, b, relative_tolerance=1e-8, impl="orc")
-        xb, rb = checkers.pcg(ro, ci, v, b, relative_tolerance=1e-8, impl="ref")
-        assert ra == rb
-        assert np.array_equal(xa, xb)
+        for pre in (True, False):   # Jacobi PCG and plain CG
+            xa, ra = checkers.pcg(ro, ci, v, b, relative_tolerance=1e-8, preconditioned=pre, impl="orc")
+            xb, rb = checkers.pcg(ro, ci, v, b, relative_tolerance=1e-8, preconditioned=pre, impl="ref")
+            assert ra == rb and ra["converged"]
+            assert np.array_equal(xa, xb)
 
 
 def test_pcg_error_paths(checkers):
